@@ -1,0 +1,98 @@
+"""ctypes binding of the C ABI in include/gpk_b200.h (libgpk_b200.so).
+
+This is the Python-side stub a maintainer would bind against the library;
+it raises instead of falling back to anything when the library or a B200 is
+missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .thermo import CThermoDesc
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpk_b200.so")
+
+GPK_OK = 0
+ERRORS = {
+    1: "invalid argument", 2: "unsupported thermodynamic model", 3: "CUDA error",
+    4: "out of device memory", 5: "label out of range", 6: "device wait timed out",
+    7: "no usable CUDA device", 8: "device consistency check failed",
+}
+
+
+class GPKError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"gpk_b200 error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libgpk_b200.so (building it first when only sources are present)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _build
+        _build.build()
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, u64, dbl, sz = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double, C.c_size_t
+    sigs = {
+        "gpk_version": ([], C.c_char_p),
+        "gpk_last_error": ([], C.c_char_p),
+        "gpk_device_init": ([i32], i32),
+        "gpk_thermo_desc_init": ([vp, C.c_int32], None),
+        "gpk_grid_create": ([i32, i32, i32, dbl, vp, dbl, dbl, i32, C.POINTER(vp)], i32),
+        "gpk_grid_destroy": ([vp], i32),
+        "gpk_grid_set_thermo": ([vp, vp], i32),
+        "gpk_grid_upload": ([vp, i32, vp, sz], i32),
+        "gpk_grid_download": ([vp, i32, vp, sz], i32),
+        "gpk_grid_device_ptr": ([vp, i32, C.POINTER(vp)], i32),
+        "gpk_grid_get_time": ([vp, C.POINTER(dbl)], i32),
+        "gpk_grid_set_time": ([vp, dbl], i32),
+        "gpk_grid_get_step_id": ([vp, C.POINTER(u64)], i32),
+        "gpk_grid_set_step_id": ([vp, u64], i32),
+        "gpk_grid_step": ([vp, dbl, dbl, C.POINTER(dbl)], i32),
+        "gpk_grid_step_n": ([vp, i32, dbl, dbl, C.POINTER(dbl)], i32),
+        "gpk_grid_run": ([vp, dbl, dbl, i32, C.POINTER(i32)], i32),
+        "gpk_grid_sync": ([vp], i32),
+        "gpk_grid_max_dt": ([vp, C.POINTER(dbl)], i32),
+        "gpk_grid_phase_volume": ([vp, C.c_int32, C.POINTER(dbl)], i32),
+        "gpk_grid_n_grains": ([vp, C.POINTER(i32)], i32),
+        "gpk_grid_interface_fraction": ([vp, C.POINTER(dbl)], i32),
+        "gpk_grid_counters": ([vp, C.POINTER(u64)], i32),
+        "gpk_grid_topology_simple_move": ([vp, i32, C.c_int32, C.POINTER(i32)], i32),
+        "gpk_grid_device_bytes": ([vp, C.POINTER(sz)], i32),
+        "gpk_grid_launch_count": ([vp, C.POINTER(u64)], i32),
+        "gpk_voronoi_init": ([i32, i32, i32, i32, u64, vp, vp, C.POINTER(i32)], i32),
+    }
+    for name, (args, res) in sigs.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def check(code: int) -> None:
+    if code != GPK_OK:
+        msg = lib().gpk_last_error().decode(errors="replace")
+        raise GPKError(code, msg)
+
+
+def exported_symbols() -> list:
+    """Names of every entry point declared in include/gpk_b200.h and gpk_init.h."""
+    import re
+    names = []
+    inc = os.path.join(HERE, "..", "include")
+    for h in ("gpk_b200.h", "gpk_init.h"):
+        text = open(os.path.join(inc, h)).read()
+        names += re.findall(r"^\s*(?:const\s+)?\w[\w\s\*]*?\b(gpk_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+__all__ = ["lib", "check", "GPKError", "CThermoDesc", "exported_symbols"]

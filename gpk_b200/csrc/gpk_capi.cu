@@ -1,0 +1,598 @@
+// gpk_capi.cu — the C ABI of include/gpk_b200.h: grid lifetime, host-built
+// tap tables, state transfer and diagnostics.
+#include <cuda_runtime.h>
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gpk_grid.h"
+
+using namespace gpk_dev;
+
+static thread_local std::string g_last_error;
+void gpk_set_error(const std::string& msg) { g_last_error = msg; }
+
+extern "C" const char* gpk_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char* gpk_version(void) { return "gpk_b200 0.1 (sm_100a)"; }
+
+// literal in the grid's real type: the float value for the reference's FP32
+// arithmetic, the double value for the FP64 variant
+template <typename real> static inline real L(float f, double d);
+template <> inline float L<float>(float f, double) { return f; }
+template <> inline double L<double>(float, double d) { return d; }
+
+static bool g_device_ok = false;
+
+extern "C" int gpk_device_init(int device) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        gpk_set_error("no CUDA device available");
+        return GPK_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) {
+        gpk_set_error("device index out of range");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    GPK_CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp p;
+    GPK_CUDA_TRY(cudaGetDeviceProperties(&p, device));
+    if (p.major != 10) {
+        gpk_set_error("gpk_b200 is built for sm_100a (B200); found sm_" + std::to_string(p.major) +
+                      std::to_string(p.minor));
+        return GPK_ERR_NO_DEVICE;
+    }
+    g_device_ok = true;
+    return GPK_OK;
+}
+
+extern "C" void gpk_thermo_desc_init(gpk_thermo_desc* d, int32_t model) {
+    std::memset(d, 0, sizeof(*d));
+    d->model = model;
+    d->sigma0 = 0.5f; d->eps4 = 0.f; d->M0 = 1e-8f; d->Q = 0.f; d->Rgas = 8.314f;
+    d->noise_scale = 1.0f; d->kB = 1.380649e-23f;
+    d->k_partition = 1.0f;
+    d->elastic_smooth_iters = 8;
+}
+
+int gpk_alloc(gpk_grid* G, void** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        gpk_set_error("cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+        *p = nullptr;
+        return GPK_ERR_OUT_OF_MEMORY;
+    }
+    G->allocations.push_back(*p);
+    G->device_bytes += bytes;
+    return GPK_OK;
+}
+
+static void gpk_free(gpk_grid* G, void* p) {
+    if (!p) return;
+    auto it = std::find(G->allocations.begin(), G->allocations.end(), p);
+    if (it != G->allocations.end()) G->allocations.erase(it);
+    cudaFree(p);
+}
+
+__global__ static void k_fill_u32(int32_t* p, int n, int32_t v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+template <typename real>
+__global__ static void k_fill_real(real* p, int n, real v) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+__global__ static void k_histogram(int N, const int32_t* __restrict__ phi, int32_t* __restrict__ count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) atomicAdd(&count[phi[i]], 1);
+}
+
+int gpk_ensure_label_capacity(gpk_grid* G, int cap) {
+    if (cap <= G->label_cap) return GPK_OK;
+    int nc = std::max(cap, 64);
+    gpk_free(G, G->count); gpk_free(G, G->minF); gpk_free(G, G->minL); gpk_free(G, G->unres);
+    GPK_TRY(gpk_alloc(G, (void**)&G->count, sizeof(int32_t) * nc));
+    GPK_TRY(gpk_alloc(G, (void**)&G->minF, sizeof(int32_t) * nc));
+    GPK_TRY(gpk_alloc(G, (void**)&G->minL, sizeof(int32_t) * nc));
+    GPK_TRY(gpk_alloc(G, (void**)&G->unres, nc));
+    k_fill_u32<<<(nc + 255) / 256, 256, 0, G->stream>>>(G->minF, nc, 0x7fffffff);
+    k_fill_u32<<<(nc + 255) / 256, 256, 0, G->stream>>>(G->minL, nc, 0x7fffffff);
+    G->label_cap = nc;
+    return gpk_recount_labels(G);
+}
+
+int gpk_recount_labels(gpk_grid* G) {
+    GPK_CUDA_TRY(cudaMemsetAsync(G->count, 0, sizeof(int32_t) * G->label_cap, G->stream));
+    k_histogram<<<G->num_sms * 8, 256, 0, G->stream>>>(G->d.N, G->phi, G->count);
+    G->launches++;
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+// ---- host-built kernels (include/gpk_core.hpp:37-55, src/gpk_geometry.cpp:12-36) ----
+template <typename real>
+static void gauss_kernel(real sigma, std::vector<real>& w, int& radius, real& sigma_cells) {
+    sigma_cells = std::max(sigma, L<real>(0.5f, 0.5));
+    sigma = sigma_cells;
+    radius = (int)std::ceil(L<real>(3.5f, 3.5) * sigma);
+    const int sz = 2 * radius + 1;
+    w.assign(sz, (real)0);
+    real sum = 0;
+    for (int i = 0; i < sz; ++i) {
+        const real x = (real)(i - radius);
+        w[i] = std::exp(-x * x / (L<real>(2.f, 2.0) * sigma * sigma));
+        sum += w[i];
+    }
+    for (auto& v : w) v /= sum;
+}
+
+template <typename real>
+int gpk_build_tables(gpk_grid* G) {
+    HostKernels<real>* hk = new HostKernels<real>();
+    G->host_kernels = hk;
+    const real gs = (real)G->sigma;
+    gauss_kernel<real>(gs, hk->gauss_w, hk->gauss_radius, hk->gauss_sigma);
+    std::vector<real> tmp;
+    int r_unused;
+    const real vs_in = G->d.Nz > 1 ? std::clamp(L<real>(0.375f, 0.375) * gs, L<real>(0.85f, 0.85), L<real>(3.00f, 3.00))
+                                   : L<real>(0.85f, 0.85);
+    const real rs_in = G->d.Nz > 1 ? std::clamp(L<real>(0.125f, 0.125) * gs, L<real>(0.70f, 0.70), L<real>(1.00f, 1.00))
+                                   : L<real>(0.70f, 0.70);
+    gauss_kernel<real>(vs_in, tmp, r_unused, hk->vel_sigma);
+    gauss_kernel<real>(rs_in, tmp, r_unused, hk->remap_sigma);
+    // derivative-of-Gaussian taps
+    const int R = hk->gauss_radius + 2;
+    hk->geom_radius = R;
+    const int W = 2 * R + 1;
+    hk->w0.assign(W, (real)0); hk->w1.assign(W, (real)0); hk->w2.assign(W, (real)0);
+    const int first_offset[4] = {-2, -1, 1, 2};
+    const real first_coeff[4] = {L<real>(1.f, 1.0) / L<real>(12.f, 12.0), -L<real>(8.f, 8.0) / L<real>(12.f, 12.0),
+                                 L<real>(8.f, 8.0) / L<real>(12.f, 12.0), -L<real>(1.f, 1.0) / L<real>(12.f, 12.0)};
+    const int second_offset[5] = {-2, -1, 0, 1, 2};
+    const real second_coeff[5] = {-L<real>(1.f, 1.0) / L<real>(12.f, 12.0), L<real>(16.f, 16.0) / L<real>(12.f, 12.0),
+                                  -L<real>(30.f, 30.0) / L<real>(12.f, 12.0), L<real>(16.f, 16.0) / L<real>(12.f, 12.0),
+                                  -L<real>(1.f, 1.0) / L<real>(12.f, 12.0)};
+    auto gat = [&](int o) -> real {
+        if (o < -hk->gauss_radius || o > hk->gauss_radius) return (real)0;
+        return hk->gauss_w[o + hk->gauss_radius];
+    };
+    for (int o = -R; o <= R; ++o) {
+        const int j = o + R;
+        hk->w0[j] = gat(o);
+        for (int k = 0; k < 4; ++k) hk->w1[j] += first_coeff[k] * gat(o - first_offset[k]);
+        for (int k = 0; k < 5; ++k) hk->w2[j] += second_coeff[k] * gat(o - second_offset[k]);
+    }
+    hk->global_separable = G->d.Nz > 1 && R > 18;
+    // per-tap products, formed as the reference forms them: (gx*gy)*gz
+    const bool is3d = G->d.Nz > 1;
+    const int nz_taps = is3d ? W : 1;
+    hk->geom_table.assign((size_t)nz_taps * W * W * 12, (real)0);
+    for (int jz = 0; jz < nz_taps; ++jz) {
+        const real gz0 = is3d ? hk->w0[jz] : (real)1;
+        const real gz1 = is3d ? hk->w1[jz] : (real)0;
+        const real gz2 = is3d ? hk->w2[jz] : (real)0;
+        for (int jy = 0; jy < W; ++jy) {
+            const real gy0 = hk->w0[jy], gy1 = hk->w1[jy], gy2 = hk->w2[jy];
+            for (int jx = 0; jx < W; ++jx) {
+                const real gx0 = hk->w0[jx], gx1 = hk->w1[jx], gx2 = hk->w2[jx];
+                real* t = &hk->geom_table[(((size_t)jz * W + jy) * W + jx) * 12];
+                volatile real p;  // keep each product a separate rounded operation
+                p = gx1 * gy0; t[0] = p * gz0;
+                p = gx0 * gy1; t[1] = p * gz0;
+                p = gx2 * gy0; t[2] = p * gz0;
+                p = gx0 * gy2; t[3] = p * gz0;
+                p = gx1 * gy1; t[4] = p * gz0;
+                p = gx0 * gy0; t[5] = p * gz1;
+                p = gx0 * gy0; t[6] = p * gz2;
+                p = gx1 * gy0; t[7] = p * gz1;
+                p = gx0 * gy1; t[8] = p * gz1;
+            }
+        }
+    }
+    // projection / remap weights by squared distance
+    auto weights = [&](real s, int& radius, std::vector<double>& w) {
+        radius = std::max(1, (int)std::ceil(L<real>(3.f, 3.0) * s));
+        const real inv_two_sigma2 = L<real>(0.5f, 0.5) / (s * s);
+        const int r2max = 3 * radius * radius;
+        w.assign(r2max + 1, 0.0);
+        for (int r2 = 0; r2 <= r2max; ++r2) {
+            const real rr = (real)r2;
+            w[r2] = (double)std::exp(-rr * inv_two_sigma2);
+        }
+    };
+    weights(hk->vel_sigma, hk->proj_radius, hk->proj_w);
+    weights(hk->remap_sigma, hk->remap_radius, hk->remap_w);
+    // upload
+    GPK_TRY(gpk_alloc(G, &G->d_geom_table, sizeof(real) * hk->geom_table.size()));
+    GPK_CUDA_TRY(cudaMemcpy(G->d_geom_table, hk->geom_table.data(), sizeof(real) * hk->geom_table.size(),
+                            cudaMemcpyHostToDevice));
+    GPK_TRY(gpk_alloc(G, &G->d_gauss, sizeof(real) * hk->gauss_w.size()));
+    GPK_CUDA_TRY(cudaMemcpy(G->d_gauss, hk->gauss_w.data(), sizeof(real) * hk->gauss_w.size(), cudaMemcpyHostToDevice));
+    GPK_TRY(gpk_alloc(G, (void**)&G->d_proj_w, sizeof(double) * hk->proj_w.size()));
+    GPK_CUDA_TRY(cudaMemcpy(G->d_proj_w, hk->proj_w.data(), sizeof(double) * hk->proj_w.size(), cudaMemcpyHostToDevice));
+    GPK_TRY(gpk_alloc(G, (void**)&G->d_remap_w, sizeof(double) * hk->remap_w.size()));
+    GPK_CUDA_TRY(cudaMemcpy(G->d_remap_w, hk->remap_w.data(), sizeof(double) * hk->remap_w.size(),
+                            cudaMemcpyHostToDevice));
+    return GPK_OK;
+}
+
+template <typename real>
+static int init_fields(gpk_grid* G) {
+    const int N = G->d.N;
+    const int gN = std::min((N + 255) / 256, G->num_sms * 8);
+    struct Init { int f; double v; };
+    const Init inits[] = {{GPK_FIELD_ALPHA, 1.0}, {GPK_FIELD_T, 800.0}};
+    for (int f = 0; f < GPK_NUM_FIELDS; ++f)
+        if (G->f[f]) GPK_CUDA_TRY(cudaMemsetAsync(G->f[f], 0, G->rsz * N, G->stream));
+    for (const Init& in : inits) k_fill_real<real><<<gN, 256, 0, G->stream>>>((real*)G->f[in.f], N, (real)in.v);
+    GPK_CUDA_TRY(cudaMemsetAsync(G->phi, 0, sizeof(int32_t) * N, G->stream));
+    GPK_CUDA_TRY(cudaMemsetAsync(G->phi_comp, 0, sizeof(int32_t) * N, G->stream));
+    GPK_CUDA_TRY(cudaMemsetAsync(G->mask, 0, N, G->stream));
+    k_fill_u32<<<gN, 256, 0, G->stream>>>(G->pmap, N, -1);
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+static int validate_thermo(const gpk_thermo_desc* t) {
+    if (!t) { gpk_set_error("thermo descriptor is null"); return GPK_ERR_INVALID_ARGUMENT; }
+    if (t->model < 0 || t->model >= GPK_NUM_MODELS) {
+        gpk_set_error("unknown thermodynamic model tag " + std::to_string(t->model));
+        return GPK_ERR_UNSUPPORTED_MODEL;
+    }
+    if (t->model == GPK_MODEL_PRECIPITATION && (t->p[0] < 0 || t->p[0] > GPK_MAX_PHASES)) {
+        gpk_set_error("PrecipitationThermo: at most 8 phases");
+        return GPK_ERR_UNSUPPORTED_MODEL;
+    }
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_create(int Nz, int Ny, int Nx, double dx, const gpk_thermo_desc* thermo, double D,
+                               double gaussian_sigma, int precision, gpk_grid** out) {
+    if (!out) { gpk_set_error("out is null"); return GPK_ERR_INVALID_ARGUMENT; }
+    *out = nullptr;
+    if (Nz < 1 || Ny < 1 || Nx < 1 || (long long)Nz * Ny * Nx >= (1LL << 30)) {
+        gpk_set_error("grid dimensions must be positive with fewer than 2^30 cells");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    if (precision != GPK_PREC_F32 && precision != GPK_PREC_F64) {
+        gpk_set_error("precision must be GPK_PREC_F32 or GPK_PREC_F64");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    GPK_TRY(validate_thermo(thermo));
+    if (!g_device_ok) GPK_TRY(gpk_device_init(0));
+    gpk_grid* G = new gpk_grid();
+    G->d = Dims{Nz, Ny, Nx, Nz * Ny * Nx};
+    G->precision = precision;
+    G->rsz = precision == GPK_PREC_F32 ? 4 : 8;
+    G->dx = dx; G->D = D; G->sigma = gaussian_sigma;
+    G->th = *thermo;
+    cudaGetDevice(&G->device);
+    cudaDeviceGetAttribute(&G->num_sms, cudaDevAttrMultiProcessorCount, G->device);
+    int rc = GPK_OK;
+    auto fail = [&](int code) {
+        gpk_grid_destroy(G);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        gpk_set_error("cudaStreamCreate failed");
+        return fail(GPK_ERR_CUDA);
+    }
+    const size_t N = G->d.N;
+    const size_t rb = G->rsz * N;
+#define ALLOC(ptr, bytes) do { if ((rc = gpk_alloc(G, (void**)&(ptr), (bytes))) != GPK_OK) return fail(rc); } while (0)
+    ALLOC(G->phi, 4 * N);
+    ALLOC(G->phi_comp, 4 * N);
+    ALLOC(G->mask, N);
+    for (int f = 0; f < GPK_NUM_FIELDS; ++f) {
+        if (f == GPK_FIELD_PHI || f == GPK_FIELD_PHI_COMP || f == GPK_FIELD_MASK) continue;
+        ALLOC(G->f[f], rb);
+    }
+    ALLOC(G->vn2, rb);
+    ALLOC(G->c_new, rb);
+    ALLOC(G->active, 4 * N);
+    G->ntiles = (int)((N + 2047) / 2048);
+    ALLOC(G->tile_off, 4 * (size_t)(2 * G->ntiles + 8));
+    ALLOC(G->alpha_new_a, rb + 16);
+    ALLOC(G->cand, 4 * N);
+    ALLOC(G->cand_info, 16 * N);
+    ALLOC(G->pmap, 4 * N);
+    ALLOC(G->stamp, 4 * N);
+    ALLOC(G->ff_stack, 4 * (2 * N + 64));
+    ALLOC(G->bgr_res, rb);
+    ALLOC(G->bgr_best, rb);
+    ALLOC(G->key_a, 8 * N);
+    ALLOC(G->key_b, 8 * N);
+    ALLOC(G->val_a, 4 * N);
+    ALLOC(G->val_b, 4 * N);
+    ALLOC(G->exch, 16 * N);
+    ALLOC(G->ero_target, 4 * N);
+    ALLOC(G->ero_g, rb);
+    ALLOC(G->scal, sizeof(StepScalars));
+    {
+        size_t b1 = 0, b2 = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, b1, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                        (const int32_t*)nullptr, (int32_t*)nullptr, (int)N, 0, 64);
+        cub::DeviceRadixSort::SortPairs(nullptr, b2, (const int32_t*)nullptr, (int32_t*)nullptr,
+                                        (const unsigned long long*)nullptr, (unsigned long long*)nullptr, (int)N, 0, 32);
+        G->cub_tmp_bytes = std::max(b1, b2) + 256;
+        ALLOC(G->cub_tmp, G->cub_tmp_bytes);
+    }
+#undef ALLOC
+    if (cudaMallocHost((void**)&G->h_scal, sizeof(StepScalars)) != cudaSuccess) {
+        gpk_set_error("cudaMallocHost failed");
+        return fail(GPK_ERR_OUT_OF_MEMORY);
+    }
+    std::memset(G->h_scal, 0, sizeof(StepScalars));
+    if (cudaMemsetAsync(G->scal, 0, sizeof(StepScalars), G->stream) != cudaSuccess) return fail(GPK_ERR_CUDA);
+    rc = precision == GPK_PREC_F32 ? gpk_build_tables<float>(G) : gpk_build_tables<double>(G);
+    if (rc != GPK_OK) return fail(rc);
+    bool sep = precision == GPK_PREC_F32 ? ((HostKernels<float>*)G->host_kernels)->global_separable
+                                         : ((HostKernels<double>*)G->host_kernels)->global_separable;
+    if (sep) {
+        if ((rc = gpk_alloc(G, &G->sep_I, rb)) || (rc = gpk_alloc(G, &G->sep_t1, rb)) ||
+            (rc = gpk_alloc(G, &G->sep_t2, rb)) || (rc = gpk_alloc(G, &G->sep_S, rb)))
+            return fail(rc);
+    }
+    rc = precision == GPK_PREC_F32 ? init_fields<float>(G) : init_fields<double>(G);
+    if (rc != GPK_OK) return fail(rc);
+    if ((rc = gpk_ensure_label_capacity(G, 64)) != GPK_OK) return fail(rc);
+    if (cudaStreamSynchronize(G->stream) != cudaSuccess) {
+        gpk_set_error(std::string("grid initialisation failed: ") + cudaGetErrorString(cudaGetLastError()));
+        return fail(GPK_ERR_CUDA);
+    }
+    *out = G;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_destroy(gpk_grid* G) {
+    if (!G) return GPK_OK;
+    if (G->stream) cudaStreamSynchronize(G->stream);
+    for (void* p : G->allocations) cudaFree(p);
+    G->allocations.clear();
+    if (G->h_scal) cudaFreeHost(G->h_scal);
+    if (G->stream) cudaStreamDestroy(G->stream);
+    if (G->host_kernels) {
+        if (G->precision == GPK_PREC_F32) delete (HostKernels<float>*)G->host_kernels;
+        else delete (HostKernels<double>*)G->host_kernels;
+    }
+    delete G;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_set_thermo(gpk_grid* G, const gpk_thermo_desc* thermo) {
+    if (!G) return GPK_ERR_INVALID_ARGUMENT;
+    GPK_TRY(validate_thermo(thermo));
+    G->th = *thermo;
+    return GPK_OK;
+}
+
+static int check_field(gpk_grid* G, int field, size_t count) {
+    if (!G) { gpk_set_error("grid is null"); return GPK_ERR_INVALID_ARGUMENT; }
+    if (field < 0 || field >= GPK_NUM_FIELDS) {
+        gpk_set_error("unknown field id " + std::to_string(field));
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    if (count != (size_t)G->d.N) {
+        gpk_set_error("field transfer of " + std::to_string(count) + " elements; the grid has " +
+                      std::to_string(G->d.N));
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    return GPK_OK;
+}
+
+static void* field_ptr(gpk_grid* G, int field, size_t* esz) {
+    switch (field) {
+    case GPK_FIELD_PHI: *esz = 4; return G->phi;
+    case GPK_FIELD_PHI_COMP: *esz = 4; return G->phi_comp;
+    case GPK_FIELD_MASK: *esz = 1; return G->mask;
+    default: *esz = G->rsz; return G->f[field];
+    }
+}
+
+extern "C" int gpk_grid_upload(gpk_grid* G, int field, const void* host, size_t count) {
+    GPK_TRY(check_field(G, field, count));
+    if (!host) { gpk_set_error("host pointer is null"); return GPK_ERR_INVALID_ARGUMENT; }
+    size_t esz;
+    void* dst = field_ptr(G, field, &esz);
+    if (field == GPK_FIELD_PHI) {
+        const int32_t* p = (const int32_t*)host;
+        int32_t mx = 0;
+        for (size_t i = 0; i < count; ++i) {
+            if (p[i] < 0 || p[i] >= (1 << 26)) {
+                gpk_set_error("label " + std::to_string(p[i]) + " at cell " + std::to_string(i) +
+                              " lies outside [0, 2^26)");
+                return GPK_ERR_LABEL_RANGE;
+            }
+            mx = std::max(mx, p[i]);
+        }
+        GPK_CUDA_TRY(cudaMemcpyAsync(dst, host, esz * count, cudaMemcpyHostToDevice, G->stream));
+        GPK_TRY(gpk_ensure_label_capacity(G, mx + 1));
+        GPK_TRY(gpk_recount_labels(G));
+    } else if (field == GPK_FIELD_PHI_COMP) {
+        const int32_t* p = (const int32_t*)host;
+        for (size_t i = 0; i < count; ++i)
+            if (p[i] < 0 || p[i] >= (1 << 26)) {
+                gpk_set_error("competitor label outside [0, 2^26)");
+                return GPK_ERR_LABEL_RANGE;
+            }
+        GPK_CUDA_TRY(cudaMemcpyAsync(dst, host, esz * count, cudaMemcpyHostToDevice, G->stream));
+    } else {
+        GPK_CUDA_TRY(cudaMemcpyAsync(dst, host, esz * count, cudaMemcpyHostToDevice, G->stream));
+    }
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_download(gpk_grid* G, int field, void* host, size_t count) {
+    GPK_TRY(check_field(G, field, count));
+    if (!host) { gpk_set_error("host pointer is null"); return GPK_ERR_INVALID_ARGUMENT; }
+    size_t esz;
+    void* src = field_ptr(G, field, &esz);
+    GPK_CUDA_TRY(cudaMemcpyAsync(host, src, esz * count, cudaMemcpyDeviceToHost, G->stream));
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_device_ptr(gpk_grid* G, int field, void** dev_ptr) {
+    GPK_TRY(check_field(G, field, G ? (size_t)G->d.N : 0));
+    size_t esz;
+    *dev_ptr = field_ptr(G, field, &esz);
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_get_time(gpk_grid* G, double* t) {
+    if (!G || !t) return GPK_ERR_INVALID_ARGUMENT;
+    GPK_TRY(gpk_sync_scalars(G));
+    *t = G->h_scal->time;
+    return GPK_OK;
+}
+extern "C" int gpk_grid_set_time(gpk_grid* G, double t) {
+    if (!G) return GPK_ERR_INVALID_ARGUMENT;
+    GPK_CUDA_TRY(cudaMemcpyAsync(&G->scal->time, &t, sizeof(double), cudaMemcpyHostToDevice, G->stream));
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    return GPK_OK;
+}
+extern "C" int gpk_grid_get_step_id(gpk_grid* G, uint64_t* s) {
+    if (!G || !s) return GPK_ERR_INVALID_ARGUMENT;
+    *s = G->step_id;
+    return GPK_OK;
+}
+extern "C" int gpk_grid_set_step_id(gpk_grid* G, uint64_t s) {
+    if (!G) return GPK_ERR_INVALID_ARGUMENT;
+    G->step_id = s;
+    return GPK_OK;
+}
+
+static int step_once(gpk_grid* G, double dt, double cap) {
+    return G->precision == GPK_PREC_F32 ? gpk_step_impl<float>(G, dt, cap) : gpk_step_impl<double>(G, dt, cap);
+}
+
+extern "C" int gpk_grid_step(gpk_grid* G, double dt, double dt_cap, double* dt_used) {
+    if (!G) return GPK_ERR_INVALID_ARGUMENT;
+    GPK_TRY(step_once(G, dt, dt_cap));
+    if (dt_used) {
+        GPK_TRY(gpk_sync_scalars(G));
+        *dt_used = G->h_scal->dt;
+    }
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_step_n(gpk_grid* G, int n, double dt, double dt_cap, double* time_out) {
+    if (!G || n < 0) return GPK_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < n; ++k) GPK_TRY(step_once(G, dt, dt_cap));
+    if (time_out) {
+        GPK_TRY(gpk_sync_scalars(G));
+        *time_out = G->h_scal->time;
+    }
+    return GPK_OK;
+}
+
+// GPKGrid::run without callback (src/gpk_simulation.cpp:60-73)
+extern "C" int gpk_grid_run(gpk_grid* G, double t_end, double dt, int max_steps, int* steps_out) {
+    if (!G) return GPK_ERR_INVALID_ARGUMENT;
+    GPK_TRY(gpk_sync_scalars(G));
+    int n = 0;
+    while (G->h_scal->time < t_end && (max_steps <= 0 || n < max_steps)) {
+        const float remaining = (float)(t_end - G->h_scal->time);
+        GPK_TRY(step_once(G, dt, (double)remaining));
+        GPK_TRY(gpk_sync_scalars(G));
+        ++n;
+    }
+    if (steps_out) *steps_out = n;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_sync(gpk_grid* G) {
+    if (!G) return GPK_ERR_INVALID_ARGUMENT;
+    return gpk_sync_scalars(G);
+}
+
+extern "C" int gpk_grid_max_dt(gpk_grid* G, double* out) {
+    if (!G || !out) return GPK_ERR_INVALID_ARGUMENT;
+    return G->precision == GPK_PREC_F32 ? gpk_max_dt_impl<float>(G, out) : gpk_max_dt_impl<double>(G, out);
+}
+
+extern "C" int gpk_grid_counters(gpk_grid* G, uint64_t c[3]) {
+    if (!G || !c) return GPK_ERR_INVALID_ARGUMENT;
+    GPK_TRY(gpk_sync_scalars(G));
+    c[0] = G->h_scal->accepted;
+    c[1] = G->h_scal->deferred;
+    c[2] = G->h_scal->exchanges;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_topology_simple_move(gpk_grid* G, int cell, int32_t new_label, int* result) {
+    if (!G || !result) return GPK_ERR_INVALID_ARGUMENT;
+    if (cell < 0 || cell >= G->d.N) { *result = 0; return GPK_OK; }
+    return gpk_topology_simple_move_impl(G, cell, new_label, result);
+}
+
+extern "C" int gpk_grid_device_bytes(gpk_grid* G, size_t* out) {
+    if (!G || !out) return GPK_ERR_INVALID_ARGUMENT;
+    *out = G->device_bytes;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_launch_count(gpk_grid* G, uint64_t* out) {
+    if (!G || !out) return GPK_ERR_INVALID_ARGUMENT;
+    *out = G->launches;
+    return GPK_OK;
+}
+
+// ---- diagnostics (src/gpk_simulation.cpp:78-124) ---------------------------
+// phase_volume is a serial double sum in flat-index order in the reference;
+// it is a diagnostic outside the step, so the state is read back and summed
+// in that order.
+template <typename real>
+static int phase_volume_t(gpk_grid* G, int32_t label, double* out) {
+    const int N = G->d.N;
+    std::vector<int32_t> phi(N), pc(N);
+    std::vector<uint8_t> m(N);
+    std::vector<real> al(N);
+    GPK_CUDA_TRY(cudaMemcpyAsync(phi.data(), G->phi, 4 * (size_t)N, cudaMemcpyDeviceToHost, G->stream));
+    GPK_CUDA_TRY(cudaMemcpyAsync(pc.data(), G->phi_comp, 4 * (size_t)N, cudaMemcpyDeviceToHost, G->stream));
+    GPK_CUDA_TRY(cudaMemcpyAsync(m.data(), G->mask, (size_t)N, cudaMemcpyDeviceToHost, G->stream));
+    GPK_CUDA_TRY(cudaMemcpyAsync(al.data(), G->f[GPK_FIELD_ALPHA], sizeof(real) * N, cudaMemcpyDeviceToHost, G->stream));
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    double v = 0.0;
+    for (int i = 0; i < N; ++i) {
+        if (phi[i] == label) v += al[i];
+        if (m[i] && pc[i] == label && pc[i] != phi[i]) v += 1.0 - al[i];
+    }
+    *out = v;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_phase_volume(gpk_grid* G, int32_t label, double* out) {
+    if (!G || !out) return GPK_ERR_INVALID_ARGUMENT;
+    return G->precision == GPK_PREC_F32 ? phase_volume_t<float>(G, label, out) : phase_volume_t<double>(G, label, out);
+}
+
+extern "C" int gpk_grid_n_grains(gpk_grid* G, int* out) {
+    if (!G || !out) return GPK_ERR_INVALID_ARGUMENT;
+    std::vector<int32_t> c(G->label_cap);
+    GPK_CUDA_TRY(cudaMemcpyAsync(c.data(), G->count, sizeof(int32_t) * G->label_cap, cudaMemcpyDeviceToHost, G->stream));
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    int n = 0;
+    for (int v : c) n += v > 0;
+    *out = n;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_interface_fraction(gpk_grid* G, double* out) {
+    if (!G || !out) return GPK_ERR_INVALID_ARGUMENT;
+    std::vector<uint8_t> m(G->d.N);
+    GPK_CUDA_TRY(cudaMemcpyAsync(m.data(), G->mask, G->d.N, cudaMemcpyDeviceToHost, G->stream));
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    int cnt = 0;
+    for (uint8_t v : m) cnt += v != 0;
+    *out = (double)((float)cnt / (float)G->d.N);
+    return GPK_OK;
+}
+
+template int gpk_build_tables<float>(gpk_grid*);
+template int gpk_build_tables<double>(gpk_grid*);

@@ -1,0 +1,113 @@
+// gpk_grid.h — host-side state of one gpk_b200 grid and the launchers that
+// the C ABI (gpk_capi.cu) strings together into GPKGrid::step().
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/gpk_b200.h"
+#include "gpk_internal.cuh"
+
+// ---- error plumbing --------------------------------------------------------
+void gpk_set_error(const std::string& msg);
+#define GPK_CUDA_TRY(expr)                                                              \
+    do {                                                                                \
+        cudaError_t _e = (expr);                                                        \
+        if (_e != cudaSuccess) {                                                        \
+            gpk_set_error(std::string(#expr " failed: ") + cudaGetErrorString(_e));      \
+            return GPK_ERR_CUDA;                                                        \
+        }                                                                               \
+    } while (0)
+#define GPK_TRY(expr)                 \
+    do {                              \
+        int _s = (expr);              \
+        if (_s != GPK_OK) return _s;  \
+    } while (0)
+
+// Host-computed kernels of the reference (include/gpk_core.hpp:37-55,
+// src/gpk_geometry.cpp:12-36) in the grid's real type.
+template <typename real>
+struct HostKernels {
+    std::vector<real> gauss_w;             // GaussKernel(sigma).w
+    int gauss_radius = 0;
+    real gauss_sigma = 0, vel_sigma = 0, remap_sigma = 0;
+    std::vector<real> w0, w1, w2;          // derivative-of-Gaussian taps
+    int geom_radius = 0;
+    bool global_separable = false;
+    int proj_radius = 0, remap_radius = 0;
+    std::vector<double> proj_w;            // weight by squared distance r2
+    std::vector<double> remap_w;
+    std::vector<real> geom_table;          // per tap: 12 products (see build)
+};
+
+struct gpk_grid {
+    gpk_dev::Dims d{};
+    int precision = GPK_PREC_F32;
+    size_t rsz = 4;                        // bytes per real
+    double dx = 1, D = 0, sigma = 2;
+    gpk_thermo_desc th{};
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    int num_sms = 148;
+    uint64_t step_id = 0;
+    double time = 0;                       // host mirror (device copy in scal)
+    uint64_t launches = 0;
+
+    // public fields
+    int32_t* phi = nullptr;
+    int32_t* phi_comp = nullptr;
+    uint8_t* mask = nullptr;
+    void* f[GPK_NUM_FIELDS] = {};          // real fields by field id (phi/phi_comp/mask: null)
+
+    // scratch
+    void* vn2 = nullptr;                   // projection output before swap
+    void* c_new = nullptr;
+    void* eps_star = nullptr; void* eps_smooth = nullptr; void* eps_tmp = nullptr;
+    void* solid_old = nullptr; void* s_new = nullptr; void* delta = nullptr; void* cL = nullptr;
+    int have_solid_old = 0;
+    int32_t* active = nullptr;             // sorted interface cells
+    int32_t* tile_off = nullptr;           // compaction tile offsets
+    int ntiles = 0;
+    void* alpha_new_a = nullptr;           // per active position
+    int32_t* cand = nullptr;               // candidate active positions
+    int32_t* cand_info = nullptr;          // packed per-candidate wave state
+    int32_t* pmap = nullptr;               // pending map (cell -> item) or -1
+    int32_t* minF = nullptr; int32_t* minL = nullptr;
+    uint32_t* stamp = nullptr; int32_t* ff_stack = nullptr;
+    // remap
+    void* bgr_res = nullptr; void* bgr_best = nullptr;   // per active position (real)
+    unsigned long long* key_a = nullptr; unsigned long long* key_b = nullptr;
+    int32_t* val_a = nullptr; int32_t* val_b = nullptr;
+    int32_t* exch = nullptr;               // exchange slots: a, b, low, high, state
+    void* cub_tmp = nullptr; size_t cub_tmp_bytes = 0;
+    // extinction
+    uint8_t* unres = nullptr; int32_t* ero_target = nullptr; void* ero_g = nullptr;
+    // separable geometry
+    void* sep_I = nullptr; void* sep_t1 = nullptr; void* sep_t2 = nullptr; void* sep_S = nullptr;
+    // labels
+    int32_t* count = nullptr;              // cells per label
+    int label_cap = 0;                     // labels live in [0, label_cap)
+    // tables
+    void* d_geom_table = nullptr; void* d_w0 = nullptr; void* d_w1 = nullptr; void* d_w2 = nullptr;
+    void* d_gauss = nullptr; double* d_proj_w = nullptr; double* d_remap_w = nullptr;
+    gpk_dev::StepScalars* scal = nullptr;  // device scalars
+    gpk_dev::StepScalars* h_scal = nullptr;  // pinned host mirror
+    void* host_kernels = nullptr;          // HostKernels<real>*
+    std::vector<void*> allocations;
+    size_t device_bytes = 0;
+};
+
+// ---- launchers (templated on the grid's real type) --------------------------
+template <typename real> int gpk_build_tables(gpk_grid* G);
+template <typename real> int gpk_step_impl(gpk_grid* G, double dt, double dt_cap);
+template <typename real> int gpk_interface_mask(gpk_grid* G);
+template <typename real> int gpk_max_dt_impl(gpk_grid* G, double* out);
+template <typename real> int gpk_phase_volume_impl(gpk_grid* G, int32_t label, double* out);
+int gpk_recount_labels(gpk_grid* G);
+int gpk_topology_simple_move_impl(gpk_grid* G, int cell, int32_t new_label, int* result);
+int gpk_alloc(gpk_grid* G, void** p, size_t bytes);
+int gpk_ensure_label_capacity(gpk_grid* G, int cap);
+int gpk_sync_scalars(gpk_grid* G);

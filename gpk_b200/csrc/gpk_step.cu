@@ -1,0 +1,1227 @@
+// gpk_step.cu — the per-step kernels of GPKGrid::step() and their sequencing.
+//
+// Reference (albert-hzbn/GPK):
+//   step order           src/gpk_simulation.cpp:31-54
+//   interface mask       src/gpk_geometry.cpp:42-82
+//   geometry (direct)    src/gpk_geometry.cpp:88-183
+//   geometry (separable) src/gpk_geometry.cpp:185-390, src/gpk_gaussian.cpp:9-72
+//   elastic proxy        src/gpk_physics.cpp:10-63
+//   velocities           src/gpk_physics.cpp:67-148
+//   pair projection      src/gpk_physics.cpp:152-193
+//   max_dt               src/gpk_simulation.cpp:11-23
+//   alpha integration    src/gpk_transitions.cpp:251-271
+//   transport, recovery  src/gpk_transport.cpp:11-152
+//
+// Every real-valued expression keeps the reference's operand order; with
+// -fmad=false the float path rounds exactly like the reference build.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+
+#include "gpk_grid.h"
+
+namespace gpk_dev {
+
+// ---------------------------------------------------------------------------
+// interface mask + ordered compaction
+// ---------------------------------------------------------------------------
+static constexpr int MASK_TPB = 256;
+static constexpr int MASK_IPT = 8;
+static constexpr int MASK_TILE = MASK_TPB * MASK_IPT;
+
+__global__ void __launch_bounds__(MASK_TPB) k_mask_tiles(Dims D, const int32_t* __restrict__ phi,
+                                                         uint8_t* __restrict__ mask, int32_t* __restrict__ tile_cnt) {
+    typedef cub::BlockReduce<int, MASK_TPB> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const int base = blockIdx.x * MASK_TILE;
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < MASK_IPT; ++k) {
+        const int i = base + k * MASK_TPB + threadIdx.x;
+        if (i < D.N) {
+            int nb[6];
+            D.faces(i, nb);
+            const int32_t v = phi[i];
+            const uint8_t act = (uint8_t)((v != phi[nb[0]]) | (v != phi[nb[1]]) | (v != phi[nb[2]]) |
+                                          (v != phi[nb[3]]) | (v != phi[nb[4]]) | (v != phi[nb[5]]));
+            mask[i] = act;
+            cnt += act;
+        }
+    }
+    const int total = BR(tmp).Sum(cnt);
+    if (threadIdx.x == 0) tile_cnt[blockIdx.x] = total;
+}
+
+// Exclusive scan of tile counts in one block; writes the total.
+__global__ void __launch_bounds__(1024) k_scan_tiles(int32_t* __restrict__ tile, int ntiles, unsigned* __restrict__ total) {
+    typedef cub::BlockScan<int, 1024> BS;
+    __shared__ typename BS::TempStorage tmp;
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < ntiles; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int v = i < ntiles ? tile[i] : 0;
+        int ex, agg;
+        BS(tmp).ExclusiveSum(v, ex, agg);
+        if (i < ntiles) tile[i] = ex + carry;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += agg;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = (unsigned)carry;
+}
+
+// Writes the flat indices of flagged cells in increasing order.
+__global__ void __launch_bounds__(MASK_TPB) k_compact_u8(int n, const uint8_t* __restrict__ flag,
+                                                         const int32_t* __restrict__ tile_off, int32_t* __restrict__ out) {
+    typedef cub::BlockScan<int, MASK_TPB> BS;
+    __shared__ typename BS::TempStorage tmp;
+    const int base = blockIdx.x * MASK_TILE;
+    int f[MASK_IPT];
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < MASK_IPT; ++k) {
+        const int i = base + threadIdx.x * MASK_IPT + k;
+        f[k] = (i < n) ? flag[i] : 0;
+        cnt += f[k];
+    }
+    int ex;
+    BS(tmp).ExclusiveSum(cnt, ex);
+    int pos = tile_off[blockIdx.x] + ex;
+#pragma unroll
+    for (int k = 0; k < MASK_IPT; ++k) {
+        const int i = base + threadIdx.x * MASK_IPT + k;
+        if (f[k]) out[pos++] = i;
+    }
+}
+
+// Tile counts of a u8 flag array whose valid length is read on the device.
+__global__ void __launch_bounds__(MASK_TPB) k_count_u8(const uint8_t* __restrict__ flag, const unsigned* __restrict__ n_ptr,
+                                                       int32_t* __restrict__ tile_cnt) {
+    typedef cub::BlockReduce<int, MASK_TPB> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const int n = (int)*n_ptr;
+    const int base = blockIdx.x * MASK_TILE;
+    int cnt = 0;
+    for (int k = 0; k < MASK_IPT; ++k) {
+        const int i = base + k * MASK_TPB + threadIdx.x;
+        if (i < n) cnt += flag[i];
+    }
+    const int total = BR(tmp).Sum(cnt);
+    if (threadIdx.x == 0) tile_cnt[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(MASK_TPB) k_compact_u8_dyn(const unsigned* __restrict__ n_ptr,
+                                                             const uint8_t* __restrict__ flag,
+                                                             const int32_t* __restrict__ tile_off,
+                                                             int32_t* __restrict__ out) {
+    typedef cub::BlockScan<int, MASK_TPB> BS;
+    __shared__ typename BS::TempStorage tmp;
+    const int n = (int)*n_ptr;
+    const int base = blockIdx.x * MASK_TILE;
+    int f[MASK_IPT];
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < MASK_IPT; ++k) {
+        const int i = base + threadIdx.x * MASK_IPT + k;
+        f[k] = (i < n) ? flag[i] : 0;
+        cnt += f[k];
+    }
+    int ex;
+    BS(tmp).ExclusiveSum(cnt, ex);
+    int pos = tile_off[blockIdx.x] + ex;
+#pragma unroll
+    for (int k = 0; k < MASK_IPT; ++k) {
+        const int i = base + threadIdx.x * MASK_IPT + k;
+        if (f[k]) out[pos++] = i;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// direct Gaussian-Hessian geometry + competitor choice
+// ---------------------------------------------------------------------------
+// table layout per tap t = ((dz+R)*W + (dy+R))*W + (dx+R), 12 reals:
+//   [0] gx1*gy0*gz0 (Ix)   [1] gx0*gy1*gz0 (Iy)  [2] gx2*gy0*gz0 (Ixx) [3] gx0*gy2*gz0 (Iyy)
+//   [4] gx1*gy1*gz0 (Ixy)  [5] gx0*gy0*gz1 (Iz)  [6] gx0*gy0*gz2 (Izz) [7] gx1*gy0*gz1 (Ixz)
+//   [8] gx0*gy1*gz1 (Iyz)  [9..11] 0
+// each product formed on the host exactly as the reference forms it, (a*b)*c.
+
+template <typename real>
+__device__ __forceinline__ void competitor_at(const Dims& D, const int32_t* __restrict__ phi, int i, real nx, real ny,
+                                              real nz, int32_t* __restrict__ phi_comp) {
+    int z, y, x;
+    D.decode(i, z, y, x);
+    int nei[6];
+    D.faces(i, nei);
+    const real score[6] = {-nx, nx, -ny, ny, -nz, nz};
+    const int nf = D.nface();
+    const bool is3d = D.is3d();
+    const int32_t pi = phi[i];
+    int best = -1, best_support = -1;
+    real best_score = (real)-2;
+    for (int k = 0; k < nf; ++k) {
+        const int32_t q = phi[nei[k]];
+        if (q == pi) continue;
+        int support = 0;
+        for (int dz = (is3d ? -1 : 0); dz <= (is3d ? 1 : 0); ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    if (!dx && !dy && !dz) continue;
+                    const int xx = wrap1(x + dx, D.Nx), yy = wrap1(y + dy, D.Ny), zz = wrap1(z + dz, D.Nz);
+                    support += phi[D.idx(zz, yy, xx)] == q;
+                }
+        if (support > best_support || (support == best_support && score[k] > best_score)) {
+            best = k; best_support = support; best_score = score[k];
+        }
+    }
+    phi_comp[i] = (best >= 0) ? phi[nei[best]] : pi;
+}
+
+template <typename real>
+__device__ __forceinline__ void finish_geometry(int i, real Ix, real Iy, real Iz, real Ixx, real Iyy, real Izz, real Ixy,
+                                                real Ixz, real Iyz, real dx, real kappa_limit, real* nxo, real* nyo,
+                                                real* nzo, real* ko, real& nxv, real& nyv, real& nzv) {
+    const real grad_sq = Ix * Ix + Iy * Iy + Iz * Iz;
+    nxv = nyv = nzv = (real)0;
+    if (grad_sq * dx * dx > (real)1e-8) {
+        const real grad = sqrt(grad_sq);
+        nxv = -Ix / grad;
+        nyv = -Iy / grad;
+        nzv = -Iz / grad;
+        const real trace_H = Ixx + Iyy + Izz;
+        const real gHg = Ix * Ix * Ixx + Iy * Iy * Iyy + Iz * Iz * Izz + (real)2 * (Ix * Iy * Ixy + Ix * Iz * Ixz + Iy * Iz * Iyz);
+        real curvature = (gHg - grad_sq * trace_H) / (grad_sq * grad);
+        if (fabs(curvature * dx) < (real)1e-6) curvature = (real)0;
+        nxo[i] = nxv; nyo[i] = nyv; nzo[i] = nzv;
+        ko[i] = dclamp(curvature, -kappa_limit, kappa_limit);
+    }
+}
+
+template <typename real, bool IS3D>
+__global__ void __launch_bounds__(128) k_geometry_direct(Dims D, const int32_t* __restrict__ active,
+                                                         const unsigned* __restrict__ n_active,
+                                                         const int32_t* __restrict__ phi, const real* __restrict__ table,
+                                                         int R, real inv_dx, real inv_dx2, real dx, real kappa_limit,
+                                                         real* __restrict__ nxo, real* __restrict__ nyo,
+                                                         real* __restrict__ nzo, real* __restrict__ ko,
+                                                         int32_t* __restrict__ phi_comp) {
+    const int na = (int)*n_active;
+    const int W = 2 * R + 1;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
+        const int i = active[a];
+        const int32_t resident = phi[i];
+        int z0, y0, x0;
+        D.decode(i, z0, y0, x0);
+        real Ix = 0, Iy = 0, Iz = 0, Ixx = 0, Iyy = 0, Izz = 0, Ixy = 0, Ixz = 0, Iyz = 0;
+        const int dzb = IS3D ? -R : 0, dze = IS3D ? R : 0;
+        for (int dz = dzb; dz <= dze; ++dz) {
+            const int z = IS3D ? wrap_any(z0 + dz, D.Nz) : z0;
+            for (int dy = -R; dy <= R; ++dy) {
+                const int y = wrap_any(y0 + dy, D.Ny);
+                const int32_t* row = phi + (size_t)(z * D.Ny + y) * D.Nx;
+                const int zoff = IS3D ? (dz + R) * W : 0;
+                const real* trow = table + (size_t)((zoff + (dy + R)) * W) * 12;
+                for (int dx = -R; dx <= R; ++dx) {
+                    int x = x0 + dx;
+                    if (x < 0 || x >= D.Nx) x = wrap_any(x, D.Nx);
+                    if (row[x] != resident) continue;
+                    const real* t = trow + (dx + R) * 12;
+                    Ix += t[0]; Iy += t[1]; Ixx += t[2]; Iyy += t[3]; Ixy += t[4];
+                    if (IS3D) { Iz += t[5]; Izz += t[6]; Ixz += t[7]; Iyz += t[8]; }
+                }
+            }
+        }
+        Ix *= inv_dx; Iy *= inv_dx; Iz *= inv_dx;
+        Ixx *= inv_dx2; Iyy *= inv_dx2; Izz *= inv_dx2;
+        Ixy *= inv_dx2; Ixz *= inv_dx2; Iyz *= inv_dx2;
+        real nxv, nyv, nzv;
+        finish_geometry<real>(i, Ix, Iy, Iz, Ixx, Iyy, Izz, Ixy, Ixz, Iyz, dx, kappa_limit, nxo, nyo, nzo, ko, nxv, nyv, nzv);
+        competitor_at<real>(D, phi, i, nxv, nyv, nzv, phi_comp);
+    }
+}
+
+// ---- separable path (broad 3-D kernels) -----------------------------------
+template <typename real>
+__global__ void k_indicator(int N, const int32_t* __restrict__ phi, int32_t p, real* __restrict__ I) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        I[i] = (phi[i] == p) ? (real)1 : (real)0;
+}
+
+// one periodic 1-D pass along axis (0 = x, 1 = y, 2 = z)
+template <typename real>
+__global__ void k_gauss_pass(Dims D, const real* __restrict__ in, real* __restrict__ out, const real* __restrict__ kw,
+                             int krad, int axis) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.N; i += gridDim.x * blockDim.x) {
+        int z, y, x;
+        D.decode(i, z, y, x);
+        real acc = 0;
+        for (int k = 0, ki = -krad; ki <= krad; ++k, ++ki) {
+            int j;
+            if (axis == 0) j = D.idx(z, y, wrap1(x + ki, D.Nx));
+            else if (axis == 1) j = D.idx(z, wrap1(y + ki, D.Ny), x);
+            else j = D.idx(wrap1(z + ki, D.Nz), y, x);
+            acc += kw[k] * in[j];
+        }
+        out[i] = acc;
+    }
+}
+
+template <typename real>
+__global__ void k_separable_eval(Dims D, const int32_t* __restrict__ phi, const uint8_t* __restrict__ mask, int32_t p,
+                                 const real* __restrict__ S, real dx, real kappa_limit, real* __restrict__ nxo,
+                                 real* __restrict__ nyo, real* __restrict__ nzo, real* __restrict__ ko) {
+    const int Nx = D.Nx, Ny = D.Ny, Nz = D.Nz;
+    const real idx12 = (real)1 / ((real)12 * dx);
+    const real idx_sq = (real)1 / (dx * dx);
+    const real idx12_sq = idx_sq / (real)12;
+    const real idx144_sq = idx_sq / (real)144;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.N; i += gridDim.x * blockDim.x) {
+        if (!mask[i] || phi[i] != p) continue;
+        int z, y, x;
+        D.decode(i, z, y, x);
+        const int xm = (x == 0 ? Nx - 1 : x - 1), xp = (x == Nx - 1 ? 0 : x + 1);
+        const int ym = (y == 0 ? Ny - 1 : y - 1), yp = (y == Ny - 1 ? 0 : y + 1);
+        const int zm = (z == 0 ? Nz - 1 : z - 1), zp = (z == Nz - 1 ? 0 : z + 1);
+        const int xmm = (x < 2 ? x + Nx - 2 : x - 2), xpp = (x >= Nx - 2 ? x - Nx + 2 : x + 2);
+        const int ymm = (y < 2 ? y + Ny - 2 : y - 2), ypp = (y >= Ny - 2 ? y - Ny + 2 : y + 2);
+        const int zmm = (z < 2 ? z + Nz - 2 : z - 2), zpp = (z >= Nz - 2 ? z - Nz + 2 : z + 2);
+        const real I0 = S[i];
+        const real Ix = (S[D.idx(z, y, xmm)] - (real)8 * S[D.idx(z, y, xm)] + (real)8 * S[D.idx(z, y, xp)] -
+                         S[D.idx(z, y, xpp)]) * idx12;
+        const real Iy = (S[D.idx(z, ymm, x)] - (real)8 * S[D.idx(z, ym, x)] + (real)8 * S[D.idx(z, yp, x)] -
+                         S[D.idx(z, ypp, x)]) * idx12;
+        const real Iz = (Nz > 1) ? (S[D.idx(zmm, y, x)] - (real)8 * S[D.idx(zm, y, x)] + (real)8 * S[D.idx(zp, y, x)] -
+                                    S[D.idx(zpp, y, x)]) * idx12
+                                 : (real)0;
+        const real Ixx = (-S[D.idx(z, y, xpp)] + (real)16 * S[D.idx(z, y, xp)] - (real)30 * I0 +
+                          (real)16 * S[D.idx(z, y, xm)] - S[D.idx(z, y, xmm)]) * idx12_sq;
+        const real Iyy = (-S[D.idx(z, ypp, x)] + (real)16 * S[D.idx(z, yp, x)] - (real)30 * I0 +
+                          (real)16 * S[D.idx(z, ym, x)] - S[D.idx(z, ymm, x)]) * idx12_sq;
+        const real Izz = (Nz > 1) ? (-S[D.idx(zpp, y, x)] + (real)16 * S[D.idx(zp, y, x)] - (real)30 * I0 +
+                                     (real)16 * S[D.idx(zm, y, x)] - S[D.idx(zmm, y, x)]) * idx12_sq
+                                  : (real)0;
+        const int xo[4] = {xmm, xm, xp, xpp};
+        const int yo[4] = {ymm, ym, yp, ypp};
+        const int zo[4] = {zmm, zm, zp, zpp};
+        const real dc[4] = {(real)1, (real)-8, (real)8, (real)-1};
+        real Ixy_sum = 0, Ixz_sum = 0, Iyz_sum = 0;
+        for (int aa = 0; aa < 4; ++aa)
+            for (int b = 0; b < 4; ++b) {
+                const real w = dc[aa] * dc[b];
+                Ixy_sum += w * S[D.idx(z, yo[b], xo[aa])];
+                if (Nz > 1) {
+                    Ixz_sum += w * S[D.idx(zo[b], y, xo[aa])];
+                    Iyz_sum += w * S[D.idx(zo[b], yo[aa], x)];
+                }
+            }
+        const real Ixy = Ixy_sum * idx144_sq;
+        const real Ixz = (Nz > 1) ? Ixz_sum * idx144_sq : (real)0;
+        const real Iyz = (Nz > 1) ? Iyz_sum * idx144_sq : (real)0;
+        const real grad_sq = Ix * Ix + Iy * Iy + Iz * Iz;
+        if (grad_sq * dx * dx > (real)1e-8) {
+            const real inv_grad = (real)1 / sqrt(grad_sq);
+            nxo[i] = -Ix * inv_grad;
+            nyo[i] = -Iy * inv_grad;
+            nzo[i] = -Iz * inv_grad;
+            const real trace_H = Ixx + Iyy + Izz;
+            const real gHg = Ix * Ix * Ixx + Iy * Iy * Iyy + Iz * Iz * Izz + (real)2 * (Ix * Iy * Ixy + Ix * Iz * Ixz + Iy * Iz * Iyz);
+            real k = (gHg - grad_sq * trace_H) / (grad_sq * sqrt(grad_sq));
+            if (fabs(k * dx) < (real)1e-6) k = (real)0;
+            ko[i] = dclamp(k, -kappa_limit, kappa_limit);
+        }
+    }
+}
+
+template <typename real>
+__global__ void k_competitor_all(Dims D, const int32_t* __restrict__ active, const unsigned* __restrict__ n_active,
+                                 const int32_t* __restrict__ phi, const real* __restrict__ nx, const real* __restrict__ ny,
+                                 const real* __restrict__ nz, int32_t* __restrict__ phi_comp) {
+    const int na = (int)*n_active;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
+        const int i = active[a];
+        competitor_at<real>(D, phi, i, nx[i], ny[i], nz[i], phi_comp);
+    }
+}
+
+__global__ void k_label_flags(int N, const int32_t* __restrict__ phi, const uint8_t* __restrict__ mask,
+                              uint8_t* __restrict__ present, int cap) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        if (mask[i]) present[phi[i]] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// constitutive laws (src/gpk_thermo.cpp:9-47, include/gpk_thermo.hpp)
+// ---------------------------------------------------------------------------
+struct ThermoDev {
+    gpk_thermo_desc t;
+    float log_pH2;   // ReductionThermo: logf(pH2_over_pH2O), formed on the host
+    float mu0;       // ThermoModel::MU0 = 4.0e-7f * pi (float)
+};
+
+template <typename real> __device__ __forceinline__ real dev_pi();
+template <> __device__ __forceinline__ float dev_pi<float>() { return 3.14159265358979323846f; }
+template <> __device__ __forceinline__ double dev_pi<double>() { return 3.14159265358979323846; }
+
+template <typename real>
+__device__ real th_sigma_base(const gpk_thermo_desc& th, real nx, real ny, real nz, real g) {
+    if ((real)th.eps4 == (real)0) return (real)th.sigma0;
+    const real cg = cos(g), sg = sin(g);
+    const real ncx = nx * cg + ny * sg;
+    const real ncy = -nx * sg + ny * cg;
+    const real ncz = nz;
+    real aniso;
+    if (ncz == (real)0) aniso = cos((real)4 * atan2(ncy, ncx));
+    else aniso = ncx * ncx * ncx * ncx + ncy * ncy * ncy * ncy + ncz * ncz * ncz * ncz - (real)0.6;
+    return (real)th.sigma0 * ((real)1 + (real)th.eps4 * aniso);
+}
+
+template <typename real>
+__device__ real th_sigma(const gpk_thermo_desc& th, real nx, real ny, real nz, real g, int32_t p, int32_t q, real c) {
+    switch (th.model) {
+    case GPK_MODEL_TENSOR_ANISO:
+    case GPK_MODEL_ANISO_OSTWALD: {
+        const real cg = cos(g), sg = sin(g);
+        const real ncx = nx * cg + ny * sg;
+        const real ncy = -nx * sg + ny * cg;
+        const real ncz = nz;
+        const real K = (real)th.p[0] * ncx * ncx + (real)th.p[1] * ncy * ncy + (real)th.p[2] * ncz * ncz;
+        return (real)th.sigma0 * sqrt(dmax(K, (real)1e-12));
+    }
+    case GPK_MODEL_GROOVING: return (p == 0 || q == 0) ? (real)th.p[1] : (real)th.p[0];
+    case GPK_MODEL_NDFEB:
+        if (p == 0 || q == 0) {
+            const real s0 = (real)th.p[1];
+            const real s = s0 * ((real)1 - (real)th.p[2] * c);
+            return dclamp(s, (real)0, s0);
+        }
+        return (real)th.p[0];
+    default: return th_sigma_base<real>(th, nx, ny, nz, g);
+    }
+}
+
+template <typename real>
+__device__ real th_mobility(const gpk_thermo_desc& th, real gp, real gq, real T) {
+    if (th.model != GPK_MODEL_BASE) return (real)th.M0;
+    const real PI = dev_pi<real>();
+    real dg = fabs(gp - gq);
+    dg = fmod(dg + PI * (real)0.5, PI * (real)0.5);
+    if (dg > PI * (real)0.25) dg = PI * (real)0.5 - dg;
+    const real theta_m = (real)15 * PI / (real)180;
+    real mis;
+    if (dg < (real)1e-6) mis = 0;
+    else if (dg >= theta_m) mis = 1;
+    else { const real frac = dg / theta_m; mis = frac * ((real)1 - log(frac)); }
+    const real arr = ((real)th.Q > (real)0) ? exp(-(real)th.Q / ((real)th.Rgas * dmax(T, (real)1))) : (real)1;
+    return (real)th.M0 * mis * arr;
+}
+
+template <typename real>
+__device__ __forceinline__ real th_precip_G(const gpk_thermo_desc& th, int q, real c, real T) {
+    return (real)th.p[2 + q] + (real)th.p[10 + q] * c + (real)th.p[18 + q] * c * c + (real)th.p[26 + q] * (T - (real)th.p[1]);
+}
+
+template <typename real>
+__device__ real th_bulk(const ThermoDev& TD, int32_t p, int32_t q, real c, real T) {
+    const gpk_thermo_desc& th = TD.t;
+    switch (th.model) {
+    case GPK_MODEL_SOLIDIFICATION: {
+        const real T_liq = (real)th.p[2] + (real)th.p[0] * c;
+        const real dT = T_liq - T;
+        const real dG = ((real)th.p[3] / (real)th.p[2]) * dT;
+        if (p == 0 && q == 1) return -dG;
+        if (p == 1 && q == 0) return +dG;
+        return 0;
+    }
+    case GPK_MODEL_RECRYSTALLISATION: {
+        const real E = (real)th.p[0];
+        if (p == 0 && q >= 1) return -E;
+        if (p >= 1 && q == 0) return +E;
+        return 0;
+    }
+    case GPK_MODEL_OSTWALD:
+        if (p == 0) return (real)th.p[1] * ((real)th.p[0] - c);
+        if (p >= 1) return (real)th.p[1] * (c - (real)th.p[0]);
+        return 0;
+    case GPK_MODEL_TENSOR_ANISO: {
+        const real bias = (real)th.p[3];
+        if (bias == (real)0) return 0;
+        return (p != 0) ? bias : -bias;
+    }
+    case GPK_MODEL_ANISO_OSTWALD:
+        if (p == 0) return (real)th.p[4] * ((real)th.p[3] - c);
+        return (real)th.p[4] * (c - (real)th.p[3]);
+    case GPK_MODEL_PRECIPITATION: {
+        const int np = (int)th.p[0];
+        if (p < 0 || p >= np || q < 0 || q >= np) return 0;
+        return th_precip_G<real>(th, q, c, T) - th_precip_G<real>(th, p, c, T);
+    }
+    case GPK_MODEL_REDUCTION: {
+        const real dG_mol = (real)th.p[1] - (real)8.314 * T * (real)TD.log_pH2;
+        const real dG_vol = dG_mol / (real)th.p[2];
+        if (p == 0 && q >= 1) return dG_vol;
+        if (p >= 1 && q == 0) return -dG_vol;
+        return 0;
+    }
+    case GPK_MODEL_NDFEB:
+        if (p != 0) return (real)th.p[4] * ((real)th.p[3] - c);
+        return (real)th.p[4] * (c - (real)th.p[3]);
+    default: return 0;
+    }
+}
+
+template <typename real>
+__device__ __forceinline__ real th_iface_comp(const gpk_thermo_desc& th, int32_t p, int32_t q, real cp, real cq) {
+    if (th.model == GPK_MODEL_OSTWALD || th.model == GPK_MODEL_ANISO_OSTWALD) {
+        if (p == 0) return cp;
+        if (q == 0) return cq;
+    }
+    return cp;
+}
+
+template <typename real>
+__device__ int th_select(const gpk_thermo_desc& th, int32_t p, real c, real T, const int32_t* cand, int n) {
+    if (th.model != GPK_MODEL_PRECIPITATION) return -1;
+    const int np = (int)th.p[0];
+    real best = (real)1e30;
+    int best_q = -1;
+    for (int k = 0; k < n; ++k) {
+        const int32_t q = cand[k];
+        if (q < 0 || q >= np || q == p) continue;
+        const real dG = th_precip_G<real>(th, q, c, T) - th_precip_G<real>(th, p, c, T);
+        if (dG < best) { best = dG; best_q = q; }
+    }
+    return best_q;
+}
+
+template <typename real>
+__device__ __forceinline__ real th_Emag(const ThermoDev& TD, real g) {
+    const gpk_thermo_desc& th = TD.t;
+    if (!th.magnetic_enabled) return 0;
+    const real c1 = cos(g - (real)th.g_easy_ref);
+    const real c2 = cos(g - (real)th.H_theta);
+    return -(real)th.Ku * c1 * c1 - (real)TD.mu0 * (real)th.Ms * (real)th.H_ext * c2;
+}
+
+// ---------------------------------------------------------------------------
+// velocities (src/gpk_physics.cpp:67-148)
+// ---------------------------------------------------------------------------
+template <typename real>
+__global__ void k_velocities(Dims D, ThermoDev TD, const int32_t* __restrict__ active, const unsigned* __restrict__ n_active,
+                             const int32_t* __restrict__ phi, int32_t* __restrict__ phi_comp, const real* __restrict__ c,
+                             const real* __restrict__ T, const real* __restrict__ g, const real* __restrict__ rho,
+                             const real* __restrict__ nx, const real* __restrict__ ny, const real* __restrict__ nz,
+                             const real* __restrict__ kappa, const real* __restrict__ E_el, real* __restrict__ vn,
+                             real* __restrict__ g_comp) {
+    const gpk_thermo_desc& th = TD.t;
+    const int na = (int)*n_active;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
+        const int i = active[a];
+        int nei[6];
+        D.faces(i, nei);
+        const int32_t pi = phi[i];
+        if (th.phase_selection) {
+            int32_t cand[6];
+            int ncand = 0;
+            for (int k = 0; k < 6; ++k) {
+                const int32_t q = phi[nei[k]];
+                if (q == pi) continue;
+                bool seen = false;
+                for (int cc = 0; cc < ncand; ++cc)
+                    if (cand[cc] == q) { seen = true; break; }
+                if (!seen) cand[ncand++] = q;
+            }
+            const int sel = th_select<real>(th, pi, c[i], T[i], cand, ncand);
+            if (sel >= 0) phi_comp[i] = sel;
+        }
+        const int32_t qid = phi_comp[i];
+        const real g_p = g[i];
+        real g_q = g_p, c_q = c[i];
+        int qk = -1;
+        for (int k = 0; k < 6; ++k)
+            if (phi[nei[k]] == qid) { qk = nei[k]; break; }
+        if (qk >= 0) { g_q = g[qk]; c_q = c[qk]; }
+        g_comp[i] = g_q;
+        const real c_iface = th_iface_comp<real>(th, pi, qid, c[i], c_q);
+        real dG = th_bulk<real>(TD, pi, qid, c_iface, T[i]);
+        const real sig = th_sigma<real>(th, nx[i], ny[i], nz[i], g_p, pi, qid, c[i]);
+        const real mob = th_mobility<real>(th, g_p, g_q, T[i]);
+        if (th.elastic_enabled) {
+            const real E_prod = qk >= 0 ? E_el[qk] : E_el[i];
+            dG += (E_prod - E_el[i]);
+        }
+        if (th.dislocation_enabled) {
+            const real rho_prod = qk >= 0 ? rho[qk] : rho[i];
+            dG += (real)th.disloc_coeff * (rho_prod - rho[i]);
+        }
+        if (th.magnetic_enabled) dG += th_Emag<real>(TD, g_q) - th_Emag<real>(TD, g_p);
+        vn[i] = mob * (dG - sig * kappa[i]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pair projection (src/gpk_physics.cpp:152-193): double accumulation,
+// weights (double)expf(-r2/(2 s^2)) tabulated on the host by r2.
+// ---------------------------------------------------------------------------
+template <typename real>
+__global__ void k_projection(Dims D, const int32_t* __restrict__ active, const unsigned* __restrict__ n_active,
+                             const int32_t* __restrict__ phi, const int32_t* __restrict__ phi_comp,
+                             const uint8_t* __restrict__ mask, const real* __restrict__ vn, real* __restrict__ vn_out,
+                             const double* __restrict__ wtab, int radius) {
+    const int na = (int)*n_active;
+    const bool is3d = D.is3d();
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
+        const int i = active[a];
+        const int32_t pi = phi[i], qi = phi_comp[i];
+        real out = vn[i];
+        if (pi != qi) {
+            const int32_t low = min(pi, qi), high = max(pi, qi);
+            const real orient_i = pi == low ? (real)1 : (real)-1;
+            int z0, y0, x0;
+            D.decode(i, z0, y0, x0);
+            double num = 0.0, den = 0.0;
+            const int dz0 = is3d ? -radius : 0, dz1 = is3d ? radius : 0;
+            for (int dz = dz0; dz <= dz1; ++dz) {
+                const int z = wrap_any(z0 + dz, D.Nz);
+                for (int dy = -radius; dy <= radius; ++dy) {
+                    const int y = wrap_any(y0 + dy, D.Ny);
+                    for (int dx = -radius; dx <= radius; ++dx) {
+                        const int x = wrap_any(x0 + dx, D.Nx);
+                        const int j = D.idx(z, y, x);
+                        if (!mask[j]) continue;
+                        const int32_t pj = phi[j], qj = phi_comp[j];
+                        if (pj == qj || min(pj, qj) != low || max(pj, qj) != high) continue;
+                        const double w = wtab[dx * dx + dy * dy + dz * dz];
+                        const real oj = pj == low ? (real)1 : (real)-1;
+                        num += w * (double)oj * (double)vn[j];
+                        den += w;
+                    }
+                }
+            }
+            if (den > 0.0) out = orient_i * (real)(num / den);
+        }
+        vn_out[i] = out;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// max_dt (src/gpk_simulation.cpp:11-23)
+// ---------------------------------------------------------------------------
+template <typename real> struct RealBits;
+template <> struct RealBits<float> {
+    typedef unsigned int U;
+    __device__ static U bits(float v) { return __float_as_uint(v); }
+    __device__ static float val(U u) { return __uint_as_float(u); }
+};
+template <> struct RealBits<double> {
+    typedef unsigned long long U;
+    __device__ static U bits(double v) { return (U)__double_as_longlong(v); }
+    __device__ static double val(U u) { return __longlong_as_double((long long)u); }
+};
+
+template <typename real>
+__global__ void k_vmax(const int32_t* __restrict__ active, const unsigned* __restrict__ n_active,
+                       const real* __restrict__ vn, typename RealBits<real>::U* out) {
+    typedef typename RealBits<real>::U U;
+    const int na = (int)*n_active;
+    real m = (real)0;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x)
+        m = dmax(m, (real)fabs(vn[active[a]]));
+    typedef cub::BlockReduce<U, 256> BR;
+    __shared__ typename BR::TempStorage tmp;
+    // non-negative reals order like their bit patterns
+    const U agg = BR(tmp).Reduce(RealBits<real>::bits(m), cub::Max());
+    if (threadIdx.x == 0) atomicMax(out, agg);
+}
+
+// dt selection of GPKGrid::step (src/gpk_simulation.cpp:31-37)
+template <typename real>
+__global__ void k_select_dt(StepScalars* s, const typename RealBits<real>::U* vbits, real dx, real D, int is3d,
+                            double dt_req_d, double dt_cap_d) {
+    real vmax = (real)1e-30;
+    vmax = dmax(vmax, RealBits<real>::val(*vbits));
+    const real neighbors = is3d ? (real)6 : (real)4;
+    const real dt_iface = (real)0.125 * dx / vmax;
+    const real dt_diff = (D > (real)0) ? (real)0.4 * dx * dx / (neighbors * D) : (real)1e30;
+    const real dt_stable = dmin(dt_iface, dt_diff);
+    real dt = (real)dt_req_d;
+    if (dt < (real)0) dt = dt_stable;
+    else dt = dmin(dt, dt_stable);
+    dt = dmin(dt, (real)dt_cap_d);
+    s->dt = (double)dt;
+    s->vmax = (double)vmax;
+}
+
+// ---------------------------------------------------------------------------
+// alpha integration + crossing candidates (src/gpk_transitions.cpp:251-292)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+    x ^= x >> 30; x *= 0xbf58476d1ce4e5b9ULL;
+    x ^= x >> 27; x *= 0x94d049bb133111ebULL;
+    x ^= x >> 31;
+    return x;
+}
+template <typename real>
+__device__ __forceinline__ real u01_from_u64(uint64_t x) {
+    const uint64_t m = (x >> 11) | 1ULL;
+    return (real)((double)(m & ((1ULL << 53) - 1)) * (1.0 / (double)(1ULL << 53)));
+}
+template <typename real>
+__device__ __forceinline__ real normal_from_cell_step(int i, uint64_t step_id, uint64_t salt) {
+    const uint64_t a = mix64(((uint64_t)i + 0x9e3779b97f4a7c15ULL) ^ (step_id << 1) ^ salt);
+    const uint64_t b = mix64(((uint64_t)i + 0xd2b74407b1ce6e93ULL) ^ (step_id << 3) ^ (salt + 17ULL));
+    const real u1 = dmax((real)1e-12, u01_from_u64<real>(a));
+    const real u2 = u01_from_u64<real>(b);
+    return sqrt((real)-2 * log(u1)) * cos((real)2 * dev_pi<real>() * u2);
+}
+
+template <typename real>
+__global__ void k_alpha(Dims D, const int32_t* __restrict__ active, const unsigned* __restrict__ n_active,
+                        const int32_t* __restrict__ phi, const int32_t* __restrict__ phi_comp,
+                        const real* __restrict__ vn, const real* __restrict__ T, real* __restrict__ alpha,
+                        real* __restrict__ alpha_new_a, uint8_t* __restrict__ cand_flag, const StepScalars* s, real dx,
+                        int do_noise_flag, real M0, real kB, real noise_scale, uint64_t step_id) {
+    const real dt = (real)s->dt;
+    const real idt = dt / dx;
+    const real cell_vol = dx * dx * dx;
+    const real inv_dt = (dt > (real)0) ? ((real)1 / dt) : (real)0;
+    const bool do_noise = do_noise_flag && dt > (real)0;
+    const real noise_amp = do_noise ? noise_scale * sqrt((real)2 * M0 * kB * inv_dt / dmax(cell_vol, (real)1e-30)) : (real)0;
+    const int na = (int)*n_active;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
+        const int i = active[a];
+        real vn_eff = vn[i];
+        if (do_noise) vn_eff += noise_amp * sqrt(dmax(T[i], (real)1)) * normal_from_cell_step<real>(i, step_id, 0xabcddcbaULL);
+        const real an = dmin(alpha[i] + vn_eff * idt, (real)1);
+        alpha_new_a[a] = an;
+        const bool cand = an <= (real)1e-6 && phi_comp[i] != phi[i];
+        cand_flag[a] = cand ? 1 : 0;
+        if (!cand) alpha[i] = an;
+    }
+}
+
+// crossings without region identity: every candidate is accepted
+template <typename real>
+__global__ void k_accept_all(const int32_t* __restrict__ active, const int32_t* __restrict__ cpos, int m,
+                             int32_t* __restrict__ phi, const int32_t* __restrict__ phi_comp, real* __restrict__ g,
+                             const real* __restrict__ g_comp, real* __restrict__ alpha, real* __restrict__ rho,
+                             int32_t* __restrict__ count, StepScalars* s, int sweep_rho, real rho_rex) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const int i = active[cpos[k]];
+        const int32_t o = phi[i], n = phi_comp[i];
+        phi[i] = n;
+        g[i] = g_comp[i];
+        alpha[i] = (real)1;
+        atomicSub(&count[o], 1);
+        atomicAdd(&count[n], 1);
+        if (sweep_rho) rho[i] = rho_rex;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) s->accepted = (unsigned long long)m;
+}
+
+// ---------------------------------------------------------------------------
+// elastic proxy (src/gpk_physics.cpp:10-63)
+// ---------------------------------------------------------------------------
+template <typename real>
+__global__ void k_elastic_init(int N, ThermoDev TD, const real* __restrict__ c, const real* __restrict__ g,
+                               real* __restrict__ es, real* __restrict__ sm) {
+    const gpk_thermo_desc& th = TD.t;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        real eps = (real)th.eigenstrain_coeff * (c[i] - (real)th.c_ref);
+        if ((real)th.lambda_s != (real)0) {
+            const real cg = cos(g[i] - (real)th.H_theta);
+            eps += (real)1.5 * (real)th.lambda_s * (cg * cg - ((real)1 / (real)3));
+        }
+        es[i] = eps;
+        sm[i] = eps;
+    }
+}
+template <typename real>
+__global__ void k_elastic_jacobi(Dims D, const real* __restrict__ src, real* __restrict__ dst) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.N; i += gridDim.x * blockDim.x) {
+        int nb[6];
+        D.faces(i, nb);
+        real avg = src[nb[0]] + src[nb[1]] + src[nb[2]] + src[nb[3]];
+        if (D.Nz > 1) { avg += src[nb[4]] + src[nb[5]]; avg /= (real)6; }
+        else avg /= (real)4;
+        dst[i] = (real)0.5 * src[i] + (real)0.5 * avg;
+    }
+}
+template <typename real>
+__global__ void k_elastic_energy(int N, real E, const real* __restrict__ es, const real* __restrict__ sm, real* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const real d = es[i] - sm[i];
+        out[i] = (real)0.5 * E * d * d;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// transport (src/gpk_transport.cpp:11-135) and recovery (:143-152)
+// ---------------------------------------------------------------------------
+template <typename real>
+__global__ void k_diffusion(Dims D, const real* __restrict__ c, real* __restrict__ c_new, const uint8_t* __restrict__ mask,
+                            const real* __restrict__ alpha, real Dc, const StepScalars* s, real dx2) {
+    const real dt = (real)s->dt;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.N; i += gridDim.x * blockDim.x) {
+        int nb[6];
+        D.faces(i, nb);
+        real lap = c[nb[1]] + c[nb[0]] + c[nb[3]] + c[nb[2]];
+        if (D.Nz > 1) lap += c[nb[5]] + c[nb[4]] - (real)6 * c[i];
+        else lap -= (real)4 * c[i];
+        const real D_eff = mask[i] ? Dc * alpha[i] : Dc;
+        c_new[i] = c[i] + dt * D_eff * lap / dx2;
+    }
+}
+
+template <typename real>
+__global__ void k_solid_fraction(int N, const int32_t* __restrict__ phi, const real* __restrict__ alpha, real* __restrict__ s) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        s[i] = (phi[i] != 0) ? alpha[i] : (real)1 - alpha[i];
+}
+
+// neighbour order of the transport routines: x+, x-, y+, y-, z+, z-
+__device__ __forceinline__ int faces_transport(const Dims& D, int i, int nb[6]) {
+    int z, y, x;
+    D.decode(i, z, y, x);
+    int nn = 0;
+    nb[nn++] = D.idx(z, y, x == D.Nx - 1 ? 0 : x + 1);
+    nb[nn++] = D.idx(z, y, x == 0 ? D.Nx - 1 : x - 1);
+    nb[nn++] = D.idx(z, y == D.Ny - 1 ? 0 : y + 1, x);
+    nb[nn++] = D.idx(z, y == 0 ? D.Ny - 1 : y - 1, x);
+    if (D.Nz > 1) {
+        nb[nn++] = D.idx(z == D.Nz - 1 ? 0 : z + 1, y, x);
+        nb[nn++] = D.idx(z == 0 ? D.Nz - 1 : z - 1, y, x);
+    }
+    return nn;
+}
+
+// per-source rejected solute q and liquid weight sum (0 when it rejects nothing)
+template <typename real>
+__global__ void k_rejection_source(Dims D, const int32_t* __restrict__ phi, const real* __restrict__ c,
+                                   const real* __restrict__ s_old, const real* __restrict__ s_new, real k,
+                                   real* __restrict__ q_out, real* __restrict__ wsum_out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.N; i += gridDim.x * blockDim.x) {
+        real qv = 0, wsum = 0;
+        const real ds = s_new[i] - s_old[i];
+        if (ds > (real)0) {
+            const real s0 = dclamp(s_old[i], (real)0, (real)1);
+            const real cL = c[i] / dmax((real)1 - s0 * ((real)1 - k), (real)1e-6);
+            real q = ((real)1 - k) * cL * dmin(ds, (real)1);
+            q = dmin(q, c[i]);
+            if (q > (real)0) {
+                int nb[6];
+                const int nn = faces_transport(D, i, nb);
+                for (int a = 0; a < nn; ++a) {
+                    const int j = nb[a];
+                    const real w = (phi[j] == 0) ? dmax((real)1 - s_new[j], (real)0) : (real)0;
+                    wsum += w;
+                }
+                if (wsum > (real)0) qv = q;
+            }
+        }
+        q_out[i] = qv;
+        wsum_out[i] = wsum;
+    }
+}
+
+// gathers delta[j] in the reference's scatter order (increasing source index,
+// then neighbour slot) and applies c += delta
+template <typename real>
+__global__ void k_rejection_gather(Dims D, const int32_t* __restrict__ phi, const real* __restrict__ s_new,
+                                   const real* __restrict__ q, const real* __restrict__ wsum, real* __restrict__ c) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < D.N; j += gridDim.x * blockDim.x) {
+        int src[7];
+        int ns = 0;
+        int nbj[6];
+        const int nn = faces_transport(D, j, nbj);
+        src[ns++] = j;
+        for (int a = 0; a < nn; ++a) {
+            bool dup = false;
+            for (int b = 0; b < ns; ++b) dup |= src[b] == nbj[a];
+            if (!dup) src[ns++] = nbj[a];
+        }
+        for (int a = 1; a < ns; ++a) {  // insertion sort, at most 7 entries
+            const int v = src[a];
+            int b = a - 1;
+            while (b >= 0 && src[b] > v) { src[b + 1] = src[b]; --b; }
+            src[b + 1] = v;
+        }
+        real delta = 0;
+        for (int t = 0; t < ns; ++t) {
+            const int sidx = src[t];
+            const real qs = q[sidx];
+            if (!(qs > (real)0)) continue;
+            if (sidx == j) delta -= qs;
+            int nbs[6];
+            const int ms = faces_transport(D, sidx, nbs);
+            for (int a = 0; a < ms; ++a) {
+                if (nbs[a] != j) continue;
+                const real w = (phi[j] == 0) ? dmax((real)1 - s_new[j], (real)0) : (real)0;
+                if (w > (real)0) delta += qs * w / wsum[sidx];
+            }
+        }
+        c[j] += delta;
+    }
+}
+
+template <typename real>
+__global__ void k_liquid_comp(int N, const real* __restrict__ c, const real* __restrict__ s, real k, real* __restrict__ cL) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        cL[i] = c[i] / dmax((real)1 - s[i] * ((real)1 - k), (real)1e-6);
+}
+
+template <typename real>
+__global__ void k_diffusion_partitioned(Dims D, const real* __restrict__ c, const real* __restrict__ s,
+                                        const real* __restrict__ cL, real* __restrict__ c_new, real Dc,
+                                        const StepScalars* st, real dx) {
+    const real dt = (real)st->dt;
+    const real coef = dt * Dc / (dx * dx);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.N; i += gridDim.x * blockDim.x) {
+        int nb[6];
+        const int nn = faces_transport(D, i, nb);
+        const real li = (real)1 - s[i];
+        real flux = 0;
+        for (int a = 0; a < nn; ++a) {
+            const int j = nb[a];
+            const real lf = dmin(li, (real)1 - s[j]);
+            if (lf > (real)0) flux += lf * (cL[j] - cL[i]);
+        }
+        c_new[i] = c[i] + coef * flux;
+    }
+}
+
+template <typename real>
+__global__ void k_scale(int N, real* __restrict__ v, real f) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) v[i] *= f;
+}
+
+__global__ void k_advance_time(StepScalars* s) { s->time += s->dt; }
+
+__global__ void k_reset_step(StepScalars* s) {
+    s->accepted = 0; s->deferred = 0; s->exchanges = 0; s->exch_pass = 0;
+    s->n_cand = 0; s->n_prop = 0; s->waves = 0;
+}
+
+}  // namespace gpk_dev
+
+using namespace gpk_dev;
+
+template <typename real> int gpk_crossings(gpk_grid* G, int m);
+template <typename real> int gpk_remap_pass(gpk_grid* G);
+template <typename real> int gpk_extinction(gpk_grid* G);
+
+static inline int grid_for(gpk_grid* G, long long n, int block = 256) {
+    long long b = (n + block - 1) / block;
+    long long cap = (long long)G->num_sms * 8;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+// mask + sorted interface list (src/gpk_geometry.cpp:42-82)
+template <typename real>
+int gpk_interface_mask(gpk_grid* G) {
+    const int nt = (G->d.N + MASK_TILE - 1) / MASK_TILE;
+    k_mask_tiles<<<nt, MASK_TPB, 0, G->stream>>>(G->d, G->phi, G->mask, G->tile_off);
+    k_scan_tiles<<<1, 1024, 0, G->stream>>>(G->tile_off, nt, &G->scal->n_active);
+    k_compact_u8<<<nt, MASK_TPB, 0, G->stream>>>(G->d.N, G->mask, G->tile_off, G->active);
+    G->launches += 3;
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+template <typename real>
+static int geometry(gpk_grid* G) {
+    HostKernels<real>* hk = (HostKernels<real>*)G->host_kernels;
+    const Dims D = G->d;
+    const size_t nb = G->rsz * D.N;
+    for (int f : {GPK_FIELD_NX, GPK_FIELD_NY, GPK_FIELD_NZ, GPK_FIELD_KAPPA})
+        GPK_CUDA_TRY(cudaMemsetAsync(G->f[f], 0, nb, G->stream));
+    const real dx = (real)G->dx;
+    const real kappa_limit = (real)1 / (hk->gauss_sigma * dx);
+    real* nx = (real*)G->f[GPK_FIELD_NX];
+    real* ny = (real*)G->f[GPK_FIELD_NY];
+    real* nz = (real*)G->f[GPK_FIELD_NZ];
+    real* kp = (real*)G->f[GPK_FIELD_KAPPA];
+    if (!hk->global_separable) {
+        const real inv_dx = (real)1 / dx;
+        const real inv_dx2 = inv_dx * inv_dx;
+        const int grid = G->num_sms * 16;
+        if (D.is3d())
+            k_geometry_direct<real, true><<<grid, 128, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi,
+                                                                       (const real*)G->d_geom_table, hk->geom_radius,
+                                                                       inv_dx, inv_dx2, dx, kappa_limit, nx, ny, nz, kp,
+                                                                       G->phi_comp);
+        else
+            k_geometry_direct<real, false><<<grid, 128, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi,
+                                                                        (const real*)G->d_geom_table, hk->geom_radius,
+                                                                        inv_dx, inv_dx2, dx, kappa_limit, nx, ny, nz,
+                                                                        kp, G->phi_comp);
+        G->launches++;
+        GPK_CUDA_TRY(cudaGetLastError());
+        return GPK_OK;
+    }
+    // separable path: one smoothed indicator per distinct interface label
+    uint8_t* present = G->unres;  // label-indexed scratch
+    GPK_CUDA_TRY(cudaMemsetAsync(present, 0, G->label_cap, G->stream));
+    k_label_flags<<<grid_for(G, D.N), 256, 0, G->stream>>>(D.N, G->phi, G->mask, present, G->label_cap);
+    std::vector<uint8_t> hp(G->label_cap);
+    GPK_CUDA_TRY(cudaMemcpyAsync(hp.data(), present, G->label_cap, cudaMemcpyDeviceToHost, G->stream));
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    const int gN = grid_for(G, D.N);
+    for (int p = 0; p < G->label_cap; ++p) {
+        if (!hp[p]) continue;
+        k_indicator<real><<<gN, 256, 0, G->stream>>>(D.N, G->phi, p, (real*)G->sep_I);
+        k_gauss_pass<real><<<gN, 256, 0, G->stream>>>(D, (const real*)G->sep_I, (real*)G->sep_t1, (const real*)G->d_gauss,
+                                                      hk->gauss_radius, 0);
+        k_gauss_pass<real><<<gN, 256, 0, G->stream>>>(D, (const real*)G->sep_t1, (real*)G->sep_t2,
+                                                      (const real*)G->d_gauss, hk->gauss_radius, 1);
+        k_gauss_pass<real><<<gN, 256, 0, G->stream>>>(D, (const real*)G->sep_t2, (real*)G->sep_S, (const real*)G->d_gauss,
+                                                      hk->gauss_radius, 2);
+        k_separable_eval<real><<<gN, 256, 0, G->stream>>>(D, G->phi, G->mask, p, (const real*)G->sep_S, dx, kappa_limit,
+                                                          nx, ny, nz, kp);
+        G->launches += 5;
+    }
+    k_competitor_all<real><<<grid_for(G, D.N), 256, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, nx, ny,
+                                                                     nz, G->phi_comp);
+    G->launches += 2;
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+static ThermoDev make_thermo_dev(const gpk_thermo_desc& t) {
+    ThermoDev TD;
+    TD.t = t;
+    TD.log_pH2 = (t.model == GPK_MODEL_REDUCTION) ? logf(t.p[0]) : 0.f;
+    TD.mu0 = 4.0e-7f * 3.14159265358979323846f;
+    return TD;
+}
+
+template <typename real>
+static int elastic(gpk_grid* G) {
+    const gpk_thermo_desc& th = G->th;
+    const Dims D = G->d;
+    real* E = (real*)G->f[GPK_FIELD_E_EL];
+    if (!th.elastic_enabled || (real)th.elastic_modulus <= (real)0 ||
+        ((real)th.eigenstrain_coeff == (real)0 && (real)th.lambda_s == (real)0)) {
+        GPK_CUDA_TRY(cudaMemsetAsync(E, 0, G->rsz * D.N, G->stream));
+        return GPK_OK;
+    }
+    if (!G->eps_star) {
+        GPK_TRY(gpk_alloc(G, &G->eps_star, G->rsz * D.N));
+        GPK_TRY(gpk_alloc(G, &G->eps_smooth, G->rsz * D.N));
+        GPK_TRY(gpk_alloc(G, &G->eps_tmp, G->rsz * D.N));
+    }
+    const int gN = grid_for(G, D.N);
+    const ThermoDev TD = make_thermo_dev(th);
+    k_elastic_init<real><<<gN, 256, 0, G->stream>>>(D.N, TD, (const real*)G->f[GPK_FIELD_C], (const real*)G->f[GPK_FIELD_G],
+                                                    (real*)G->eps_star, (real*)G->eps_smooth);
+    const int iters = std::max(1, th.elastic_smooth_iters);
+    for (int it = 0; it < iters; ++it) {
+        k_elastic_jacobi<real><<<gN, 256, 0, G->stream>>>(D, (const real*)G->eps_smooth, (real*)G->eps_tmp);
+        std::swap(G->eps_smooth, G->eps_tmp);
+    }
+    k_elastic_energy<real><<<gN, 256, 0, G->stream>>>(D.N, (real)th.elastic_modulus, (const real*)G->eps_star,
+                                                      (const real*)G->eps_smooth, E);
+    G->launches += 2 + iters;
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+template <typename real>
+static int transport(gpk_grid* G) {
+    const Dims D = G->d;
+    const gpk_thermo_desc& th = G->th;
+    const real Dc = (real)G->D;
+    const real dx = (real)G->dx;
+    const int gN = grid_for(G, D.N);
+    if (th.solute_rejection) {
+        const real k = (real)th.k_partition;
+        if (k < (real)1 && G->have_solid_old) {
+            k_solid_fraction<real><<<gN, 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
+                                                              (real*)G->s_new);
+            k_rejection_source<real><<<gN, 256, 0, G->stream>>>(D, G->phi, (const real*)G->f[GPK_FIELD_C],
+                                                                 (const real*)G->solid_old, (const real*)G->s_new, k,
+                                                                 (real*)G->delta, (real*)G->cL);
+            k_rejection_gather<real><<<gN, 256, 0, G->stream>>>(D, G->phi, (const real*)G->s_new, (const real*)G->delta,
+                                                                (const real*)G->cL, (real*)G->f[GPK_FIELD_C]);
+            G->launches += 3;
+        }
+        if (Dc > (real)0) {
+            k_solid_fraction<real><<<gN, 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
+                                                              (real*)G->s_new);
+            k_liquid_comp<real><<<gN, 256, 0, G->stream>>>(D.N, (const real*)G->f[GPK_FIELD_C], (const real*)G->s_new,
+                                                           (real)th.k_partition, (real*)G->cL);
+            k_diffusion_partitioned<real><<<gN, 256, 0, G->stream>>>(D, (const real*)G->f[GPK_FIELD_C],
+                                                                     (const real*)G->s_new, (const real*)G->cL,
+                                                                     (real*)G->c_new, Dc, G->scal, dx);
+            std::swap(G->f[GPK_FIELD_C], G->c_new);
+            G->launches += 3;
+        }
+    } else if (Dc > (real)0) {
+        k_diffusion<real><<<gN, 256, 0, G->stream>>>(D, (const real*)G->f[GPK_FIELD_C], (real*)G->c_new, G->mask,
+                                                     (const real*)G->f[GPK_FIELD_ALPHA], Dc, G->scal, dx * dx);
+        std::swap(G->f[GPK_FIELD_C], G->c_new);
+        G->launches++;
+    }
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+int gpk_sync_scalars(gpk_grid* G) {
+    GPK_CUDA_TRY(cudaMemcpyAsync(G->h_scal, G->scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, G->stream));
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    if (G->h_scal->error) {
+        const unsigned e = G->h_scal->error;
+        gpk_set_error(e == GPK_ERR_TIMEOUT ? "a bounded device wait gave up" : "device consistency check failed");
+        return (int)e;
+    }
+    return GPK_OK;
+}
+
+// GPKGrid::step (src/gpk_simulation.cpp:31-54)
+template <typename real>
+int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
+    HostKernels<real>* hk = (HostKernels<real>*)G->host_kernels;
+    const Dims D = G->d;
+    const gpk_thermo_desc& th = G->th;
+    const int ga = G->num_sms * 8;
+    k_reset_step<<<1, 1, 0, G->stream>>>(G->scal);
+    G->launches++;
+    // flood-fill stamps: restart before the 32-bit cursor can wrap
+    if (G->h_scal->stamp > 0x70000000u) {
+        GPK_CUDA_TRY(cudaMemsetAsync(G->stamp, 0, sizeof(uint32_t) * D.N, G->stream));
+        GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->stamp, 0, sizeof(unsigned), G->stream));
+        G->h_scal->stamp = 0;
+    }
+    GPK_TRY(gpk_interface_mask<real>(G));
+    GPK_TRY(geometry<real>(G));
+    GPK_TRY(elastic<real>(G));
+    const ThermoDev TD = make_thermo_dev(th);
+    GPK_CUDA_TRY(cudaMemsetAsync(G->f[GPK_FIELD_VN], 0, G->rsz * D.N, G->stream));
+    k_velocities<real><<<ga, 256, 0, G->stream>>>(
+        D, TD, G->active, &G->scal->n_active, G->phi, G->phi_comp, (const real*)G->f[GPK_FIELD_C],
+        (const real*)G->f[GPK_FIELD_T], (const real*)G->f[GPK_FIELD_G], (const real*)G->f[GPK_FIELD_RHO],
+        (const real*)G->f[GPK_FIELD_NX], (const real*)G->f[GPK_FIELD_NY], (const real*)G->f[GPK_FIELD_NZ],
+        (const real*)G->f[GPK_FIELD_KAPPA], (const real*)G->f[GPK_FIELD_E_EL], (real*)G->f[GPK_FIELD_VN],
+        (real*)G->f[GPK_FIELD_G_COMP]);
+    // projection into vn2 (zero at bulk cells), then swap
+    GPK_CUDA_TRY(cudaMemsetAsync(G->vn2, 0, G->rsz * D.N, G->stream));
+    k_projection<real><<<ga, 256, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, G->phi_comp, G->mask,
+                                                  (const real*)G->f[GPK_FIELD_VN], (real*)G->vn2, G->d_proj_w,
+                                                  hk->proj_radius);
+    std::swap(G->f[GPK_FIELD_VN], G->vn2);
+    // stable dt
+    typedef typename RealBits<real>::U U;
+    U* vbits = (U*)&G->scal->vmax;
+    GPK_CUDA_TRY(cudaMemsetAsync(vbits, 0, sizeof(double), G->stream));
+    k_vmax<real><<<ga, 256, 0, G->stream>>>(G->active, &G->scal->n_active, (const real*)G->f[GPK_FIELD_VN], vbits);
+    k_select_dt<real><<<1, 1, 0, G->stream>>>(G->scal, vbits, (real)G->dx, (real)G->D, D.is3d() ? 1 : 0, dt_req, dt_cap);
+    G->launches += 4;
+    if (th.solute_rejection) {
+        if (!G->solid_old) {
+            GPK_TRY(gpk_alloc(G, &G->solid_old, G->rsz * D.N));
+            GPK_TRY(gpk_alloc(G, &G->s_new, G->rsz * D.N));
+            GPK_TRY(gpk_alloc(G, &G->delta, G->rsz * D.N));
+            GPK_TRY(gpk_alloc(G, &G->cL, G->rsz * D.N));
+        }
+        k_solid_fraction<real><<<grid_for(G, D.N), 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
+                                                                         (real*)G->solid_old);
+        G->have_solid_old = 1;
+        G->launches++;
+    }
+    // alpha integration and candidates
+    uint8_t* cflag = (uint8_t*)G->ero_target;  // active-indexed scratch flags
+    k_alpha<real><<<ga, 256, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, G->phi_comp,
+                                             (const real*)G->f[GPK_FIELD_VN], (const real*)G->f[GPK_FIELD_T],
+                                             (real*)G->f[GPK_FIELD_ALPHA], (real*)G->alpha_new_a, cflag, G->scal,
+                                             (real)G->dx, th.stochastic, (real)th.M0, (real)th.kB, (real)th.noise_scale,
+                                             G->step_id);
+    const int nt = (D.N + MASK_TILE - 1) / MASK_TILE;
+    int32_t* ctile = G->tile_off + nt + 1;
+    k_count_u8<<<nt, MASK_TPB, 0, G->stream>>>(cflag, &G->scal->n_active, ctile);
+    k_scan_tiles<<<1, 1024, 0, G->stream>>>(ctile, nt, &G->scal->n_cand);
+    k_compact_u8_dyn<<<nt, MASK_TPB, 0, G->stream>>>(&G->scal->n_active, cflag, ctile, G->cand);
+    G->launches += 4;
+    GPK_CUDA_TRY(cudaGetLastError());
+    GPK_TRY(gpk_sync_scalars(G));
+    const int m = (int)G->h_scal->n_cand;
+    if (m > 0) {
+        if (th.grain_network) {
+            GPK_TRY(gpk_crossings<real>(G, m));
+        } else {
+            k_accept_all<real><<<grid_for(G, m), 256, 0, G->stream>>>(
+                G->active, G->cand, m, G->phi, G->phi_comp, (real*)G->f[GPK_FIELD_G], (const real*)G->f[GPK_FIELD_G_COMP],
+                (real*)G->f[GPK_FIELD_ALPHA], (real*)G->f[GPK_FIELD_RHO], G->count, G->scal, th.dislocation_enabled,
+                (real)th.rho_rex);
+            G->launches++;
+        }
+        GPK_CUDA_TRY(cudaGetLastError());
+        GPK_TRY(gpk_sync_scalars(G));
+    }
+    // balanced Gaussian remap, twice in 3-D when the first pass exchanged
+    if (G->h_scal->accepted > 0) {
+        GPK_TRY(gpk_interface_mask<real>(G));
+        GPK_TRY(gpk_remap_pass<real>(G));
+        GPK_TRY(gpk_interface_mask<real>(G));
+        GPK_TRY(gpk_sync_scalars(G));
+        const unsigned long long first = G->h_scal->exch_pass;
+        unsigned long long total = first;
+        if (D.is3d() && first > 0) {
+            GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->exch_pass, 0, sizeof(unsigned long long), G->stream));
+            GPK_TRY(gpk_remap_pass<real>(G));
+            GPK_TRY(gpk_interface_mask<real>(G));
+            GPK_TRY(gpk_sync_scalars(G));
+            total += G->h_scal->exch_pass;
+        }
+        G->h_scal->exchanges = total;
+        GPK_CUDA_TRY(cudaMemcpyAsync(&G->scal->exchanges, &G->h_scal->exchanges, sizeof(unsigned long long),
+                                     cudaMemcpyHostToDevice, G->stream));
+    }
+    if (th.grain_network && (G->step_id & 7ULL) == 0ULL) GPK_TRY(gpk_extinction<real>(G));
+    GPK_TRY(transport<real>(G));
+    if (th.dislocation_enabled && (real)th.recovery_rate > (real)0) {
+        GPK_TRY(gpk_sync_scalars(G));
+        const real dt = (real)G->h_scal->dt;
+        if (dt > (real)0) {
+            const real decay = (sizeof(real) == 4) ? (real)expf(-(float)th.recovery_rate * (float)dt)
+                                                   : (real)exp(-(double)th.recovery_rate * (double)dt);
+            k_scale<real><<<grid_for(G, D.N), 256, 0, G->stream>>>(D.N, (real*)G->f[GPK_FIELD_RHO], decay);
+            G->launches++;
+        }
+    }
+    k_advance_time<<<1, 1, 0, G->stream>>>(G->scal);
+    G->launches++;
+    GPK_CUDA_TRY(cudaGetLastError());
+    ++G->step_id;
+    return GPK_OK;
+}
+
+template <typename real>
+int gpk_max_dt_impl(gpk_grid* G, double* out) {
+    // the reference evaluates max_dt on its current interface list and vn_f
+    typedef typename RealBits<real>::U U;
+    U* vbits = (U*)G->alpha_new_a;  // scratch word
+    GPK_CUDA_TRY(cudaMemsetAsync(vbits, 0, sizeof(U), G->stream));
+    k_vmax<real><<<G->num_sms * 8, 256, 0, G->stream>>>(G->active, &G->scal->n_active, (const real*)G->f[GPK_FIELD_VN], vbits);
+    U h = 0;
+    GPK_CUDA_TRY(cudaMemcpyAsync(&h, vbits, sizeof(U), cudaMemcpyDeviceToHost, G->stream));
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    real v;
+    memcpy(&v, &h, sizeof(real));
+    real vmax = dmax((real)1e-30, v);
+    const real dx = (real)G->dx, Dc = (real)G->D;
+    const real neighbors = G->d.is3d() ? (real)6 : (real)4;
+    const real dt_iface = (real)0.125 * dx / vmax;
+    const real dt_diff = (Dc > (real)0) ? (real)0.4 * dx * dx / (neighbors * Dc) : (real)1e30;
+    *out = (double)dmin(dt_iface, dt_diff);
+    return GPK_OK;
+}
+
+template int gpk_interface_mask<float>(gpk_grid*);
+template int gpk_interface_mask<double>(gpk_grid*);
+template int gpk_step_impl<float>(gpk_grid*, double, double);
+template int gpk_step_impl<double>(gpk_grid*, double, double);
+template int gpk_max_dt_impl<float>(gpk_grid*, double*);
+template int gpk_max_dt_impl<double>(gpk_grid*, double*);

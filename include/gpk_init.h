@@ -1,0 +1,30 @@
+/*
+ * gpk_init.h — host-side initial conditions for gpk_b200 label grids.
+ *
+ * The reference builds its polycrystals in the driver, voronoi_init
+ * (demos/gpk.cpp:51-189 of albert-hzbn/GPK).  This is the same construction
+ * with this library's own seeded random stream, exported so that drivers,
+ * tests and benchmarks can produce identical input buffers for the GPU path
+ * and for CPU checkers.
+ */
+#ifndef GPK_INIT_H
+#define GPK_INIT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Fills phi (labels 1..n_seeds) and, when g is not null, g (one orientation
+ * per grain in [0, pi/2)) for an Nz x Ny x Nx periodic grid.  Returns 0 on
+ * success, 1 on bad arguments, 2 if the normalisation stalls.  *reassigned
+ * (may be null) receives the number of raster-tie cells that were moved to
+ * make every label one face-connected component.                          */
+int gpk_voronoi_init(int Nz, int Ny, int Nx, int n_seeds, uint64_t seed, int32_t* phi, float* g, int* reassigned);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPK_INIT_H */

@@ -1,0 +1,260 @@
+"""CPU checkers for the gpk_b200 CUDA path (test infrastructure only).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package.  Two checkers are exposed with the same
+interface:
+
+* :class:`OracleGrid` — the C restatement in ``oracle/gpk_oracle.c`` of the
+  reference's ``GPKGrid::step`` (float build = the reference's FP32
+  arithmetic, double build = the FP64 variant).
+* :class:`RefGrid` — the reference's own sources (src/*.cpp of
+  albert-hzbn/GPK) compiled into ``oracle/_ref/libgpk_ref.so`` behind
+  ``oracle/ref_harness.cpp``.
+
+Both wrap the public fields of ``GPKGrid`` (include/gpk_core.hpp:211-228) as
+numpy arrays copied in and out through plain pointers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from gpk_b200.thermo import ThermoDesc, FIELD_IDS, INT_FIELDS, U8_FIELDS
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_ORACLE_SO = os.path.join(_HERE, "liboracle.so")
+_REF_SO = os.path.join(_HERE, "_ref", "libgpk_ref.so")
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the oracle (and the reference harness where its sources exist)."""
+    out = subprocess.run(["make", "-f", os.path.join(_HERE, "Makefile")],
+                         capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+_libs: dict = {}
+
+
+def _load(path: str) -> C.CDLL:
+    if path not in _libs:
+        if not os.path.exists(path):
+            if path == _ORACLE_SO:
+                build()
+            else:
+                raise FileNotFoundError(path)
+        _libs[path] = C.CDLL(path)
+    return _libs[path]
+
+
+def ref_available() -> bool:
+    return os.path.exists(_REF_SO)
+
+
+class _GridBase:
+    """Shared numpy field access over a C grid handle."""
+
+    real_dtype = np.float32
+
+    def __init__(self, Nz: int, Ny: int, Nx: int):
+        self.Nz, self.Ny, self.Nx = Nz, Ny, Nx
+        self.N = Nz * Ny * Nx
+
+    def _dtype(self, name: str):
+        if name in INT_FIELDS:
+            return np.int32
+        if name in U8_FIELDS:
+            return np.uint8
+        return self.real_dtype
+
+    def _ptr(self, name: str) -> int:
+        raise NotImplementedError
+
+    def get(self, name: str) -> np.ndarray:
+        dt = self._dtype(name)
+        ptr = self._ptr(name)
+        buf = (C.c_byte * (self.N * np.dtype(dt).itemsize)).from_address(ptr)
+        return np.frombuffer(buf, dtype=dt).copy().reshape(self.Nz, self.Ny, self.Nx)
+
+    def set(self, name: str, value) -> None:
+        dt = self._dtype(name)
+        arr = np.ascontiguousarray(np.broadcast_to(np.asarray(value, dtype=dt),
+                                                   (self.Nz, self.Ny, self.Nx)))
+        C.memmove(self._ptr(name), arr.ctypes.data, arr.nbytes)
+
+
+class OracleGrid(_GridBase):
+    """C restatement of GPKGrid (float or double build)."""
+
+    def __init__(self, Nz, Ny, Nx, dx, thermo: ThermoDesc, D=0.0, sigma=2.0, precision="f32"):
+        super().__init__(Nz, Ny, Nx)
+        self.lib = _load(_ORACLE_SO)
+        self.sfx = precision
+        self.real_dtype = np.float32 if precision == "f32" else np.float64
+        f = self._fn
+        f("or_create").restype = C.c_void_p
+        f("or_create").argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p,
+                                   C.c_double, C.c_double]
+        f("or_field").restype = C.c_void_p
+        f("or_field").argtypes = [C.c_void_p, C.c_int]
+        f("or_step").restype = C.c_double
+        f("or_step").argtypes = [C.c_void_p, C.c_double, C.c_double]
+        for n in ("or_get_time", "or_max_dt", "or_interface_fraction"):
+            f(n).restype = C.c_double
+            f(n).argtypes = [C.c_void_p]
+        f("or_phase_volume").restype = C.c_double
+        f("or_phase_volume").argtypes = [C.c_void_p, C.c_int32]
+        f("or_set_time").argtypes = [C.c_void_p, C.c_double]
+        f("or_counters").argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
+        f("or_n_grains").argtypes = [C.c_void_p]
+        f("or_topology_simple_move").argtypes = [C.c_void_p, C.c_int, C.c_int32]
+        f("or_run").argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
+        f("or_set_thermo").argtypes = [C.c_void_p, C.c_void_p]
+        f("or_destroy").argtypes = [C.c_void_p]
+        f("or_interface_mask").argtypes = [C.c_void_p]
+        self._thermo = thermo.to_c()
+        self.h = f("or_create")(Nz, Ny, Nx, float(dx), C.byref(self._thermo), float(D), float(sigma))
+        if not self.h:
+            raise RuntimeError("or_create failed")
+
+    def _fn(self, name):
+        return getattr(self.lib, f"{name}_{self.sfx}")
+
+    def _ptr(self, name):
+        return self._fn("or_field")(self.h, FIELD_IDS[name])
+
+    def step(self, dt=-1.0, dt_cap=1e30) -> float:
+        return self._fn("or_step")(self.h, dt, dt_cap)
+
+    def run(self, t_end, dt=-1.0, max_steps=0) -> int:
+        return self._fn("or_run")(self.h, t_end, dt, max_steps)
+
+    @property
+    def time(self) -> float:
+        return self._fn("or_get_time")(self.h)
+
+    @time.setter
+    def time(self, t):
+        self._fn("or_set_time")(self.h, t)
+
+    def counters(self):
+        out = (C.c_uint64 * 3)()
+        self._fn("or_counters")(self.h, out)
+        return tuple(int(v) for v in out)
+
+    def set_thermo(self, thermo: ThermoDesc):
+        self._thermo = thermo.to_c()
+        self._fn("or_set_thermo")(self.h, C.byref(self._thermo))
+
+    def max_dt(self):
+        return self._fn("or_max_dt")(self.h)
+
+    def phase_volume(self, label):
+        return self._fn("or_phase_volume")(self.h, label)
+
+    def n_grains(self):
+        return self._fn("or_n_grains")(self.h)
+
+    def interface_fraction(self):
+        return self._fn("or_interface_fraction")(self.h)
+
+    def topology_simple_move(self, cell, label):
+        return bool(self._fn("or_topology_simple_move")(self.h, cell, label))
+
+    def interface_mask(self):
+        self._fn("or_interface_mask")(self.h)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self._fn("or_destroy")(h)
+            self.h = None
+
+
+class RefGrid(_GridBase):
+    """The reference's own GPKGrid (compiled from its sources), float only."""
+
+    def __init__(self, Nz, Ny, Nx, dx, thermo: ThermoDesc, D=0.0, sigma=2.0):
+        super().__init__(Nz, Ny, Nx)
+        self.lib = _load(_REF_SO)
+        L = self.lib
+        L.ref_create.restype = C.c_void_p
+        L.ref_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_double, C.c_double]
+        L.ref_field.restype = C.c_void_p
+        L.ref_field.argtypes = [C.c_void_p, C.c_int]
+        L.ref_step.restype = C.c_double
+        L.ref_step.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.ref_time_steps.restype = C.c_double
+        L.ref_time_steps.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
+        for n in ("ref_get_time", "ref_max_dt", "ref_interface_fraction"):
+            getattr(L, n).restype = C.c_double
+            getattr(L, n).argtypes = [C.c_void_p]
+        L.ref_phase_volume.restype = C.c_double
+        L.ref_phase_volume.argtypes = [C.c_void_p, C.c_int32]
+        L.ref_set_time.argtypes = [C.c_void_p, C.c_double]
+        L.ref_counters.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
+        L.ref_n_grains.argtypes = [C.c_void_p]
+        L.ref_topology_simple_move.argtypes = [C.c_void_p, C.c_int, C.c_int32]
+        L.ref_run.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.ref_destroy.argtypes = [C.c_void_p]
+        self._thermo = thermo.to_c()
+        self.h = L.ref_create(Nz, Ny, Nx, float(dx), C.byref(self._thermo), float(D), float(sigma))
+        if not self.h:
+            raise RuntimeError("ref_create failed (unknown model tag)")
+
+    def _ptr(self, name):
+        return self.lib.ref_field(self.h, FIELD_IDS[name])
+
+    def step(self, dt=-1.0, dt_cap=1e30) -> float:
+        return self.lib.ref_step(self.h, dt, dt_cap)
+
+    def run(self, t_end, dt=-1.0) -> int:
+        return self.lib.ref_run(self.h, t_end, dt)
+
+    def time_steps(self, n, dt=-1.0, threads=0) -> float:
+        return self.lib.ref_time_steps(self.h, n, dt, threads)
+
+    @staticmethod
+    def max_threads() -> int:
+        lib = _load(_REF_SO)
+        return lib.ref_max_threads()
+
+    @property
+    def time(self) -> float:
+        return self.lib.ref_get_time(self.h)
+
+    @time.setter
+    def time(self, t):
+        self.lib.ref_set_time(self.h, t)
+
+    def counters(self):
+        out = (C.c_uint64 * 3)()
+        self.lib.ref_counters(self.h, out)
+        return tuple(int(v) for v in out)
+
+    def max_dt(self):
+        return self.lib.ref_max_dt(self.h)
+
+    def phase_volume(self, label):
+        return self.lib.ref_phase_volume(self.h, label)
+
+    def n_grains(self):
+        return self.lib.ref_n_grains(self.h)
+
+    def interface_fraction(self):
+        return self.lib.ref_interface_fraction(self.h)
+
+    def topology_simple_move(self, cell, label):
+        return bool(self.lib.ref_topology_simple_move(self.h, cell, label))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.lib.ref_destroy(h)
+            self.h = None
