@@ -68,6 +68,10 @@ def lib() -> C.CDLL:
         "gpk_grid_topology_simple_move": ([vp, i32, C.c_int32, C.POINTER(i32)], i32),
         "gpk_grid_device_bytes": ([vp, C.POINTER(sz)], i32),
         "gpk_grid_launch_count": ([vp, C.POINTER(u64)], i32),
+        "gpk_gaussian_filter_3d": ([vp, vp, i32, i32, i32, vp, i32], i32),
+        "gpk_grid_stream": ([vp, C.POINTER(vp)], i32),
+        "gpk_grid_profile": ([vp, i32], i32),
+        "gpk_grid_stage_times": ([vp, C.POINTER(dbl), C.POINTER(u64)], i32),
         "gpk_voronoi_init": ([i32, i32, i32, i32, u64, vp, vp, C.POINTER(i32)], i32),
     }
     for name, (args, res) in sigs.items():

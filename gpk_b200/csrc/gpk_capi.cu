@@ -596,3 +596,27 @@ extern "C" int gpk_grid_interface_fraction(gpk_grid* G, double* out) {
 
 template int gpk_build_tables<float>(gpk_grid*);
 template int gpk_build_tables<double>(gpk_grid*);
+
+extern "C" int gpk_grid_stream(gpk_grid* G, void** stream) {
+    if (!G || !stream) return GPK_ERR_INVALID_ARGUMENT;
+    *stream = (void*)G->stream;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_profile(gpk_grid* G, int enable) {
+    if (!G) return GPK_ERR_INVALID_ARGUMENT;
+    G->profile = enable != 0;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_stage_times(gpk_grid* G, double ms[GPK_NUM_STAGES], uint64_t calls[GPK_NUM_STAGES]) {
+    if (!G || !ms || !calls) return GPK_ERR_INVALID_ARGUMENT;
+    GPK_TRY(gpk_stage_collect(G));
+    for (int k = 0; k < GPK_NUM_STAGES; ++k) {
+        ms[k] = G->stage_ms[k];
+        calls[k] = G->stage_calls[k];
+        G->stage_ms[k] = 0;
+        G->stage_calls[k] = 0;
+    }
+    return GPK_OK;
+}

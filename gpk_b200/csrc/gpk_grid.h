@@ -98,7 +98,19 @@ struct gpk_grid {
     void* host_kernels = nullptr;          // HostKernels<real>*
     std::vector<void*> allocations;
     size_t device_bytes = 0;
+    // stage timing (gpk_grid_profile)
+    int profile = 0;
+    cudaEvent_t ev[GPK_NUM_STAGES][2] = {};
+    double stage_ms[GPK_NUM_STAGES] = {};
+    uint64_t stage_calls[GPK_NUM_STAGES] = {};
+    bool stage_open[GPK_NUM_STAGES] = {};
 };
+
+// brackets a stage with events when profiling is on; the elapsed time is
+// collected at the next stream synchronisation point of the step
+int gpk_stage_begin(gpk_grid* G, int stage);
+int gpk_stage_end(gpk_grid* G, int stage);
+int gpk_stage_collect(gpk_grid* G);
 
 // ---- launchers (templated on the grid's real type) --------------------------
 template <typename real> int gpk_build_tables(gpk_grid* G);

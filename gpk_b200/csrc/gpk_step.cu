@@ -259,9 +259,9 @@ __global__ void k_gauss_pass(Dims D, const real* __restrict__ in, real* __restri
         real acc = 0;
         for (int k = 0, ki = -krad; ki <= krad; ++k, ++ki) {
             int j;
-            if (axis == 0) j = D.idx(z, y, wrap1(x + ki, D.Nx));
-            else if (axis == 1) j = D.idx(z, wrap1(y + ki, D.Ny), x);
-            else j = D.idx(wrap1(z + ki, D.Nz), y, x);
+            if (axis == 0) j = D.idx(z, y, wrap_any(x + ki, D.Nx));
+            else if (axis == 1) j = D.idx(z, wrap_any(y + ki, D.Ny), x);
+            else j = D.idx(wrap_any(z + ki, D.Nz), y, x);
             acc += kw[k] * in[j];
         }
         out[i] = acc;
@@ -1069,6 +1069,37 @@ static int transport(gpk_grid* G) {
     return GPK_OK;
 }
 
+int gpk_stage_begin(gpk_grid* G, int stage) {
+    if (!G->profile) return GPK_OK;
+    if (!G->ev[stage][0]) {
+        GPK_CUDA_TRY(cudaEventCreate(&G->ev[stage][0]));
+        GPK_CUDA_TRY(cudaEventCreate(&G->ev[stage][1]));
+    }
+    GPK_CUDA_TRY(cudaEventRecord(G->ev[stage][0], G->stream));
+    return GPK_OK;
+}
+
+int gpk_stage_end(gpk_grid* G, int stage) {
+    if (!G->profile) return GPK_OK;
+    GPK_CUDA_TRY(cudaEventRecord(G->ev[stage][1], G->stream));
+    G->stage_open[stage] = true;
+    return GPK_OK;
+}
+
+int gpk_stage_collect(gpk_grid* G) {
+    if (!G->profile) return GPK_OK;
+    for (int k = 0; k < GPK_NUM_STAGES; ++k) {
+        if (!G->stage_open[k]) continue;
+        GPK_CUDA_TRY(cudaEventSynchronize(G->ev[k][1]));
+        float ms = 0.f;
+        GPK_CUDA_TRY(cudaEventElapsedTime(&ms, G->ev[k][0], G->ev[k][1]));
+        G->stage_ms[k] += ms;
+        G->stage_calls[k] += 1;
+        G->stage_open[k] = false;
+    }
+    return GPK_OK;
+}
+
 int gpk_sync_scalars(gpk_grid* G) {
     GPK_CUDA_TRY(cudaMemcpyAsync(G->h_scal, G->scal, sizeof(StepScalars), cudaMemcpyDeviceToHost, G->stream));
     GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
@@ -1095,8 +1126,13 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
         GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->stamp, 0, sizeof(unsigned), G->stream));
         G->h_scal->stamp = 0;
     }
+    GPK_TRY(gpk_stage_begin(G, GPK_STAGE_MASK));
     GPK_TRY(gpk_interface_mask<real>(G));
+    GPK_TRY(gpk_stage_end(G, GPK_STAGE_MASK));
+    GPK_TRY(gpk_stage_begin(G, GPK_STAGE_GEOMETRY));
     GPK_TRY(geometry<real>(G));
+    GPK_TRY(gpk_stage_end(G, GPK_STAGE_GEOMETRY));
+    GPK_TRY(gpk_stage_begin(G, GPK_STAGE_VELOCITY));
     GPK_TRY(elastic<real>(G));
     const ThermoDev TD = make_thermo_dev(th);
     GPK_CUDA_TRY(cudaMemsetAsync(G->f[GPK_FIELD_VN], 0, G->rsz * D.N, G->stream));
@@ -1106,7 +1142,9 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
         (const real*)G->f[GPK_FIELD_NX], (const real*)G->f[GPK_FIELD_NY], (const real*)G->f[GPK_FIELD_NZ],
         (const real*)G->f[GPK_FIELD_KAPPA], (const real*)G->f[GPK_FIELD_E_EL], (real*)G->f[GPK_FIELD_VN],
         (real*)G->f[GPK_FIELD_G_COMP]);
+    GPK_TRY(gpk_stage_end(G, GPK_STAGE_VELOCITY));
     // projection into vn2 (zero at bulk cells), then swap
+    GPK_TRY(gpk_stage_begin(G, GPK_STAGE_PROJECTION));
     GPK_CUDA_TRY(cudaMemsetAsync(G->vn2, 0, G->rsz * D.N, G->stream));
     k_projection<real><<<ga, 256, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, G->phi_comp, G->mask,
                                                   (const real*)G->f[GPK_FIELD_VN], (real*)G->vn2, G->d_proj_w,
@@ -1119,6 +1157,8 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
     k_vmax<real><<<ga, 256, 0, G->stream>>>(G->active, &G->scal->n_active, (const real*)G->f[GPK_FIELD_VN], vbits);
     k_select_dt<real><<<1, 1, 0, G->stream>>>(G->scal, vbits, (real)G->dx, (real)G->D, D.is3d() ? 1 : 0, dt_req, dt_cap);
     G->launches += 4;
+    GPK_TRY(gpk_stage_end(G, GPK_STAGE_PROJECTION));
+    GPK_TRY(gpk_stage_begin(G, GPK_STAGE_ALPHA));
     if (th.solute_rejection) {
         if (!G->solid_old) {
             GPK_TRY(gpk_alloc(G, &G->solid_old, G->rsz * D.N));
@@ -1145,8 +1185,10 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
     k_compact_u8_dyn<<<nt, MASK_TPB, 0, G->stream>>>(&G->scal->n_active, cflag, ctile, G->cand);
     G->launches += 4;
     GPK_CUDA_TRY(cudaGetLastError());
+    GPK_TRY(gpk_stage_end(G, GPK_STAGE_ALPHA));
     GPK_TRY(gpk_sync_scalars(G));
     const int m = (int)G->h_scal->n_cand;
+    GPK_TRY(gpk_stage_begin(G, GPK_STAGE_CROSSINGS));
     if (m > 0) {
         if (th.grain_network) {
             GPK_TRY(gpk_crossings<real>(G, m));
@@ -1158,10 +1200,12 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
             G->launches++;
         }
         GPK_CUDA_TRY(cudaGetLastError());
+        GPK_TRY(gpk_stage_end(G, GPK_STAGE_CROSSINGS));
         GPK_TRY(gpk_sync_scalars(G));
     }
     // balanced Gaussian remap, twice in 3-D when the first pass exchanged
     if (G->h_scal->accepted > 0) {
+        GPK_TRY(gpk_stage_begin(G, GPK_STAGE_REMAP));
         GPK_TRY(gpk_interface_mask<real>(G));
         GPK_TRY(gpk_remap_pass<real>(G));
         GPK_TRY(gpk_interface_mask<real>(G));
@@ -1178,8 +1222,14 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
         G->h_scal->exchanges = total;
         GPK_CUDA_TRY(cudaMemcpyAsync(&G->scal->exchanges, &G->h_scal->exchanges, sizeof(unsigned long long),
                                      cudaMemcpyHostToDevice, G->stream));
+        GPK_TRY(gpk_stage_end(G, GPK_STAGE_REMAP));
     }
-    if (th.grain_network && (G->step_id & 7ULL) == 0ULL) GPK_TRY(gpk_extinction<real>(G));
+    if (th.grain_network && (G->step_id & 7ULL) == 0ULL) {
+        GPK_TRY(gpk_stage_begin(G, GPK_STAGE_EXTINCTION));
+        GPK_TRY(gpk_extinction<real>(G));
+        GPK_TRY(gpk_stage_end(G, GPK_STAGE_EXTINCTION));
+    }
+    GPK_TRY(gpk_stage_begin(G, GPK_STAGE_TRANSPORT));
     GPK_TRY(transport<real>(G));
     if (th.dislocation_enabled && (real)th.recovery_rate > (real)0) {
         GPK_TRY(gpk_sync_scalars(G));
@@ -1191,9 +1241,11 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
             G->launches++;
         }
     }
+    GPK_TRY(gpk_stage_end(G, GPK_STAGE_TRANSPORT));
     k_advance_time<<<1, 1, 0, G->stream>>>(G->scal);
     G->launches++;
     GPK_CUDA_TRY(cudaGetLastError());
+    GPK_TRY(gpk_stage_collect(G));
     ++G->step_id;
     return GPK_OK;
 }
@@ -1217,6 +1269,49 @@ int gpk_max_dt_impl(gpk_grid* G, double* out) {
     const real dt_diff = (Dc > (real)0) ? (real)0.4 * dx * dx / (neighbors * Dc) : (real)1e30;
     *out = (double)dmin(dt_iface, dt_diff);
     return GPK_OK;
+}
+
+// gaussian_filter_3d (src/gpk_gaussian.cpp:9-72): host buffers in and out,
+// the three periodic passes on the device.
+extern "C" int gpk_gaussian_filter_3d(const float* in, float* out, int Nz, int Ny, int Nx, const float* taps,
+                                      int radius) {
+    if (!in || !out || !taps || Nz < 1 || Ny < 1 || Nx < 1 || radius < 0) {
+        gpk_set_error("gpk_gaussian_filter_3d: bad arguments");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    const Dims D{Nz, Ny, Nx, Nz * Ny * Nx};
+    const size_t nb = sizeof(float) * (size_t)D.N;
+    float *a = nullptr, *b = nullptr, *w = nullptr;
+    cudaStream_t st = nullptr;
+    int rc = GPK_OK;
+    auto done = [&](int code) {
+        if (st) cudaStreamSynchronize(st);
+        cudaFree(a); cudaFree(b); cudaFree(w);
+        if (st) cudaStreamDestroy(st);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess || cudaMalloc(&a, nb) != cudaSuccess ||
+        cudaMalloc(&b, nb) != cudaSuccess || cudaMalloc(&w, sizeof(float) * (2 * radius + 1)) != cudaSuccess) {
+        gpk_set_error("gpk_gaussian_filter_3d: device allocation failed");
+        return done(GPK_ERR_OUT_OF_MEMORY);
+    }
+    const int grid = std::min((D.N + 255) / 256, 148 * 8);
+    if (cudaMemcpyAsync(a, in, nb, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(w, taps, sizeof(float) * (2 * radius + 1), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return done(GPK_ERR_CUDA);
+    k_gauss_pass<float><<<grid, 256, 0, st>>>(D, a, b, w, radius, 0);
+    k_gauss_pass<float><<<grid, 256, 0, st>>>(D, b, a, w, radius, 1);
+    float* res = a;
+    if (Nz > 1) {
+        k_gauss_pass<float><<<grid, 256, 0, st>>>(D, a, b, w, radius, 2);
+        res = b;
+    }
+    if (cudaGetLastError() != cudaSuccess || cudaMemcpyAsync(out, res, nb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        gpk_set_error("gpk_gaussian_filter_3d: CUDA failure");
+        rc = GPK_ERR_CUDA;
+    }
+    return done(rc);
 }
 
 template int gpk_interface_mask<float>(gpk_grid*);

@@ -161,9 +161,11 @@ __device__ __forceinline__ bool bounded_branches_connected(const Dims& D, const 
 // ---------------------------------------------------------------------------
 // global flood fill (src/gpk_connectivity.cpp:79-115)
 // ---------------------------------------------------------------------------
+// `cap` bounds the stack; overflowing it (only possible if the label counts
+// were wrong) records GPK_ERR_INTERNAL instead of writing out of bounds.
 __device__ bool global_branches_connected(const Dims& D, const int32_t* __restrict__ phi, int cell, int32_t label,
                                           bool exclude_centre, uint32_t* __restrict__ stamp, int32_t* __restrict__ stack,
-                                          uint32_t my_stamp) {
+                                          uint32_t my_stamp, int cap, unsigned* err) {
     int nb6[6];
     D.faces(cell, nb6);
     const int nf = D.nface();
@@ -191,6 +193,7 @@ __device__ bool global_branches_connected(const Dims& D, const int32_t* __restri
             for (int t = 0; t < nt; ++t)
                 if (targets[t] == next) { targets[t] = targets[--nt]; break; }
             if (nt == 0) return true;
+            if (sp >= cap) { atomicCAS(err, 0u, (unsigned)GPK_ERR_INTERNAL); return false; }
             stack[sp++] = next;
         }
     }
@@ -212,7 +215,7 @@ struct CrossArgs {
     int4* cinfo;             // cell, old label, new label, state
     const int32_t* cpos;     // active position of the candidate
     const void* alpha_new_a; void* alpha; void* g; const void* g_comp; void* rho;
-    uint32_t* stamp; int32_t* ff_stack;
+    uint32_t* stamp; int32_t* ff_stack; long long pool_size;
     StepScalars* s;
     int sweep_rho; float rho_rex_f; double rho_rex_d;
   };
@@ -243,6 +246,7 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
     const Dims D = a.D;
     const bool is3d = D.is3d();
     unsigned* rem = a.s->wave_rem;  // three rotating counters
+    unsigned prev_left = (unsigned)m;
     for (int w = 0; w < max_waves; ++w) {
         // ---- phase A: locality test, topological numbers, global-read flags
         if (tid == 0) { rem[(w + 1) % 3] = 0; a.s->ff_pool = 0; }
@@ -297,19 +301,26 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
             const int to = (ci.w >> CS_TO_SHIFT) & 3, tn = (ci.w >> CS_TN_SHIFT) & 3;
             bool acc = true;
             uint32_t base = 0, my_stamp = 0;
+            int cap = 0;
             if (to > 1 || tn > 1) {
-                const int cap = max(to > 1 ? a.count[ci.y] : 0, tn > 1 ? a.count[ci.z] : 0) + 1;
+                cap = max(to > 1 ? a.count[ci.y] : 0, tn > 1 ? a.count[ci.z] : 0) + 1;
                 base = atomicAdd(&a.s->ff_pool, (unsigned)cap);
                 my_stamp = atomicAdd(&a.s->stamp, 2u) + 1u;
+                if ((long long)base + cap > (long long)a.pool_size) {
+                    atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
+                    cap = 0;
+                    base = 0;
+                }
             }
             if (to == 0) acc = a.count[ci.y] <= 1;
             else if (to > 1)
-                acc = global_branches_connected(D, a.phi, ci.x, ci.y, true, a.stamp, a.ff_stack + base, my_stamp);
+                acc = global_branches_connected(D, a.phi, ci.x, ci.y, true, a.stamp, a.ff_stack + base, my_stamp, cap,
+                                                &a.s->error);
             if (acc) {
                 if (tn == 0) acc = false;
                 else if (tn > 1)
                     acc = global_branches_connected(D, a.phi, ci.x, ci.z, false, a.stamp, a.ff_stack + base,
-                                                    my_stamp + 1u);
+                                                    my_stamp + 1u, cap, &a.s->error);
             }
             a.cinfo[k].w = ci.w | CS_READY | (acc ? CS_ACCEPT : 0);
         }
@@ -334,6 +345,14 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
             if (tid == 0) a.s->waves = w + 1;
             return;
         }
+        // the earliest pending item is always ready, so every wave applies
+        // at least one; every thread holds the previous count in a register
+        // (the shared counter of wave w-1 is recycled by wave w+1)
+        if (left >= prev_left) {
+            if (threadIdx.x == 0) atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
+            return;
+        }
+        prev_left = left;
     }
     if (tid == 0) atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
 }
@@ -545,6 +564,7 @@ __global__ void __launch_bounds__(256) k_bgr_exchange_waves(ExchArgs a, int n, i
     const bool is3d = D.is3d();
     real* g = (real*)a.g;
     unsigned* rem = a.s->wave_rem;
+    unsigned prev_left = 0xffffffffu;  // slots without an exchange are never pending
     for (int w = 0; w < max_waves; ++w) {
         if (tid == 0) rem[(w + 1) % 3] = 0;
         // ---- phase 1: readiness (no earlier pending exchange of an
@@ -623,6 +643,11 @@ __global__ void __launch_bounds__(256) k_bgr_exchange_waves(ExchArgs a, int n, i
             if (tid == 0) a.s->waves = w + 1;
             return;
         }
+        if (left >= prev_left) {
+            if (threadIdx.x == 0) atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
+            return;
+        }
+        prev_left = left;
     }
     if (tid == 0) atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
 }
@@ -695,7 +720,7 @@ __global__ void k_erosion_commit(int N, int32_t* __restrict__ phi, real* __restr
 // topology_simple_move diagnostic (src/gpk_connectivity.cpp:198-208)
 __global__ void k_topology_simple_move(Dims D, const int32_t* __restrict__ phi, const int32_t* __restrict__ count,
                                        int cell, int32_t new_label, uint32_t* stamp, int32_t* stack,
-                                       uint32_t my_stamp, int* out) {
+                                       uint32_t my_stamp, int* out, unsigned* err) {
     const int32_t old_label = phi[cell];
     bool r = true;
     if (old_label == new_label) r = false;
@@ -703,11 +728,13 @@ __global__ void k_topology_simple_move(Dims D, const int32_t* __restrict__ phi, 
         const int to = topological_number(D, phi, cell, old_label);
         const bool ext = count[old_label] <= 1;
         if (to == 0 && !ext) r = false;
-        else if (to > 1 && !global_branches_connected(D, phi, cell, old_label, true, stamp, stack, my_stamp)) r = false;
+        else if (to > 1 && !global_branches_connected(D, phi, cell, old_label, true, stamp, stack, my_stamp, D.N, err))
+            r = false;
         else {
             const int tn = topological_number(D, phi, cell, new_label);
             if (tn == 0) r = false;
-            else if (tn > 1 && !global_branches_connected(D, phi, cell, new_label, false, stamp, stack, my_stamp + 1))
+            else if (tn > 1 &&
+                     !global_branches_connected(D, phi, cell, new_label, false, stamp, stack, my_stamp + 1, D.N, err))
                 r = false;
         }
     }
@@ -758,7 +785,7 @@ int gpk_crossings(gpk_grid* G, int m) {
     a.cinfo = (int4*)G->cand_info; a.cpos = G->cand;
     a.alpha_new_a = G->alpha_new_a; a.alpha = G->f[GPK_FIELD_ALPHA]; a.g = G->f[GPK_FIELD_G];
     a.g_comp = G->f[GPK_FIELD_G_COMP]; a.rho = G->f[GPK_FIELD_RHO];
-    a.stamp = G->stamp; a.ff_stack = G->ff_stack; a.s = G->scal;
+    a.stamp = G->stamp; a.ff_stack = G->ff_stack; a.pool_size = 2LL * G->d.N + 64; a.s = G->scal;
     a.sweep_rho = G->th.dislocation_enabled; a.rho_rex_f = G->th.rho_rex; a.rho_rex_d = (double)G->th.rho_rex;
     int max_waves = m + 1;
     void* args[] = {&a, &m, &max_waves};
@@ -875,7 +902,7 @@ int gpk_topology_simple_move_impl(gpk_grid* G, int cell, int32_t new_label, int*
     GPK_CUDA_TRY(cudaMemcpyAsync(&G->scal->stamp, &G->h_scal->stamp, sizeof(unsigned), cudaMemcpyHostToDevice,
                                  G->stream));
     k_topology_simple_move<<<1, 1, 0, G->stream>>>(G->d, G->phi, G->count, cell, new_label, G->stamp,
-                                                   G->ff_stack + 1, st, d_out);
+                                                   G->ff_stack + 1, st, d_out, &G->scal->error);
     G->launches++;
     GPK_CUDA_TRY(cudaGetLastError());
     GPK_CUDA_TRY(cudaMemcpyAsync(result, d_out, sizeof(int), cudaMemcpyDeviceToHost, G->stream));

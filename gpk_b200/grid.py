@@ -199,6 +199,23 @@ class GPKGrid:
         check(lib().gpk_grid_device_bytes(self._h, C.byref(v)))
         return v.value
 
+    STAGES = ("mask", "geometry", "velocity", "projection", "alpha", "crossings", "remap",
+              "extinction", "transport")
+
+    def stream_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib().gpk_grid_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    def profile(self, enable: bool = True) -> None:
+        check(lib().gpk_grid_profile(self._h, 1 if enable else 0))
+
+    def stage_times(self) -> dict:
+        ms = (C.c_double * len(self.STAGES))()
+        calls = (C.c_uint64 * len(self.STAGES))()
+        check(lib().gpk_grid_stage_times(self._h, ms, calls))
+        return {s: (ms[k], int(calls[k])) for k, s in enumerate(self.STAGES)}
+
     def launch_count(self) -> int:
         v = C.c_uint64()
         check(lib().gpk_grid_launch_count(self._h, C.byref(v)))

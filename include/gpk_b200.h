@@ -187,6 +187,33 @@ int gpk_grid_device_bytes(gpk_grid* grid, size_t* out);
 /* Cumulative kernel-launch count issued by this grid (instrumentation).   */
 int gpk_grid_launch_count(gpk_grid* grid, uint64_t* out);
 
+/* gaussian_filter_3d (src/gpk_gaussian.cpp:9-72 of the reference): periodic
+ * separable filter of an Nz x Ny x Nx float field with 2*radius+1 taps,
+ * x then y then z (no z pass when Nz == 1), host buffers in and out.      */
+int gpk_gaussian_filter_3d(const float* in, float* out, int Nz, int Ny, int Nx,
+                           const float* taps, int radius);
+
+/* ---- instrumentation ------------------------------------------------------ */
+/* The CUDA stream (cudaStream_t) all of this grid's work is queued on.     */
+int gpk_grid_stream(gpk_grid* grid, void** stream);
+/* Stage timing with CUDA events on the grid's stream.  enable != 0 records
+ * an event pair around each stage of every following step; the per-stage
+ * device milliseconds accumulate until read.  Stages (GPK_STAGE_*):       */
+#define GPK_STAGE_MASK        0  /* interface mask + compaction          */
+#define GPK_STAGE_GEOMETRY    1  /* Gaussian-Hessian geometry + competitor */
+#define GPK_STAGE_VELOCITY    2  /* elastic proxy + constitutive velocity */
+#define GPK_STAGE_PROJECTION  3  /* pair projection + stable dt          */
+#define GPK_STAGE_ALPHA       4  /* alpha integration + candidates       */
+#define GPK_STAGE_CROSSINGS   5  /* certified label crossings            */
+#define GPK_STAGE_REMAP       6  /* balanced Gaussian remap              */
+#define GPK_STAGE_EXTINCTION  7  /* unresolved-grain extinction          */
+#define GPK_STAGE_TRANSPORT   8  /* diffusion / partitioning / recovery  */
+#define GPK_NUM_STAGES        9
+int gpk_grid_profile(gpk_grid* grid, int enable);
+/* ms[k] = device milliseconds of stage k summed over profiled steps;
+ * calls[k] = profiled steps; both reset after reading.                     */
+int gpk_grid_stage_times(gpk_grid* grid, double ms[GPK_NUM_STAGES], uint64_t calls[GPK_NUM_STAGES]);
+
 #ifdef __cplusplus
 }
 #endif
