@@ -321,7 +321,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpk_b200")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--size", type=int, default=SIZE, help="cube side (profiling of smaller cases)")
+    ap.add_argument("--grains", type=int, default=GRAINS)
     args = ap.parse_args()
+    globals()["SIZE"], globals()["GRAINS"] = args.size, args.grains
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_gpu_arm(args)
