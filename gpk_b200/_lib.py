@@ -69,6 +69,7 @@ def lib() -> C.CDLL:
         "gpk_grid_device_bytes": ([vp, C.POINTER(sz)], i32),
         "gpk_grid_launch_count": ([vp, C.POINTER(u64)], i32),
         "gpk_gaussian_filter_3d": ([vp, vp, i32, i32, i32, vp, i32], i32),
+        "gpk_gaussian_filter_3d_noalloc": ([vp, vp, i32, i32, i32, vp, i32], i32),
         "gpk_grid_stream": ([vp, C.POINTER(vp)], i32),
         "gpk_grid_profile": ([vp, i32], i32),
         "gpk_grid_stage_times": ([vp, C.POINTER(dbl), C.POINTER(u64)], i32),

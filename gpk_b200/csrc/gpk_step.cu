@@ -1320,3 +1320,87 @@ template int gpk_step_impl<float>(gpk_grid*, double, double);
 template int gpk_step_impl<double>(gpk_grid*, double, double);
 template int gpk_max_dt_impl<float>(gpk_grid*, double*);
 template int gpk_max_dt_impl<double>(gpk_grid*, double*);
+
+// ---------------------------------------------------------------------------
+// Allocation-free separable Gaussian filter.
+//
+// Some callers cannot call cudaMalloc: processes whose device memory is
+// owned up front by another allocator (a framework pool or a fixed budget),
+// latency-critical loops that must not allocate, and hosts that only link
+// this library without managing device memory themselves.  This entry point
+// runs the same three periodic passes as gpk_gaussian_filter_3d on host
+// input and output buffers, but its device scratch is the file-scope array
+// below instead of cudaMalloc'd buffers, and it creates no stream.
+//
+//  - The array holds taps plus two fields of at most GPK_NOALLOC_MAX_CELLS
+//    floats (16 MiB in all).  Every GPU that loads the library holds it until
+//    the process exits.  Larger grids are rejected with
+//    GPK_ERR_INVALID_ARGUMENT.
+//  - The first call on a device looks up the array's device address with
+//    cudaGetSymbolAddress while that device is current; make that first call
+//    before any stream capture on the device.
+//  - Every call overwrites the part of the array it reads before reading it,
+//    so no region has to start at zero; the array keeps the last call's
+//    contents.  All calls share the one array: calls in this process are
+//    serialised by a mutex, and calls that overlap on the GPU from any other
+//    route would race.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+static constexpr int NOALLOC_TAP_PAD = 512;  // taps region, a multiple of 64 floats
+static __device__ __align__(256) float g_noalloc_scratch[NOALLOC_TAP_PAD + 2 * (size_t)GPK_NOALLOC_MAX_CELLS];
+
+static std::mutex g_noalloc_mutex;
+static float* g_noalloc_ptr[64] = {};
+
+extern "C" int gpk_gaussian_filter_3d_noalloc(const float* in, float* out, int Nz, int Ny, int Nx, const float* taps,
+                                              int radius) {
+    if (!in || !out || !taps || Nz < 1 || Ny < 1 || Nx < 1 || radius < 0) {
+        gpk_set_error("gpk_gaussian_filter_3d_noalloc: bad arguments");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    const long long cells = (long long)Nz * Ny * Nx;
+    if (cells > GPK_NOALLOC_MAX_CELLS || 2 * radius + 1 > NOALLOC_TAP_PAD) {
+        gpk_set_error("gpk_gaussian_filter_3d_noalloc: " + std::to_string(cells) + " cells and " +
+                      std::to_string(2 * radius + 1) + " taps exceed the static scratch limits of " +
+                      std::to_string(GPK_NOALLOC_MAX_CELLS) + " cells and " + std::to_string(NOALLOC_TAP_PAD) +
+                      " taps");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    int dev = 0;
+    GPK_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        gpk_set_error("gpk_gaussian_filter_3d_noalloc: device index beyond 63");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    if (!g_noalloc_ptr[dev]) {
+        // set-up, once per device, with that device current
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            gpk_set_error(std::string("gpk_gaussian_filter_3d_noalloc: cudaGetSymbolAddress failed: ") +
+                          cudaGetErrorString(e));
+            return GPK_ERR_CUDA;
+        }
+        g_noalloc_ptr[dev] = (float*)p;
+    }
+    float* w = g_noalloc_ptr[dev];
+    float* a = w + NOALLOC_TAP_PAD;
+    float* b = a + GPK_NOALLOC_MAX_CELLS;
+    const Dims D{Nz, Ny, Nx, (int)cells};
+    const size_t nb = sizeof(float) * (size_t)cells;
+    GPK_CUDA_TRY(cudaMemcpy(w, taps, sizeof(float) * (2 * radius + 1), cudaMemcpyHostToDevice));
+    GPK_CUDA_TRY(cudaMemcpy(a, in, nb, cudaMemcpyHostToDevice));
+    const int grid = std::min((D.N + 255) / 256, 148 * 8);
+    k_gauss_pass<float><<<grid, 256>>>(D, a, b, w, radius, 0);
+    k_gauss_pass<float><<<grid, 256>>>(D, b, a, w, radius, 1);
+    float* res = a;
+    if (Nz > 1) {
+        k_gauss_pass<float><<<grid, 256>>>(D, a, b, w, radius, 2);
+        res = b;
+    }
+    GPK_CUDA_TRY(cudaGetLastError());
+    GPK_CUDA_TRY(cudaMemcpy(out, res, nb, cudaMemcpyDeviceToHost));
+    return GPK_OK;
+}

@@ -193,6 +193,23 @@ int gpk_grid_launch_count(gpk_grid* grid, uint64_t* out);
 int gpk_gaussian_filter_3d(const float* in, float* out, int Nz, int Ny, int Nx,
                            const float* taps, int radius);
 
+/* Allocation-free variant of gpk_gaussian_filter_3d (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc — processes whose
+ * device memory belongs to another allocator or a fixed budget, loops that
+ * must not allocate, hosts that only link this library — it takes the same
+ * host buffers and returns the same result, but uses a file-scope static
+ * device array (taps + two fields of at most GPK_NOALLOC_MAX_CELLS floats,
+ * 16 MiB held by every GPU that loads the library until exit) instead of
+ * cudaMalloc, and no stream of its own.  Larger grids return
+ * GPK_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress) with that device current: make it before
+ * any stream capture.  Calls share the array and keep the last call's
+ * contents; calls in one process are serialised, calls overlapping on the GPU
+ * by any other route race.                                                 */
+#define GPK_NOALLOC_MAX_CELLS (1 << 21)
+int gpk_gaussian_filter_3d_noalloc(const float* in, float* out, int Nz, int Ny, int Nx,
+                                   const float* taps, int radius);
+
 /* ---- instrumentation ------------------------------------------------------ */
 /* The CUDA stream (cudaStream_t) all of this grid's work is queued on.     */
 int gpk_grid_stream(gpk_grid* grid, void** stream);
