@@ -71,6 +71,8 @@ def lib() -> C.CDLL:
         "gpk_gaussian_filter_3d": ([vp, vp, i32, i32, i32, vp, i32], i32),
         "gpk_gaussian_filter_3d_noalloc": ([vp, vp, i32, i32, i32, vp, i32], i32),
         "gpk_grid_stream": ([vp, C.POINTER(vp)], i32),
+        "gpk_grid_wave_stats": ([vp, C.POINTER(u64)], i32),
+        "gpk_grid_set_geometry_kernel": ([vp, i32], i32),
         "gpk_grid_profile": ([vp, i32], i32),
         "gpk_grid_stage_times": ([vp, C.POINTER(dbl), C.POINTER(u64)], i32),
         "gpk_voronoi_init": ([i32, i32, i32, i32, u64, vp, vp, C.POINTER(i32)], i32),

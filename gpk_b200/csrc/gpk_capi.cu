@@ -95,10 +95,14 @@ int gpk_ensure_label_capacity(gpk_grid* G, int cap) {
     if (cap <= G->label_cap) return GPK_OK;
     int nc = std::max(cap, 64);
     gpk_free(G, G->count); gpk_free(G, G->minF); gpk_free(G, G->minL); gpk_free(G, G->unres);
+    gpk_free(G, G->count0); gpk_free(G, G->n_old);
     GPK_TRY(gpk_alloc(G, (void**)&G->count, sizeof(int32_t) * nc));
     GPK_TRY(gpk_alloc(G, (void**)&G->minF, sizeof(int32_t) * nc));
     GPK_TRY(gpk_alloc(G, (void**)&G->minL, sizeof(int32_t) * nc));
     GPK_TRY(gpk_alloc(G, (void**)&G->unres, nc));
+    GPK_TRY(gpk_alloc(G, (void**)&G->count0, sizeof(int32_t) * nc));
+    GPK_TRY(gpk_alloc(G, (void**)&G->n_old, sizeof(int32_t) * nc));
+    GPK_CUDA_TRY(cudaMemsetAsync(G->n_old, 0, sizeof(int32_t) * nc, G->stream));
     k_fill_u32<<<(nc + 255) / 256, 256, 0, G->stream>>>(G->minF, nc, 0x7fffffff);
     k_fill_u32<<<(nc + 255) / 256, 256, 0, G->stream>>>(G->minL, nc, 0x7fffffff);
     G->label_cap = nc;
@@ -233,6 +237,9 @@ static int init_fields(gpk_grid* G) {
     GPK_CUDA_TRY(cudaMemsetAsync(G->phi_comp, 0, sizeof(int32_t) * N, G->stream));
     GPK_CUDA_TRY(cudaMemsetAsync(G->mask, 0, N, G->stream));
     k_fill_u32<<<gN, 256, 0, G->stream>>>(G->pmap, N, -1);
+    // flood-fill visit marks: stamps start at 1, so 0 means "never visited"
+    GPK_CUDA_TRY(cudaMemsetAsync(G->stamp, 0, sizeof(uint32_t) * N, G->stream));
+    GPK_CUDA_TRY(cudaMemsetAsync(G->stamp_rev, 0, sizeof(uint32_t) * N, G->stream));
     GPK_CUDA_TRY(cudaGetLastError());
     return GPK_OK;
 }
@@ -301,7 +308,8 @@ extern "C" int gpk_grid_create(int Nz, int Ny, int Nx, double dx, const gpk_ther
     ALLOC(G->cand_info, 16 * N);
     ALLOC(G->pmap, 4 * N);
     ALLOC(G->stamp, 4 * N);
-    ALLOC(G->ff_stack, 4 * (2 * N + 64));
+    ALLOC(G->stamp_rev, 4 * N);
+    ALLOC(G->ff_stack, 4 * (5 * N + 64));  // flood-fill queues: cells + search ids
     ALLOC(G->bgr_res, rb);
     ALLOC(G->bgr_best, rb);
     ALLOC(G->key_a, 8 * N);
@@ -618,5 +626,26 @@ extern "C" int gpk_grid_stage_times(gpk_grid* G, double ms[GPK_NUM_STAGES], uint
         G->stage_ms[k] = 0;
         G->stage_calls[k] = 0;
     }
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_wave_stats(gpk_grid* G, uint64_t out[8]) {
+    if (!G || !out) return GPK_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 4; ++k) {
+        out[k] = G->wave_stats[k];
+        G->wave_stats[k] = 0;
+    }
+    GPK_TRY(gpk_sync_scalars(G));
+    out[4] = G->h_scal->flood_tasks;
+    out[5] = G->h_scal->flood_cells;
+    out[6] = G->h_scal->count_tasks;
+    out[7] = G->h_scal->count_scanned;
+    GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->flood_tasks, 0, 4 * sizeof(unsigned long long), G->stream));
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_set_geometry_kernel(gpk_grid* G, int kind) {
+    if (!G || kind < 0 || kind > 1) return GPK_ERR_INVALID_ARGUMENT;
+    G->geometry_kernel = kind;
     return GPK_OK;
 }

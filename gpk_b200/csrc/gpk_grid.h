@@ -76,7 +76,7 @@ struct gpk_grid {
     int32_t* cand_info = nullptr;          // packed per-candidate wave state
     int32_t* pmap = nullptr;               // pending map (cell -> item) or -1
     int32_t* minF = nullptr; int32_t* minL = nullptr;
-    uint32_t* stamp = nullptr; int32_t* ff_stack = nullptr;
+    uint32_t* stamp = nullptr; uint32_t* stamp_rev = nullptr; int32_t* ff_stack = nullptr;
     // remap
     void* bgr_res = nullptr; void* bgr_best = nullptr;   // per active position (real)
     unsigned long long* key_a = nullptr; unsigned long long* key_b = nullptr;
@@ -89,6 +89,8 @@ struct gpk_grid {
     void* sep_I = nullptr; void* sep_t1 = nullptr; void* sep_t2 = nullptr; void* sep_S = nullptr;
     // labels
     int32_t* count = nullptr;              // cells per label
+    int32_t* count0 = nullptr;             // cells per label when the crossing sweep started
+    int32_t* n_old = nullptr;              // crossing candidates per old label (zero between sweeps)
     int label_cap = 0;                     // labels live in [0, label_cap)
     // tables
     void* d_geom_table = nullptr; void* d_w0 = nullptr; void* d_w1 = nullptr; void* d_w2 = nullptr;
@@ -98,6 +100,12 @@ struct gpk_grid {
     void* host_kernels = nullptr;          // HostKernels<real>*
     std::vector<void*> allocations;
     size_t device_bytes = 0;
+    // waves of the crossing sweeps, waves of the remap exchange loops,
+    // crossing candidates, remap proposals (summed since last read)
+    uint64_t wave_stats[4] = {};
+    // geometry kernel choice: 0 = tiled (per-cell kernel where no tiled
+    // instantiation exists), 1 = per-cell kernel
+    int geometry_kernel = 0;
     // stage timing (gpk_grid_profile)
     int profile = 0;
     cudaEvent_t ev[GPK_NUM_STAGES][2] = {};
@@ -118,6 +126,8 @@ template <typename real> int gpk_step_impl(gpk_grid* G, double dt, double dt_cap
 template <typename real> int gpk_interface_mask(gpk_grid* G);
 template <typename real> int gpk_max_dt_impl(gpk_grid* G, double* out);
 template <typename real> int gpk_phase_volume_impl(gpk_grid* G, int32_t label, double* out);
+template <typename real>
+int gpk_geometry_tiled(gpk_grid* G, int R, real inv_dx, real inv_dx2, real dx, real kappa_limit);
 int gpk_recount_labels(gpk_grid* G);
 int gpk_topology_simple_move_impl(gpk_grid* G, int cell, int32_t new_label, int* result);
 int gpk_alloc(gpk_grid* G, void** p, size_t bytes);

@@ -79,8 +79,10 @@ struct StepScalars {
     unsigned bar_gen;       // grid barrier generation
     unsigned wave_rem[3];   // rotating "items left" counters of a wave loop
     unsigned present_labels;  // labels with at least one cell (extinction)
-    unsigned n_unres_cells; // unused
+    unsigned n_tasks;       // crossing candidates queued for warp-wide work
     unsigned pad;
+    // instrumentation of the label-wide work (summed until read)
+    unsigned long long flood_tasks, flood_cells, count_tasks, count_scanned;
 };
 
 // bounded grid-wide barrier for persistent kernels launched cooperatively.

@@ -947,6 +947,10 @@ static int geometry(gpk_grid* G) {
     if (!hk->global_separable) {
         const real inv_dx = (real)1 / dx;
         const real inv_dx2 = inv_dx * inv_dx;
+        if (G->geometry_kernel == 0) {
+            const int rc = gpk_geometry_tiled<real>(G, hk->geom_radius, inv_dx, inv_dx2, dx, kappa_limit);
+            if (rc != -1) return rc;
+        }
         const int grid = G->num_sms * 16;
         if (D.is3d())
             k_geometry_direct<real, true><<<grid, 128, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi,
@@ -1123,6 +1127,7 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
     // flood-fill stamps: restart before the 32-bit cursor can wrap
     if (G->h_scal->stamp > 0x70000000u) {
         GPK_CUDA_TRY(cudaMemsetAsync(G->stamp, 0, sizeof(uint32_t) * D.N, G->stream));
+        GPK_CUDA_TRY(cudaMemsetAsync(G->stamp_rev, 0, sizeof(uint32_t) * D.N, G->stream));
         GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->stamp, 0, sizeof(unsigned), G->stream));
         G->h_scal->stamp = 0;
     }
@@ -1202,22 +1207,30 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
         GPK_CUDA_TRY(cudaGetLastError());
         GPK_TRY(gpk_stage_end(G, GPK_STAGE_CROSSINGS));
         GPK_TRY(gpk_sync_scalars(G));
+        G->wave_stats[0] += G->h_scal->waves;
+        G->wave_stats[2] += (uint64_t)m;
     }
     // balanced Gaussian remap, twice in 3-D when the first pass exchanged
     if (G->h_scal->accepted > 0) {
         GPK_TRY(gpk_stage_begin(G, GPK_STAGE_REMAP));
         GPK_TRY(gpk_interface_mask<real>(G));
+        GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->waves, 0, sizeof(unsigned), G->stream));
         GPK_TRY(gpk_remap_pass<real>(G));
         GPK_TRY(gpk_interface_mask<real>(G));
         GPK_TRY(gpk_sync_scalars(G));
+        G->wave_stats[1] += G->h_scal->waves;
+        G->wave_stats[3] += G->h_scal->n_prop;
         const unsigned long long first = G->h_scal->exch_pass;
         unsigned long long total = first;
         if (D.is3d() && first > 0) {
             GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->exch_pass, 0, sizeof(unsigned long long), G->stream));
+            GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->waves, 0, sizeof(unsigned), G->stream));
             GPK_TRY(gpk_remap_pass<real>(G));
             GPK_TRY(gpk_interface_mask<real>(G));
             GPK_TRY(gpk_sync_scalars(G));
             total += G->h_scal->exch_pass;
+            G->wave_stats[1] += G->h_scal->waves;
+            G->wave_stats[3] += G->h_scal->n_prop;
         }
         G->h_scal->exchanges = total;
         GPK_CUDA_TRY(cudaMemcpyAsync(&G->scal->exchanges, &G->h_scal->exchanges, sizeof(unsigned long long),

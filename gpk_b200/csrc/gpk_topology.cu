@@ -9,15 +9,23 @@
 // The reference decides crossings one at a time in increasing flat index,
 // each against the state left by the previous commits, and the remap
 // exchanges one at a time in (label pair, rank) order.  Here both run as
-// waves of a persistent kernel.  An item (crossing or exchange) is decided in
-// a wave only when no earlier, still undecided item can change what it
-// reads, and no later item it could be affected by has been applied before
-// it.  For a crossing the reads are the 3^d box of its cell (topological
-// numbers) and, only when its certificate needs them, the region or the
-// count of its old/new label (global flood fill, extinction).  For a remap
-// exchange the reads are the 5^d boxes of its two cells.  Items whose reads
-// are disjoint from every earlier pending item's writes commute with them,
-// so every decision equals the serial one and labels stay bit-identical.
+// waves of a persistent kernel.
+//
+// Crossings: every decision reads a "serial-time view" of the labels, in
+// which a cell committed by a later candidate (higher index) shows its old
+// label again.  Later commits therefore never change an earlier decision,
+// and a candidate only has to wait for the earlier candidates it actually
+// reads: those within Chebyshev distance 2 that share one of its labels
+// (topological numbers read the 3^d box, bounded proofs the 5^d box), and,
+// only when its certificate needs a label-wide read (a global flood fill that
+// the bounded 5^d proof could not replace, or an exact label count near
+// extinction), every earlier candidate that touches that label.  A bounded
+// proof that succeeds implies the global flood fill succeeds, so using it
+// first changes no decision.
+//
+// Remap exchanges read the 5^d boxes of their two cells; an exchange waits
+// for earlier pending exchanges with an intersecting label pair within
+// Chebyshev distance 2 (in both directions, since exchanges commit in place).
 #include <cub/cub.cuh>
 
 #include "gpk_grid.h"
@@ -25,6 +33,36 @@
 namespace gpk_dev {
 
 static constexpr int32_t INT_BIG = 0x7fffffff;
+
+// ---- label readers ---------------------------------------------------------------
+struct PhiReader {  // the current labels, with at most one overridden cell
+    const int32_t* phi;
+    int ov_cell;
+    int32_t ov_label;
+    __device__ __forceinline__ int32_t operator()(int j) const { return j == ov_cell ? ov_label : phi[j]; }
+    __device__ __forceinline__ int32_t get(int j, bool& reverted) const {
+        reverted = false;
+        return (*this)(j);
+    }
+};
+// labels as the serial sweep saw them when it reached candidate k: cells
+// accepted by a later candidate read back their old label ("reverted")
+struct SerialView {
+    const int32_t* phi;
+    const int32_t* cmap;   // cell -> candidate index, -1 elsewhere
+    const int8_t* cres;    // 0 pending, 1 deferred, 2 accepted
+    const int4* cinfo;     // cell, old label, new label, state
+    int k;
+    __device__ __forceinline__ int32_t get(int j, bool& reverted) const {
+        const int c = cmap[j];
+        reverted = c > k && cres[c] == 2;
+        return reverted ? cinfo[c].y : phi[j];
+    }
+    __device__ __forceinline__ int32_t operator()(int j) const {
+        bool r;
+        return get(j, r);
+    }
+};
 
 // ---------------------------------------------------------------------------
 // 3^d topological number with 27-bit occupancy masks
@@ -59,7 +97,7 @@ __device__ __forceinline__ int count_face_components(uint32_t occ, bool is3d) {
     while (rem & faces) {
         uint32_t comp = (rem & faces) & (0u - (rem & faces));  // lowest face bit
         for (;;) {
-            uint32_t nxt = dilate3(comp, is3d) & occ;
+            const uint32_t nxt = dilate3(comp, is3d) & occ;
             if (nxt == comp) break;
             comp = nxt;
         }
@@ -69,10 +107,8 @@ __device__ __forceinline__ int count_face_components(uint32_t occ, bool is3d) {
     return count;
 }
 
-// Occupancy of `label` in the 3^d box around `cell` (centre cleared), with
-// an optional override of one cell's label (ov_cell < 0: none).
-__device__ __forceinline__ uint32_t box3_occupancy(const Dims& D, const int32_t* __restrict__ phi, int cell,
-                                                   int32_t label, int ov_cell, int32_t ov_label) {
+template <class Lab>
+__device__ __forceinline__ int topological_number(const Dims& D, const Lab& lab, int cell, int32_t label) {
     int z0, y0, x0;
     D.decode(cell, z0, y0, x0);
     const bool is3d = D.is3d();
@@ -84,19 +120,12 @@ __device__ __forceinline__ uint32_t box3_occupancy(const Dims& D, const int32_t*
             const int y = wrap1(y0 + ly - 1, D.Ny);
             for (int lx = 0; lx < 3; ++lx) {
                 const int x = wrap1(x0 + lx - 1, D.Nx);
-                const int j = D.idx(z, y, x);
-                const int32_t v = (j == ov_cell) ? ov_label : phi[j];
-                occ |= (uint32_t)(v == label) << (lz * 9 + ly * 3 + lx);
+                occ |= (uint32_t)(lab(D.idx(z, y, x)) == label) << (lz * 9 + ly * 3 + lx);
             }
         }
     }
-    const int centre = is3d ? 13 : 4;
-    return occ & ~(1u << centre);
-}
-
-__device__ __forceinline__ int topological_number(const Dims& D, const int32_t* __restrict__ phi, int cell,
-                                                  int32_t label, int ov_cell = -1, int32_t ov_label = 0) {
-    return count_face_components(box3_occupancy(D, phi, cell, label, ov_cell, ov_label), D.is3d());
+    occ &= ~(1u << (is3d ? 13 : 4));
+    return count_face_components(occ, is3d);
 }
 
 // ---------------------------------------------------------------------------
@@ -106,9 +135,9 @@ typedef unsigned __int128 u128;
 
 __device__ __forceinline__ u128 bit128(int b) { return ((u128)1) << b; }
 
-__device__ __forceinline__ bool bounded_branches_connected(const Dims& D, const int32_t* __restrict__ phi, int cell,
-                                                           int32_t label, bool exclude_centre, int ov_cell,
-                                                           int32_t ov_label) {
+template <class Lab>
+__device__ __forceinline__ bool bounded_branches_connected(const Dims& D, const Lab& lab, int cell, int32_t label,
+                                                           bool exclude_centre) {
     int z0, y0, x0;
     D.decode(cell, z0, y0, x0);
     const bool is3d = D.is3d();
@@ -122,10 +151,8 @@ __device__ __forceinline__ bool bounded_branches_connected(const Dims& D, const 
             const int y = wrap_any(y0 + ly - 2, D.Ny);
             for (int lx = 0; lx < 5; ++lx) {
                 const int x = wrap_any(x0 + lx - 2, D.Nx);
-                const int j = D.idx(z, y, x);
-                const int32_t v = (j == ov_cell) ? ov_label : phi[j];
                 const int b = lz * 25 + ly * 5 + lx;
-                if (v == label) occ |= bit128(b);
+                if (lab(D.idx(z, y, x)) == label) occ |= bit128(b);
                 if (lx == 0) lx0 |= bit128(b);
                 if (lx == 4) lx4 |= bit128(b);
                 if (ly == 0) ly0 |= bit128(b);
@@ -159,19 +186,20 @@ __device__ __forceinline__ bool bounded_branches_connected(const Dims& D, const 
 }
 
 // ---------------------------------------------------------------------------
-// global flood fill (src/gpk_connectivity.cpp:79-115)
+// global flood fill (src/gpk_connectivity.cpp:79-115).  `cap` bounds the
+// stack; overflowing it (only possible if the label counts were wrong)
+// records GPK_ERR_INTERNAL instead of writing out of bounds.
 // ---------------------------------------------------------------------------
-// `cap` bounds the stack; overflowing it (only possible if the label counts
-// were wrong) records GPK_ERR_INTERNAL instead of writing out of bounds.
-__device__ bool global_branches_connected(const Dims& D, const int32_t* __restrict__ phi, int cell, int32_t label,
-                                          bool exclude_centre, uint32_t* __restrict__ stamp, int32_t* __restrict__ stack,
-                                          uint32_t my_stamp, int cap, unsigned* err) {
+template <class Lab>
+__device__ bool global_branches_connected(const Dims& D, const Lab& lab, int cell, int32_t label, bool exclude_centre,
+                                          uint32_t* __restrict__ stamp, int32_t* __restrict__ stack, uint32_t my_stamp,
+                                          int cap, unsigned* err) {
     int nb6[6];
     D.faces(cell, nb6);
     const int nf = D.nface();
     int branches[6], nbr = 0;
     for (int k = 0; k < nf; ++k)
-        if (phi[nb6[k]] == label) branches[nbr++] = nb6[k];
+        if (lab(nb6[k]) == label) branches[nbr++] = nb6[k];
     if (nbr <= 1) return true;
     int targets[6], nt = 0;
     for (int k = 1; k < nbr; ++k) {
@@ -179,6 +207,7 @@ __device__ bool global_branches_connected(const Dims& D, const int32_t* __restri
         for (int t = 0; t < nt; ++t) dup |= targets[t] == branches[k];
         if (!dup) targets[nt++] = branches[k];
     }
+    if (cap < 1) { atomicCAS(err, 0u, (unsigned)GPK_ERR_INTERNAL); return false; }
     int sp = 0;
     stack[sp++] = branches[0];
     stamp[branches[0]] = my_stamp;
@@ -188,7 +217,7 @@ __device__ bool global_branches_connected(const Dims& D, const int32_t* __restri
         D.faces(cur, nx);
         for (int k = 0; k < nf; ++k) {
             const int next = nx[k];
-            if (phi[next] != label || (exclude_centre && next == cell) || stamp[next] == my_stamp) continue;
+            if ((exclude_centre && next == cell) || stamp[next] == my_stamp || lab(next) != label) continue;
             stamp[next] = my_stamp;
             for (int t = 0; t < nt; ++t)
                 if (targets[t] == next) { targets[t] = targets[--nt]; break; }
@@ -203,22 +232,30 @@ __device__ bool global_branches_connected(const Dims& D, const int32_t* __restri
 // ---------------------------------------------------------------------------
 // crossing sweep
 // ---------------------------------------------------------------------------
-// candidate state bits
 enum : int32_t {
-    CS_PENDING = 1, CS_LOCAL = 2, CS_FO = 4, CS_FN = 8, CS_READY = 16, CS_ACCEPT = 32,
-    CS_TO_SHIFT = 8, CS_TN_SHIFT = 12  // 2-bit capped topological numbers
+    CS_LOCAL = 1,      // no earlier pending candidate among its local reads
+    CS_GO = 2,         // needs the global flood fill of the old label
+    CS_GN = 4,         // needs the global flood fill of the new label
+    CS_GC = 8,         // needs the exact count of the old label
+    CS_CNT_REJECT = 16,  // old label isolated and provably not its last cell
+    CS_OLD_LOCAL = 32, // old-label branches proven connected inside 5^d
+    CS_NEW_LOCAL = 64, // new-label branches proven connected inside 5^d
+    CS_READY = 128, CS_ACCEPT = 256,
+    CS_TO_SHIFT = 12, CS_TN_SHIFT = 16  // 2-bit capped topological numbers
 };
 
 struct CrossArgs {
     Dims D;
-    int32_t* phi; int32_t* pmap; int32_t* minF; int32_t* minL; int32_t* count;
-    int4* cinfo;             // cell, old label, new label, state
-    const int32_t* cpos;     // active position of the candidate
+    int32_t* phi; int32_t* cmap; int8_t* cres; int32_t* minL; int32_t* count; const int32_t* count0;
+    const int32_t* n_old;  // candidates per old label
+    int4* cinfo;           // cell, old label, new label, state
+    const int32_t* cpos;   // active position of the candidate
     const void* alpha_new_a; void* alpha; void* g; const void* g_comp; void* rho;
-    uint32_t* stamp; int32_t* ff_stack; long long pool_size;
+    uint32_t* stamp; uint32_t* stamp_rev; int32_t* ff_stack; long long pool_size;
+    int32_t* tasks;        // candidates whose decision needs label-wide reads
     StepScalars* s;
     int sweep_rho; float rho_rex_f; double rho_rex_d;
-  };
+};
 
 template <typename real>
 __device__ __forceinline__ void cross_commit(const CrossArgs& a, int k, int4 ci, bool accept) {
@@ -236,6 +273,250 @@ __device__ __forceinline__ void cross_commit(const CrossArgs& a, int k, int4 ci,
         alpha[ci.x] = dmax(an, (real)1e-6);
         atomicAdd(&a.s->deferred, 1ull);
     }
+    a.cres[k] = accept ? 2 : 1;
+}
+
+// Exact count of `label` at candidate k's serial time; every earlier
+// candidate touching the label has been decided.
+__device__ int serial_count(const CrossArgs& a, int k, int32_t label) {
+    int c = a.count0[label];
+    for (int j = 0; j < k; ++j) {
+        if (a.cres[j] != 2) continue;
+        const int4 cj = a.cinfo[j];
+        c += (cj.z == label) - (cj.y == label);
+    }
+    return c;
+}
+
+// The same count with the 32 lanes of a warp splitting the earlier candidates.
+__device__ int warp_serial_count(const CrossArgs& a, int k, int32_t label) {
+    const int lane = threadIdx.x & 31;
+    int c = 0;
+    for (int j = lane; j < k; j += 32) {
+        if (a.cres[j] != 2) continue;
+        const int4 cj = a.cinfo[j];
+        c += (cj.z == label) - (cj.y == label);
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    return a.count0[label] + c;
+}
+
+// Warp-cooperative breadth-first form of global_branches_connected: are all
+// face branches of `label` around `cell` connected within the label's region
+// (minus the centre when exclude_centre)?  The answer does not depend on the
+// visiting order.  All 32 lanes call it with the same arguments; `queue`
+// holds `cap` cells.
+//
+// Visit marks: flood fills running in the same wave cover distinct labels,
+// but in the serial-time view a cell accepted by candidate m shows its old
+// label to candidates before m and its new label to candidates after m, so
+// it can lie in two regions at once — never in two regions as the same kind
+// of cell.  Reverted cells therefore carry their marks in a second array.
+template <class Lab>
+__device__ bool warp_branches_connected(const Dims& D, const Lab& lab, int cell, int32_t label, bool exclude_centre,
+                                        uint32_t* __restrict__ stamp, uint32_t* __restrict__ stamp_rev,
+                                        int32_t* __restrict__ queue, int cap, uint32_t my_stamp, unsigned* err,
+                                        int& visited) {
+    visited = 0;
+    const int lane = threadIdx.x & 31;
+    int nb6[6];
+    D.faces(cell, nb6);
+    const int nf = D.nface();
+    int branches[6], nbr = 0;
+    for (int k = 0; k < nf; ++k)
+        if (lab(nb6[k]) == label) branches[nbr++] = nb6[k];
+    if (nbr <= 1) return true;
+    int targets[6], nt = 0;
+    for (int k = 1; k < nbr; ++k) {
+        bool dup = false;
+        for (int t = 0; t < nt; ++t) dup |= targets[t] == branches[k];
+        if (!dup) targets[nt++] = branches[k];
+    }
+    if (cap < 1) {
+        if (lane == 0) atomicCAS(err, 0u, (unsigned)GPK_ERR_INTERNAL);
+        return false;
+    }
+    const unsigned all = (1u << nt) - 1u;
+    unsigned found = 0;
+    if (lane == 0) {
+        bool rev;
+        lab.get(branches[0], rev);
+        queue[0] = branches[0];
+        (rev ? stamp_rev : stamp)[branches[0]] = my_stamp;
+    }
+    __syncwarp();
+    int head = 0, tail = 1;
+    while (head < tail) {
+        const int n = min(32, tail - head);
+        int fresh[6];
+        int nfresh = 0;
+        if (lane < n) {
+            const int cur = queue[head + lane];
+            int nx[6];
+            D.faces(cur, nx);
+            for (int k = 0; k < nf; ++k) {
+                const int next = nx[k];
+                if (exclude_centre && next == cell) continue;
+                bool rev;
+                if (lab.get(next, rev) != label) continue;
+                uint32_t* mark = rev ? &stamp_rev[next] : &stamp[next];
+                if (*mark == my_stamp || atomicExch(mark, my_stamp) == my_stamp) continue;  // seen / taken by a lane
+                fresh[nfresh++] = next;
+            }
+        }
+        head += n;
+        unsigned hit = 0;
+        for (int q = 0; q < nfresh; ++q)
+            for (int t = 0; t < nt; ++t) hit |= (fresh[q] == targets[t]) ? (1u << t) : 0u;
+        found |= __reduce_or_sync(0xffffffffu, hit);
+        visited = tail;
+        if (found == all) return true;
+        int incl = nfresh;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (tail + total > cap) {
+            if (lane == 0) atomicCAS(err, 0u, (unsigned)GPK_ERR_INTERNAL);
+            return false;
+        }
+        const int off = tail + incl - nfresh;
+        for (int q = 0; q < nfresh; ++q) queue[off + q] = fresh[q];
+        tail += total;
+        __syncwarp();
+    }
+    visited = tail;
+    return found == all;
+}
+
+// Multi-source form of the same test: one breadth-first search grows from
+// every branch at once (search i marks its cells with my_stamp + i); when a
+// search reaches a cell of another search the two are united.  All branches
+// connected <=> all searches end up united; a group of united searches whose
+// frontier empties before that proves the branches disconnected.  A failed
+// test therefore costs about the smaller side instead of the whole region.
+// Needs distinct branch cells (always so unless a grid side is shorter than
+// three cells; callers fall back to warp_branches_connected then).  `queue`
+// holds 2*cap entries (cells, then search ids); stamps my_stamp..my_stamp+7.
+template <class Lab>
+__device__ bool warp_branches_connected_ms(const Dims& D, const Lab& lab, int cell, int32_t label, bool exclude_centre,
+                                           uint32_t* __restrict__ stamp, uint32_t* __restrict__ stamp_rev,
+                                           int32_t* __restrict__ queue, int cap, uint32_t my_stamp, unsigned* err,
+                                           int& visited) {
+    const int lane = threadIdx.x & 31;
+    visited = 0;
+    int nb6[6];
+    D.faces(cell, nb6);
+    const int nf = D.nface();
+    int br[6], nbr = 0;
+    for (int k = 0; k < nf; ++k)
+        if (lab(nb6[k]) == label) br[nbr++] = nb6[k];
+    if (nbr <= 1) return true;
+    for (int i = 0; i < nbr; ++i)
+        for (int j = i + 1; j < nbr; ++j)
+            if (br[i] == br[j])
+                return warp_branches_connected(D, lab, cell, label, exclude_centre, stamp, stamp_rev, queue, cap,
+                                               my_stamp, err, visited);
+    if (cap < nbr) {
+        if (lane == 0) atomicCAS(err, 0u, (unsigned)GPK_ERR_INTERNAL);
+        return false;
+    }
+    int32_t* qcell = queue;
+    int32_t* qsid = queue + cap;
+    int root[6], pend[6];
+    for (int i = 0; i < 6; ++i) { root[i] = i; pend[i] = i < nbr ? 1 : 0; }
+    if (lane < nbr) {
+        bool rev;
+        lab.get(br[lane], rev);
+        (rev ? stamp_rev : stamp)[br[lane]] = my_stamp + (uint32_t)lane;
+        qcell[lane] = br[lane];
+        qsid[lane] = lane;
+    }
+    __syncwarp();
+    int head = 0, tail = nbr;
+    while (head < tail) {
+        const int n = min(32, tail - head);
+        int fresh[6];
+        int nfresh = 0, sid = -1;
+        uint64_t unions = 0;  // bit 6*i + j: search i touched search j
+        if (lane < n) {
+            const int cur = qcell[head + lane];
+            sid = qsid[head + lane];
+            int nx[6];
+            D.faces(cur, nx);
+            for (int k = 0; k < nf; ++k) {
+                const int next = nx[k];
+                if (exclude_centre && next == cell) continue;
+                bool rev;
+                if (lab.get(next, rev) != label) continue;
+                uint32_t* mark = rev ? &stamp_rev[next] : &stamp[next];
+                const uint32_t seen = *mark - my_stamp;
+                if (seen < 8u) {  // already claimed by a search of this test
+                    if ((int)seen != sid) unions |= 1ull << (6 * sid + (int)seen);
+                    continue;
+                }
+                const uint32_t old = atomicExch(mark, my_stamp + (uint32_t)sid) - my_stamp;
+                if (old < 8u) {  // another lane claimed it first
+                    if ((int)old != sid) unions |= 1ull << (6 * sid + (int)old);
+                    continue;
+                }
+                fresh[nfresh++] = next;
+            }
+        }
+        head += n;
+        // processed entries leave their search's frontier, fresh ones join it
+        for (int i = 0; i < nbr; ++i) {
+            pend[i] -= __reduce_add_sync(0xffffffffu, (sid == i) ? 1 : 0);
+            pend[i] += __reduce_add_sync(0xffffffffu, (sid == i) ? nfresh : 0);
+        }
+        const uint32_t ulo = __reduce_or_sync(0xffffffffu, (uint32_t)unions);
+        const uint32_t uhi = __reduce_or_sync(0xffffffffu, (uint32_t)(unions >> 32));
+        uint64_t u = ((uint64_t)uhi << 32) | ulo;
+        while (u) {
+            const int b = __ffsll((long long)u) - 1;
+            u &= u - 1;
+            int ri = root[b / 6], rj = root[b % 6];
+            if (ri != rj) {
+                const int lo = min(ri, rj), hi = max(ri, rj);
+                for (int i = 0; i < 6; ++i)
+                    if (root[i] == hi) root[i] = lo;
+            }
+        }
+        // one group left: connected; a group with an empty frontier: not
+        bool single = true, closed = false;
+        for (int i = 0; i < nbr; ++i) single &= root[i] == root[0];
+        for (int r = 0; r < nbr && !single; ++r) {
+            if (root[r] != r) continue;
+            int p = 0;
+            for (int i = 0; i < nbr; ++i) p += (root[i] == r) ? pend[i] : 0;
+            closed |= p == 0;
+        }
+        int incl = nfresh;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        visited = tail + total;
+        if (single) return true;
+        if (closed) return false;
+        if (tail + total > cap) {
+            if (lane == 0) atomicCAS(err, 0u, (unsigned)GPK_ERR_INTERNAL);
+            return false;
+        }
+        const int off = tail + incl - nfresh;
+        for (int q = 0; q < nfresh; ++q) {
+            qcell[off + q] = fresh[q];
+            qsid[off + q] = sid;
+        }
+        tail += total;
+        __syncwarp();
+    }
+    // every frontier empty without one group: not connected
+    bool single = true;
+    for (int i = 0; i < nbr; ++i) single &= root[i] == root[0];
+    return single;
 }
 
 template <typename real>
@@ -248,96 +529,143 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
     unsigned* rem = a.s->wave_rem;  // three rotating counters
     unsigned prev_left = (unsigned)m;
     for (int w = 0; w < max_waves; ++w) {
-        // ---- phase A: locality test, topological numbers, global-read flags
+        // ---- phase A: locality, local certificate parts, label-wide needs;
+        //      earliest pending candidate touching each label
         if (tid == 0) { rem[(w + 1) % 3] = 0; a.s->ff_pool = 0; }
         for (int k = tid; k < m; k += nthr) {
-            int4 ci = a.cinfo[k];
-            if (!(ci.w & CS_PENDING)) continue;
+            if (a.cres[k] != 0) continue;
+            const int4 ci = a.cinfo[k];
+            atomicMin(&a.minL[ci.y], k);
+            atomicMin(&a.minL[ci.z], k);
             int z0, y0, x0;
             D.decode(ci.x, z0, y0, x0);
             bool local = true;
-            for (int dz = (is3d ? -1 : 0); dz <= (is3d ? 1 : 0) && local; ++dz)
-                for (int dy = -1; dy <= 1 && local; ++dy)
-                    for (int dx = -1; dx <= 1; ++dx) {
+            for (int dz = (is3d ? -2 : 0); dz <= (is3d ? 2 : 0) && local; ++dz)
+                for (int dy = -2; dy <= 2 && local; ++dy)
+                    for (int dx = -2; dx <= 2; ++dx) {
                         if (!dz && !dy && !dx) continue;
-                        const int j = D.idx(is3d ? wrap1(z0 + dz, D.Nz) : z0, wrap1(y0 + dy, D.Ny), wrap1(x0 + dx, D.Nx));
-                        const int q = a.pmap[j];
-                        if (q >= 0 && q < k) {
+                        const int j = D.idx(is3d ? wrap_any(z0 + dz, D.Nz) : z0, wrap_any(y0 + dy, D.Ny),
+                                            wrap_any(x0 + dx, D.Nx));
+                        const int q = a.cmap[j];
+                        if (q >= 0 && q < k && a.cres[q] == 0) {
                             const int4 cq = a.cinfo[q];
                             if (cq.y == ci.y || cq.y == ci.z || cq.z == ci.y || cq.z == ci.z) { local = false; break; }
                         }
                     }
-            int st = ci.w & CS_PENDING;
+            int st = 0;
             if (local) {
-                const int to = topological_number(D, a.phi, ci.x, ci.y);
-                const int tn = topological_number(D, a.phi, ci.x, ci.z);
-                st |= CS_LOCAL | (min(to, 2) << CS_TO_SHIFT) | (min(tn, 2) << CS_TN_SHIFT);
-                if (to != 1) st |= CS_FO;
-                if (tn > 1) st |= CS_FN;
-            } else {
-                st |= CS_FO | CS_FN;
+                const SerialView view{a.phi, a.cmap, a.cres, a.cinfo, k};
+                const int to = topological_number(D, view, ci.x, ci.y);
+                const int tn = topological_number(D, view, ci.x, ci.z);
+                st = CS_LOCAL | (min(to, 2) << CS_TO_SHIFT) | (min(tn, 2) << CS_TN_SHIFT);
+                if (to == 0) {
+                    // at k's serial time the label holds at least count0 - (its other candidates) cells
+                    if (a.count0[ci.y] - (a.n_old[ci.y] - 1) >= 2) st |= CS_CNT_REJECT;
+                    else st |= CS_GC;
+                } else if (to > 1) {
+                    if (bounded_branches_connected(D, view, ci.x, ci.y, true)) st |= CS_OLD_LOCAL;
+                    else st |= CS_GO;
+                }
+                if (tn > 1) {
+                    if (bounded_branches_connected(D, view, ci.x, ci.z, false)) st |= CS_NEW_LOCAL;
+                    else st |= CS_GN;
+                }
             }
             a.cinfo[k].w = st;
         }
         if (!grid_barrier(a.s, nblocks)) return;
-        // ---- phase B: earliest pending item per label (global reads / any touch)
+        // ---- phase B: readiness; decisions that need only local reads
         for (int k = tid; k < m; k += nthr) {
+            if (a.cres[k] != 0) continue;
             const int4 ci = a.cinfo[k];
-            if (!(ci.w & CS_PENDING)) continue;
-            if (ci.w & CS_FO) atomicMin(&a.minF[ci.y], k);
-            if (ci.w & CS_FN) atomicMin(&a.minF[ci.z], k);
-            atomicMin(&a.minL[ci.y], k);
-            atomicMin(&a.minL[ci.z], k);
+            const int st = ci.w;
+            if (!(st & CS_LOCAL)) continue;
+            if ((st & (CS_GO | CS_GC)) && a.minL[ci.y] < k) continue;
+            if ((st & CS_GN) && a.minL[ci.z] < k) continue;
+            if (st & (CS_GO | CS_GN | CS_GC)) {
+                // label-wide work: one warp per candidate in phase B2
+                a.tasks[atomicAdd(&a.s->n_tasks, 1u)] = k;
+                continue;
+            }
+            const int to = (st >> CS_TO_SHIFT) & 3, tn = (st >> CS_TN_SHIFT) & 3;
+            // to == 0 without GC is CS_CNT_REJECT; to > 1 without GO passed the 5^d proof
+            bool acc = to != 0;
+            if (acc && tn == 0) acc = false;
+            a.cinfo[k].w = st | CS_READY | (acc ? CS_ACCEPT : 0);
         }
         if (!grid_barrier(a.s, nblocks)) return;
-        // ---- phase C: readiness and decision on the current state
-        for (int k = tid; k < m; k += nthr) {
-            int4 ci = a.cinfo[k];
-            if (!(ci.w & CS_PENDING) || !(ci.w & CS_LOCAL)) continue;
-            const bool fo = ci.w & CS_FO, fn = ci.w & CS_FN;
-            if (a.minF[ci.y] < k || a.minF[ci.z] < k) continue;
-            if (fo && a.minL[ci.y] < k) continue;
-            if (fn && a.minL[ci.z] < k) continue;
-            const int to = (ci.w >> CS_TO_SHIFT) & 3, tn = (ci.w >> CS_TN_SHIFT) & 3;
-            bool acc = true;
-            uint32_t base = 0, my_stamp = 0;
-            int cap = 0;
-            if (to > 1 || tn > 1) {
-                cap = max(to > 1 ? a.count[ci.y] : 0, tn > 1 ? a.count[ci.z] : 0) + 1;
-                base = atomicAdd(&a.s->ff_pool, (unsigned)cap);
-                my_stamp = atomicAdd(&a.s->stamp, 2u) + 1u;
-                if ((long long)base + cap > (long long)a.pool_size) {
-                    atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
-                    cap = 0;
-                    base = 0;
+        // ---- phase B2: global flood fills and exact counts, a warp per candidate
+        {
+            const int lane = threadIdx.x & 31;
+            const int gwarp = tid >> 5, nwarps = nthr >> 5;
+            const unsigned ntask = *((volatile unsigned*)&a.s->n_tasks);
+            for (unsigned t = gwarp; t < ntask; t += nwarps) {
+                const int k = a.tasks[t];
+                const int4 ci = a.cinfo[k];
+                const int st = ci.w;
+                const SerialView view{a.phi, a.cmap, a.cres, a.cinfo, k};
+                const int to = (st >> CS_TO_SHIFT) & 3, tn = (st >> CS_TN_SHIFT) & 3;
+                int base = 0, cap = 0;
+                uint32_t my_stamp = 0;
+                if (st & (CS_GO | CS_GN)) {
+                    // the view of a label holds at most its count plus its later candidates' cells
+                    cap = max((st & CS_GO) ? a.count[ci.y] + a.n_old[ci.y] : 0,
+                              (st & CS_GN) ? a.count[ci.z] + a.n_old[ci.z] : 0) + 1;
+                    if (lane == 0) {
+                        // queue of cap cells plus cap search ids; 8 stamps per flood fill
+                        base = (int)atomicAdd(&a.s->ff_pool, (unsigned)(2 * cap));
+                        my_stamp = atomicAdd(&a.s->stamp, 16u) + 1u;
+                    }
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    my_stamp = __shfl_sync(0xffffffffu, my_stamp, 0);
+                    if ((long long)base + 2 * cap > a.pool_size) {
+                        if (lane == 0) atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
+                        cap = 0;
+                        base = 0;
+                    }
+                }
+                bool acc = true;
+                int visited = 0, vis = 0;
+                if (to == 0) {
+                    if (st & CS_CNT_REJECT) acc = false;
+                    else {
+                        acc = warp_serial_count(a, k, ci.y) <= 1;
+                        if (lane == 0) {
+                            atomicAdd(&a.s->count_tasks, 1ull);
+                            atomicAdd(&a.s->count_scanned, (unsigned long long)k);
+                        }
+                    }
+                } else if (to > 1 && !(st & CS_OLD_LOCAL)) {
+                    acc = warp_branches_connected_ms(D, view, ci.x, ci.y, true, a.stamp, a.stamp_rev,
+                                                     a.ff_stack + base, cap, my_stamp, &a.s->error, vis);
+                    visited += vis;
+                }
+                if (acc) {
+                    if (tn == 0) acc = false;
+                    else if (tn > 1 && !(st & CS_NEW_LOCAL))
+                        acc = warp_branches_connected_ms(D, view, ci.x, ci.z, false, a.stamp, a.stamp_rev,
+                                                         a.ff_stack + base, cap, my_stamp + 8u, &a.s->error, vis);
+                    visited += vis;
+                }
+                if (lane == 0) {
+                    a.cinfo[k].w = st | CS_READY | (acc ? CS_ACCEPT : 0);
+                    if (st & (CS_GO | CS_GN)) {
+                        atomicAdd(&a.s->flood_tasks, 1ull);
+                        atomicAdd(&a.s->flood_cells, (unsigned long long)visited);
+                    }
                 }
             }
-            if (to == 0) acc = a.count[ci.y] <= 1;
-            else if (to > 1)
-                acc = global_branches_connected(D, a.phi, ci.x, ci.y, true, a.stamp, a.ff_stack + base, my_stamp, cap,
-                                                &a.s->error);
-            if (acc) {
-                if (tn == 0) acc = false;
-                else if (tn > 1)
-                    acc = global_branches_connected(D, a.phi, ci.x, ci.z, false, a.stamp, a.ff_stack + base,
-                                                    my_stamp + 1u, cap, &a.s->error);
-            }
-            a.cinfo[k].w = ci.w | CS_READY | (acc ? CS_ACCEPT : 0);
         }
         if (!grid_barrier(a.s, nblocks)) return;
-        // ---- phase D: commit ready items, reset per-label minima
+        if (tid == 0) a.s->n_tasks = 0;
+        // ---- phase C: commit ready candidates, reset per-label minima
         for (int k = tid; k < m; k += nthr) {
+            if (a.cres[k] != 0) continue;
             const int4 ci = a.cinfo[k];
-            if (!(ci.w & CS_PENDING)) continue;
-            a.minF[ci.y] = INT_BIG; a.minF[ci.z] = INT_BIG;
-            a.minL[ci.y] = INT_BIG; a.minL[ci.z] = INT_BIG;
-            if (ci.w & CS_READY) {
-                cross_commit<real>(a, k, ci, (ci.w & CS_ACCEPT) != 0);
-                a.pmap[ci.x] = -1;
-                a.cinfo[k].w = 0;
-            } else {
-                atomicAdd(&rem[w % 3], 1u);
-            }
+            a.minL[ci.y] = INT_BIG;
+            a.minL[ci.z] = INT_BIG;
+            if (ci.w & CS_READY) cross_commit<real>(a, k, ci, (ci.w & CS_ACCEPT) != 0);
+            else atomicAdd(&rem[w % 3], 1u);
         }
         if (!grid_barrier(a.s, nblocks)) return;
         const unsigned left = *((volatile unsigned*)&rem[w % 3]);
@@ -345,9 +673,9 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
             if (tid == 0) a.s->waves = w + 1;
             return;
         }
-        // the earliest pending item is always ready, so every wave applies
-        // at least one; every thread holds the previous count in a register
-        // (the shared counter of wave w-1 is recycled by wave w+1)
+        // the earliest pending candidate is always ready, so every wave
+        // decides at least one; every thread holds the previous count in a
+        // register (the shared counter of wave w-1 is recycled by wave w+1)
         if (left >= prev_left) {
             if (threadIdx.x == 0) atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
             return;
@@ -357,16 +685,28 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
     if (tid == 0) atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
 }
 
-// Gathers the candidates (in active order) and arms the pending map.
-template <typename real>
-__global__ void k_cross_setup(Dims D, const int32_t* __restrict__ active, const int32_t* __restrict__ cpos, int m,
+// Gathers the candidates (in active order), maps their cells and counts
+// the candidates per old label.
+__global__ void k_cross_setup(const int32_t* __restrict__ active, const int32_t* __restrict__ cpos, int m,
                               const int32_t* __restrict__ phi, const int32_t* __restrict__ phi_comp, int4* cinfo,
-                              int32_t* pmap) {
+                              int32_t* cmap, int8_t* cres, int32_t* n_old) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= m) return;
     const int cell = active[cpos[k]];
-    cinfo[k] = make_int4(cell, phi[cell], phi_comp[cell], CS_PENDING);
-    pmap[cell] = k;
+    const int32_t o = phi[cell];
+    cinfo[k] = make_int4(cell, o, phi_comp[cell], 0);
+    cmap[cell] = k;
+    cres[k] = 0;
+    atomicAdd(&n_old[o], 1);
+}
+
+// Clears the cell map and the per-label candidate counts after the sweep.
+__global__ void k_cross_cleanup(int m, const int4* __restrict__ cinfo, int32_t* cmap, int32_t* n_old) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const int4 ci = cinfo[k];
+    cmap[ci.x] = -1;
+    n_old[ci.y] = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -497,7 +837,7 @@ __global__ void k_bgr_match(int n, const unsigned long long* __restrict__ key1, 
             e.y = val[rstart + r];
             e.z = (int)(k >> 37);
             e.w = (int)((k >> 11) & ((1ull << 26) - 1));
-            st = CS_PENDING;
+            st = 1;  // pending (ES_PENDING)
             pmap[e.x] = t;
             pmap[e.y] = t;
         }
@@ -534,13 +874,14 @@ __device__ __forceinline__ int mismatch_count(const Dims& D, const int32_t* phi,
 __device__ __forceinline__ bool certificate_local(const Dims& D, const int32_t* phi, int cell, int32_t old_label,
                                                   int32_t new_label, int old_count, int ov_cell, int32_t ov_label) {
     if (old_label == new_label) return false;
-    const int old_object = topological_number(D, phi, cell, old_label, ov_cell, ov_label);
+    const PhiReader lab{phi, ov_cell, ov_label};
+    const int old_object = topological_number(D, lab, cell, old_label);
     const bool old_ext = old_count <= 1;
     if (old_object == 0 && !old_ext) return false;
-    if (old_object > 1 && !bounded_branches_connected(D, phi, cell, old_label, true, ov_cell, ov_label)) return false;
-    const int new_object = topological_number(D, phi, cell, new_label, ov_cell, ov_label);
+    if (old_object > 1 && !bounded_branches_connected(D, lab, cell, old_label, true)) return false;
+    const int new_object = topological_number(D, lab, cell, new_label);
     if (new_object == 0) return false;
-    if (new_object > 1 && !bounded_branches_connected(D, phi, cell, new_label, false, ov_cell, ov_label)) return false;
+    if (new_object > 1 && !bounded_branches_connected(D, lab, cell, new_label, false)) return false;
     return true;
 }
 
@@ -722,19 +1063,20 @@ __global__ void k_topology_simple_move(Dims D, const int32_t* __restrict__ phi, 
                                        int cell, int32_t new_label, uint32_t* stamp, int32_t* stack,
                                        uint32_t my_stamp, int* out, unsigned* err) {
     const int32_t old_label = phi[cell];
+    const PhiReader lab{phi, -1, 0};
     bool r = true;
     if (old_label == new_label) r = false;
     else {
-        const int to = topological_number(D, phi, cell, old_label);
+        const int to = topological_number(D, lab, cell, old_label);
         const bool ext = count[old_label] <= 1;
         if (to == 0 && !ext) r = false;
-        else if (to > 1 && !global_branches_connected(D, phi, cell, old_label, true, stamp, stack, my_stamp, D.N, err))
+        else if (to > 1 && !global_branches_connected(D, lab, cell, old_label, true, stamp, stack, my_stamp, D.N, err))
             r = false;
         else {
-            const int tn = topological_number(D, phi, cell, new_label);
+            const int tn = topological_number(D, lab, cell, new_label);
             if (tn == 0) r = false;
             else if (tn > 1 &&
-                     !global_branches_connected(D, phi, cell, new_label, false, stamp, stack, my_stamp + 1, D.N, err))
+                     !global_branches_connected(D, lab, cell, new_label, false, stamp, stack, my_stamp + 1, D.N, err))
                 r = false;
         }
     }
@@ -775,23 +1117,35 @@ template <typename real>
 int gpk_crossings(gpk_grid* G, int m) {
     if (m == 0) return GPK_OK;
     const int B = 256;
-    k_cross_setup<real><<<(m + B - 1) / B, B, 0, G->stream>>>(G->d, G->active, G->cand, m, G->phi, G->phi_comp,
-                                                             (int4*)G->cand_info, G->pmap);
+    // label counts at the start of the sweep (exact counts near extinction)
+    GPK_CUDA_TRY(cudaMemcpyAsync(G->count0, G->count, sizeof(int32_t) * G->label_cap, cudaMemcpyDeviceToDevice,
+                                 G->stream));
+    int8_t* cres = (int8_t*)G->val_a;  // candidate results, scratch until the remap
+    k_cross_setup<<<(m + B - 1) / B, B, 0, G->stream>>>(G->active, G->cand, m, G->phi, G->phi_comp,
+                                                        (int4*)G->cand_info, G->pmap, cres, G->n_old);
     G->launches++;
     GPK_CUDA_TRY(cudaGetLastError());
     CrossArgs a;
     a.D = G->d;
-    a.phi = G->phi; a.pmap = G->pmap; a.minF = G->minF; a.minL = G->minL; a.count = G->count;
+    a.phi = G->phi; a.cmap = G->pmap; a.cres = cres; a.minL = G->minL; a.count = G->count; a.count0 = G->count0;
+    a.n_old = G->n_old;
     a.cinfo = (int4*)G->cand_info; a.cpos = G->cand;
     a.alpha_new_a = G->alpha_new_a; a.alpha = G->f[GPK_FIELD_ALPHA]; a.g = G->f[GPK_FIELD_G];
     a.g_comp = G->f[GPK_FIELD_G_COMP]; a.rho = G->f[GPK_FIELD_RHO];
-    a.stamp = G->stamp; a.ff_stack = G->ff_stack; a.pool_size = 2LL * G->d.N + 64; a.s = G->scal;
+    a.stamp = G->stamp; a.stamp_rev = G->stamp_rev; a.ff_stack = G->ff_stack; a.pool_size = 5LL * G->d.N + 64;
+    a.s = G->scal;
+    a.tasks = (int32_t*)G->key_a;  // free until the remap
+    GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->n_tasks, 0, sizeof(unsigned), G->stream));
     a.sweep_rho = G->th.dislocation_enabled; a.rho_rex_f = G->th.rho_rex; a.rho_rex_d = (double)G->th.rho_rex;
     int max_waves = m + 1;
     void* args[] = {&a, &m, &max_waves};
     const void* kern = (const void*)k_crossing_sweep<real>;
     const int grid = coop_grid(G, kern, 256, m);
-    return launch_coop(G, kern, grid, 256, args);
+    GPK_TRY(launch_coop(G, kern, grid, 256, args));
+    k_cross_cleanup<<<(m + B - 1) / B, B, 0, G->stream>>>(m, (const int4*)G->cand_info, G->pmap, G->n_old);
+    G->launches++;
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
 }
 
 // One balanced-remap pass.  Precondition: the interface mask and the active

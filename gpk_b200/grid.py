@@ -202,6 +202,16 @@ class GPKGrid:
     STAGES = ("mask", "geometry", "velocity", "projection", "alpha", "crossings", "remap",
               "extinction", "transport")
 
+    def wave_stats(self) -> dict:
+        out = (C.c_uint64 * 8)()
+        check(lib().gpk_grid_wave_stats(self._h, out))
+        return {"crossing_waves": int(out[0]), "remap_waves": int(out[1]), "candidates": int(out[2]),
+                "remap_proposals": int(out[3]), "flood_fills": int(out[4]), "flood_cells": int(out[5]),
+                "exact_counts": int(out[6]), "count_scanned": int(out[7])}
+
+    def set_geometry_kernel(self, kind: str) -> None:
+        check(lib().gpk_grid_set_geometry_kernel(self._h, {"tiled": 0, "per_cell": 1}[kind]))
+
     def stream_ptr(self) -> int:
         p = C.c_void_p()
         check(lib().gpk_grid_stream(self._h, C.byref(p)))

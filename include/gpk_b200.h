@@ -230,6 +230,15 @@ int gpk_grid_profile(gpk_grid* grid, int enable);
 /* ms[k] = device milliseconds of stage k summed over profiled steps;
  * calls[k] = profiled steps; both reset after reading.                     */
 int gpk_grid_stage_times(gpk_grid* grid, double ms[GPK_NUM_STAGES], uint64_t calls[GPK_NUM_STAGES]);
+/* out = {waves of the crossing sweeps, waves of the remap exchange loops,
+ * crossing candidates, remap proposals, global flood fills, cells they
+ * visited, exact label counts, candidates those counts scanned}, summed
+ * since the last read.                                                     */
+int gpk_grid_wave_stats(gpk_grid* grid, uint64_t out[8]);
+/* Geometry kernel selection (both give identical results): 0 = tiled
+ * shared-memory kernel where an instantiation exists (default), 1 = the
+ * per-interface-cell kernel.                                               */
+int gpk_grid_set_geometry_kernel(gpk_grid* grid, int kind);
 
 #ifdef __cplusplus
 }
