@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
               "-ftz=false", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-ffp-contract=off,-fopenmp,-O2"]
-SOURCES = ["gpk_capi.cu", "gpk_step.cu", "gpk_geometry.cu", "gpk_topology.cu", "gpk_init.cpp", "gpk_core_shim.cpp"]
+SOURCES = ["gpk_capi.cu", "gpk_step.cu", "gpk_geometry.cu", "gpk_local.cu", "gpk_topology.cu", "gpk_init.cpp", "gpk_core_shim.cpp"]
 
 
 def _nvcc() -> str:

@@ -102,10 +102,56 @@ constexpr size_t geo_smem_bytes() {
     return (size_t)2 * S::PLANE * sizeof(real) + (size_t)S::NLAB * 4 + (size_t)S::NCELL * 2 + 64;
 }
 
+// One row of W taps (fixed dz, dy).  The Gaussian factor w0(o) is exactly 0
+// for |o| in {R-1, R} (the Gaussian has radius R-2), so a product with such
+// a factor is +-0 and adding it is an exact no-op (see the file comment):
+//   x factor zero (|dx| >= R-1): Iy, Iyy, Iz, Izz, Iyz have no contribution
+//   y factor zero (ZY0):         Ix, Ixx, Iz, Izz, Ixz
+//   z factor zero (ZZ0):         Ix, Iy, Ixx, Iyy, Ixy
+// Components: 0 Ix, 1 Iy, 2 Ixx, 3 Iyy, 4 Ixy, 5 Iz, 6 Izz, 7 Ixz, 8 Iyz.
+template <typename real, int R, bool IS3D, int SLOTS, bool ZY0, bool ZZ0>
+__device__ __forceinline__ void geo_row(const int32_t* __restrict__ lab, const real* __restrict__ trow, int yoff,
+                                        real acc[SLOTS][9], const int base[SLOTS], const int32_t res[SLOTS]) {
+    constexpr int W = 2 * R + 1;
+#pragma unroll
+    for (int dxs = 0; dxs < W; ++dxs) {
+        const bool zx0 = dxs <= 1 || dxs >= W - 2;  // compile-time after unrolling
+        bool live[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) live[k] = IS3D || k < 5;
+        if (zx0) live[1] = live[3] = live[5] = live[6] = live[8] = false;
+        if (ZY0) live[0] = live[2] = live[5] = live[6] = live[7] = false;
+        if (ZZ0) live[0] = live[1] = live[2] = live[3] = live[4] = false;
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) any |= live[k];
+        if (!any) continue;
+        const real* t = trow + dxs * 12;
+        real w[9];
+        if (sizeof(real) == 4) {
+            const float4 t0 = *reinterpret_cast<const float4*>(t);
+            const float4 t1 = *reinterpret_cast<const float4*>(t + 4);
+            w[0] = t0.x; w[1] = t0.y; w[2] = t0.z; w[3] = t0.w;
+            w[4] = t1.x; w[5] = t1.y; w[6] = t1.z; w[7] = t1.w;
+            w[8] = live[8] ? t[8] : (real)0;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) w[k] = live[k] ? t[k] : (real)0;
+        }
+#pragma unroll
+        for (int s = 0; s < SLOTS; ++s) {
+            const real m = (lab[base[s] + yoff + dxs] == res[s]) ? (real)1 : (real)0;
+#pragma unroll
+            for (int k = 0; k < 9; ++k)
+                if (live[k]) acc[s][k] = fma_rn<real>(w[k], m, acc[s][k]);
+        }
+    }
+}
+
 template <typename real, int R, bool IS3D, int SLOTS>
 __device__ __forceinline__ void geo_accumulate(const GeoArgs<real>& a, const int32_t* __restrict__ lab,
                                                const real* __restrict__ tab0, const real* __restrict__ tab1,
-                                               uint64_t* bars, const int16_t* cells, int ncell, int tid,
+                                               uint64_t* bars, const int16_t* cells, int nact, int tid,
                                                real acc[SLOTS][9], int base[SLOTS], int32_t res[SLOTS], bool& ok) {
     typedef GeoShape<R, IS3D> S;
     constexpr int W = S::W;
@@ -127,41 +173,22 @@ __device__ __forceinline__ void geo_accumulate(const GeoArgs<real>& a, const int
             mbar_expect_tx(&bars[(p + 1) & 1], S::PLANE * sizeof(real));
             bulk_g2s(dst, a.table + (size_t)(p + 1) * S::PLANE, S::PLANE * sizeof(real), &bars[(p + 1) & 1]);
         }
-        if (ok) {
+        if (ok && tid < nact) {
             const int zoff = p * S::HY * S::HXP;
+            // rows whose y or z Gaussian factor is exactly zero run
+            // specialised bodies without the corresponding products
+            const bool zz0 = IS3D && (p <= 1 || p >= W - 2);
 #pragma unroll 1
             for (int dy = 0; dy < W; ++dy) {
                 const real* trow = tab + dy * W * 12;
                 const int yoff = zoff + dy * S::HXP;
-#pragma unroll
-                for (int dxs = 0; dxs < W; ++dxs) {
-                    const real* t = trow + dxs * 12;
-                    real w[9];
-                    if (sizeof(real) == 4) {
-                        const float4 t0 = *reinterpret_cast<const float4*>(t);
-                        const float4 t1 = *reinterpret_cast<const float4*>(t + 4);
-                        w[0] = t0.x; w[1] = t0.y; w[2] = t0.z; w[3] = t0.w;
-                        w[4] = t1.x; w[5] = t1.y; w[6] = t1.z; w[7] = t1.w;
-                        w[8] = t[8];
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < 9; ++k) w[k] = t[k];
-                    }
-#pragma unroll
-                    for (int s = 0; s < SLOTS; ++s) {
-                        const real m = (lab[base[s] + yoff + dxs] == res[s]) ? (real)1 : (real)0;
-                        acc[s][0] = fma_rn<real>(w[0], m, acc[s][0]);
-                        acc[s][1] = fma_rn<real>(w[1], m, acc[s][1]);
-                        acc[s][2] = fma_rn<real>(w[2], m, acc[s][2]);
-                        acc[s][3] = fma_rn<real>(w[3], m, acc[s][3]);
-                        acc[s][4] = fma_rn<real>(w[4], m, acc[s][4]);
-                        if (IS3D) {
-                            acc[s][5] = fma_rn<real>(w[5], m, acc[s][5]);
-                            acc[s][6] = fma_rn<real>(w[6], m, acc[s][6]);
-                            acc[s][7] = fma_rn<real>(w[7], m, acc[s][7]);
-                            acc[s][8] = fma_rn<real>(w[8], m, acc[s][8]);
-                        }
-                    }
+                const bool yy0 = dy <= 1 || dy >= W - 2;
+                if (zz0) {
+                    if (yy0) geo_row<real, R, IS3D, SLOTS, true, true>(lab, trow, yoff, acc, base, res);
+                    else geo_row<real, R, IS3D, SLOTS, false, true>(lab, trow, yoff, acc, base, res);
+                } else {
+                    if (yy0) geo_row<real, R, IS3D, SLOTS, true, false>(lab, trow, yoff, acc, base, res);
+                    else geo_row<real, R, IS3D, SLOTS, false, false>(lab, trow, yoff, acc, base, res);
                 }
             }
         }
@@ -281,14 +308,19 @@ __global__ void __launch_bounds__(256) k_geometry_tiled(GeoArgs<real> a) {
     }
     __syncthreads();
 
+    // The tile's cells go to the fewest threads that hold them at `slots`
+    // cells each: thread t < nact takes cells t, t + nact, ...  Warps whose
+    // threads all lie beyond nact skip the arithmetic, leaving their issue
+    // slots to the other resident CTA instead of computing dummy cells.
     const int slots = (ncell + 255) / 256;
+    const int nact = (ncell + slots - 1) / slots;
     bool ok = true;
     int base[4], myc[4];
     int32_t res[4];
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
-        const int k = tid + 256 * s;
-        myc[s] = (k < ncell) ? cells[k] : -1;
+        const int k = tid + nact * s;
+        myc[s] = (tid < nact && k < ncell) ? cells[k] : -1;
         const int c = myc[s] < 0 ? cells[0] : myc[s];
         const int lx = c % S::TX, ly = (c / S::TX) % S::TY, lz = c / (S::TX * S::TY);
         // label of tap (dz,dy,dx) at lab[base + (dz+R)*plane + (dy+R)*HXP + (dx+R)]
@@ -298,10 +330,10 @@ __global__ void __launch_bounds__(256) k_geometry_tiled(GeoArgs<real> a) {
 
     real acc[4][9];
     switch (slots) {
-    case 1: geo_accumulate<real, R, IS3D, 1>(a, lab, tab0, tab1, bars, cells, ncell, tid, (real(*)[9])acc, base, res, ok); break;
-    case 2: geo_accumulate<real, R, IS3D, 2>(a, lab, tab0, tab1, bars, cells, ncell, tid, (real(*)[9])acc, base, res, ok); break;
-    case 3: geo_accumulate<real, R, IS3D, 3>(a, lab, tab0, tab1, bars, cells, ncell, tid, (real(*)[9])acc, base, res, ok); break;
-    default: geo_accumulate<real, R, IS3D, 4>(a, lab, tab0, tab1, bars, cells, ncell, tid, (real(*)[9])acc, base, res, ok); break;
+    case 1: geo_accumulate<real, R, IS3D, 1>(a, lab, tab0, tab1, bars, cells, nact, tid, (real(*)[9])acc, base, res, ok); break;
+    case 2: geo_accumulate<real, R, IS3D, 2>(a, lab, tab0, tab1, bars, cells, nact, tid, (real(*)[9])acc, base, res, ok); break;
+    case 3: geo_accumulate<real, R, IS3D, 3>(a, lab, tab0, tab1, bars, cells, nact, tid, (real(*)[9])acc, base, res, ok); break;
+    default: geo_accumulate<real, R, IS3D, 4>(a, lab, tab0, tab1, bars, cells, nact, tid, (real(*)[9])acc, base, res, ok); break;
     }
     if (!ok) return;
 #pragma unroll

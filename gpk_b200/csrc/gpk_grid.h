@@ -128,6 +128,8 @@ template <typename real> int gpk_max_dt_impl(gpk_grid* G, double* out);
 template <typename real> int gpk_phase_volume_impl(gpk_grid* G, int32_t label, double* out);
 template <typename real>
 int gpk_geometry_tiled(gpk_grid* G, int R, real inv_dx, real inv_dx2, real dx, real kappa_limit);
+template <typename real> int gpk_bgr_scores_tiled(gpk_grid* G, int radius, real* res, real* best);
+template <typename real> int gpk_projection_tiled(gpk_grid* G, int radius);
 int gpk_recount_labels(gpk_grid* G);
 int gpk_topology_simple_move_impl(gpk_grid* G, int cell, int32_t new_label, int* result);
 int gpk_alloc(gpk_grid* G, void** p, size_t bytes);

@@ -1,0 +1,286 @@
+// gpk_local.cu — tiled kernels for the small-radius Gaussian boxes of a step:
+// the pair velocity projection (src/gpk_physics.cpp:152-193) and the
+// balanced-remap scores (src/gpk_transitions.cpp:53-91).
+//
+// Both visit a (2R+1)^d box (R = 3 at the configured sigmas) around every
+// interface cell and accumulate, in double and in the reference's z -> y -> x
+// tap order, the weights (double)expf(-r2/(2 s^2)) of the taps that satisfy a
+// label condition.  One CTA stages its tile's labels (and, for the
+// projection, each cell's label pair and signed velocity) with an R-cell
+// periodic halo in shared memory and walks the tile's interface cells.  The
+// conditional additions are written as fma(w, m, acc) with m in {0, 1}; a sum
+// that starts at +0 is never -0 in round-to-nearest, so adding a signed zero
+// changes nothing and the result is bit-identical to `if (cond) acc += w`.
+#include <cuda_runtime.h>
+
+#include <cub/cub.cuh>
+
+#include "gpk_grid.h"
+
+namespace gpk_dev {
+
+template <bool IS3D> struct LocTile;
+template <> struct LocTile<true> { static constexpr int TX = 16, TY = 8, TZ = 8; };
+template <> struct LocTile<false> { static constexpr int TX = 32, TY = 32, TZ = 1; };
+
+template <int R, bool IS3D>
+struct LocShape {
+    static constexpr int TX = LocTile<IS3D>::TX, TY = LocTile<IS3D>::TY, TZ = LocTile<IS3D>::TZ;
+    static constexpr int HX = TX + 2 * R, HY = TY + 2 * R, HZ = IS3D ? TZ + 2 * R : 1;
+    static constexpr int NH = HX * HY * HZ;
+    static constexpr int NCELL = TX * TY * TZ;
+    static constexpr int R2MAX = (IS3D ? 3 : 2) * R * R;
+};
+
+// Compacts the tile's interface cells (flat tile order) into `cells`; returns
+// their number.  All threads of the 256-thread block call it.
+template <int R, bool IS3D>
+__device__ __forceinline__ int tile_interface_cells(const Dims& D, const uint8_t* __restrict__ mask, int x0, int y0,
+                                                    int z0, int16_t* cells) {
+    typedef LocShape<R, IS3D> S;
+    typedef cub::BlockScan<int, 256> BS;
+    __shared__ typename BS::TempStorage scan;
+    __shared__ int s_total;
+    constexpr int PER = (S::NCELL + 255) / 256;
+    int flags[PER];
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int c = threadIdx.x * PER + k;
+        int f = 0;
+        if (c < S::NCELL) {
+            const int lx = c % S::TX, ly = (c / S::TX) % S::TY, lz = c / (S::TX * S::TY);
+            const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+            if (x < D.Nx && y < D.Ny && z < D.Nz) f = mask[D.idx(z, y, x)];
+        }
+        flags[k] = f;
+        cnt += f;
+    }
+    int ex, total;
+    BS(scan).ExclusiveSum(cnt, ex, total);
+#pragma unroll
+    for (int k = 0; k < PER; ++k)
+        if (flags[k]) cells[ex++] = (int16_t)(threadIdx.x * PER + k);
+    if (threadIdx.x == 0) s_total = total;
+    __syncthreads();
+    return s_total;
+}
+
+// ---------------------------------------------------------------------------
+// balanced-remap scores
+// ---------------------------------------------------------------------------
+// Weighted support of the resident label and of the first NC candidates over
+// the box (tap order z -> y -> x).  Unused candidate slots hold -1 and match
+// nothing, so running fewer slots than 6 changes no sum.
+template <int R, bool IS3D, int NC, int HX, int HY>
+__device__ __forceinline__ void score_box_impl(const int32_t* __restrict__ lab, int base, const double* __restrict__ w,
+                                               int32_t pi, const int32_t cand[6], double& resident, double sup[6]) {
+#pragma unroll 1
+    for (int dz = (IS3D ? -R : 0); dz <= (IS3D ? R : 0); ++dz)
+#pragma unroll 1
+        for (int dy = -R; dy <= R; ++dy) {
+            const int rowb = base + ((IS3D ? dz + R : 0) * HY + dy + R) * HX + R;
+            const int r2yz = dy * dy + dz * dz;
+#pragma unroll
+            for (int dx = -R; dx <= R; ++dx) {
+                const int32_t v = lab[rowb + dx];
+                const double wt = w[r2yz + dx * dx];
+                resident = __fma_rn(wt, v == pi ? 1.0 : 0.0, resident);
+#pragma unroll
+                for (int q = 0; q < NC; ++q) sup[q] = __fma_rn(wt, v == cand[q] ? 1.0 : 0.0, sup[q]);
+            }
+        }
+}
+template <int R, bool IS3D, int NC>
+__device__ __forceinline__ void score_box(const int32_t* __restrict__ lab, int base, const double* __restrict__ w,
+                                          int32_t pi, const int32_t cand[6], double& resident, double sup[6]) {
+    typedef LocShape<R, IS3D> S;
+    score_box_impl<R, IS3D, NC, S::HX, S::HY>(lab, base, w, pi, cand, resident, sup);
+}
+template <typename real, int R, bool IS3D>
+__global__ void __launch_bounds__(256) k_bgr_scores_tiled(Dims D, const int32_t* __restrict__ phi,
+                                                          const uint8_t* __restrict__ mask, int ntx, int nty,
+                                                          const double* __restrict__ wtab, int32_t* __restrict__ phi_comp,
+                                                          real* __restrict__ res_out, real* __restrict__ best_out) {
+    typedef LocShape<R, IS3D> S;
+    __shared__ int32_t lab[S::NH];
+    __shared__ int16_t cells[S::NCELL];
+    __shared__ double w[S::R2MAX + 1];
+    const int t = blockIdx.x;
+    const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
+    const int x0 = tx * S::TX, y0 = ty * S::TY, z0 = tz * S::TZ;
+    const int ncell = tile_interface_cells<R, IS3D>(D, mask, x0, y0, z0, cells);
+    if (ncell == 0) return;
+    for (int e = threadIdx.x; e < S::NH; e += 256) {
+        const int hx = e % S::HX, hy = (e / S::HX) % S::HY, hz = e / (S::HX * S::HY);
+        const int x = wrap_any(x0 + hx - R, D.Nx), y = wrap_any(y0 + hy - R, D.Ny);
+        const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
+        lab[e] = phi[D.idx(z, y, x)];
+    }
+    for (int e = threadIdx.x; e <= S::R2MAX; e += 256) w[e] = wtab[e];
+    __syncthreads();
+    const int plane = S::HX * S::HY;
+    for (int c = threadIdx.x; c < ncell; c += 256) {
+        const int lc = cells[c];
+        const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
+        const int cb = ((IS3D ? lz + R : 0) * S::HY + ly + R) * S::HX + lx + R;
+        const int32_t pi = lab[cb];
+        // distinct unlike face-neighbour labels in face order; -1 pads
+        const int fo[6] = {-1, +1, -S::HX, +S::HX, -plane, +plane};
+        int32_t cand[6] = {-1, -1, -1, -1, -1, -1};
+        int nc = 0;
+        for (int k = 0; k < (IS3D ? 6 : 4); ++k) {
+            const int32_t v = lab[cb + fo[k]];
+            if (v == pi) continue;
+            bool known = false;
+            for (int q = 0; q < nc; ++q) known |= cand[q] == v;
+            if (!known) cand[nc++] = v;
+        }
+        double resident = 0.0, sup[6] = {0, 0, 0, 0, 0, 0};
+        const int base = cb - (IS3D ? R * plane : 0) - R * S::HX - R;
+        // candidate slots beyond the warp's largest count are skipped
+        const int ncw = __reduce_max_sync(__activemask(), nc);
+        switch (ncw) {
+        case 0: score_box<R, IS3D, 0>(lab, base, w, pi, cand, resident, sup); break;
+        case 1: score_box<R, IS3D, 1>(lab, base, w, pi, cand, resident, sup); break;
+        case 2: score_box<R, IS3D, 2>(lab, base, w, pi, cand, resident, sup); break;
+        case 3: score_box<R, IS3D, 3>(lab, base, w, pi, cand, resident, sup); break;
+        default: score_box<R, IS3D, 6>(lab, base, w, pi, cand, resident, sup); break;
+        }
+        double best = -1.0;
+        int32_t best_label = pi;
+        for (int q = 0; q < nc; ++q)
+            if (sup[q] > best) { best = sup[q]; best_label = cand[q]; }
+        const int i = D.idx(z0 + lz, y0 + ly, x0 + lx);
+        res_out[i] = (real)resident;
+        best_out[i] = (real)best;
+        phi_comp[i] = best_label;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pair projection
+// ---------------------------------------------------------------------------
+// Staged per halo cell: its unordered label pair (low, high), or (-1, -1) when
+// it is not an interface cell or has no competitor, and orientation*vn.
+template <typename real, int R, bool IS3D>
+__global__ void __launch_bounds__(256) k_projection_tiled(Dims D, const int32_t* __restrict__ phi,
+                                                          const int32_t* __restrict__ phi_comp,
+                                                          const uint8_t* __restrict__ mask, const real* __restrict__ vn,
+                                                          real* __restrict__ vn_out, int ntx, int nty,
+                                                          const double* __restrict__ wtab) {
+    typedef LocShape<R, IS3D> S;
+    extern __shared__ __align__(16) unsigned char dyn[];
+    int2* pair = reinterpret_cast<int2*>(dyn);          // S::NH entries
+    real* svn = reinterpret_cast<real*>(pair + S::NH);  // S::NH entries
+    __shared__ int16_t cells[S::NCELL];
+    __shared__ double w[S::R2MAX + 1];
+    const int t = blockIdx.x;
+    const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
+    const int x0 = tx * S::TX, y0 = ty * S::TY, z0 = tz * S::TZ;
+    const int ncell = tile_interface_cells<R, IS3D>(D, mask, x0, y0, z0, cells);
+    if (ncell == 0) return;
+    for (int e = threadIdx.x; e < S::NH; e += 256) {
+        const int hx = e % S::HX, hy = (e / S::HX) % S::HY, hz = e / (S::HX * S::HY);
+        const int x = wrap_any(x0 + hx - R, D.Nx), y = wrap_any(y0 + hy - R, D.Ny);
+        const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
+        const int j = D.idx(z, y, x);
+        const int32_t pj = phi[j], qj = phi_comp[j];
+        if (mask[j] && pj != qj) {
+            const int32_t lo = min(pj, qj);
+            pair[e] = make_int2(lo, max(pj, qj));
+            svn[e] = (pj == lo) ? vn[j] : -vn[j];
+        } else {
+            pair[e] = make_int2(-1, -1);
+            svn[e] = (real)0;
+        }
+    }
+    for (int e = threadIdx.x; e <= S::R2MAX; e += 256) w[e] = wtab[e];
+    __syncthreads();
+    const int plane = S::HX * S::HY;
+    for (int c = threadIdx.x; c < ncell; c += 256) {
+        const int lc = cells[c];
+        const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
+        const int cb = ((IS3D ? lz + R : 0) * S::HY + ly + R) * S::HX + lx + R;
+        const int i = D.idx(z0 + lz, y0 + ly, x0 + lx);
+        const int2 pr = pair[cb];
+        real out = vn[i];
+        if (pr.x >= 0) {
+            // interface cell with a competitor: average over the same pair
+            const real orient_i = (phi[i] == pr.x) ? (real)1 : (real)-1;
+            double num = 0.0, den = 0.0;
+            const int base = cb - (IS3D ? R * plane : 0) - R * S::HX - R;
+#pragma unroll
+            for (int dz = (IS3D ? -R : 0); dz <= (IS3D ? R : 0); ++dz)
+#pragma unroll
+                for (int dy = -R; dy <= R; ++dy)
+#pragma unroll
+                    for (int dx = -R; dx <= R; ++dx) {
+                        const int e = base + ((IS3D ? dz + R : 0) * S::HY + dy + R) * S::HX + dx + R;
+                        const int2 pj = pair[e];
+                        const double m = (pj.x == pr.x && pj.y == pr.y) ? 1.0 : 0.0;
+                        const double wt = w[dx * dx + dy * dy + dz * dz];
+                        // reference: (w * orientation_j) * vn_j == w * (orientation_j * vn_j), exactly
+                        num = __fma_rn(wt * (double)svn[e], m, num);
+                        den = __fma_rn(wt, m, den);
+                    }
+            if (den > 0.0) out = orient_i * (real)(num / den);
+        }
+        vn_out[i] = out;
+    }
+}
+
+template <typename real, int R, bool IS3D>
+static int launch_scores(gpk_grid* G, real* res, real* best) {
+    typedef LocShape<R, IS3D> S;
+    const Dims D = G->d;
+    const int ntx = (D.Nx + S::TX - 1) / S::TX, nty = (D.Ny + S::TY - 1) / S::TY, ntz = (D.Nz + S::TZ - 1) / S::TZ;
+    k_bgr_scores_tiled<real, R, IS3D><<<ntx * nty * ntz, 256, 0, G->stream>>>(D, G->phi, G->mask, ntx, nty,
+                                                                               G->d_remap_w, G->phi_comp, res, best);
+    G->launches++;
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+template <typename real, int R, bool IS3D>
+static int launch_projection(gpk_grid* G) {
+    typedef LocShape<R, IS3D> S;
+    const Dims D = G->d;
+    const int ntx = (D.Nx + S::TX - 1) / S::TX, nty = (D.Ny + S::TY - 1) / S::TY, ntz = (D.Nz + S::TZ - 1) / S::TZ;
+    const size_t smem = (size_t)S::NH * (sizeof(int2) + sizeof(real));
+    static bool attr_set = false;
+    if (!attr_set) {
+        GPK_CUDA_TRY(cudaFuncSetAttribute(k_projection_tiled<real, R, IS3D>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    k_projection_tiled<real, R, IS3D><<<ntx * nty * ntz, 256, smem, G->stream>>>(
+        D, G->phi, G->phi_comp, G->mask, (const real*)G->f[GPK_FIELD_VN], (real*)G->vn2, ntx, nty, G->d_proj_w);
+    G->launches++;
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+}  // namespace gpk_dev
+
+using namespace gpk_dev;
+
+// Tiled remap scores / projection for radius 3 (the radius at every sigma up
+// to 8 cells for the projection and at every sigma for the remap); -1 when
+// no tiled instantiation applies.
+template <typename real>
+int gpk_bgr_scores_tiled(gpk_grid* G, int radius, real* res, real* best) {
+    if (radius != 3) return -1;
+    return G->d.is3d() ? launch_scores<real, 3, true>(G, res, best) : launch_scores<real, 3, false>(G, res, best);
+}
+
+template <typename real>
+int gpk_projection_tiled(gpk_grid* G, int radius) {
+    if (radius != 3) return -1;
+    return G->d.is3d() ? launch_projection<real, 3, true>(G) : launch_projection<real, 3, false>(G);
+}
+
+template int gpk_bgr_scores_tiled<float>(gpk_grid*, int, float*, float*);
+template int gpk_bgr_scores_tiled<double>(gpk_grid*, int, double*, double*);
+template int gpk_projection_tiled<float>(gpk_grid*, int);
+template int gpk_projection_tiled<double>(gpk_grid*, int);

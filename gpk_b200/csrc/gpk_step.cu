@@ -1151,9 +1151,13 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
     // projection into vn2 (zero at bulk cells), then swap
     GPK_TRY(gpk_stage_begin(G, GPK_STAGE_PROJECTION));
     GPK_CUDA_TRY(cudaMemsetAsync(G->vn2, 0, G->rsz * D.N, G->stream));
-    k_projection<real><<<ga, 256, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, G->phi_comp, G->mask,
-                                                  (const real*)G->f[GPK_FIELD_VN], (real*)G->vn2, G->d_proj_w,
-                                                  hk->proj_radius);
+    const int prc = G->geometry_kernel == 0 ? gpk_projection_tiled<real>(G, hk->proj_radius) : -1;
+    if (prc == -1)
+        k_projection<real><<<ga, 256, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, G->phi_comp, G->mask,
+                                                      (const real*)G->f[GPK_FIELD_VN], (real*)G->vn2, G->d_proj_w,
+                                                      hk->proj_radius);
+    else if (prc != GPK_OK)
+        return prc;
     std::swap(G->f[GPK_FIELD_VN], G->vn2);
     // stable dt
     typedef typename RealBits<real>::U U;

@@ -757,8 +757,8 @@ __global__ void k_bgr_scores(Dims D, const int32_t* __restrict__ active, const u
         int32_t best_label = pi;
         for (int q = 0; q < nc; ++q)
             if (sup[q] > best) { best = sup[q]; best_label = cand[q]; }
-        res_a[a] = (real)resident;
-        best_a[a] = (real)best;
+        res_a[i] = (real)resident;
+        best_a[i] = (real)best;
         phi_comp[i] = best_label;
     }
 }
@@ -775,7 +775,7 @@ __global__ void k_bgr_proposals(const int32_t* __restrict__ active, const unsign
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
         const int i = active[a];
         const int32_t p = phi[i], q = phi_comp[i];
-        const real gain = best_a[a] - res_a[a];
+        const real gain = best_a[i] - res_a[i];  // scores are stored by cell
         if (p == q || !(gain > (real)1e-7)) continue;
         const unsigned slot = atomicAdd(&s->n_prop, 1u);
         unsigned long long gbits;
@@ -1158,9 +1158,15 @@ int gpk_remap_pass(gpk_grid* G) {
     const int grid = 4 * G->num_sms;
     // phi_comp <- phi everywhere, then the best candidate at interface cells
     GPK_CUDA_TRY(cudaMemcpyAsync(G->phi_comp, G->phi, sizeof(int32_t) * D.N, cudaMemcpyDeviceToDevice, G->stream));
-    k_bgr_scores<real><<<grid, B, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, G->phi_comp,
-                                                  (real*)G->bgr_res, (real*)G->bgr_best, G->d_remap_w,
-                                                  hk->remap_radius);
+    const int rc = G->geometry_kernel == 0
+                       ? gpk_bgr_scores_tiled<real>(G, hk->remap_radius, (real*)G->bgr_res, (real*)G->bgr_best)
+                       : -1;
+    if (rc == -1)
+        k_bgr_scores<real><<<grid, B, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, G->phi_comp,
+                                                      (real*)G->bgr_res, (real*)G->bgr_best, G->d_remap_w,
+                                                      hk->remap_radius);
+    else if (rc != GPK_OK)
+        return rc;
     GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->n_prop, 0, sizeof(unsigned), G->stream));
     k_bgr_proposals<real><<<grid, B, 0, G->stream>>>(G->active, &G->scal->n_active, G->phi, G->phi_comp,
                                                      (const real*)G->bgr_res, (const real*)G->bgr_best, G->key_b,
