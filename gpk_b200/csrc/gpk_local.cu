@@ -210,20 +210,23 @@ __global__ void __launch_bounds__(256) k_projection_tiled(Dims D, const int32_t*
             const real orient_i = (phi[i] == pr.x) ? (real)1 : (real)-1;
             double num = 0.0, den = 0.0;
             const int base = cb - (IS3D ? R * plane : 0) - R * S::HX - R;
-#pragma unroll
+#pragma unroll 1
             for (int dz = (IS3D ? -R : 0); dz <= (IS3D ? R : 0); ++dz)
-#pragma unroll
-                for (int dy = -R; dy <= R; ++dy)
+#pragma unroll 1
+                for (int dy = -R; dy <= R; ++dy) {
+                    const int rowb = base + ((IS3D ? dz + R : 0) * S::HY + dy + R) * S::HX + R;
+                    const int r2yz = dy * dy + dz * dz;
 #pragma unroll
                     for (int dx = -R; dx <= R; ++dx) {
-                        const int e = base + ((IS3D ? dz + R : 0) * S::HY + dy + R) * S::HX + dx + R;
+                        const int e = rowb + dx;
                         const int2 pj = pair[e];
                         const double m = (pj.x == pr.x && pj.y == pr.y) ? 1.0 : 0.0;
-                        const double wt = w[dx * dx + dy * dy + dz * dz];
+                        const double wt = w[r2yz + dx * dx];
                         // reference: (w * orientation_j) * vn_j == w * (orientation_j * vn_j), exactly
                         num = __fma_rn(wt * (double)svn[e], m, num);
                         den = __fma_rn(wt, m, den);
                     }
+                }
             if (den > 0.0) out = orient_i * (real)(num / den);
         }
         vn_out[i] = out;
