@@ -184,16 +184,23 @@ int gpk_build_tables(gpk_grid* G) {
             for (int jx = 0; jx < W; ++jx) {
                 const real gx0 = hk->w0[jx], gx1 = hk->w1[jx], gx2 = hk->w2[jx];
                 real* t = &hk->geom_table[(((size_t)jz * W + jy) * W + jx) * 12];
+                // three quads: A = (Ix, Ixx, Ixy, Ixz), B = (Iy, Iyy, Ixy, Iyz),
+                // C = (Iz, Izz, Ixz, Iyz); a tap whose x (y, z) Gaussian factor is
+                // zero needs quad A (B, C) alone
                 volatile real p;  // keep each product a separate rounded operation
-                p = gx1 * gy0; t[0] = p * gz0;
-                p = gx0 * gy1; t[1] = p * gz0;
-                p = gx2 * gy0; t[2] = p * gz0;
-                p = gx0 * gy2; t[3] = p * gz0;
-                p = gx1 * gy1; t[4] = p * gz0;
-                p = gx0 * gy0; t[5] = p * gz1;
-                p = gx0 * gy0; t[6] = p * gz2;
-                p = gx1 * gy0; t[7] = p * gz1;
-                p = gx0 * gy1; t[8] = p * gz1;
+                real ix, iy, ixx, iyy, ixy, iz, izz, ixz, iyz;
+                p = gx1 * gy0; ix = p * gz0;
+                p = gx0 * gy1; iy = p * gz0;
+                p = gx2 * gy0; ixx = p * gz0;
+                p = gx0 * gy2; iyy = p * gz0;
+                p = gx1 * gy1; ixy = p * gz0;
+                p = gx0 * gy0; iz = p * gz1;
+                p = gx0 * gy0; izz = p * gz2;
+                p = gx1 * gy0; ixz = p * gz1;
+                p = gx0 * gy1; iyz = p * gz1;
+                t[0] = ix; t[1] = ixx; t[2] = ixy; t[3] = ixz;
+                t[4] = iy; t[5] = iyy; t[6] = ixy; t[7] = iyz;
+                t[8] = iz; t[9] = izz; t[10] = ixz; t[11] = iyz;
             }
         }
     }
@@ -645,7 +652,7 @@ extern "C" int gpk_grid_wave_stats(gpk_grid* G, uint64_t out[8]) {
 }
 
 extern "C" int gpk_grid_set_geometry_kernel(gpk_grid* G, int kind) {
-    if (!G || kind < 0 || kind > 1) return GPK_ERR_INVALID_ARGUMENT;
+    if (!G || kind < 0 || kind > 2) return GPK_ERR_INVALID_ARGUMENT;
     G->geometry_kernel = kind;
     return GPK_OK;
 }

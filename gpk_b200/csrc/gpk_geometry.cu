@@ -1,27 +1,36 @@
-// gpk_geometry.cu — tiled, branch-free Gaussian-Hessian geometry for sm_100a.
+// gpk_geometry.cu — tiled Gaussian-Hessian geometry on label bitmaps, sm_100a.
 //
 // Same result, bit for bit, as the direct masked tensor stencil of the
 // reference (src/gpk_geometry.cpp:88-152): for every interface cell the nine
 // sums Ix..Iyz run over the (2R+1)^d taps in z -> y -> x order, each tap
 // adding its precomputed product (formed on the host exactly as (a*b)*c)
-// when the tap's label equals the cell's label.
+// when the tap's label equals the cell's label.  Here that test is one bit
+// of a per-label bitmap, and the additions are predicated on it, so every
+// sum is the reference's sequence of correctly rounded additions.
 //
-// Exactness of the branch-free form: each sum starts at +0 and in round-to-
-// nearest a sum that starts at +0 can never become -0 (x + (-x) = +0, and
-// +0 + -0 = +0).  Adding a signed zero to such a sum is therefore an exact
-// no-op, so fma(w, m, acc) with m in {0, 1} rounds exactly like the
-// reference's `if (match) acc += w`: for m = 1 it is one correctly rounded
-// addition of w, for m = 0 it adds +-0.
+// Zero products: the Gaussian factor w0(o) is exactly 0 for |o| in
+// {R-1, R} (the Gaussian has radius R-2), so some products of those taps
+// are +-0.  Each sum starts at +0, and in round-to-nearest a sum that starts
+// at +0 never becomes -0 (x + (-x) = +0 and +0 + -0 = +0), so adding +-0 to
+// it is an exact no-op and such products are skipped.
 //
-// Layout: one CTA per TX x TY x TZ tile of cells.  The CTA stages the tile's
-// labels with an R-cell periodic halo in shared memory (row pitch padded by
-// one word so that rows start in different banks), compacts the tile's
-// interface cells, and gives each thread 1..4 of them.  The product table is
-// streamed one z-plane at a time (W*W taps x 12 reals) into a double buffer
-// by TMA bulk copies (cp.async.bulk + mbarrier), overlapping the next
-// plane's copy with the current plane's arithmetic.  All warps read the
-// same table entry at the same time (broadcast), and each thread's label
-// reads are one LDS per cell and tap.
+// Layout: one CTA per tile of TX x TY x TZ cells with TX = 32 - 2R, so a row
+// of the tile's halo (x from x0-R to x0+TX+R-1) is exactly 32 cells and, for
+// one label, one 32-bit word.  The CTA
+//   1. compacts the tile's interface cells and lists their distinct labels;
+//   2. for each batch of labels, builds one word per halo row and label
+//      (warp-per-row ballots over the labels read from global memory);
+//   3. streams the product table one z-plane (W*W taps x 12 reals) at a time
+//      into a double buffer with TMA bulk copies (cp.async.bulk + mbarrier),
+//      overlapping the next plane's copy with the current plane's arithmetic;
+//   4. gives each thread 2..4 of the batch's cells: per tap row it loads one
+//      bitmap word per cell, and per tap it tests a bit and adds the live
+//      products.  All warps read the same table entry at the same time
+//      (broadcast), so the shared-memory traffic per tap is 1-3 LDS.128 for
+//      all of a thread's cells.
+// Table entry of a tap (12 reals, three quads):
+//   A = (Ix, Ixx, Ixy, Ixz)   B = (Iy, Iyy, Ixy, Iyz)   C = (Iz, Izz, Ixz, Iyz)
+// so a tap with a zero x (y, z) Gaussian factor needs quad A (B, C) alone.
 #include <cuda_runtime.h>
 
 #include <cub/cub.cuh>
@@ -63,13 +72,67 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-template <typename real> __device__ __forceinline__ real fma_rn(real a, real b, real c);
-template <> __device__ __forceinline__ float fma_rn<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-template <> __device__ __forceinline__ double fma_rn<double>(double a, double b, double c) { return __fma_rn(a, b, c); }
+// ---- predicated additions: acc_k += w_k when bit != 0 -----------------------
+// One setp per tap and cell; the additions are plain IEEE round-to-nearest
+// adds (no flush to zero), exactly the reference's `if (match) acc += w`.
+// acc operands are %0..%n-1, the bit %n, the weights follow
+__device__ __forceinline__ void padd(uint32_t b, float& a0, float w0) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %1, 0;\n\t" "@p add.rn.f32 %0, %0, %2;\n\t" "}"
+        : "+f"(a0)
+        : "r"(b), "f"(w0));
+}
+__device__ __forceinline__ void padd(uint32_t b, float& a0, float& a1, float w0, float w1) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %2, 0;\n\t" "@p add.rn.f32 %0, %0, %3;\n\t""@p add.rn.f32 %1, %1, %4;\n\t" "}"
+        : "+f"(a0), "+f"(a1)
+        : "r"(b), "f"(w0), "f"(w1));
+}
+__device__ __forceinline__ void padd(uint32_t b, float& a0, float& a1, float& a2, float w0, float w1, float w2) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %3, 0;\n\t" "@p add.rn.f32 %0, %0, %4;\n\t""@p add.rn.f32 %1, %1, %5;\n\t""@p add.rn.f32 %2, %2, %6;\n\t" "}"
+        : "+f"(a0), "+f"(a1), "+f"(a2)
+        : "r"(b), "f"(w0), "f"(w1), "f"(w2));
+}
+__device__ __forceinline__ void padd(uint32_t b, float& a0, float& a1, float& a2, float& a3, float w0, float w1, float w2, float w3) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t" "@p add.rn.f32 %0, %0, %5;\n\t""@p add.rn.f32 %1, %1, %6;\n\t""@p add.rn.f32 %2, %2, %7;\n\t""@p add.rn.f32 %3, %3, %8;\n\t" "}"
+        : "+f"(a0), "+f"(a1), "+f"(a2), "+f"(a3)
+        : "r"(b), "f"(w0), "f"(w1), "f"(w2), "f"(w3));
+}
+__device__ __forceinline__ void padd(uint32_t b, double& a0, double w0) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %1, 0;\n\t" "@p add.rn.f64 %0, %0, %2;\n\t" "}"
+        : "+d"(a0)
+        : "r"(b), "d"(w0));
+}
+__device__ __forceinline__ void padd(uint32_t b, double& a0, double& a1, double w0, double w1) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %2, 0;\n\t" "@p add.rn.f64 %0, %0, %3;\n\t""@p add.rn.f64 %1, %1, %4;\n\t" "}"
+        : "+d"(a0), "+d"(a1)
+        : "r"(b), "d"(w0), "d"(w1));
+}
+__device__ __forceinline__ void padd(uint32_t b, double& a0, double& a1, double& a2, double w0, double w1, double w2) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %3, 0;\n\t" "@p add.rn.f64 %0, %0, %4;\n\t""@p add.rn.f64 %1, %1, %5;\n\t""@p add.rn.f64 %2, %2, %6;\n\t" "}"
+        : "+d"(a0), "+d"(a1), "+d"(a2)
+        : "r"(b), "d"(w0), "d"(w1), "d"(w2));
+}
+__device__ __forceinline__ void padd(uint32_t b, double& a0, double& a1, double& a2, double& a3, double w0, double w1, double w2, double w3) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t" "@p add.rn.f64 %0, %0, %5;\n\t""@p add.rn.f64 %1, %1, %6;\n\t""@p add.rn.f64 %2, %2, %7;\n\t""@p add.rn.f64 %3, %3, %8;\n\t" "}"
+        : "+d"(a0), "+d"(a1), "+d"(a2), "+d"(a3)
+        : "r"(b), "d"(w0), "d"(w1), "d"(w2), "d"(w3));
+}
 
-template <bool IS3D> struct GeoTile;
-template <> struct GeoTile<true> { static constexpr int TX = 16, TY = 8, TZ = 8; };
-template <> struct GeoTile<false> { static constexpr int TX = 32, TY = 32, TZ = 1; };
+template <typename real> struct Quad;
+template <> struct Quad<float> {
+    float x, y, z, w;
+    __device__ __forceinline__ static Quad load(const float* p) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        return {v.x, v.y, v.z, v.w};
+    }
+};
+template <> struct Quad<double> {
+    double x, y, z, w;
+    __device__ __forceinline__ static Quad load(const double* p) {
+        const double2 u = reinterpret_cast<const double2*>(p)[0];
+        const double2 v = reinterpret_cast<const double2*>(p)[1];
+        return {u.x, u.y, v.x, v.y};
+    }
+};
 
 template <typename real>
 struct GeoArgs {
@@ -78,6 +141,7 @@ struct GeoArgs {
     const uint8_t* mask;
     const real* table;  // W^dz planes of W*W taps x 12 reals
     int ntx, nty, ntz;
+    int nl_cap;         // labels per bitmap batch at most (tests force small batches)
     real inv_dx, inv_dx2, dx, kappa_limit;
     real *nx, *ny, *nz, *kappa;
     int32_t* phi_comp;
@@ -87,72 +151,116 @@ struct GeoArgs {
 template <int R, bool IS3D>
 struct GeoShape {
     static constexpr int W = 2 * R + 1;
-    static constexpr int TX = GeoTile<IS3D>::TX, TY = GeoTile<IS3D>::TY, TZ = GeoTile<IS3D>::TZ;
-    static constexpr int HX = TX + 2 * R, HXP = HX + 1, HY = TY + 2 * R, HZ = IS3D ? TZ + 2 * R : 1;
-    static constexpr int NLAB = HZ * HY * HXP;
+    static constexpr int TX = 32 - 2 * R;  // halo row = 32 cells = one bitmap word
+    static constexpr int TY = IS3D ? 8 : 1024 / TX;
+    static constexpr int TZ = IS3D ? 1024 / (TX * 8) : 1;
+    static constexpr int HY = TY + 2 * R, HZ = IS3D ? TZ + 2 * R : 1;
+    static constexpr int NROW = HZ * HY;
+    static constexpr int NROWP = NROW | 1;  // odd pitch: one row's words for several labels hit distinct banks
     static constexpr int NCELL = TX * TY * TZ;
+    static constexpr int CX = TX + 2, CY = TY + 2, CZ = IS3D ? TZ + 2 : 1;  // tile labels with a 1-cell halo
+    static constexpr int NCORE = CX * CY * CZ;
     static constexpr int PLANE = W * W * 12;  // reals per table plane
     static constexpr int NPLANES = IS3D ? W : 1;
+    static constexpr int BM_WORDS = 6912;
+    static constexpr int NLB = BM_WORDS / NROWP;  // labels per bitmap batch
+    static_assert(NCELL <= 1024 && NLB >= 1, "tile shape");
 };
 
 template <typename real, int R, bool IS3D>
 constexpr size_t geo_smem_bytes() {
     typedef GeoShape<R, IS3D> S;
-    // table planes (16-byte aligned) | labels | cell list | 2 mbarriers
-    return (size_t)2 * S::PLANE * sizeof(real) + (size_t)S::NLAB * 4 + (size_t)S::NCELL * 2 + 64;
+    // table planes | bitmaps | core labels | distinct labels | cells | cell label
+    // index | batch cells | 2 mbarriers
+    return (size_t)2 * S::PLANE * sizeof(real) + (size_t)S::BM_WORDS * 4 + (size_t)S::NCORE * 4 + (size_t)S::NCELL * 4 +
+           (size_t)S::NCELL * 2 * 3 + 64;
 }
 
-// One row of W taps (fixed dz, dy).  The Gaussian factor w0(o) is exactly 0
-// for |o| in {R-1, R} (the Gaussian has radius R-2), so a product with such
-// a factor is +-0 and adding it is an exact no-op (see the file comment):
-//   x factor zero (|dx| >= R-1): Iy, Iyy, Iz, Izz, Iyz have no contribution
-//   y factor zero (ZY0):         Ix, Ixx, Iz, Izz, Ixz
-//   z factor zero (ZZ0):         Ix, Iy, Ixx, Iyy, Ixy
+// One row of W taps (fixed dz, dy) for SLOTS cells; wd[s] holds bit j set
+// when tap x-offset j - R of cell s matches its label.
+//   x factor zero (|dx| >= R-1): only Ix, Ixx, Ixy, Ixz live   (quad A)
+//   y factor zero (ZY0):         only Iy, Iyy, Ixy, Iyz live   (quad B)
+//   z factor zero (ZZ0):         only Iz, Izz, Ixz, Iyz live   (quad C)
 // Components: 0 Ix, 1 Iy, 2 Ixx, 3 Iyy, 4 Ixy, 5 Iz, 6 Izz, 7 Ixz, 8 Iyz.
 template <typename real, int R, bool IS3D, int SLOTS, bool ZY0, bool ZZ0>
-__device__ __forceinline__ void geo_row(const int32_t* __restrict__ lab, const real* __restrict__ trow, int yoff,
-                                        real acc[SLOTS][9], const int base[SLOTS], const int32_t res[SLOTS]) {
+__device__ __forceinline__ void geo_row(const real* __restrict__ trow, const uint32_t wd[SLOTS], real acc[SLOTS][9]) {
     constexpr int W = 2 * R + 1;
 #pragma unroll
-    for (int dxs = 0; dxs < W; ++dxs) {
-        const bool zx0 = dxs <= 1 || dxs >= W - 2;  // compile-time after unrolling
-        bool live[9];
+    for (int j = 0; j < W; ++j) {
+        const bool zx0 = j <= 1 || j >= W - 2;  // compile-time after unrolling
+        const real* t = trow + j * 12;
+        const uint32_t bit = 1u << j;
+        if (!IS3D) {
+            if (!zx0 && !ZY0) {
+                const Quad<real> A = Quad<real>::load(t), B = Quad<real>::load(t + 4);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) live[k] = IS3D || k < 5;
-        if (zx0) live[1] = live[3] = live[5] = live[6] = live[8] = false;
-        if (ZY0) live[0] = live[2] = live[5] = live[6] = live[7] = false;
-        if (ZZ0) live[0] = live[1] = live[2] = live[3] = live[4] = false;
-        bool any = false;
+                for (int s = 0; s < SLOTS; ++s) {
+                    padd(wd[s] & bit, acc[s][0], acc[s][2], acc[s][4], A.x, A.y, A.z);
+                    padd(wd[s] & bit, acc[s][1], acc[s][3], B.x, B.y);
+                }
+            } else if (zx0 && !ZY0) {
+                const Quad<real> A = Quad<real>::load(t);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) any |= live[k];
-        if (!any) continue;
-        const real* t = trow + dxs * 12;
-        real w[9];
-        if (sizeof(real) == 4) {
-            const float4 t0 = *reinterpret_cast<const float4*>(t);
-            const float4 t1 = *reinterpret_cast<const float4*>(t + 4);
-            w[0] = t0.x; w[1] = t0.y; w[2] = t0.z; w[3] = t0.w;
-            w[4] = t1.x; w[5] = t1.y; w[6] = t1.z; w[7] = t1.w;
-            w[8] = live[8] ? t[8] : (real)0;
-        } else {
+                for (int s = 0; s < SLOTS; ++s) padd(wd[s] & bit, acc[s][0], acc[s][2], acc[s][4], A.x, A.y, A.z);
+            } else if (!zx0 && ZY0) {
+                const Quad<real> B = Quad<real>::load(t + 4);
 #pragma unroll
-            for (int k = 0; k < 9; ++k) w[k] = live[k] ? t[k] : (real)0;
+                for (int s = 0; s < SLOTS; ++s) padd(wd[s] & bit, acc[s][1], acc[s][3], acc[s][4], B.x, B.y, B.z);
+            } else {
+                const real wxy = t[2];
+#pragma unroll
+                for (int s = 0; s < SLOTS; ++s) padd(wd[s] & bit, acc[s][4], wxy);
+            }
+            continue;
         }
+        if (!zx0 && !ZY0 && !ZZ0) {
+            const Quad<real> A = Quad<real>::load(t), B = Quad<real>::load(t + 4), C = Quad<real>::load(t + 8);
 #pragma unroll
-        for (int s = 0; s < SLOTS; ++s) {
-            const real m = (lab[base[s] + yoff + dxs] == res[s]) ? (real)1 : (real)0;
+            for (int s = 0; s < SLOTS; ++s) {
+                padd(wd[s] & bit, acc[s][0], acc[s][2], acc[s][4], acc[s][7], A.x, A.y, A.z, A.w);
+                padd(wd[s] & bit, acc[s][1], acc[s][3], acc[s][8], B.x, B.y, B.w);
+                padd(wd[s] & bit, acc[s][5], acc[s][6], C.x, C.y);
+            }
+        } else if (zx0 && !ZY0 && !ZZ0) {
+            const Quad<real> A = Quad<real>::load(t);
 #pragma unroll
-            for (int k = 0; k < 9; ++k)
-                if (live[k]) acc[s][k] = fma_rn<real>(w[k], m, acc[s][k]);
+            for (int s = 0; s < SLOTS; ++s)
+                padd(wd[s] & bit, acc[s][0], acc[s][2], acc[s][4], acc[s][7], A.x, A.y, A.z, A.w);
+        } else if (!zx0 && ZY0 && !ZZ0) {
+            const Quad<real> B = Quad<real>::load(t + 4);
+#pragma unroll
+            for (int s = 0; s < SLOTS; ++s)
+                padd(wd[s] & bit, acc[s][1], acc[s][3], acc[s][4], acc[s][8], B.x, B.y, B.z, B.w);
+        } else if (!zx0 && !ZY0 && ZZ0) {
+            const Quad<real> C = Quad<real>::load(t + 8);
+#pragma unroll
+            for (int s = 0; s < SLOTS; ++s)
+                padd(wd[s] & bit, acc[s][5], acc[s][6], acc[s][7], acc[s][8], C.x, C.y, C.z, C.w);
+        } else if (zx0 && ZY0 && !ZZ0) {
+            const real wxy = t[2];
+#pragma unroll
+            for (int s = 0; s < SLOTS; ++s) padd(wd[s] & bit, acc[s][4], wxy);
+        } else if (zx0 && !ZY0 && ZZ0) {
+            const real wxz = t[3];
+#pragma unroll
+            for (int s = 0; s < SLOTS; ++s) padd(wd[s] & bit, acc[s][7], wxz);
+        } else if (!zx0 && ZY0 && ZZ0) {
+            const real wyz = t[7];
+#pragma unroll
+            for (int s = 0; s < SLOTS; ++s) padd(wd[s] & bit, acc[s][8], wyz);
         }
     }
 }
 
+// The tap planes of one label batch.  gp0 = planes streamed before this
+// batch (buffer of global plane g: g & 1, its phase parity: (g >> 1) & 1);
+// gp_total = planes of all batches (the last plane prefetches nothing).
 template <typename real, int R, bool IS3D, int SLOTS>
-__device__ __forceinline__ void geo_accumulate(const GeoArgs<real>& a, const int32_t* __restrict__ lab,
+__device__ __forceinline__ void geo_accumulate(const GeoArgs<real>& a, const uint32_t* __restrict__ bm,
                                                const real* __restrict__ tab0, const real* __restrict__ tab1,
-                                               uint64_t* bars, const int16_t* cells, int nact, int tid,
-                                               real acc[SLOTS][9], int base[SLOTS], int32_t res[SLOTS], bool& ok) {
+                                               uint64_t* bars, int gp0, int gp_total, int nact, int tid,
+                                               real acc[SLOTS][9], const int bmrow[SLOTS], const int lx[SLOTS],
+                                               const uint32_t vmask[SLOTS], bool& ok) {
     typedef GeoShape<R, IS3D> S;
     constexpr int W = S::W;
 #pragma unroll
@@ -160,35 +268,43 @@ __device__ __forceinline__ void geo_accumulate(const GeoArgs<real>& a, const int
 #pragma unroll
         for (int k = 0; k < 9; ++k) acc[s][k] = (real)0;
     for (int p = 0; p < S::NPLANES; ++p) {
-        const real* tab = (p & 1) ? tab1 : tab0;
-        if (!mbar_wait(&bars[p & 1], (uint32_t)((p >> 1) & 1))) {
+        const int g = gp0 + p;
+        const real* tab = (g & 1) ? tab1 : tab0;
+        if (!mbar_wait(&bars[g & 1], (uint32_t)((g >> 1) & 1))) {
             ok = false;
             atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_TIMEOUT);
         }
-        if (tid == 0 && p + 1 < S::NPLANES) {
-            // the other buffer was last read in plane p-1, which every thread
+        if (tid == 0 && g + 1 < gp_total) {
+            // the other buffer was last read in plane g-1, which every thread
             // finished before the barrier at the end of that plane
             fence_proxy_async();
-            real* dst = ((p + 1) & 1) ? (real*)tab1 : (real*)tab0;
-            mbar_expect_tx(&bars[(p + 1) & 1], S::PLANE * sizeof(real));
-            bulk_g2s(dst, a.table + (size_t)(p + 1) * S::PLANE, S::PLANE * sizeof(real), &bars[(p + 1) & 1]);
+            real* dst = ((g + 1) & 1) ? (real*)tab1 : (real*)tab0;
+            const int pn = (g + 1) % S::NPLANES;
+            mbar_expect_tx(&bars[(g + 1) & 1], S::PLANE * sizeof(real));
+            bulk_g2s(dst, a.table + (size_t)pn * S::PLANE, S::PLANE * sizeof(real), &bars[(g + 1) & 1]);
         }
         if (ok && tid < nact) {
-            const int zoff = p * S::HY * S::HXP;
             // rows whose y or z Gaussian factor is exactly zero run
             // specialised bodies without the corresponding products
             const bool zz0 = IS3D && (p <= 1 || p >= W - 2);
 #pragma unroll 1
             for (int dy = 0; dy < W; ++dy) {
+                uint32_t wd[SLOTS];
+                uint32_t any = 0;
+#pragma unroll
+                for (int s = 0; s < SLOTS; ++s) {
+                    wd[s] = (bm[bmrow[s] + p * S::HY + dy] >> lx[s]) & vmask[s];
+                    any |= wd[s];
+                }
+                if (!any) continue;
                 const real* trow = tab + dy * W * 12;
-                const int yoff = zoff + dy * S::HXP;
                 const bool yy0 = dy <= 1 || dy >= W - 2;
                 if (zz0) {
-                    if (yy0) geo_row<real, R, IS3D, SLOTS, true, true>(lab, trow, yoff, acc, base, res);
-                    else geo_row<real, R, IS3D, SLOTS, false, true>(lab, trow, yoff, acc, base, res);
+                    if (yy0) geo_row<real, R, IS3D, SLOTS, true, true>(trow, wd, acc);
+                    else geo_row<real, R, IS3D, SLOTS, false, true>(trow, wd, acc);
                 } else {
-                    if (yy0) geo_row<real, R, IS3D, SLOTS, true, false>(lab, trow, yoff, acc, base, res);
-                    else geo_row<real, R, IS3D, SLOTS, false, false>(lab, trow, yoff, acc, base, res);
+                    if (yy0) geo_row<real, R, IS3D, SLOTS, true, false>(trow, wd, acc);
+                    else geo_row<real, R, IS3D, SLOTS, false, false>(trow, wd, acc);
                 }
             }
         }
@@ -198,7 +314,7 @@ __device__ __forceinline__ void geo_accumulate(const GeoArgs<real>& a, const int
 
 template <typename real>
 __device__ __forceinline__ void geo_finish(const GeoArgs<real>& a, int i, const real* acc, const int32_t* __restrict__ lab,
-                                           int cbase, int HXP, int HY, bool is3d) {
+                                           int cbase, int pitch, int rows, bool is3d) {
     real Ix = acc[0] * a.inv_dx, Iy = acc[1] * a.inv_dx, Iz = acc[5] * a.inv_dx;
     real Ixx = acc[2] * a.inv_dx2, Iyy = acc[3] * a.inv_dx2, Izz = acc[6] * a.inv_dx2;
     real Ixy = acc[4] * a.inv_dx2, Ixz = acc[7] * a.inv_dx2, Iyz = acc[8] * a.inv_dx2;
@@ -219,8 +335,8 @@ __device__ __forceinline__ void geo_finish(const GeoArgs<real>& a, int i, const 
     }
     // competitor choice (src/gpk_geometry.cpp:154-182) from the staged labels
     const int32_t pi = lab[cbase];
-    const int plane = HY * HXP;
-    const int fo[6] = {-1, +1, -HXP, +HXP, -plane, +plane};
+    const int plane = rows * pitch;
+    const int fo[6] = {-1, +1, -pitch, +pitch, -plane, +plane};
     const real score[6] = {-nxv, nxv, -nyv, nyv, -nzv, nzv};
     const int nf = is3d ? 6 : 4;
     int best = -1, best_support = -1;
@@ -233,7 +349,7 @@ __device__ __forceinline__ void geo_finish(const GeoArgs<real>& a, int i, const 
             for (int dy = -1; dy <= 1; ++dy)
                 for (int dxs = -1; dxs <= 1; ++dxs) {
                     if (!dxs && !dy && !dz) continue;
-                    support += lab[cbase + dz * plane + dy * HXP + dxs] == q;
+                    support += lab[cbase + dz * plane + dy * pitch + dxs] == q;
                 }
         if (support > best_support || (support == best_support && score[k] > best_score)) {
             best = k; best_support = support; best_score = score[k];
@@ -242,30 +358,39 @@ __device__ __forceinline__ void geo_finish(const GeoArgs<real>& a, int i, const 
     a.phi_comp[i] = (best >= 0) ? lab[cbase + fo[best]] : pi;
 }
 
+// Fewest cells per thread; with one cell per thread the three table loads of
+// a tap would be shared by a single cell's additions.
+constexpr int GEO_MIN_SLOTS = 2;
+
+// three CTAs per SM in float (80 registers); two in double, whose 36
+// accumulators of a 4-cell thread take 72 registers
 template <typename real, int R, bool IS3D>
-__global__ void __launch_bounds__(256) k_geometry_tiled(GeoArgs<real> a) {
+__global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) k_geometry_tiled(GeoArgs<real> a) {
     typedef GeoShape<R, IS3D> S;
     extern __shared__ __align__(128) unsigned char smem[];
     real* tab0 = reinterpret_cast<real*>(smem);
     real* tab1 = tab0 + S::PLANE;
-    int32_t* lab = reinterpret_cast<int32_t*>(tab1 + S::PLANE);
-    int16_t* cells = reinterpret_cast<int16_t*>(lab + S::NLAB);
-    uint64_t* bars = reinterpret_cast<uint64_t*>((reinterpret_cast<uintptr_t>(cells + S::NCELL) + 15) & ~(uintptr_t)15);
-    __shared__ int s_count;
-    const int tid = threadIdx.x;
+    uint32_t* bm = reinterpret_cast<uint32_t*>(tab1 + S::PLANE);
+    int32_t* core = reinterpret_cast<int32_t*>(bm + S::BM_WORDS);
+    int32_t* dl = core + S::NCORE;                      // distinct labels of the tile's interface cells
+    int16_t* cells = reinterpret_cast<int16_t*>(dl + S::NCELL);
+    uint16_t* cli = reinterpret_cast<uint16_t*>(cells + S::NCELL);  // index into dl per cell
+    int16_t* bcell = reinterpret_cast<int16_t*>(cli + S::NCELL);    // cells of the current batch
+    uint64_t* bars = reinterpret_cast<uint64_t*>((reinterpret_cast<uintptr_t>(bcell + S::NCELL) + 15) & ~(uintptr_t)15);
+    int32_t* cand = reinterpret_cast<int32_t*>(bm);      // label candidates, before the first bitmap
+    __shared__ int s_count, s_ncand, s_nl;
+    typedef cub::BlockScan<int, 256> BS;
+    __shared__ typename BS::TempStorage scan;
+    constexpr int PER = (S::NCELL + 255) / 256;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const Dims D = a.D;
 
     const int t = blockIdx.x;
     const int tx = t % a.ntx, ty = (t / a.ntx) % a.nty, tz = t / (a.ntx * a.nty);
     const int x0 = tx * S::TX, y0 = ty * S::TY, z0 = tz * S::TZ;
 
-    // interface cells of the tile, in flat order
-    if (tid == 0) s_count = 0;
-    __syncthreads();
+    // 1. interface cells of the tile, in flat order
     {
-        typedef cub::BlockScan<int, 256> BS;
-        __shared__ typename BS::TempStorage scan;
-        constexpr int PER = (S::NCELL + 255) / 256;
         int flags[PER];
         int cnt = 0;
 #pragma unroll
@@ -285,7 +410,11 @@ __global__ void __launch_bounds__(256) k_geometry_tiled(GeoArgs<real> a) {
 #pragma unroll
         for (int k = 0; k < PER; ++k)
             if (flags[k]) cells[ex++] = (int16_t)(tid * PER + k);
-        if (tid == 0) s_count = total;
+        if (tid == 0) {
+            s_count = total;
+            s_ncand = 0;
+            s_nl = 0;
+        }
     }
     __syncthreads();
     const int ncell = s_count;
@@ -299,51 +428,131 @@ __global__ void __launch_bounds__(256) k_geometry_tiled(GeoArgs<real> a) {
         mbar_expect_tx(&bars[0], S::PLANE * sizeof(real));
         bulk_g2s(tab0, a.table, S::PLANE * sizeof(real), &bars[0]);
     }
-    // labels with a periodic halo of R cells
-    for (int e = tid; e < S::HZ * S::HY * S::HX; e += 256) {
-        const int hx = e % S::HX, hy = (e / S::HX) % S::HY, hz = e / (S::HX * S::HY);
-        const int x = wrap_any(x0 + hx - R, D.Nx), y = wrap_any(y0 + hy - R, D.Ny);
-        const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
-        lab[(hz * S::HY + hy) * S::HXP + hx] = a.phi[D.idx(z, y, x)];
+    // tile labels with a periodic halo of one cell (competitor choice)
+    for (int e = tid; e < S::NCORE; e += 256) {
+        const int cx = e % S::CX, cy = (e / S::CX) % S::CY, cz = e / (S::CX * S::CY);
+        const int x = wrap_any(x0 + cx - 1, D.Nx), y = wrap_any(y0 + cy - 1, D.Ny);
+        const int z = IS3D ? wrap_any(z0 + cz - 1, D.Nz) : 0;
+        core[e] = a.phi[D.idx(z, y, x)];
     }
     __syncthreads();
 
-    // The tile's cells go to the fewest threads that hold them at `slots`
-    // cells each: thread t < nact takes cells t, t + nact, ...  Warps whose
-    // threads all lie beyond nact skip the arithmetic, leaving their issue
-    // slots to the other resident CTA instead of computing dummy cells.
-    const int slots = (ncell + 255) / 256;
-    const int nact = (ncell + slots - 1) / slots;
+    // 2. distinct labels of the interface cells: one candidate per label and
+    //    warp (match_any leaders), then the first occurrence of each candidate
+    auto core_of = [&](int c) {
+        const int lx = c % S::TX, ly = (c / S::TX) % S::TY, lz = c / (S::TX * S::TY);
+        return ((IS3D ? lz + 1 : 0) * S::CY + ly + 1) * S::CX + lx + 1;
+    };
+    for (int k0 = 0; k0 < ncell; k0 += 256) {
+        const int k = k0 + tid;
+        const bool v = k < ncell;
+        const unsigned am = __ballot_sync(0xffffffffu, v);
+        if (v) {
+            const int32_t lab = core[core_of(cells[k])];
+            const unsigned grp = __match_any_sync(am, lab);
+            if (lane == __ffs(grp) - 1) cand[atomicAdd(&s_ncand, 1)] = lab;
+        }
+    }
+    __syncthreads();
+    const int ncand = s_ncand;
+    for (int e = tid; e < ncand; e += 256) {
+        const int32_t lab = cand[e];
+        bool first = true;
+        for (int j = 0; j < e && first; ++j) first = cand[j] != lab;
+        if (first) dl[atomicAdd(&s_nl, 1)] = lab;
+    }
+    __syncthreads();
+    const int nl = s_nl;
+    for (int k = tid; k < ncell; k += 256) {
+        const int32_t lab = core[core_of(cells[k])];
+        int li = 0;
+        while (li < nl - 1 && dl[li] != lab) ++li;  // every cell label is listed
+        cli[k] = (uint16_t)li;
+    }
+    const int nlb = a.nl_cap < S::NLB ? a.nl_cap : S::NLB;
+    const int nbatch = (nl + nlb - 1) / nlb;
+    const int gp_total = nbatch * S::NPLANES;
     bool ok = true;
-    int base[4], myc[4];
-    int32_t res[4];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        const int k = tid + nact * s;
-        myc[s] = (tid < nact && k < ncell) ? cells[k] : -1;
-        const int c = myc[s] < 0 ? cells[0] : myc[s];
-        const int lx = c % S::TX, ly = (c / S::TX) % S::TY, lz = c / (S::TX * S::TY);
-        // label of tap (dz,dy,dx) at lab[base + (dz+R)*plane + (dy+R)*HXP + (dx+R)]
-        base[s] = (lz * S::HY + ly) * S::HXP + lx;
-        res[s] = lab[base[s] + ((IS3D ? R : 0) * S::HY + R) * S::HXP + R];
-    }
 
-    real acc[4][9];
-    switch (slots) {
-    case 1: geo_accumulate<real, R, IS3D, 1>(a, lab, tab0, tab1, bars, cells, nact, tid, (real(*)[9])acc, base, res, ok); break;
-    case 2: geo_accumulate<real, R, IS3D, 2>(a, lab, tab0, tab1, bars, cells, nact, tid, (real(*)[9])acc, base, res, ok); break;
-    case 3: geo_accumulate<real, R, IS3D, 3>(a, lab, tab0, tab1, bars, cells, nact, tid, (real(*)[9])acc, base, res, ok); break;
-    default: geo_accumulate<real, R, IS3D, 4>(a, lab, tab0, tab1, bars, cells, nact, tid, (real(*)[9])acc, base, res, ok); break;
-    }
-    if (!ok) return;
+    for (int b = 0; b < nbatch; ++b) {
+        const int lb0 = b * nlb;
+        const int nb = nl - lb0 < nlb ? nl - lb0 : nlb;
+        __syncthreads();  // bitmaps, candidates and batch cells of the previous pass are free
+
+        // 3. one word per halo row and label of the batch
+        for (int r = warp; r < S::NROW; r += 8) {
+            const int hz = r / S::HY, hy = r % S::HY;
+            const int x = wrap_any(x0 - R + lane, D.Nx), y = wrap_any(y0 + hy - R, D.Ny);
+            const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
+            const int32_t g = a.phi[D.idx(z, y, x)];
+            for (int L0 = 0; L0 < nb; L0 += 32) {
+                const int cnt = nb - L0 < 32 ? nb - L0 : 32;
+                uint32_t mine = 0;
+                for (int L = 0; L < cnt; ++L) {
+                    const uint32_t bits = __ballot_sync(0xffffffffu, g == dl[lb0 + L0 + L]);
+                    if (lane == L) mine = bits;
+                }
+                if (lane < cnt) bm[(L0 + lane) * S::NROWP + r] = mine;
+            }
+        }
+        // cells of the batch
+        int nbc = ncell;
+        if (nbatch > 1) {
+            int flags[PER];
+            int cnt = 0;
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        if (s >= slots || myc[s] < 0) continue;
-        const int c = myc[s];
-        const int lx = c % S::TX, ly = (c / S::TX) % S::TY, lz = c / (S::TX * S::TY);
-        const int i = D.idx(z0 + lz, y0 + ly, x0 + lx);
-        const int cbase = base[s] + ((IS3D ? R : 0) * S::HY + R) * S::HXP + R;
-        geo_finish<real>(a, i, acc[s], lab, cbase, S::HXP, S::HY, IS3D);
+            for (int k = 0; k < PER; ++k) {
+                const int e = tid * PER + k;
+                flags[k] = e < ncell && (int)cli[e] >= lb0 && (int)cli[e] < lb0 + nb;
+                cnt += flags[k];
+            }
+            int ex, total;
+            BS(scan).ExclusiveSum(cnt, ex, total);
+#pragma unroll
+            for (int k = 0; k < PER; ++k)
+                if (flags[k]) bcell[ex++] = (int16_t)(tid * PER + k);
+            nbc = total;
+        }
+        __syncthreads();
+
+        // 4. each thread takes `slots` of the batch's cells: thread t < nact
+        //    takes cells t, t + nact, ...; warps beyond nact leave their issue
+        //    slots to the other resident CTAs
+        int slots = (nbc + 255) / 256;
+        if (slots < GEO_MIN_SLOTS) slots = GEO_MIN_SLOTS;
+        const int nact = (nbc + slots - 1) / slots;
+        int bmrow[4], lx[4], kc[4];
+        uint32_t vmask[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const int kk = tid + nact * s;
+            const bool valid = s < slots && tid < nact && kk < nbc;
+            const int k = valid ? (nbatch > 1 ? bcell[kk] : kk) : (nbatch > 1 ? bcell[0] : 0);
+            const int c = cells[k];
+            const int cx = c % S::TX, cy = (c / S::TX) % S::TY, cz = c / (S::TX * S::TY);
+            // bitmap word of halo row (cz + dz + R, cy + dy + R): bmrow + (dz+R)*HY + (dy+R)
+            bmrow[s] = ((int)cli[k] - lb0) * S::NROWP + (IS3D ? cz : 0) * S::HY + cy;
+            lx[s] = cx;
+            kc[s] = valid ? c : -1;
+            vmask[s] = valid ? 0xffffffffu : 0u;
+        }
+        real acc[4][9];
+        const int gp0 = b * S::NPLANES;
+        switch (slots) {
+        case 2: geo_accumulate<real, R, IS3D, 2>(a, bm, tab0, tab1, bars, gp0, gp_total, nact, tid, acc, bmrow, lx, vmask, ok); break;
+        case 3: geo_accumulate<real, R, IS3D, 3>(a, bm, tab0, tab1, bars, gp0, gp_total, nact, tid, acc, bmrow, lx, vmask, ok); break;
+        default: geo_accumulate<real, R, IS3D, 4>(a, bm, tab0, tab1, bars, gp0, gp_total, nact, tid, acc, bmrow, lx, vmask, ok); break;
+        }
+        if (ok) {
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                if (kc[s] < 0) continue;
+                const int c = kc[s];
+                const int cx = c % S::TX, cy = (c / S::TX) % S::TY, cz = c / (S::TX * S::TY);
+                const int i = D.idx(z0 + cz, y0 + cy, x0 + cx);
+                geo_finish<real>(a, i, acc[s], core, core_of(c), S::CX, S::CY, IS3D);
+            }
+        }
     }
 }
 
@@ -372,9 +581,8 @@ static int launch_tiled(gpk_grid* G, const GeoArgs<real>& a0) {
 
 using namespace gpk_dev;
 
-// Tiled geometry for the common kernel radii; returns -1 when the radius or
-// the shared-memory footprint has no tiled instantiation (the caller then uses
-// the per-cell kernel).
+// Tiled geometry for kernel radii 4..10 (Gaussian radius 2..8); returns -1
+// for other radii (the caller then uses the per-cell kernel).
 template <typename real>
 int gpk_geometry_tiled(gpk_grid* G, int R, real inv_dx, real inv_dx2, real dx, real kappa_limit) {
     GeoArgs<real> a;
@@ -382,22 +590,27 @@ int gpk_geometry_tiled(gpk_grid* G, int R, real inv_dx, real inv_dx2, real dx, r
     a.phi = G->phi;
     a.mask = G->mask;
     a.table = (const real*)G->d_geom_table;
+    a.nl_cap = G->geometry_kernel == 2 ? 1 : (1 << 30);
     a.inv_dx = inv_dx; a.inv_dx2 = inv_dx2; a.dx = dx; a.kappa_limit = kappa_limit;
     a.nx = (real*)G->f[GPK_FIELD_NX]; a.ny = (real*)G->f[GPK_FIELD_NY]; a.nz = (real*)G->f[GPK_FIELD_NZ];
     a.kappa = (real*)G->f[GPK_FIELD_KAPPA];
     a.phi_comp = G->phi_comp;
     a.s = G->scal;
-    const bool is3d = G->d.is3d();
-    if (is3d) {
+    if (G->d.is3d()) {
         switch (R) {
+        case 4: return launch_tiled<real, 4, true>(G, a);
+        case 5: return launch_tiled<real, 5, true>(G, a);
         case 6: return launch_tiled<real, 6, true>(G, a);
         case 7: return launch_tiled<real, 7, true>(G, a);
         case 8: return launch_tiled<real, 8, true>(G, a);
-        case 9: return sizeof(real) == 4 ? launch_tiled<real, 9, true>(G, a) : -1;
+        case 9: return launch_tiled<real, 9, true>(G, a);
+        case 10: return launch_tiled<real, 10, true>(G, a);
         default: return -1;
         }
     }
     switch (R) {
+    case 4: return launch_tiled<real, 4, false>(G, a);
+    case 5: return launch_tiled<real, 5, false>(G, a);
     case 6: return launch_tiled<real, 6, false>(G, a);
     case 7: return launch_tiled<real, 7, false>(G, a);
     case 8: return launch_tiled<real, 8, false>(G, a);

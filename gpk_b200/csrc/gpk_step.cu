@@ -228,8 +228,9 @@ __global__ void __launch_bounds__(128) k_geometry_direct(Dims D, const int32_t* 
                     if (x < 0 || x >= D.Nx) x = wrap_any(x, D.Nx);
                     if (row[x] != resident) continue;
                     const real* t = trow + (dx + R) * 12;
-                    Ix += t[0]; Iy += t[1]; Ixx += t[2]; Iyy += t[3]; Ixy += t[4];
-                    if (IS3D) { Iz += t[5]; Izz += t[6]; Ixz += t[7]; Iyz += t[8]; }
+                    // table entry: (Ix, Ixx, Ixy, Ixz), (Iy, Iyy, Ixy, Iyz), (Iz, Izz, Ixz, Iyz)
+                    Ix += t[0]; Iy += t[4]; Ixx += t[1]; Iyy += t[5]; Ixy += t[2];
+                    if (IS3D) { Iz += t[8]; Izz += t[9]; Ixz += t[3]; Iyz += t[7]; }
                 }
             }
         }
@@ -947,7 +948,7 @@ static int geometry(gpk_grid* G) {
     if (!hk->global_separable) {
         const real inv_dx = (real)1 / dx;
         const real inv_dx2 = inv_dx * inv_dx;
-        if (G->geometry_kernel == 0) {
+        if (G->geometry_kernel != 1) {
             const int rc = gpk_geometry_tiled<real>(G, hk->geom_radius, inv_dx, inv_dx2, dx, kappa_limit);
             if (rc != -1) return rc;
         }
@@ -1151,7 +1152,7 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
     // projection into vn2 (zero at bulk cells), then swap
     GPK_TRY(gpk_stage_begin(G, GPK_STAGE_PROJECTION));
     GPK_CUDA_TRY(cudaMemsetAsync(G->vn2, 0, G->rsz * D.N, G->stream));
-    const int prc = G->geometry_kernel == 0 ? gpk_projection_tiled<real>(G, hk->proj_radius) : -1;
+    const int prc = G->geometry_kernel != 1 ? gpk_projection_tiled<real>(G, hk->proj_radius) : -1;
     if (prc == -1)
         k_projection<real><<<ga, 256, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, G->phi_comp, G->mask,
                                                       (const real*)G->f[GPK_FIELD_VN], (real*)G->vn2, G->d_proj_w,

@@ -1158,7 +1158,7 @@ int gpk_remap_pass(gpk_grid* G) {
     const int grid = 4 * G->num_sms;
     // phi_comp <- phi everywhere, then the best candidate at interface cells
     GPK_CUDA_TRY(cudaMemcpyAsync(G->phi_comp, G->phi, sizeof(int32_t) * D.N, cudaMemcpyDeviceToDevice, G->stream));
-    const int rc = G->geometry_kernel == 0
+    const int rc = G->geometry_kernel != 1
                        ? gpk_bgr_scores_tiled<real>(G, hk->remap_radius, (real*)G->bgr_res, (real*)G->bgr_best)
                        : -1;
     if (rc == -1)

@@ -210,7 +210,7 @@ class GPKGrid:
                 "exact_counts": int(out[6]), "count_scanned": int(out[7])}
 
     def set_geometry_kernel(self, kind: str) -> None:
-        check(lib().gpk_grid_set_geometry_kernel(self._h, {"tiled": 0, "per_cell": 1}[kind]))
+        check(lib().gpk_grid_set_geometry_kernel(self._h, {"tiled": 0, "per_cell": 1, "tiled_batched": 2}[kind]))
 
     def stream_ptr(self) -> int:
         p = C.c_void_p()

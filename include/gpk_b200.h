@@ -235,9 +235,10 @@ int gpk_grid_stage_times(gpk_grid* grid, double ms[GPK_NUM_STAGES], uint64_t cal
  * visited, exact label counts, candidates those counts scanned}, summed
  * since the last read.                                                     */
 int gpk_grid_wave_stats(gpk_grid* grid, uint64_t out[8]);
-/* Geometry kernel selection (both give identical results): 0 = tiled
- * shared-memory kernel where an instantiation exists (default), 1 = the
- * per-interface-cell kernel.                                               */
+/* Kernel selection (all give identical results): 0 = tiled shared-memory
+ * kernels where an instantiation exists (default), 1 = the per-interface-
+ * cell kernels, 2 = tiled kernels with one label per geometry bitmap batch
+ * (exercises the many-label path of the tiled geometry kernel).           */
 int gpk_grid_set_geometry_kernel(gpk_grid* grid, int kind);
 
 #ifdef __cplusplus

@@ -58,16 +58,36 @@ def test_polycrystal_3d_bitexact(oracle_mod):
     _lockstep(gpu, ora, 10)
 
 
-@pytest.mark.parametrize("sigma", [1.0, 1.5, 2.0])
+# sigma 0.5 / 1.0 / 1.5 / 2.0 / 2.2 give geometry radii 4 / 6 / 8 / 9 / 10
+@pytest.mark.parametrize("sigma", [0.5, 1.0, 1.5, 2.0, 2.2])
 def test_geometry_kernels_agree_3d(oracle_mod, sigma):
-    """Tiled and per-cell geometry kernels give the oracle's fields bit for bit."""
+    """Tiled (one and many bitmap batches) and per-cell kernels give the
+    oracle's fields bit for bit."""
     phi, g = polycrystal(24, 30, 36, 20, 12)
     ora = oracle_mod.OracleGrid(24, 30, 36, 1.0, thermo.isotropic(1.0, 1.0), 0.0, sigma)
     _load((ora,), phi=phi, g=g, alpha=1.0)
     for _ in range(10):
         ora.step()
-    for kind in ("tiled", "per_cell"):
+    for kind in ("tiled", "per_cell", "tiled_batched"):
         gpu = GPKGrid(24, 30, 36, 1.0, thermo.isotropic(1.0, 1.0), 0.0, sigma)
+        gpu.set_geometry_kernel(kind)
+        _load((gpu,), phi=phi, g=g, alpha=1.0)
+        for _ in range(10):
+            gpu.step()
+        assert not compare_all(gpu, ora), kind
+
+
+@pytest.mark.parametrize("sigma", [0.5, 1.5, 2.2])
+def test_geometry_kernels_agree_2d(oracle_mod, sigma):
+    """2-D tiles (TX = 32 - 2R, 1024 / TX rows) on a grid that no tile
+    width divides, against the oracle."""
+    phi, g = polycrystal(1, 70, 90, 40, 5)
+    ora = oracle_mod.OracleGrid(1, 70, 90, 1.0, thermo.isotropic(1.0, 1.0), 0.0, sigma)
+    _load((ora,), phi=phi, g=g, alpha=1.0)
+    for _ in range(10):
+        ora.step()
+    for kind in ("tiled", "tiled_batched"):
+        gpu = GPKGrid(1, 70, 90, 1.0, thermo.isotropic(1.0, 1.0), 0.0, sigma)
         gpu.set_geometry_kernel(kind)
         _load((gpu,), phi=phi, g=g, alpha=1.0)
         for _ in range(10):
