@@ -254,12 +254,14 @@ def run_gpu_arm(args):
                 traffic = float(line.split(":")[1])
     clocks = clk.summary()
     tap_adds = n_active * W ** 3 * 9 / (geo_ms / 1e3)
-    roofline = {"kernel": "k_geometry_direct (Gaussian-Hessian tensor stencil + competitor)",
+    roofline = {"kernel": "k_geometry_tiled (label-bitmap Gaussian-Hessian tensor stencil + competitor)",
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": geo_bytes, "ms_per_launch": geo_ms,
                 "note": "the reference-exact tensor stencil adds 9 products per matching tap over (2R+1)^3 "
-                        "taps per interface cell in a fixed order; it is FP32-add bound, see compute",
+                        "taps per interface cell in a fixed order; it is bound by FP32 add issue, not HBM "
+                        "(compute: the reference's W^3 x 9 tap-adds per interface cell per second)",
+                "traffic_note": "scaled from a 160^3 ncu capture by cell count (profiles/geometry_256_traffic.txt)",
                 "compute": {"tap_adds_per_s": tap_adds,
                             "peak_fp32_adds_per_s": _fp32_add_peak(clocks["sm_mhz"] or 1965.0),
                             "frac": tap_adds / _fp32_add_peak(clocks["sm_mhz"] or 1965.0)}}
