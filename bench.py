@@ -190,6 +190,104 @@ def run_reference_arm(args):
     return 0
 
 
+def spectral_measurement(with_cpu: bool):
+    """FP64 spectral micro-elasticity solve on the 128^3 solidification grid
+    (cubic 108/62/28 GPa, 0.5% dilatational misfit, nucleus radius 4), inputs
+    resident on the device, 10 timed solves after 3 warm-up solves."""
+    import torch
+    from gpk_b200.spectral import SpectralElasticity, variant_eigenstrains
+    n = 128
+    g = torch.arange(n, device="cuda", dtype=torch.int32) - n // 2
+    r2 = g[:, None, None] ** 2 + g[None, :, None] ** 2 + g[None, None, :] ** 2
+    vf = torch.zeros((3, n, n, n), dtype=torch.float64, device="cuda")
+    vf[0][r2 <= 16] = 1.0
+    s = SpectralElasticity((n, n, n), 1.0, 108e9, 62e9, 28e9, variant_eigenstrains(0.005, 0.005))
+    for _ in range(3):
+        out = s.solve(vf, want_residual=False)
+    residual = s.solve(vf)[3]
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(10):
+        out = s.solve(vf, want_residual=False)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / 10
+    cells = n ** 3
+    # algorithmic bytes per cell: eigenstrain 24 + 48, Green's kernel 48 + 96,
+    # epilogue 96 + 24 + 40, and 9 complex FP64 transforms of one read and one
+    # write of 16 bytes each (288)
+    per_cell = 72 + 144 + 160 + 288
+    peak, peak_kind = _peaks()
+    achieved = per_cell * cells / (ms / 1e3) / 1e9
+    res = {"workload": "spectral elasticity 128^3 FP64 (3 fwd + 6 inv Z2Z cuFFT, Green's-function and "
+                       "epilogue kernels)", "ms_per_solve": ms, "cells_per_s": cells / (ms / 1e3),
+           "residual": residual, "algorithmic_bytes_per_cell": per_cell,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_kind": peak_kind},
+           "own_kernels_per_solve": 4, "library_calls_per_solve": "2 cufftExecZ2Z (batched 3 and 6)"}
+    if with_cpu:
+        import types
+        from oracle import spectral_oracle
+        host = vf.cpu().numpy()
+        p = types.SimpleNamespace(dx=1.0, c11=108e9, c12=62e9, c44=28e9, eigen_small=0.005, eigen_large=0.005)
+        t0 = time.perf_counter()
+        spectral_oracle.spectral_elasticity(host, p)
+        cpu_s = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": cells / cpu_s, "unit": "cells/s", "cores": 1, "kind": "port",
+                               "sample": "one 128^3 solve of the numpy restatement (numpy.fft, one thread)"}
+    s.close()
+    return res
+
+
+def batched_measurement(n_inst: int = 512, steps: int = 10, warmup: int = 3):
+    """The lamellar-precipitate sweep: n_inst 2-D instances of sides
+    U{64..512} (FP64, OstwaldThermo), advanced together by the batch engine
+    and, for comparison, as a plain loop over instances (one worker)."""
+    import torch
+    from gpk_b200 import GPKBatch
+    from gpk_b200.sweep import lamellar_grid
+    grids = [lamellar_grid(5000 + i, precision="f64")[0] for i in range(n_inst)]
+    cells = sum(g.Nx * g.Ny * g.Nz for g in grids)
+    streams = [torch.cuda.ExternalStream(g.stream_ptr()) for g in grids]
+    batch = GPKBatch(grids)
+    workers, tune_steps = batch.autotune(trial_steps=1)
+    batch.step(warmup)
+
+    def timed(nsteps):
+        ts = torch.cuda.Stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(ts)
+        for st in streams:
+            st.wait_event(e0)
+        l0 = sum(g.launch_count() for g in grids)
+        batch.step(nsteps)
+        for st in streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            ts.wait_event(ev)
+        e1.record(ts)
+        e1.synchronize()
+        return e0.elapsed_time(e1), sum(g.launch_count() for g in grids) - l0
+
+    ms_b, launches = timed(steps)
+    batch.workers = 1
+    ms_p, _ = timed(steps)
+    batch.close()
+    for g in grids:
+        g.close()
+    return {"workload": f"{n_inst} lamellar-precipitate 2-D instances, sides U{{64..512}}, stripe thickness "
+                        "U{4..16}, spacing/thickness U[2,12], OstwaldThermo, FP64, sigma 1.5",
+            "instances": n_inst, "cells": cells, "steps": steps, "warmup": warmup + tune_steps,
+            "value": cells * steps / (ms_b / 1e3), "unit": "cell-updates/s", "ms": ms_b,
+            "plain_value": cells * steps / (ms_p / 1e3), "plain_ms": ms_p, "speedup_vs_plain": ms_p / ms_b,
+            "workers": workers, "gpu_launches": launches,
+            "how": "native worker pool, one CUDA stream per instance, worker count autotuned; plain = "
+                   "the same instances stepped one after another"}
+
+
 def run_gpu_arm(args):
     ws, rank, local = _dist()
     import torch
@@ -304,6 +402,16 @@ def run_gpu_arm(args):
             cpu.pop("seconds", None)
         except Exception as exc:  # the GPU number stands on its own
             cpu = {"error": str(exc)}
+    spectral = batched = None
+    if rank == 0:
+        try:
+            spectral = spectral_measurement(not args.no_cpu and ws == 1)
+        except Exception as exc:  # reported, never silent
+            spectral = {"error": str(exc)}
+        try:
+            batched = batched_measurement()
+        except Exception as exc:
+            batched = {"error": str(exc)}
     if rank == 0:
         line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -313,7 +421,7 @@ def run_gpu_arm(args):
                 "stages_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in stages.items()},
                 "interface_fraction": iface, "counters_last_step": list(grid.counters()),
                 "per_step_topology": waves,
-                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
+                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "spectral": spectral, "batched": batched,
                 "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": io,
                         "d2h_bytes_per_step": io, "steps": e2e_steps,
                         "path": "GPKGrid drop-in semantics: upload phi/alpha/g, step, download phi/alpha/g"}}
@@ -334,8 +442,19 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--size", type=int, default=SIZE, help="cube side (profiling of smaller cases)")
     ap.add_argument("--grains", type=int, default=GRAINS)
+    ap.add_argument("--batched-only", action="store_true",
+                    help="time only the lamellar sweep, batched and plain")
+    ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--spectral-only", action="store_true",
+                    help="time only the 128^3 spectral elasticity solve (profiling its kernels)")
     args = ap.parse_args()
     globals()["SIZE"], globals()["GRAINS"] = args.size, args.grains
+    if args.spectral_only:
+        print(json.dumps({"spectral": spectral_measurement(not args.no_cpu)}))
+        return 0
+    if args.batched_only:
+        print(json.dumps({"batched": batched_measurement(args.instances)}))
+        return 0
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_gpu_arm(args)

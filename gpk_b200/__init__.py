@@ -8,5 +8,8 @@ fields, and one descriptor factory per ``ThermoModel`` subclass in
 from . import thermo
 from .grid import GPKGrid, voronoi
 from ._lib import GPKError, lib
+from .spectral import SpectralElasticity, spectral_elasticity
+from .batch import GPKBatch
 
-__all__ = ["GPKGrid", "voronoi", "thermo", "GPKError", "lib"]
+__all__ = ["GPKGrid", "voronoi", "thermo", "GPKError", "lib", "SpectralElasticity", "spectral_elasticity",
+           "GPKBatch"]

@@ -76,6 +76,20 @@ def lib() -> C.CDLL:
         "gpk_grid_profile": ([vp, i32], i32),
         "gpk_grid_stage_times": ([vp, C.POINTER(dbl), C.POINTER(u64)], i32),
         "gpk_voronoi_init": ([i32, i32, i32, i32, u64, vp, vp, C.POINTER(i32)], i32),
+        "gpk_spectral_create": ([i32, C.POINTER(i32), dbl, dbl, dbl, dbl, C.POINTER(dbl), C.POINTER(vp)], i32),
+        "gpk_spectral_destroy": ([vp], i32),
+        "gpk_spectral_set_constants": ([vp, dbl, dbl, dbl, dbl, C.POINTER(dbl)], i32),
+        "gpk_spectral_set_stream": ([vp, vp], i32),
+        "gpk_spectral_solve": ([vp, vp, vp, vp, vp, C.POINTER(dbl)], i32),
+        "gpk_spectral_solve_host": ([vp, vp, vp, vp, vp, C.POINTER(dbl)], i32),
+        "gpk_spectral_info": ([vp, C.POINTER(i64), C.POINTER(i64)], i32),
+        "gpk_batch_create": ([i32, C.POINTER(vp), i32, C.POINTER(vp)], i32),
+        "gpk_batch_destroy": ([vp], i32),
+        "gpk_batch_set_workers": ([vp, i32], i32),
+        "gpk_batch_workers": ([vp, C.POINTER(i32)], i32),
+        "gpk_batch_step": ([vp, i32, dbl, dbl], i32),
+        "gpk_batch_run": ([vp, dbl, dbl, i32, C.POINTER(i32)], i32),
+        "gpk_batch_autotune": ([vp, i32, C.POINTER(i32), C.POINTER(i32)], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)
@@ -92,11 +106,11 @@ def check(code: int) -> None:
 
 
 def exported_symbols() -> list:
-    """Names of every entry point declared in include/gpk_b200.h and gpk_init.h."""
+    """Names of every entry point declared in the headers under include/."""
     import re
     names = []
     inc = os.path.join(HERE, "..", "include")
-    for h in ("gpk_b200.h", "gpk_init.h"):
+    for h in ("gpk_b200.h", "gpk_init.h", "gpk_spectral.h", "gpk_batch.h"):
         text = open(os.path.join(inc, h)).read()
         names += re.findall(r"^\s*(?:const\s+)?\w[\w\s\*]*?\b(gpk_\w+)\s*\(", text, flags=re.M)
     return sorted(set(names))

@@ -21,7 +21,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
               "-ftz=false", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-ffp-contract=off,-fopenmp,-O2"]
-SOURCES = ["gpk_capi.cu", "gpk_step.cu", "gpk_geometry.cu", "gpk_local.cu", "gpk_topology.cu", "gpk_init.cpp", "gpk_core_shim.cpp"]
+SOURCES = ["gpk_capi.cu", "gpk_step.cu", "gpk_geometry.cu", "gpk_local.cu", "gpk_topology.cu", "gpk_spectral.cu",
+           "gpk_batch.cu", "gpk_init.cpp", "gpk_core_shim.cpp"]
 
 
 def _nvcc() -> str:
@@ -65,7 +66,7 @@ def build(force: bool = False, verbose: bool = False, extra: list | None = None)
         return LIB
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         objs = list(ex.map(lambda s: _compile(s, extra), SOURCES))
-    cmd = [_nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lgomp", "-lcudart"]
+    cmd = [_nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lgomp", "-lcufft", "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

@@ -2,6 +2,8 @@
 // tap tables, state transfer and diagnostics.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -26,7 +28,7 @@ template <typename real> static inline real L(float f, double d);
 template <> inline float L<float>(float f, double) { return f; }
 template <> inline double L<double>(float, double d) { return d; }
 
-static bool g_device_ok = false;
+static std::atomic<bool> g_device_ok{false};
 
 extern "C" int gpk_device_init(int device) {
     int n = 0;

@@ -564,12 +564,10 @@ static int launch_tiled(gpk_grid* G, const GeoArgs<real>& a0) {
     a.nty = (G->d.Ny + S::TY - 1) / S::TY;
     a.ntz = (G->d.Nz + S::TZ - 1) / S::TZ;
     const size_t smem = geo_smem_bytes<real, R, IS3D>();
-    static bool attr_set = false;
-    if (!attr_set) {
-        GPK_CUDA_TRY(cudaFuncSetAttribute(k_geometry_tiled<real, R, IS3D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
-        attr_set = true;
-    }
+    // set once per process (thread-safe initialisation of a function-local static)
+    static const cudaError_t attr_rc = cudaFuncSetAttribute(
+        k_geometry_tiled<real, R, IS3D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    GPK_CUDA_TRY(attr_rc);
     const int ntiles = a.ntx * a.nty * a.ntz;
     k_geometry_tiled<real, R, IS3D><<<ntiles, 256, smem, G->stream>>>(a);
     G->launches++;

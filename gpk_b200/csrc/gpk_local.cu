@@ -251,12 +251,10 @@ static int launch_projection(gpk_grid* G) {
     const Dims D = G->d;
     const int ntx = (D.Nx + S::TX - 1) / S::TX, nty = (D.Ny + S::TY - 1) / S::TY, ntz = (D.Nz + S::TZ - 1) / S::TZ;
     const size_t smem = (size_t)S::NH * (sizeof(int2) + sizeof(real));
-    static bool attr_set = false;
-    if (!attr_set) {
-        GPK_CUDA_TRY(cudaFuncSetAttribute(k_projection_tiled<real, R, IS3D>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
+    // set once per process (thread-safe initialisation of a function-local static)
+    static const cudaError_t attr_rc = cudaFuncSetAttribute(
+        k_projection_tiled<real, R, IS3D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    GPK_CUDA_TRY(attr_rc);
     k_projection_tiled<real, R, IS3D><<<ntx * nty * ntz, 256, smem, G->stream>>>(
         D, G->phi, G->phi_comp, G->mask, (const real*)G->f[GPK_FIELD_VN], (real*)G->vn2, ntx, nty, G->d_proj_w);
     G->launches++;
