@@ -288,6 +288,63 @@ def batched_measurement(n_inst: int = 512, steps: int = 10, warmup: int = 3):
                    "the same instances stepped one after another"}
 
 
+def adjoint_measurement(with_cpu: bool, evals: int = 20):
+    """Gradients of the calibration loss on the 512^2 polycrystal (256 grains,
+    64 precipitates of radius 6-20): 3 eigenstrain + 4 anisotropy + 256
+    mobility derivatives per gradient, FP64."""
+    import torch
+    from gpk_b200 import GPKGrid, thermo
+    from gpk_b200.adjoint import AdjointProblem, calibration_case
+    n, grains = 512, 256
+    phi, g, mob_index = calibration_case(n, grains, 64, 11, (6, 20))
+    grid = GPKGrid(1, n, n, 1.0, thermo.isotropic(1.0, 1.0), 0.0, 1.5, precision="f64")
+    grid.set("phi", phi)
+    grid.set("g", g)
+    const = dict(m_fixed=1.0, sigma0=1e-3, c11=1.08, c12=0.62, c44=0.28, energy_weight=1e-6)
+    prob = AdjointProblem(grid, mob_index, grains, **const)
+    rng = np.random.default_rng(11)
+    theta = np.concatenate([[0.01, -0.004, 0.003], [0.05, -0.02, 0.01, 0.005],
+                            1.0 + 0.1 * rng.standard_normal(grains)])
+    star = theta * 1.05
+    prob.set_target(prob.forward(star, want_v=True)[1])
+    for _ in range(3):
+        prob.gradient(theta)
+    stream = torch.cuda.ExternalStream(grid.stream_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(evals):
+        prob.gradient(theta)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / evals
+    f0 = time.perf_counter()
+    for _ in range(evals):
+        prob.forward(theta)
+    fwd_ms = (time.perf_counter() - f0) * 1e3 / evals
+    res = {"workload": "adjoint calibration 512^2, 256 Voronoi grains + 64 precipitates, FP64; gradient = "
+                       "forward + adjoint (2 spectral solves, projection and its transpose)",
+           "params": len(theta), "ms_per_gradient": ms, "gradients_per_s": 1e3 / ms,
+           "derivatives_per_s": len(theta) * 1e3 / ms, "forward_ms_wall": fwd_ms,
+           "central_difference_gradients_per_s_gpu": 1e3 / (2 * len(theta) * fwd_ms)}
+    if with_cpu:
+        from oracle import adjoint_oracle
+        f = {k: grid.get(k)[0] for k in ("phi", "phi_comp", "mask", "nx_f", "ny_f", "kappa_f", "g")}
+        inv = 0.5 / (0.85 * 0.85)
+        t0 = time.perf_counter()
+        adjoint_oracle.forward(f["phi"], f["phi_comp"], f["mask"], f["nx_f"], f["ny_f"], f["kappa_f"], f["g"],
+                               mob_index, theta, const["c11"], const["c12"], const["c44"], const["sigma0"],
+                               const["m_fixed"], const["energy_weight"], 1.0, np.zeros((n, n)), 3,
+                               lambda r2: float(np.exp(-r2 * inv)))
+        cpu_s = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": 1.0 / (2 * len(theta) * cpu_s), "unit": "gradients/s", "cores": 1,
+                               "kind": "port", "sample": "one forward of the numpy restatement timed; a "
+                               "central-difference gradient costs 2 x 263 of them"}
+    prob.close()
+    grid.close()
+    return res
+
+
 def run_gpu_arm(args):
     ws, rank, local = _dist()
     import torch
@@ -402,7 +459,7 @@ def run_gpu_arm(args):
             cpu.pop("seconds", None)
         except Exception as exc:  # the GPU number stands on its own
             cpu = {"error": str(exc)}
-    spectral = batched = None
+    spectral = batched = adjoint = None
     if rank == 0:
         try:
             spectral = spectral_measurement(not args.no_cpu and ws == 1)
@@ -412,6 +469,10 @@ def run_gpu_arm(args):
             batched = batched_measurement()
         except Exception as exc:
             batched = {"error": str(exc)}
+        try:
+            adjoint = adjoint_measurement(not args.no_cpu and ws == 1)
+        except Exception as exc:
+            adjoint = {"error": str(exc)}
     if rank == 0:
         line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -421,7 +482,7 @@ def run_gpu_arm(args):
                 "stages_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in stages.items()},
                 "interface_fraction": iface, "counters_last_step": list(grid.counters()),
                 "per_step_topology": waves,
-                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "spectral": spectral, "batched": batched,
+                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "spectral": spectral, "batched": batched, "adjoint": adjoint,
                 "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": io,
                         "d2h_bytes_per_step": io, "steps": e2e_steps,
                         "path": "GPKGrid drop-in semantics: upload phi/alpha/g, step, download phi/alpha/g"}}
@@ -445,12 +506,16 @@ def main():
     ap.add_argument("--batched-only", action="store_true",
                     help="time only the lamellar sweep, batched and plain")
     ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--adjoint-only", action="store_true", help="time only the 512^2 adjoint gradient")
     ap.add_argument("--spectral-only", action="store_true",
                     help="time only the 128^3 spectral elasticity solve (profiling its kernels)")
     args = ap.parse_args()
     globals()["SIZE"], globals()["GRAINS"] = args.size, args.grains
     if args.spectral_only:
         print(json.dumps({"spectral": spectral_measurement(not args.no_cpu)}))
+        return 0
+    if args.adjoint_only:
+        print(json.dumps({"adjoint": adjoint_measurement(not args.no_cpu)}))
         return 0
     if args.batched_only:
         print(json.dumps({"batched": batched_measurement(args.instances)}))

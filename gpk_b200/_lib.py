@@ -60,6 +60,7 @@ def lib() -> C.CDLL:
         "gpk_grid_step_n": ([vp, i32, dbl, dbl, C.POINTER(dbl)], i32),
         "gpk_grid_run": ([vp, dbl, dbl, i32, C.POINTER(i32)], i32),
         "gpk_grid_sync": ([vp], i32),
+        "gpk_grid_geometry": ([vp], i32),
         "gpk_grid_max_dt": ([vp, C.POINTER(dbl)], i32),
         "gpk_grid_phase_volume": ([vp, C.c_int32, C.POINTER(dbl)], i32),
         "gpk_grid_n_grains": ([vp, C.POINTER(i32)], i32),
@@ -90,6 +91,12 @@ def lib() -> C.CDLL:
         "gpk_batch_step": ([vp, i32, dbl, dbl], i32),
         "gpk_batch_run": ([vp, dbl, dbl, i32, C.POINTER(i32)], i32),
         "gpk_batch_autotune": ([vp, i32, C.POINTER(i32), C.POINTER(i32)], i32),
+        "gpk_adjoint_create": ([vp, i32, C.POINTER(C.c_int32), i32, dbl, dbl, dbl, dbl, dbl, dbl, C.POINTER(vp)], i32),
+        "gpk_adjoint_destroy": ([vp], i32),
+        "gpk_adjoint_num_params": ([vp, C.POINTER(i32)], i32),
+        "gpk_adjoint_set_target": ([vp, C.POINTER(dbl)], i32),
+        "gpk_adjoint_forward": ([vp, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(dbl)], i32),
+        "gpk_adjoint_gradient": ([vp, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(dbl)], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)
@@ -110,7 +117,7 @@ def exported_symbols() -> list:
     import re
     names = []
     inc = os.path.join(HERE, "..", "include")
-    for h in ("gpk_b200.h", "gpk_init.h", "gpk_spectral.h", "gpk_batch.h"):
+    for h in ("gpk_b200.h", "gpk_init.h", "gpk_spectral.h", "gpk_batch.h", "gpk_adjoint.h"):
         text = open(os.path.join(inc, h)).read()
         names += re.findall(r"^\s*(?:const\s+)?\w[\w\s\*]*?\b(gpk_\w+)\s*\(", text, flags=re.M)
     return sorted(set(names))

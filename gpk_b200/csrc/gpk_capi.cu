@@ -498,6 +498,11 @@ extern "C" int gpk_grid_step(gpk_grid* G, double dt, double dt_cap, double* dt_u
     return GPK_OK;
 }
 
+extern "C" int gpk_grid_geometry(gpk_grid* G) {
+    if (!G) return GPK_ERR_INVALID_ARGUMENT;
+    return G->precision == GPK_PREC_F64 ? gpk_geometry_only<double>(G) : gpk_geometry_only<float>(G);
+}
+
 extern "C" int gpk_grid_step_n(gpk_grid* G, int n, double dt, double dt_cap, double* time_out) {
     if (!G || n < 0) return GPK_ERR_INVALID_ARGUMENT;
     for (int k = 0; k < n; ++k) GPK_TRY(step_once(G, dt, dt_cap));

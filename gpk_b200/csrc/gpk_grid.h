@@ -123,6 +123,7 @@ int gpk_stage_collect(gpk_grid* G);
 // ---- launchers (templated on the grid's real type) --------------------------
 template <typename real> int gpk_build_tables(gpk_grid* G);
 template <typename real> int gpk_step_impl(gpk_grid* G, double dt, double dt_cap);
+template <typename real> int gpk_geometry_only(gpk_grid* G);
 template <typename real> int gpk_interface_mask(gpk_grid* G);
 template <typename real> int gpk_max_dt_impl(gpk_grid* G, double* out);
 template <typename real> int gpk_phase_volume_impl(gpk_grid* G, int32_t label, double* out);

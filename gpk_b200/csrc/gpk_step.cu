@@ -1336,6 +1336,18 @@ template int gpk_interface_mask<float>(gpk_grid*);
 template int gpk_interface_mask<double>(gpk_grid*);
 template int gpk_step_impl<float>(gpk_grid*, double, double);
 template int gpk_step_impl<double>(gpk_grid*, double, double);
+
+// The mask and geometry stages of GPKGrid::step on the current labels
+// (src/gpk_geometry.cpp:42-183), without moving any interface.
+template <typename real>
+int gpk_geometry_only(gpk_grid* G) {
+    GPK_TRY(gpk_interface_mask<real>(G));
+    GPK_TRY(geometry<real>(G));
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    return GPK_OK;
+}
+template int gpk_geometry_only<float>(gpk_grid*);
+template int gpk_geometry_only<double>(gpk_grid*);
 template int gpk_max_dt_impl<float>(gpk_grid*, double*);
 template int gpk_max_dt_impl<double>(gpk_grid*, double*);
 

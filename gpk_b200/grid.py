@@ -212,6 +212,10 @@ class GPKGrid:
     def set_geometry_kernel(self, kind: str) -> None:
         check(lib().gpk_grid_set_geometry_kernel(self._h, {"tiled": 0, "per_cell": 1, "tiled_batched": 2}[kind]))
 
+    def geometry(self) -> None:
+        """Mask and geometry of the current labels, without stepping."""
+        check(lib().gpk_grid_geometry(self._h))
+
     def stream_ptr(self) -> int:
         p = C.c_void_p()
         check(lib().gpk_grid_stream(self._h, C.byref(p)))

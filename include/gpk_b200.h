@@ -170,6 +170,10 @@ int gpk_grid_run(gpk_grid* grid, double t_end, double dt, int max_steps,
                  int* steps_out);
 /* Waits for all work queued on the grid's stream.                          */
 int gpk_grid_sync(gpk_grid* grid);
+/* The interface mask and geometry of the current labels (the first two
+ * stages of GPKGrid::step, src/gpk_geometry.cpp:42-183) without stepping:
+ * fills mask, nx/ny/nz, kappa and phi_comp.  Returns when done.           */
+int gpk_grid_geometry(gpk_grid* grid);
 
 /* ---- diagnostics (src/gpk_simulation.cpp:11-144) ------------------------- */
 int gpk_grid_max_dt(gpk_grid* grid, double* out);

@@ -1,0 +1,111 @@
+"""The adjoint module: the CUDA FP64 forward against the numpy oracle, and
+the hand-written adjoint gradient against FP64 central differences
+(h = 1e-6) of the forward.
+
+Tolerances: forward loss and velocity within 1e-10 relative of the oracle;
+each gradient component within 1e-6 of the largest component plus 1e-4 of
+itself, against central differences.
+"""
+import numpy as np
+import pytest
+
+from gpk_b200 import GPKError, GPKGrid, thermo
+from gpk_b200.adjoint import AdjointProblem, calibration_case, gpk_loss
+from oracle import adjoint_oracle
+
+pytestmark = pytest.mark.gpu
+H = 1e-6
+CONST = dict(m_fixed=1.0, sigma0=1e-3, c11=1.08, c12=0.62, c44=0.28, energy_weight=1e-6)
+
+
+def _problem(n, grains, precipitates, seed, r_range):
+    phi, g, mob_index = calibration_case(n, grains, precipitates, seed, r_range)
+    grid = GPKGrid(1, n, n, 1.0, thermo.isotropic(1.0, 1.0), 0.0, 1.5, precision="f64")
+    grid.set("phi", phi)
+    grid.set("g", g)
+    prob = AdjointProblem(grid, mob_index, grains, **CONST)
+    rng = np.random.default_rng(seed)
+    theta = np.concatenate([[0.01, -0.004, 0.003], [0.05, -0.02, 0.01, 0.005], 1.0 + 0.1 * rng.standard_normal(grains)])
+    star = theta.copy()
+    star[:3] *= 1.1
+    star[3:7] += 0.01
+    star[7:] *= 1.0 + 0.05 * rng.standard_normal(grains)
+    _, v_star = prob.forward(star, want_v=True)
+    prob.set_target(v_star)
+    return grid, prob, theta, mob_index, v_star
+
+
+def _oracle_forward(grid, mob_index, theta, target):
+    f = {k: grid.get(k)[0] for k in ("phi", "phi_comp", "mask", "nx_f", "ny_f", "kappa_f", "g")}
+    inv = 0.5 / (0.85 * 0.85)
+    return adjoint_oracle.forward(f["phi"], f["phi_comp"], f["mask"], f["nx_f"], f["ny_f"], f["kappa_f"], f["g"],
+                                  mob_index, theta, CONST["c11"], CONST["c12"], CONST["c44"], CONST["sigma0"],
+                                  CONST["m_fixed"], CONST["energy_weight"], 1.0, target, 3,
+                                  lambda r2: float(np.exp(-r2 * inv)))
+
+
+def _check_grad(g, fd):
+    scale = np.max(np.abs(fd))
+    assert np.all(np.abs(g - fd) <= 1e-6 * scale + 1e-4 * np.abs(fd)), np.max(np.abs(g - fd)) / scale
+
+
+def test_forward_matches_oracle_and_gradient_matches_central_differences():
+    grid, prob, theta, mob_index, v_star = _problem(72, 12, 4, 3, (4, 8))
+    loss, v = prob.forward(theta, want_v=True)
+    lo, vo = _oracle_forward(grid, mob_index, theta, v_star)
+    assert abs(loss - lo) <= 1e-10 * abs(lo)
+    assert np.max(np.abs(v - vo)) <= 1e-10 * np.max(np.abs(vo))
+    loss2, g = prob.gradient(theta)
+    assert loss2 == loss
+    fd = np.empty_like(theta)
+    for k in range(len(theta)):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += H
+        tm[k] -= H
+        fd[k] = (_oracle_forward(grid, mob_index, tp, v_star)[0] - _oracle_forward(grid, mob_index, tm, v_star)[0]) / (2 * H)
+    _check_grad(g, fd)
+
+
+def test_calibration_512_gradient_all_components():
+    """The 512^2 case: 256 grains, 64 precipitates of radius 6-20; every one of
+    the 263 gradient components against central differences of the GPU forward."""
+    grid, prob, theta, mob_index, v_star = _problem(512, 256, 64, 11, (6, 20))
+    loss, g = prob.gradient(theta)
+    assert loss > 0 and np.all(np.isfinite(g))
+    fd = np.empty_like(theta)
+    for k in range(len(theta)):
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += H
+        tm[k] -= H
+        fd[k] = (prob.forward(tp) - prob.forward(tm)) / (2 * H)
+    _check_grad(g, fd)
+    # deterministic reductions: the same bits every call
+    assert np.array_equal(prob.gradient(theta)[1], g)
+
+
+def test_autograd_function():
+    torch = pytest.importorskip("torch")
+    grid, prob, theta, mob_index, v_star = _problem(64, 10, 3, 5, (4, 7))
+    eig = torch.tensor(theta[:3], dtype=torch.float64, requires_grad=True)
+    an = torch.tensor(theta[3:7], dtype=torch.float64, requires_grad=True)
+    mob = torch.tensor(theta[7:], dtype=torch.float64, requires_grad=True)
+    loss = gpk_loss(prob, eig, an, mob)
+    (2.0 * loss).backward()
+    lref, gref = prob.gradient(theta)
+    assert float(loss.detach()) == lref
+    assert np.array_equal(eig.grad.numpy(), 2.0 * gref[:3])
+    assert np.array_equal(an.grad.numpy(), 2.0 * gref[3:7])
+    assert np.array_equal(mob.grad.numpy(), 2.0 * gref[7:])
+
+
+def test_rejects_unsupported_grids():
+    g3 = GPKGrid(8, 8, 8, 1.0, thermo.isotropic(1.0, 1.0), 0.0, 1.5, precision="f64")
+    with pytest.raises(GPKError):
+        AdjointProblem(g3, np.zeros(2, np.int32), 1)
+    g32 = GPKGrid(1, 16, 16, 1.0, thermo.isotropic(1.0, 1.0), 0.0, 1.5, precision="f32")
+    with pytest.raises(GPKError):
+        AdjointProblem(g32, np.zeros(2, np.int32), 1)
+    g64 = GPKGrid(1, 16, 16, 1.0, thermo.isotropic(1.0, 1.0), 0.0, 1.5, precision="f64")
+    g64.set("phi", 3)
+    with pytest.raises(GPKError):
+        AdjointProblem(g64, np.zeros(2, np.int32), 1)  # label 3 outside the table
