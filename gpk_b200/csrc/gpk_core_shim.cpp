@@ -81,6 +81,57 @@ void base_fields(const ThermoModel& m, gpk_thermo_desc& d) {
     d.H_theta = m.H_theta; d.g_easy_ref = m.g_easy_ref; d.lambda_s = m.lambda_s;
 }
 
+// A subclass not known by name is described by behaviour: each virtual the
+// step calls is evaluated on the host at a fixed sample set and compared, bit
+// for bit, with a law the device implements.  Described: no bulk driving
+// force, the parent's interface composition, no product-phase selection, the
+// base interfacial energy (sigma0, eps4; src/gpk_thermo.cpp:9-30), the base
+// magnetic energy, and a mobility that is either a constant (the
+// AnisotropicGrowthThermo law) or the base Read-Shockley law
+// (src/gpk_thermo.cpp:32-47).  Anything else is left undescribed.
+bool describe_by_behaviour(const ThermoModel& m, gpk_thermo_desc& d) {
+    if (m.phase_selection) return false;
+    const int pairs[4][2] = {{0, 1}, {1, 0}, {2, 3}, {5, 2}};
+    const float cs[3] = {0.f, 0.15f, 0.9f}, Ts[3] = {300.f, 800.f, 1250.f};
+    for (const auto& pq : pairs)
+        for (float c : cs)
+            for (float T : Ts) {
+                if (m.bulk_driving_force(pq[0], pq[1], c, T) != 0.f) return false;
+                if (m.interface_composition(pq[0], pq[1], c, 0.5f * c + 0.1f) != c) return false;
+            }
+    const float nrm[8][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {0.6f, 0.8f, 0}, {-0.28f, 0.96f, 0},
+                             {0.48f, 0.6f, 0.64f}, {-0.36f, -0.48f, 0.8f}, {0.8f, 0, -0.6f}};
+    const float gs[5] = {0.f, 0.3f, 1.1f, -0.7f, 2.5f};
+    for (const auto& n : nrm)
+        for (float g : gs) {
+            if (m.interfacial_energy_pair_comp(n[0], n[1], n[2], g, 1, 2, 0.1f) !=
+                m.ThermoModel::interfacial_energy(n[0], n[1], n[2], g))
+                return false;
+            if (m.E_mag(g) != m.ThermoModel::E_mag(g)) return false;
+        }
+    bool constant = true, base = true;
+    float first = 0.f;
+    int k = 0;
+    for (const auto& n : nrm)
+        for (float gp : gs)
+            for (float gq : gs)
+                for (float T : Ts) {
+                    const float v = m.mobility(n[0], n[1], n[2], gp, gq, T);
+                    if (k++ == 0) first = v;
+                    constant = constant && v == first;
+                    base = base && v == m.ThermoModel::mobility(n[0], n[1], n[2], gp, gq, T);
+                }
+    if (!constant && !base) return false;
+    base_fields(m, d);
+    if (constant) {
+        d.model = GPK_MODEL_ANISOTROPIC;
+        d.M0 = first;
+    } else {
+        d.model = GPK_MODEL_BASE;
+    }
+    return true;
+}
+
 }  // namespace
 
 gpk_thermo_desc describe_thermo(const ThermoModel& m) {
@@ -104,9 +155,12 @@ gpk_thermo_desc describe_thermo(const ThermoModel& m) {
     else if (t == mangled("MagneticAnnealingThermo")) model = GPK_MODEL_MAGNETIC_ANNEAL;
     else if (t == mangled("MagnetoelasticThermo")) model = GPK_MODEL_MAGNETOELASTIC;
     else if (t == mangled("NdFeBGrainBoundaryThermo")) model = GPK_MODEL_NDFEB;
-    if (model < 0)
+    if (model < 0) {
+        if (describe_by_behaviour(m, d)) return d;
         throw std::runtime_error(std::string("gpk_b200: ThermoModel subclass '") + t +
-                                 "' has no device form; override ThermoModel::gpk_describe");
+                                 "' has no device form (its virtual functions match no device law); "
+                                 "override ThermoModel::gpk_describe");
+    }
     d.model = model;
     base_fields(m, d);
     float* p = d.p;
@@ -180,33 +234,43 @@ GPKGrid::GPKGrid(int Nz_, int Ny_, int Nx_, float dx_, std::shared_ptr<ThermoMod
       nz_f(Nz_ * Ny_ * Nx_, 0.f), kappa_f(Nz_ * Ny_ * Nx_, 0.f), vn_f(Nz_ * Ny_ * Nx_, 0.f),
       E_el(Nz_ * Ny_ * Nx_, 0.f), phi_comp(Nz_ * Ny_ * Nx_, 0), g_comp(Nz_ * Ny_ * Nx_, 0.f),
       mask(Nz_ * Ny_ * Nx_, 0), thermo_(std::move(thermo)), D_(D), gaussian_sigma_(gaussian_sigma) {
-    const gpk_thermo_desc d = describe_thermo(*thermo_);
-    throw_if(gpk_grid_create(Nz, Ny, Nx, (double)dx, &d, (double)D, (double)gaussian_sigma, GPK_PREC_F32, &grid_),
-             "grid creation");
+    dev();
 }
 
-GPKGrid::~GPKGrid() {
-    if (grid_) gpk_grid_destroy(grid_);
+void GPKGrid::DeviceGrid::release() {
+    if (p) gpk_grid_destroy(p);
+    p = nullptr;
 }
+
+gpk_grid* GPKGrid::dev() const {
+    if (!grid_.p) {
+        const gpk_thermo_desc d = describe_thermo(*thermo_);
+        throw_if(gpk_grid_create(Nz, Ny, Nx, (double)dx, &d, (double)D_, (double)gaussian_sigma_, GPK_PREC_F32,
+                                 &grid_.p),
+                 "grid creation");
+    }
+    return grid_.p;
+}
+
 
 void GPKGrid::push_thermo() {
     const gpk_thermo_desc d = describe_thermo(*thermo_);
-    throw_if(gpk_grid_set_thermo(grid_, &d), "thermo update");
+    throw_if(gpk_grid_set_thermo(dev(), &d), "thermo update");
 }
 
 void GPKGrid::push_state() {
     const size_t n = (size_t)N();
-    throw_if(gpk_grid_upload(grid_, GPK_FIELD_PHI, phi.data(), n), "upload phi");
-    throw_if(gpk_grid_upload(grid_, GPK_FIELD_ALPHA, alpha.data(), n), "upload alpha");
-    throw_if(gpk_grid_upload(grid_, GPK_FIELD_C, c.data(), n), "upload c");
-    throw_if(gpk_grid_upload(grid_, GPK_FIELD_T, T.data(), n), "upload T");
-    throw_if(gpk_grid_upload(grid_, GPK_FIELD_G, g.data(), n), "upload g");
-    throw_if(gpk_grid_upload(grid_, GPK_FIELD_RHO, rho.data(), n), "upload rho");
+    throw_if(gpk_grid_upload(dev(), GPK_FIELD_PHI, phi.data(), n), "upload phi");
+    throw_if(gpk_grid_upload(dev(), GPK_FIELD_ALPHA, alpha.data(), n), "upload alpha");
+    throw_if(gpk_grid_upload(dev(), GPK_FIELD_C, c.data(), n), "upload c");
+    throw_if(gpk_grid_upload(dev(), GPK_FIELD_T, T.data(), n), "upload T");
+    throw_if(gpk_grid_upload(dev(), GPK_FIELD_G, g.data(), n), "upload g");
+    throw_if(gpk_grid_upload(dev(), GPK_FIELD_RHO, rho.data(), n), "upload rho");
     // phi_comp keeps stale values outside the interface in the reference;
     // upload it so those cells read back unchanged
-    throw_if(gpk_grid_upload(grid_, GPK_FIELD_PHI_COMP, phi_comp.data(), n), "upload phi_comp");
-    throw_if(gpk_grid_set_time(grid_, time), "set time");
-    throw_if(gpk_grid_set_step_id(grid_, step_id_), "set step id");
+    throw_if(gpk_grid_upload(dev(), GPK_FIELD_PHI_COMP, phi_comp.data(), n), "upload phi_comp");
+    throw_if(gpk_grid_set_time(dev(), time), "set time");
+    throw_if(gpk_grid_set_step_id(dev(), step_id_), "set step id");
 }
 
 void GPKGrid::pull_state() {
@@ -220,20 +284,20 @@ void GPKGrid::pull_state() {
                     {GPK_FIELD_VN, vn_f.data()},       {GPK_FIELD_E_EL, E_el.data()},
                     {GPK_FIELD_PHI_COMP, phi_comp.data()}, {GPK_FIELD_G_COMP, g_comp.data()},
                     {GPK_FIELD_MASK, mask.data()}};
-    for (const F& f : fs) throw_if(gpk_grid_download(grid_, f.id, f.p, n), "download");
+    for (const F& f : fs) throw_if(gpk_grid_download(dev(), f.id, f.p, n), "download");
     uint64_t cnt[3];
-    throw_if(gpk_grid_counters(grid_, cnt), "counters");
+    throw_if(gpk_grid_counters(dev(), cnt), "counters");
     topology_accepted_last = cnt[0];
     topology_deferred_last = cnt[1];
     gaussian_remap_exchanges_last = cnt[2];
-    throw_if(gpk_grid_get_time(grid_, &time), "time");
+    throw_if(gpk_grid_get_time(dev(), &time), "time");
 }
 
 float GPKGrid::step(float dt, float dt_cap) {
     push_thermo();
     push_state();
     double used = 0.0;
-    throw_if(gpk_grid_step(grid_, (double)dt, (double)dt_cap, &used), "step");
+    throw_if(gpk_grid_step(dev(), (double)dt, (double)dt_cap, &used), "step");
     ++step_id_;
     pull_state();
     return (float)used;
@@ -247,7 +311,7 @@ int GPKGrid::run(double t_end, float dt, std::function<void(const GPKGrid&, int)
     while (t < t_end) {
         const float remaining = static_cast<float>(t_end - t);
         double used = 0.0;
-        throw_if(gpk_grid_step(grid_, (double)dt, (double)remaining, &used), "step");
+        throw_if(gpk_grid_step(dev(), (double)dt, (double)remaining, &used), "step");
         ++step_id_;
         t += (double)(float)used;
         ++step_count;
@@ -316,9 +380,9 @@ std::size_t GPKGrid::allocated_array_bytes() const {
 bool GPKGrid::topology_simple_move(int cell, int32_t new_label) const {
     if (cell < 0 || cell >= N()) return false;
     // evaluate on the labels currently held in the host mirror
-    throw_if(gpk_grid_upload(grid_, GPK_FIELD_PHI, phi.data(), (size_t)N()), "upload phi");
+    throw_if(gpk_grid_upload(dev(), GPK_FIELD_PHI, phi.data(), (size_t)N()), "upload phi");
     int r = 0;
-    throw_if(gpk_grid_topology_simple_move(grid_, cell, new_label, &r), "topology_simple_move");
+    throw_if(gpk_grid_topology_simple_move(dev(), cell, new_label, &r), "topology_simple_move");
     return r != 0;
 }
 

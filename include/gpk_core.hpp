@@ -165,9 +165,11 @@ public:
 
     GPKGrid(int Nz, int Ny, int Nx, float dx, std::shared_ptr<ThermoModel> thermo, float D = 0.f,
             float gaussian_sigma = 2.0f);
-    ~GPKGrid();
-    GPKGrid(const GPKGrid&) = delete;
-    GPKGrid& operator=(const GPKGrid&) = delete;
+    // Copyable like the reference's GPKGrid: a copy takes every public
+    // member and builds its own device grid from them at its first use.
+    ~GPKGrid() = default;
+    GPKGrid(const GPKGrid&) = default;
+    GPKGrid& operator=(const GPKGrid&) = default;
 
     float step(float dt = -1.f, float dt_cap = 1.0e30f);
     int run(double t_end, float dt = -1.f, std::function<void(const GPKGrid&, int)> cb = nullptr,
@@ -191,15 +193,33 @@ public:
     }
 
     // The device grid behind this object (no counterpart in the reference).
-    gpk_grid* device_grid() const { return grid_; }
+    gpk_grid* device_grid() const { return dev(); }
+    // Host members -> device, and device -> host members, for code that
+    // advances device_grid() directly (e.g. a gpk_batch); step() and run()
+    // do both themselves.  No counterpart in the reference.
+    void to_device() { push_state(); }
+    void from_device() { pull_state(); }
 
 private:
     std::shared_ptr<ThermoModel> thermo_;
     float D_;
     float gaussian_sigma_;
-    gpk_grid* grid_ = nullptr;
+    // owns one device grid; a copy or assignment starts without one
+    struct DeviceGrid {
+        gpk_grid* p = nullptr;
+        DeviceGrid() = default;
+        DeviceGrid(const DeviceGrid&) {}
+        DeviceGrid& operator=(const DeviceGrid&) {
+            release();
+            return *this;
+        }
+        ~DeviceGrid() { release(); }
+        void release();
+    };
+    mutable DeviceGrid grid_;
     uint64_t step_id_ = 0;
 
+    gpk_grid* dev() const;  // the device grid, created on first use
     void push_state();      // host mirrors -> device (state + time)
     void pull_state();      // device -> host mirrors (every public field)
     void push_thermo();     // ThermoModel -> gpk_thermo_desc
