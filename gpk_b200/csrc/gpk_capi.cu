@@ -89,8 +89,37 @@ template <typename real>
 __global__ static void k_fill_real(real* p, int n, real v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
 }
+// cells per label; the lanes of a warp holding the same label add once
 __global__ static void k_histogram(int N, const int32_t* __restrict__ phi, int32_t* __restrict__ count) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) atomicAdd(&count[phi[i]], 1);
+    for (int base = blockIdx.x * blockDim.x; base < N; base += gridDim.x * blockDim.x) {
+        const int i = base + threadIdx.x;
+        const bool v = i < N;
+        const int32_t label = v ? phi[i] : -1;
+        const unsigned act = __ballot_sync(0xffffffffu, v);
+        if (v) {
+            const unsigned grp = __match_any_sync(act, label);
+            if ((threadIdx.x & 31) == __ffs(grp) - 1) atomicAdd(&count[label], (int)__popc(grp));
+        }
+    }
+}
+// out[0] = lowest cell index whose label lies outside [0, 2^26) (or ~0u),
+// out[1] = largest label in range
+__global__ static void k_label_scan(int N, const int32_t* __restrict__ p, unsigned* __restrict__ out) {
+    unsigned bad = 0xffffffffu, mx = 0;
+    for (int base = blockIdx.x * blockDim.x; base < N; base += gridDim.x * blockDim.x) {
+        const int i = base + threadIdx.x;
+        if (i < N) {
+            const int32_t v = p[i];
+            if (v < 0 || v >= (1 << 26)) bad = min(bad, (unsigned)i);
+            else mx = max(mx, (unsigned)v);
+        }
+    }
+    bad = __reduce_min_sync(0xffffffffu, bad);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&out[0], bad);
+        atomicMax(&out[1], mx);
+    }
 }
 
 int gpk_ensure_label_capacity(gpk_grid* G, int cap) {
@@ -325,6 +354,7 @@ extern "C" int gpk_grid_create(int Nz, int Ny, int Nx, double dx, const gpk_ther
     ALLOC(G->key_b, 8 * N);
     ALLOC(G->val_a, 4 * N);
     ALLOC(G->val_b, 4 * N);
+    ALLOC(G->upload_check, 2 * sizeof(unsigned));
     ALLOC(G->exch, 16 * N);
     ALLOC(G->ero_target, 4 * N);
     ALLOC(G->ero_g, rb);
@@ -415,28 +445,30 @@ extern "C" int gpk_grid_upload(gpk_grid* G, int field, const void* host, size_t 
     if (!host) { gpk_set_error("host pointer is null"); return GPK_ERR_INVALID_ARGUMENT; }
     size_t esz;
     void* dst = field_ptr(G, field, &esz);
-    if (field == GPK_FIELD_PHI) {
+    if (field == GPK_FIELD_PHI || field == GPK_FIELD_PHI_COMP) {
+        // labels are staged in scratch and checked on the device; the field is
+        // written only when every label lies in range
         const int32_t* p = (const int32_t*)host;
-        int32_t mx = 0;
-        for (size_t i = 0; i < count; ++i) {
-            if (p[i] < 0 || p[i] >= (1 << 26)) {
-                gpk_set_error("label " + std::to_string(p[i]) + " at cell " + std::to_string(i) +
-                              " lies outside [0, 2^26)");
-                return GPK_ERR_LABEL_RANGE;
-            }
-            mx = std::max(mx, p[i]);
+        GPK_CUDA_TRY(cudaMemcpyAsync(G->val_a, host, esz * count, cudaMemcpyHostToDevice, G->stream));
+        const unsigned init[2] = {0xffffffffu, 0u};
+        GPK_CUDA_TRY(cudaMemcpyAsync(G->upload_check, init, sizeof(init), cudaMemcpyHostToDevice, G->stream));
+        k_label_scan<<<G->num_sms * 8, 256, 0, G->stream>>>((int)count, G->val_a, G->upload_check);
+        G->launches++;
+        GPK_CUDA_TRY(cudaGetLastError());
+        unsigned res[2];
+        GPK_CUDA_TRY(cudaMemcpyAsync(res, G->upload_check, sizeof(res), cudaMemcpyDeviceToHost, G->stream));
+        GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+        if (res[0] != 0xffffffffu) {
+            gpk_set_error(std::string(field == GPK_FIELD_PHI ? "label " : "competitor label ") +
+                          std::to_string(p[res[0]]) + " at cell " + std::to_string(res[0]) +
+                          " lies outside [0, 2^26)");
+            return GPK_ERR_LABEL_RANGE;
         }
-        GPK_CUDA_TRY(cudaMemcpyAsync(dst, host, esz * count, cudaMemcpyHostToDevice, G->stream));
-        GPK_TRY(gpk_ensure_label_capacity(G, mx + 1));
-        GPK_TRY(gpk_recount_labels(G));
-    } else if (field == GPK_FIELD_PHI_COMP) {
-        const int32_t* p = (const int32_t*)host;
-        for (size_t i = 0; i < count; ++i)
-            if (p[i] < 0 || p[i] >= (1 << 26)) {
-                gpk_set_error("competitor label outside [0, 2^26)");
-                return GPK_ERR_LABEL_RANGE;
-            }
-        GPK_CUDA_TRY(cudaMemcpyAsync(dst, host, esz * count, cudaMemcpyHostToDevice, G->stream));
+        GPK_CUDA_TRY(cudaMemcpyAsync(dst, G->val_a, esz * count, cudaMemcpyDeviceToDevice, G->stream));
+        if (field == GPK_FIELD_PHI) {
+            GPK_TRY(gpk_ensure_label_capacity(G, (int)res[1] + 1));
+            GPK_TRY(gpk_recount_labels(G));
+        }
     } else {
         GPK_CUDA_TRY(cudaMemcpyAsync(dst, host, esz * count, cudaMemcpyHostToDevice, G->stream));
     }

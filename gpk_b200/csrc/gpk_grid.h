@@ -81,6 +81,7 @@ struct gpk_grid {
     void* bgr_res = nullptr; void* bgr_best = nullptr;   // per active position (real)
     unsigned long long* key_a = nullptr; unsigned long long* key_b = nullptr;
     int32_t* val_a = nullptr; int32_t* val_b = nullptr;
+    unsigned* upload_check = nullptr;      // label range check of an upload
     int32_t* exch = nullptr;               // exchange slots: a, b, low, high, state
     void* cub_tmp = nullptr; size_t cub_tmp_bytes = 0;
     // extinction

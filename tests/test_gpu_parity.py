@@ -277,7 +277,18 @@ def test_run_matches_oracle(oracle_mod):
 def test_label_range_rejected():
     from gpk_b200 import GPKError
     gpu = GPKGrid(1, 8, 8, 1.0, thermo.isotropic(1.0))
+    good = (np.arange(64, dtype=np.int32) // 16).reshape(1, 8, 8) + 1
+    gpu.set("phi", good)
+    assert gpu.n_grains() == 4
     bad = np.zeros((1, 8, 8), np.int32); bad[0, 0, 0] = -3
     with pytest.raises(GPKError) as e:
         gpu.set("phi", bad)
     assert e.value.code == 5
+    bad = good.copy(); bad[0, 5, 2] = 1 << 26; bad[0, 7, 7] = -1
+    with pytest.raises(GPKError) as e:
+        gpu.set("phi", bad)
+    assert e.value.code == 5 and "at cell 42 " in str(e.value)
+    # a rejected upload leaves the grid as it was
+    assert np.array_equal(gpu.get("phi"), good) and gpu.n_grains() == 4
+    with pytest.raises(GPKError):
+        gpu.set("phi_comp", bad)
