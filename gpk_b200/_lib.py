@@ -84,6 +84,8 @@ def lib() -> C.CDLL:
         "gpk_spectral_solve": ([vp, vp, vp, vp, vp, C.POINTER(dbl)], i32),
         "gpk_spectral_solve_host": ([vp, vp, vp, vp, vp, C.POINTER(dbl)], i32),
         "gpk_spectral_info": ([vp, C.POINTER(i64), C.POINTER(i64)], i32),
+        "gpk_spectral_couple_grid": ([vp, vp, C.c_int32, C.POINTER(dbl)], i32),
+        "gpk_grid_set_external_elastic": ([vp, i32], i32),
         "gpk_batch_create": ([i32, C.POINTER(vp), i32, C.POINTER(vp)], i32),
         "gpk_batch_destroy": ([vp], i32),
         "gpk_batch_set_workers": ([vp, i32], i32),

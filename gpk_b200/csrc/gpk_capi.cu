@@ -690,6 +690,12 @@ extern "C" int gpk_grid_wave_stats(gpk_grid* G, uint64_t out[8]) {
     return GPK_OK;
 }
 
+extern "C" int gpk_grid_set_external_elastic(gpk_grid* G, int on) {
+    if (!G) return GPK_ERR_INVALID_ARGUMENT;
+    G->external_elastic = on ? 1 : 0;
+    return GPK_OK;
+}
+
 extern "C" int gpk_grid_set_geometry_kernel(gpk_grid* G, int kind) {
     if (!G || kind < 0 || kind > 2) return GPK_ERR_INVALID_ARGUMENT;
     G->geometry_kernel = kind;

@@ -107,6 +107,8 @@ struct gpk_grid {
     // geometry kernel choice: 0 = tiled (per-cell kernel where no tiled
     // instantiation exists), 1 = per-cell kernel
     int geometry_kernel = 0;
+    // E_el supplied by the caller (gpk_grid_set_external_elastic)
+    int external_elastic = 0;
     // stage timing (gpk_grid_profile)
     int profile = 0;
     cudaEvent_t ev[GPK_NUM_STAGES][2] = {};

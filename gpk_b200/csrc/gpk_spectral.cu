@@ -23,10 +23,8 @@
 
 #include <string>
 
-#include "../../include/gpk_b200.h"
 #include "../../include/gpk_spectral.h"
-
-void gpk_set_error(const std::string& msg);
+#include "gpk_grid.h"
 
 namespace {
 
@@ -219,6 +217,19 @@ __global__ void k_epilogue(SpecConst c, const double* __restrict__ f, const doub
     }
 }
 
+// variant fractions of a label map: variant 0 = every non-matrix label
+__global__ void k_label_fractions(long long N, const int32_t* __restrict__ phi, int32_t matrix, double* __restrict__ f) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        f[i] = phi[i] != matrix ? 1.0 : 0.0;
+        f[N + i] = 0.0;
+        f[2 * N + i] = 0.0;
+    }
+}
+__global__ void k_to_float(long long N, const double* __restrict__ a, float* __restrict__ b) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
 }  // namespace
 
 struct gpk_spectral {
@@ -408,6 +419,42 @@ extern "C" int gpk_spectral_solve_host(gpk_spectral* s, const double* fractions,
     if (hydro) SPEC_CUDA_TRY(cudaMemcpyAsync(hydro, h, sizeof(double) * N, cudaMemcpyDeviceToHost, s->stream));
     SPEC_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return GPK_OK;
+}
+
+extern "C" int gpk_spectral_couple_grid(gpk_spectral* s, gpk_grid* G, int32_t matrix_label, double* residual) {
+    if (!s || !G) { gpk_set_error("spectral: null handle"); return GPK_ERR_INVALID_ARGUMENT; }
+    const bool same = s->ndim == 3 ? (s->n[0] == G->d.Nz && s->n[1] == G->d.Ny && s->n[2] == G->d.Nx)
+                                   : (G->d.Nz == 1 && s->n[0] == G->d.Ny && s->n[1] == G->d.Nx);
+    if (!same) {
+        gpk_set_error("spectral: the solve's shape differs from the grid's");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    const long long N = s->N;
+    if (!s->stage) {
+        const size_t b = sizeof(double) * 8 * N;
+        if (cudaMalloc((void**)&s->stage, b) != cudaSuccess) {
+            cudaGetLastError();
+            gpk_set_error("spectral: cudaMalloc of the coupling buffers failed");
+            return GPK_ERR_OUT_OF_MEMORY;
+        }
+        s->bytes += (long long)b;
+    }
+    double* f = s->stage;
+    double* e = f + 7 * N;  // energy when the grid holds floats
+    cudaStream_t saved = s->stream;
+    s->stream = G->stream;
+    k_label_fractions<<<s->nblocks, 256, 0, s->stream>>>(N, G->phi, matrix_label, f);
+    G->launches++;
+    double* E = G->precision == GPK_PREC_F64 ? (double*)G->f[GPK_FIELD_E_EL] : e;
+    int rc = gpk_spectral_solve(s, f, nullptr, E, nullptr, residual);
+    if (rc == GPK_OK && G->precision != GPK_PREC_F64) {
+        k_to_float<<<s->nblocks, 256, 0, s->stream>>>(N, e, (float*)G->f[GPK_FIELD_E_EL]);
+        G->launches++;
+        if (cudaGetLastError() != cudaSuccess) rc = GPK_ERR_CUDA;
+    }
+    G->launches += 4;
+    s->stream = saved;
+    return rc;
 }
 
 extern "C" int gpk_spectral_info(const gpk_spectral* s, int64_t* cells, int64_t* device_bytes) {

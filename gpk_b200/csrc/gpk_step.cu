@@ -1008,6 +1008,7 @@ static int elastic(gpk_grid* G) {
     const gpk_thermo_desc& th = G->th;
     const Dims D = G->d;
     real* E = (real*)G->f[GPK_FIELD_E_EL];
+    if (G->external_elastic) return GPK_OK;  // E_el as the caller supplied it
     if (!th.elastic_enabled || (real)th.elastic_modulus <= (real)0 ||
         ((real)th.eigenstrain_coeff == (real)0 && (real)th.lambda_s == (real)0)) {
         GPK_CUDA_TRY(cudaMemsetAsync(E, 0, G->rsz * D.N, G->stream));
@@ -1140,7 +1141,8 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
     GPK_TRY(gpk_stage_end(G, GPK_STAGE_GEOMETRY));
     GPK_TRY(gpk_stage_begin(G, GPK_STAGE_VELOCITY));
     GPK_TRY(elastic<real>(G));
-    const ThermoDev TD = make_thermo_dev(th);
+    ThermoDev TD = make_thermo_dev(th);
+    if (G->external_elastic) TD.t.elastic_enabled = 1;
     GPK_CUDA_TRY(cudaMemsetAsync(G->f[GPK_FIELD_VN], 0, G->rsz * D.N, G->stream));
     k_velocities<real><<<ga, 256, 0, G->stream>>>(
         D, TD, G->active, &G->scal->n_active, G->phi, G->phi_comp, (const real*)G->f[GPK_FIELD_C],

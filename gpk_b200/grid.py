@@ -212,6 +212,11 @@ class GPKGrid:
     def set_geometry_kernel(self, kind: str) -> None:
         check(lib().gpk_grid_set_geometry_kernel(self._h, {"tiled": 0, "per_cell": 1, "tiled_batched": 2}[kind]))
 
+    def set_external_elastic(self, on: bool = True) -> None:
+        """E_el is supplied by the caller (e.g. SpectralElasticity.couple) and
+        drives the interfaces; the model's elastic proxy is not run."""
+        check(lib().gpk_grid_set_external_elastic(self._h, 1 if on else 0))
+
     def geometry(self) -> None:
         """Mask and geometry of the current labels, without stepping."""
         check(lib().gpk_grid_geometry(self._h))

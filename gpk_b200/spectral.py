@@ -54,6 +54,15 @@ class SpectralElasticity:
         except Exception:
             pass
 
+    def couple(self, grid, matrix_label: int = 0, want_residual: bool = False):
+        """Elastic energy density of the grid's current labels (variant 0 =
+        every label but matrix_label) written into grid's E_el field, on the
+        grid's stream; returns the residual when asked."""
+        res = C.c_double(0.0)
+        check(lib().gpk_spectral_couple_grid(self._h, grid._h, int(matrix_label),
+                                             C.byref(res) if want_residual else None))
+        return res.value if want_residual else None
+
     def device_bytes(self) -> int:
         cells, nb = C.c_int64(), C.c_int64()
         check(lib().gpk_spectral_info(self._h, C.byref(cells), C.byref(nb)))

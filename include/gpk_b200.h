@@ -244,6 +244,13 @@ int gpk_grid_wave_stats(gpk_grid* grid, uint64_t out[8]);
  * cell kernels, 2 = tiled kernels with one label per geometry bitmap batch
  * (exercises the many-label path of the tiled geometry kernel).           */
 int gpk_grid_set_geometry_kernel(gpk_grid* grid, int kind);
+/* External elastic energy (no counterpart in the reference): when on, the
+ * E_el field is what the caller last wrote (an upload, a device write, or
+ * gpk_spectral_couple_grid) and enters every interface velocity as
+ * E_el(product neighbour) - E_el(cell) (src/gpk_physics.cpp:118-125), even
+ * when the thermodynamic model's elastic flag is off; the model's own elastic
+ * proxy (src/gpk_physics.cpp:10-63) is not run.                            */
+int gpk_grid_set_external_elastic(gpk_grid* grid, int on);
 
 #ifdef __cplusplus
 }

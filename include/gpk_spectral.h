@@ -31,6 +31,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "gpk_b200.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -59,6 +61,14 @@ int gpk_spectral_solve(gpk_spectral* s, const double* fractions, double* driving
 /* The same with host pointers (copies in and out; returns when done).     */
 int gpk_spectral_solve_host(gpk_spectral* s, const double* fractions, double* driving, double* energy, double* hydro,
                             double* residual);
+/* Coupling to a grid (no counterpart in the reference): variant 0 = every
+ * cell whose label is not matrix_label (variants 1, 2 empty), solved on the
+ * grid's stream, the elastic energy density written into the grid's E_el
+ * field (converted to float for a GPK_PREC_F32 grid).  With
+ * gpk_grid_set_external_elastic on, the next step drives the interfaces by
+ * it.  The solve's shape must be the grid's ((Nz, Ny, Nx), or (Ny, Nx) for
+ * Nz = 1).  residual (host) may be NULL.                                   */
+int gpk_spectral_couple_grid(gpk_spectral* s, gpk_grid* grid, int32_t matrix_label, double* residual);
 /* Cells N = product of the extents; device bytes held by the handle.      */
 int gpk_spectral_info(const gpk_spectral* s, int64_t* cells, int64_t* device_bytes);
 
