@@ -215,18 +215,18 @@ def spectral_measurement(with_cpu: bool):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / 10
     cells = n ** 3
-    # algorithmic bytes per cell: eigenstrain 24 + 48, Green's kernel 48 + 96,
-    # epilogue 96 + 24 + 40, and 9 complex FP64 transforms of one read and one
-    # write of 16 bytes each (288)
-    per_cell = 72 + 144 + 160 + 288
+    # algorithmic bytes per cell: eigenstrain 24 + 24, forward half-spectrum
+    # transforms 24 + 24, Green's kernel 24 + 48, inverse transforms 48 + 48,
+    # epilogue 48 + 24 + 40
+    per_cell = 48 + 48 + 72 + 96 + 112
     peak, peak_kind = _peaks()
     achieved = per_cell * cells / (ms / 1e3) / 1e9
-    res = {"workload": "spectral elasticity 128^3 FP64 (3 fwd + 6 inv Z2Z cuFFT, Green's-function and "
-                       "epilogue kernels)", "ms_per_solve": ms, "cells_per_s": cells / (ms / 1e3),
+    res = {"workload": "spectral elasticity 128^3 FP64 (3 D2Z + 6 Z2D cuFFT on half spectra, Green's-function "
+                       "and epilogue kernels)", "ms_per_solve": ms, "cells_per_s": cells / (ms / 1e3),
            "residual": residual, "algorithmic_bytes_per_cell": per_cell,
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                         "frac": achieved / peak, "peak_kind": peak_kind},
-           "own_kernels_per_solve": 4, "library_calls_per_solve": "2 cufftExecZ2Z (batched 3 and 6)"}
+           "own_kernels_per_solve": 4, "library_calls_per_solve": "cufftExecD2Z (batch 3), cufftExecZ2D (batch 6)"}
     if with_cpu:
         import types
         from oracle import spectral_oracle

@@ -16,10 +16,13 @@
  *   hydro      = trace(sigma) / 3
  *   residual   = rms |k . sigma^(k)| / rms |b(k)|  (the reference's audit)
  *
- * Transforms are complex-to-complex FP64 cuFFT, and the strain is the real
- * part of the inverse transform, as in the reference.  Everything else (the
- * eigenstrain assembly, the per-wave-vector 3x3 acoustic-tensor solve, the
- * stress/energy epilogue, the residual reduction) is hand-written CUDA.
+ * Transforms are real-to-complex / complex-to-real FP64 cuFFT on half
+ * spectra; the strain is the inverse transform of the Hermitian part of the
+ * reference's strain transform, which is exactly what the reference's
+ * `ifftn(...).real` keeps (the two differ only on the Nyquist planes of even
+ * extents, handled explicitly).  Everything else (the eigenstrain assembly,
+ * the per-wave-vector 3x3 acoustic-tensor solve, the stress/energy epilogue,
+ * the residual reduction) is hand-written CUDA.
  * Results agree with the reference to about 1e-15 relative (FFT rounding).
  *
  * All functions return GPK_OK (0) or a GPK_ERR_* status of gpk_b200.h; the
