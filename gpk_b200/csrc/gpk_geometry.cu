@@ -495,23 +495,27 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) k_geometry_til
                 if (lane < cnt) bm[(L0 + lane) * S::NROWP + r] = mine;
             }
         }
-        // cells of the batch
-        int nbc = ncell;
-        if (nbatch > 1) {
-            int flags[PER];
-            int cnt = 0;
+        // cells of the batch, grouped by label (flat order within a label), so
+        // that a warp's cells share a label and skip the same empty rows
+        int nbc = 0;
+        {
+            for (int L = lb0; L < lb0 + nb; ++L) {
+                int flags[PER];
+                int cnt = 0;
 #pragma unroll
-            for (int k = 0; k < PER; ++k) {
-                const int e = tid * PER + k;
-                flags[k] = e < ncell && (int)cli[e] >= lb0 && (int)cli[e] < lb0 + nb;
-                cnt += flags[k];
+                for (int k = 0; k < PER; ++k) {
+                    const int e = tid * PER + k;
+                    flags[k] = e < ncell && (int)cli[e] == L;
+                    cnt += flags[k];
+                }
+                int ex, total;
+                BS(scan).ExclusiveSum(cnt, ex, total);
+#pragma unroll
+                for (int k = 0; k < PER; ++k)
+                    if (flags[k]) bcell[nbc + ex++] = (int16_t)(tid * PER + k);
+                nbc += total;
+                __syncthreads();
             }
-            int ex, total;
-            BS(scan).ExclusiveSum(cnt, ex, total);
-#pragma unroll
-            for (int k = 0; k < PER; ++k)
-                if (flags[k]) bcell[ex++] = (int16_t)(tid * PER + k);
-            nbc = total;
         }
         __syncthreads();
 
@@ -527,7 +531,7 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) k_geometry_til
         for (int s = 0; s < 4; ++s) {
             const int kk = tid + nact * s;
             const bool valid = s < slots && tid < nact && kk < nbc;
-            const int k = valid ? (nbatch > 1 ? bcell[kk] : kk) : (nbatch > 1 ? bcell[0] : 0);
+            const int k = valid ? bcell[kk] : bcell[0];
             const int c = cells[k];
             const int cx = c % S::TX, cy = (c / S::TX) % S::TY, cz = c / (S::TX * S::TY);
             // bitmap word of halo row (cz + dz + R, cy + dy + R): bmrow + (dz+R)*HY + (dy+R)
