@@ -401,10 +401,23 @@ def run_gpu_arm(args):
     check(lib().gpk_device_init(local))
     torch.cuda.set_device(local)
 
-    phi, g = voronoi(SIZE, SIZE, SIZE, GRAINS, SEED + rank)
     grid = GPKGrid(SIZE, SIZE, SIZE, 1.0, thermo.isotropic(1.0, 1.0), 0.0, SIGMA)
-    grid.set("phi", phi); grid.set("g", g); grid.set("alpha", 1.0)
     stream = torch.cuda.ExternalStream(grid.stream_ptr())
+    # the seeded Voronoi polycrystal, built on the device (cell for cell the
+    # host construction, which is timed once beside it)
+    i0, i1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    i0.record(stream)
+    grid.voronoi(GRAINS, SEED + rank)
+    i1.record(stream)
+    i1.synchronize()
+    init = {"workload": f"periodic Voronoi polycrystal {SIZE}^3, {GRAINS} grains, with connectivity normalisation",
+            "device_ms": i0.elapsed_time(i1)}
+    if rank == 0 and not args.no_cpu:
+        t0 = time.perf_counter()
+        voronoi(SIZE, SIZE, SIZE, GRAINS, SEED + rank)
+        init["host_ms"] = (time.perf_counter() - t0) * 1e3
+        init["host_threads"] = os.cpu_count()
+    grid.set("alpha", 1.0)
     # Input preparation: from a fresh tessellation no cell crosses before
     # step 8 (|v| dt <= dx/8), so the state is first evolved SETTLE steps;
     # the timed steps then run the full pipeline, crossings and remap included.
@@ -529,7 +542,7 @@ def run_gpu_arm(args):
                 "stages_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in stages.items()},
                 "interface_fraction": iface, "counters_last_step": list(grid.counters()),
                 "per_step_topology": waves,
-                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "spectral": spectral, "batched": batched, "adjoint": adjoint, "coupled": coupled,
+                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "spectral": spectral, "batched": batched, "adjoint": adjoint, "coupled": coupled, "init": init,
                 "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": io,
                         "d2h_bytes_per_step": io, "steps": e2e_steps,
                         "path": "GPKGrid drop-in semantics: upload phi/alpha/g, step, download phi/alpha/g"}}

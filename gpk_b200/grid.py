@@ -217,6 +217,14 @@ class GPKGrid:
         drives the interfaces; the model's elastic proxy is not run."""
         check(lib().gpk_grid_set_external_elastic(self._h, 1 if on else 0))
 
+    def voronoi(self, n_grains: int, seed: int = 42) -> int:
+        """Fills phi and g with the periodic Voronoi polycrystal of
+        gpk_b200.voronoi(Nz, Ny, Nx, n_grains, seed), built on the device;
+        returns the number of tie cells the connectivity step moved."""
+        moved = C.c_int()
+        check(lib().gpk_grid_voronoi(self._h, int(n_grains), int(seed), C.byref(moved)))
+        return moved.value
+
     def geometry(self) -> None:
         """Mask and geometry of the current labels, without stepping."""
         check(lib().gpk_grid_geometry(self._h))

@@ -23,6 +23,13 @@ extern "C" {
  * make every label one face-connected component.                          */
 int gpk_voronoi_init(int Nz, int Ny, int Nx, int n_seeds, uint64_t seed, int32_t* phi, float* g, int* reassigned);
 
+/* The same polycrystal built on the device, straight into a grid's phi and
+ * g fields (and its label counts): cell for cell the result of
+ * gpk_voronoi_init for the grid's dimensions, n_seeds and seed.  Returns a
+ * GPK_* status (gpk_b200.h).                                               */
+typedef struct gpk_grid gpk_grid;
+int gpk_grid_voronoi(gpk_grid* grid, int n_seeds, uint64_t seed, int* reassigned);
+
 #ifdef __cplusplus
 }
 #endif
