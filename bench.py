@@ -134,7 +134,8 @@ def _allmax(v: float, ws: int) -> float:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -241,15 +242,20 @@ def spectral_measurement(with_cpu: bool):
     return res
 
 
-def batched_measurement(n_inst: int = 512, steps: int = 10, warmup: int = 3):
+def batched_measurement(n_inst: int = 512, steps: int = 10, warmup: int = 3, ws: int = 1, rank: int = 0):
     """The lamellar-precipitate sweep: n_inst 2-D instances of sides
     U{64..512} (FP64, OstwaldThermo), advanced together by the batch engine
-    and, for comparison, as a plain loop over instances (one worker)."""
+    and, for comparison, as a plain loop over instances (one worker).  With
+    ws > 1 ranks the instances are sharded by cell count (no exchange); the
+    time is the max over ranks and the plain loop is not run."""
     import torch
     from gpk_b200 import GPKBatch
-    from gpk_b200.sweep import lamellar_grid
-    grids = [lamellar_grid(5000 + i, precision="f64")[0] for i in range(n_inst)]
-    cells = sum(g.Nx * g.Ny * g.Nz for g in grids)
+    from gpk_b200.sweep import lamellar_grid, lamellar_side, shard
+    seeds = [5000 + i for i in range(n_inst)]
+    sizes = [lamellar_side(s) ** 2 for s in seeds]
+    mine = shard(sizes, ws)[rank] if ws > 1 else list(range(n_inst))
+    grids = [lamellar_grid(seeds[i], precision="f64")[0] for i in mine]
+    cells = sum(sizes)
     streams = [torch.cuda.ExternalStream(g.stream_ptr()) for g in grids]
     batch = GPKBatch(grids)
     workers, tune_steps = batch.autotune(trial_steps=1)
@@ -272,20 +278,24 @@ def batched_measurement(n_inst: int = 512, steps: int = 10, warmup: int = 3):
         e1.synchronize()
         return e0.elapsed_time(e1), sum(g.launch_count() for g in grids) - l0
 
+    _barrier(ws)
     ms_b, launches = timed(steps)
-    batch.workers = 1
-    ms_p, _ = timed(steps)
+    ms_b = _allmax(ms_b, ws)
+    res = {"workload": f"{n_inst} lamellar-precipitate 2-D instances, sides U{{64..512}}, stripe thickness "
+                       "U{4..16}, spacing/thickness U[2,12], OstwaldThermo, FP64, sigma 1.5",
+           "instances": n_inst, "cells": cells, "steps": steps, "warmup": warmup + tune_steps,
+           "value": cells * steps / (ms_b / 1e3), "unit": "cell-updates/s", "ms": ms_b,
+           "workers": workers, "gpu_launches_rank0": launches, "ranks": ws,
+           "how": "native worker pool, one CUDA stream per instance, worker count autotuned; plain = "
+                  "the same instances stepped one after another"}
+    if ws == 1:
+        batch.workers = 1
+        ms_p, _ = timed(steps)
+        res.update({"plain_value": cells * steps / (ms_p / 1e3), "plain_ms": ms_p, "speedup_vs_plain": ms_p / ms_b})
     batch.close()
     for g in grids:
         g.close()
-    return {"workload": f"{n_inst} lamellar-precipitate 2-D instances, sides U{{64..512}}, stripe thickness "
-                        "U{4..16}, spacing/thickness U[2,12], OstwaldThermo, FP64, sigma 1.5",
-            "instances": n_inst, "cells": cells, "steps": steps, "warmup": warmup + tune_steps,
-            "value": cells * steps / (ms_b / 1e3), "unit": "cell-updates/s", "ms": ms_b,
-            "plain_value": cells * steps / (ms_p / 1e3), "plain_ms": ms_p, "speedup_vs_plain": ms_p / ms_b,
-            "workers": workers, "gpu_launches": launches,
-            "how": "native worker pool, one CUDA stream per instance, worker count autotuned; plain = "
-                   "the same instances stepped one after another"}
+    return res
 
 
 def adjoint_measurement(with_cpu: bool, evals: int = 20):
@@ -516,15 +526,16 @@ def run_gpu_arm(args):
         except Exception as exc:  # the GPU number stands on its own
             cpu = {"error": str(exc)}
     spectral = batched = adjoint = coupled = None
+    # the sweep shards over all ranks (same collective order on every rank)
+    try:
+        batched = batched_measurement(ws=ws, rank=rank)
+    except Exception as exc:
+        batched = {"error": str(exc)}
     if rank == 0:
         try:
             spectral = spectral_measurement(not args.no_cpu and ws == 1)
         except Exception as exc:  # reported, never silent
             spectral = {"error": str(exc)}
-        try:
-            batched = batched_measurement()
-        except Exception as exc:
-            batched = {"error": str(exc)}
         try:
             adjoint = adjoint_measurement(not args.no_cpu and ws == 1)
         except Exception as exc:

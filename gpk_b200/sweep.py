@@ -30,6 +30,24 @@ def lamellar_instance(seed: int, side_range=(64, 512)) -> dict:
     return {"side": side, "h": h, "ratio": ratio, "d": d, "phi": phi, "c": c}
 
 
+def lamellar_side(seed: int, side_range=(64, 512)) -> int:
+    """The side of instance `seed` (its first random draw), without building it."""
+    return int(np.random.default_rng(seed).integers(side_range[0], side_range[1] + 1))
+
+
+def shard(sizes, n: int) -> list:
+    """Instances split over n ranks with balanced work: largest first, each
+    to the least-loaded rank (ties to the lower rank); each part ascending."""
+    order = sorted(range(len(sizes)), key=lambda i: (-sizes[i], i))
+    load = [0] * n
+    parts = [[] for _ in range(n)]
+    for i in order:
+        r = min(range(n), key=lambda q: (load[q], q))
+        parts[r].append(i)
+        load[r] += sizes[i]
+    return [sorted(p) for p in parts]
+
+
 def lamellar_grid(seed: int, sigma: float = 1.5, precision: str = "f64", side_range=(64, 512)):
     """A GPKGrid holding instance `seed` (OstwaldThermo, M0 = sigma0 = 1,
     Omega = 10, D = 0.1, dx = 1)."""
