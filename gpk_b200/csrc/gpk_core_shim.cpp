@@ -7,6 +7,13 @@
 // and downloads before each callback and at the end.  Host-side diagnostics
 // (phase_volume, n_grains, ...) read the mirrors exactly as the reference's
 // own diagnostics read its vectors (src/gpk_simulation.cpp:78-144).
+#include <condition_variable>
+#include <cstdlib>
+#include <deque>
+#include <exception>
+#include <memory>
+#include <mutex>
+#include <thread>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -303,11 +310,81 @@ float GPKGrid::step(float dt, float dt_cap) {
     return (float)used;
 }
 
+namespace {
+
+// Callbacks on a writer thread, in order, each on a snapshot copy of the
+// grid taken at its step: the snapshot I/O of a driver (CSV/VTK writers in
+// its callback) then overlaps the following steps.  At most two snapshots
+// wait at a time.  An exception from a callback stops later callbacks and is
+// rethrown by run().
+class CallbackWriter {
+public:
+    explicit CallbackWriter(const std::function<void(const GPKGrid&, int)>& cb) : cb_(cb) {
+        thread_ = std::thread([this] { loop(); });
+    }
+    ~CallbackWriter() { finish(); }
+    void push(std::unique_ptr<GPKGrid> g, int step) {
+        std::unique_lock<std::mutex> lk(m_);
+        space_.wait(lk, [this] { return q_.size() < 2; });
+        q_.emplace_back(std::move(g), step);
+        ready_.notify_one();
+    }
+    // waits for every queued callback; rethrows the first callback error
+    void finish() {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            if (done_) return;
+            done_ = true;
+        }
+        ready_.notify_all();
+        thread_.join();
+    }
+    std::exception_ptr error() const { return err_; }
+
+private:
+    void loop() {
+        while (true) {
+            std::pair<std::unique_ptr<GPKGrid>, int> item;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                ready_.wait(lk, [this] { return done_ || !q_.empty(); });
+                if (q_.empty()) return;
+                item = std::move(q_.front());
+                q_.pop_front();
+                space_.notify_one();
+            }
+            if (!err_) {
+                try {
+                    cb_(*item.first, item.second);
+                } catch (...) {
+                    err_ = std::current_exception();
+                }
+            }
+        }
+    }
+    const std::function<void(const GPKGrid&, int)>& cb_;
+    std::deque<std::pair<std::unique_ptr<GPKGrid>, int>> q_;
+    std::mutex m_;
+    std::condition_variable ready_, space_;
+    bool done_ = false;
+    std::exception_ptr err_;
+    std::thread thread_;
+};
+
+bool async_callbacks() {
+    const char* e = std::getenv("GPK_ASYNC_CALLBACKS");
+    return e && e[0] == '1';
+}
+
+}  // namespace
+
 int GPKGrid::run(double t_end, float dt, std::function<void(const GPKGrid&, int)> cb, int cb_interval) {
     push_thermo();
     push_state();
     int step_count = 0;
     double t = time;
+    std::unique_ptr<CallbackWriter> writer;
+    if (cb && async_callbacks()) writer.reset(new CallbackWriter(cb));
     while (t < t_end) {
         const float remaining = static_cast<float>(t_end - t);
         double used = 0.0;
@@ -317,10 +394,15 @@ int GPKGrid::run(double t_end, float dt, std::function<void(const GPKGrid&, int)
         ++step_count;
         if (cb && step_count % cb_interval == 0) {
             pull_state();
-            cb(*this, step_count);
+            if (writer) writer->push(std::unique_ptr<GPKGrid>(new GPKGrid(*this)), step_count);
+            else cb(*this, step_count);
         }
     }
     pull_state();
+    if (writer) {
+        writer->finish();
+        if (writer->error()) std::rethrow_exception(writer->error());
+    }
     return step_count;
 }
 

@@ -194,6 +194,12 @@ public:
 
     // The device grid behind this object (no counterpart in the reference).
     gpk_grid* device_grid() const { return dev(); }
+    // run() with a callback: when the environment variable
+    // GPK_ASYNC_CALLBACKS is 1, each callback receives a snapshot copy of the
+    // grid on a writer thread (in order) while the steps go on, so a driver's
+    // snapshot output overlaps the computation; run() returns after the last
+    // callback and rethrows a callback's exception.  (No counterpart in the
+    // reference, whose callbacks run between steps.)
     // Host members -> device, and device -> host members, for code that
     // advances device_grid() directly (e.g. a gpk_batch); step() and run()
     // do both themselves.  No counterpart in the reference.
