@@ -1,0 +1,152 @@
+"""Generates tests/golden/alcu_transport.npz from the reference itself.
+
+Imports the per-step transport and remap functions of the reference's Al-Cu
+material module, scripts/run_alcu_gpk_microstructure.py:
+
+  neighbor_competitor (260-276), precip_fraction (675-676),
+  diffuse_conservative_subcycled (679-699),
+  conservative_partition_transfer (702-737),
+  interface_matrix_composition (740-755),
+  conservative_gaussian_remap (562-594),
+
+and runs them on seeded states shaped like the module's own: int8 labels
+0..3 (alpha-Al and three theta-prime variants) with plates and spheres, one
+crossing a periodic face (scipy's `label` splits it there), two touching
+plates of different variants, single-cell specks and jagged interfaces as
+left by committed crossings.  Run it where the reference tree is present:
+
+    python tests/golden/make_alcu_golden.py [path/to/reference]
+"""
+from __future__ import annotations
+
+import importlib.util
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "alcu_transport.npz")
+
+
+def load_reference(root: str):
+    path = os.path.join(root, "scripts", "run_alcu_gpk_microstructure.py")
+    spec = importlib.util.spec_from_file_location("gpk_ref_alcu", path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["gpk_ref_alcu"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def ellipsoid(labels, centre, axes, value):
+    shape = labels.shape
+    coords = np.indices(shape)
+    d2 = 0.0
+    for a in range(len(shape)):
+        delta = np.abs(coords[a] - centre[a])
+        delta = np.minimum(delta, shape[a] - delta)  # minimum image
+        d2 = d2 + (delta / axes[a]) ** 2
+    labels[d2 <= 1.0] = value
+
+
+def make_labels(shape, rng):
+    labels = np.zeros(shape, dtype=np.int8)
+    nd = len(shape)
+    big = max(shape) / 5.0
+    if nd == 2:
+        ellipsoid(labels, (shape[0] // 4, shape[1] // 4), (big, big / 4), 1)
+        ellipsoid(labels, (0, shape[1] // 2), (big / 3, big), 2)            # crosses axis-0 face
+        ellipsoid(labels, (3 * shape[0] // 4, 2 * shape[1] // 3), (big / 1.5, big / 1.5), 1)
+        # two touching plates of different variants
+        labels[shape[0] // 2:shape[0] // 2 + 3, 4:16] = 2
+        labels[shape[0] // 2 + 3:shape[0] // 2 + 5, 6:14] = 1
+    else:
+        ellipsoid(labels, (shape[0] // 4, shape[1] // 4, shape[2] // 4), (big / 4, big, big), 1)
+        ellipsoid(labels, (shape[0] // 2, 0, shape[2] // 2), (big, big / 4, big), 2)  # crosses axis-1 face
+        ellipsoid(labels, (3 * shape[0] // 4, 2 * shape[1] // 3, 3 * shape[2] // 4), (big, big, big / 4), 3)
+        labels[2:5, shape[1] // 2:shape[1] // 2 + 6, 2:8] = 2
+        labels[5:7, shape[1] // 2 + 1:shape[1] // 2 + 5, 3:7] = 3
+    # jagged interfaces: random flips across matrix/precipitate faces
+    for _ in range(2):
+        nb_lab = np.zeros_like(labels)
+        for axis in range(nd):
+            for s in (-1, 1):
+                r = np.roll(labels, s, axis=axis)
+                nb_lab = np.where((nb_lab == 0) & (r > 0), r, nb_lab)
+        grow = (labels == 0) & (nb_lab > 0) & (rng.random(shape) < 0.25)
+        labels[grow] = nb_lab[grow]
+        has_matrix = np.zeros(shape, dtype=bool)
+        for axis in range(nd):
+            for s in (-1, 1):
+                has_matrix |= np.roll(labels, s, axis=axis) == 0
+        shrink = (labels > 0) & has_matrix & (rng.random(shape) < 0.15)
+        labels[shrink] = 0
+    # isolated specks (components of one cell are left alone by the remap)
+    for _ in range(4):
+        idx = tuple(int(rng.integers(0, n)) for n in shape)
+        labels[idx] = int(rng.integers(1, 4 if nd == 3 else 3))
+    return labels
+
+
+def make_state(shape, rng, ref, p):
+    labels = make_labels(shape, rng)
+    alpha = np.ones(shape)
+    mask, comp = ref.neighbor_competitor(labels)
+    alpha[mask] = rng.uniform(0.05, 1.0, size=int(mask.sum()))
+    precip = labels > 0
+    f0 = float(np.mean(precip))
+    cm0 = (p.c0 - f0 * p.c_theta) / (1.0 - f0)
+    ctot = np.full(shape, cm0) * (1.0 + 0.05 * rng.standard_normal(shape))
+    ctot[precip] = p.c_theta
+    return labels, alpha, ctot
+
+
+def main(root: str) -> None:
+    ref = load_reference(root)
+    rng = np.random.default_rng(20240611)
+    out = {}
+    cases = [("2d", (64, 60), 0.5e-9), ("3d", (24, 26, 22), 1.5e-9)]
+    for name, shape, dx in cases:
+        p = ref.Parameters()
+        p.dx = dx
+        labels, alpha, ctot = make_state(shape, rng, ref, p)
+        mask, comp = ref.neighbor_competitor(labels)
+        fp = ref.precip_fraction(labels, alpha, comp)
+        matrix = np.maximum(1.0 - fp, 1e-8)
+        cm = np.where(matrix > 1e-7, (ctot - fp * p.c_theta) / matrix, p.c_matrix_eq)
+        cm = np.clip(cm, 0.0, p.c_theta)
+        trace = ref.interface_matrix_composition(cm, fp, p)
+        dt = 10.0
+        c_new, cm_last, substeps = ref.diffuse_conservative_subcycled(ctot.copy(), fp, p, dt)
+        out.update({f"{name}_labels": labels, f"{name}_alpha": alpha, f"{name}_ctot": ctot,
+                    f"{name}_dx": np.float64(dx), f"{name}_dt": np.float64(dt),
+                    f"{name}_mask": mask, f"{name}_competitor": comp, f"{name}_fprec": fp,
+                    f"{name}_cm": cm, f"{name}_trace": trace, f"{name}_diffused": c_new,
+                    f"{name}_cm_last": cm_last, f"{name}_substeps": np.int64(substeps)})
+        # partition transfer: growth (correction < 0, capacity branch),
+        # dissolution (correction > 0) and no change (early return)
+        for kind in ("grow", "shrink", "none"):
+            step = np.zeros(shape)
+            if kind == "grow":
+                step[mask] = rng.uniform(0.0, 0.3, size=int(mask.sum()))
+            elif kind == "shrink":
+                step[mask] = -rng.uniform(0.0, 0.3, size=int(mask.sum()))
+            new_fp = np.clip(fp + step, -0.2, 1.2)
+            c = ctot.copy()
+            ref.conservative_partition_transfer(c, fp, new_fp, trace, p)
+            out[f"{name}_pt_{kind}_new"] = new_fp
+            out[f"{name}_pt_{kind}_out"] = c
+        for sigma in (0.70, 1.2):
+            lab = labels.copy()
+            al = alpha.copy()
+            n = ref.conservative_gaussian_remap(lab, al, sigma)
+            tag = f"{name}_cgr_{int(round(sigma * 100))}"
+            out[f"{tag}_labels"] = lab
+            out[f"{tag}_alpha"] = al
+            out[f"{tag}_changed"] = np.int64(n)
+    np.savez_compressed(OUT, **out)
+    print("wrote", OUT, {k: v.shape for k, v in out.items() if np.ndim(v)})
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

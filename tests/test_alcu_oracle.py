@@ -1,0 +1,115 @@
+"""The Al-Cu transport/remap oracle against the reference's own outputs.
+
+tests/golden/alcu_transport.npz holds what the reference's functions
+(scripts/run_alcu_gpk_microstructure.py:260-276, 562-594, 675-755) returned
+on seeded 2-D and 3-D states (make_alcu_golden.py).  The numpy restatement
+in oracle/alcu_oracle.py must reproduce every array bit for bit.  Its three
+library primitives are checked against the installed numpy and scipy: the
+pairwise sum against `np.sum`, the wrapped Gaussian against
+`scipy.ndimage.gaussian_filter`, the components against `scipy.ndimage.label`.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import alcu_oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "alcu_transport.npz")
+
+
+def params(z, name):
+    return O.AlCuParams(dx=float(z[f"{name}_dx"]))
+
+
+@pytest.fixture(scope="module")
+def z():
+    return np.load(GOLDEN)
+
+
+def same(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return a.shape == b.shape and a.dtype.kind == b.dtype.kind and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+@pytest.mark.parametrize("n", [1, 7, 8, 128, 129, 1000, 4097, 33 * 35 * 37, 64 ** 3])
+def test_pairwise_sum_is_numpy_sum(n):
+    a = np.random.default_rng(n).standard_normal(n) * 10.0 ** np.random.default_rng(n + 1).integers(-8, 8, n)
+    assert O.pairwise_sum(a) == float(np.sum(a))
+
+
+@pytest.mark.parametrize("sigma", [0.1, 0.7, 0.75, 0.85, 1.2, 2.0, 8.0 / 3.0])
+@pytest.mark.parametrize("shape", [(23, 17), (11, 13, 9), (5, 40)])
+def test_gaussian_is_scipy(sigma, shape):
+    ndi = pytest.importorskip("scipy.ndimage")
+    rng = np.random.default_rng(int(sigma * 100) + sum(shape))
+    for a in (rng.random(shape), (rng.random(shape) < 0.3).astype(float)):
+        assert same(O.gaussian_filter_wrap(a, sigma), ndi.gaussian_filter(a, sigma, mode="wrap"))
+
+
+@pytest.mark.parametrize("shape", [(40, 37), (17, 19, 23)])
+def test_components_and_dilation_are_scipy(shape):
+    ndi = pytest.importorskip("scipy.ndimage")
+    m = np.random.default_rng(len(shape)).random(shape) < 0.45
+    cc, n = ndi.label(m)
+    c2, n2 = O.face_components(m)
+    assert n == n2 and np.array_equal(cc, c2)
+    box = ndi.binary_dilation(m, structure=np.ones((3,) * m.ndim, bool), iterations=1, border_value=0)
+    assert np.array_equal(O.dilate_box(m), box)
+
+
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_oracle_competitor_fraction_composition(z, name):
+    p = params(z, name)
+    mask, comp = O.neighbor_competitor(z[f"{name}_labels"])
+    assert np.array_equal(mask, z[f"{name}_mask"]) and np.array_equal(comp, z[f"{name}_competitor"])
+    fp = O.precip_fraction(z[f"{name}_labels"], z[f"{name}_alpha"], comp)
+    assert same(fp, z[f"{name}_fprec"])
+    cm = O.matrix_composition(z[f"{name}_ctot"], fp, p)
+    assert same(cm, z[f"{name}_cm"])
+    assert same(O.interface_matrix_composition(cm, fp, p), z[f"{name}_trace"])
+
+
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_oracle_diffusion(z, name):
+    p = params(z, name)
+    c, cm, sub = O.diffuse_conservative_subcycled(z[f"{name}_ctot"].copy(), z[f"{name}_fprec"], p,
+                                                  float(z[f"{name}_dt"]))
+    assert sub == int(z[f"{name}_substeps"])
+    assert same(c, z[f"{name}_diffused"]) and same(cm, z[f"{name}_cm_last"])
+
+
+@pytest.mark.parametrize("kind", ["grow", "shrink", "none"])
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_oracle_partition_transfer(z, name, kind):
+    p = params(z, name)
+    c = z[f"{name}_ctot"].copy()
+    O.conservative_partition_transfer(c, z[f"{name}_fprec"], z[f"{name}_pt_{kind}_new"], z[f"{name}_trace"], p)
+    assert same(c, z[f"{name}_pt_{kind}_out"])
+
+
+def test_oracle_partition_transfer_errors():
+    p = O.AlCuParams()
+    shape = (12, 10)
+    old = np.zeros(shape)
+    new = np.zeros(shape)
+    new[5, 5] = 0.5  # half a cell of theta-prime from a field without Cu above equilibrium
+    c = np.full(shape, -0.5)
+    with pytest.raises(RuntimeError, match="insufficient matrix Cu"):
+        O.conservative_partition_transfer(c, old, new, np.full(shape, p.c_matrix_eq), p)
+    # everything becomes precipitate: no matrix left to draw from
+    c = np.full(shape, 0.2)
+    with pytest.raises(RuntimeError, match="empty matrix neighbourhood"):
+        O.conservative_partition_transfer(c, np.full(shape, 0.5), np.ones(shape), np.full(shape, 0.01), p)
+
+
+@pytest.mark.parametrize("sigma", [0.70, 1.2])
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_oracle_gaussian_remap(z, name, sigma):
+    lab = z[f"{name}_labels"].copy()
+    al = z[f"{name}_alpha"].copy()
+    n = O.conservative_gaussian_remap(lab, al, sigma)
+    tag = f"{name}_cgr_{int(round(sigma * 100))}"
+    assert n == int(z[f"{tag}_changed"])
+    assert np.array_equal(lab, z[f"{tag}_labels"]) and same(al, z[f"{tag}_alpha"])
