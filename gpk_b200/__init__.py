@@ -10,6 +10,7 @@ from .grid import GPKGrid, voronoi
 from ._lib import GPKError, lib
 from .spectral import SpectralElasticity, spectral_elasticity
 from .batch import GPKBatch
+from . import alcu
 
 __all__ = ["GPKGrid", "voronoi", "thermo", "GPKError", "lib", "SpectralElasticity", "spectral_elasticity",
-           "GPKBatch"]
+           "GPKBatch", "alcu"]

@@ -19,7 +19,14 @@ ERRORS = {
     1: "invalid argument", 2: "unsupported thermodynamic model", 3: "CUDA error",
     4: "out of device memory", 5: "label out of range", 6: "device wait timed out",
     7: "no usable CUDA device", 8: "device consistency check failed",
+    9: "no admissible result",
 }
+
+
+class CAlCuParams(C.Structure):
+    """gpk_alcu_params of include/gpk_alcu.h."""
+    _fields_ = [("dx", C.c_double), ("diffusivity", C.c_double), ("c_matrix_eq", C.c_double),
+                ("c_theta", C.c_double)]
 
 
 class GPKError(RuntimeError):
@@ -100,6 +107,21 @@ def lib() -> C.CDLL:
         "gpk_adjoint_set_target": ([vp, C.POINTER(dbl)], i32),
         "gpk_adjoint_forward": ([vp, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(dbl)], i32),
         "gpk_adjoint_gradient": ([vp, C.POINTER(dbl), C.POINTER(dbl), C.POINTER(dbl)], i32),
+        "gpk_alcu_create": ([i32, C.POINTER(i32), C.POINTER(CAlCuParams), C.POINTER(vp)], i32),
+        "gpk_alcu_destroy": ([vp], i32),
+        "gpk_alcu_set_params": ([vp, C.POINTER(CAlCuParams)], i32),
+        "gpk_alcu_set_stream": ([vp, vp], i32),
+        "gpk_alcu_gauss_taps": ([dbl, C.POINTER(dbl), i32, C.POINTER(i32)], i32),
+        "gpk_alcu_competitor": ([vp, vp, vp, vp], i32),
+        "gpk_alcu_precip_fraction": ([vp, vp, vp, vp, vp], i32),
+        "gpk_alcu_matrix_composition": ([vp, vp, vp, vp], i32),
+        "gpk_alcu_diffuse": ([vp, vp, vp, dbl, vp, C.POINTER(i32)], i32),
+        "gpk_alcu_partition_transfer": ([vp, vp, vp, vp, vp, C.POINTER(dbl), i32], i32),
+        "gpk_alcu_interface_composition": ([vp, vp, vp, vp, C.POINTER(dbl), i32], i32),
+        "gpk_alcu_gaussian_remap": ([vp, vp, vp, C.POINTER(dbl), i32, C.POINTER(i64)], i32),
+        "gpk_alcu_sum": ([vp, vp, C.POINTER(dbl)], i32),
+        "gpk_alcu_gaussian_filter": ([vp, vp, vp, C.POINTER(dbl), i32], i32),
+        "gpk_alcu_info": ([vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)
@@ -120,10 +142,10 @@ def exported_symbols() -> list:
     import re
     names = []
     inc = os.path.join(HERE, "..", "include")
-    for h in ("gpk_b200.h", "gpk_init.h", "gpk_spectral.h", "gpk_batch.h", "gpk_adjoint.h"):
+    for h in ("gpk_b200.h", "gpk_init.h", "gpk_spectral.h", "gpk_batch.h", "gpk_adjoint.h", "gpk_alcu.h"):
         text = open(os.path.join(inc, h)).read()
         names += re.findall(r"^\s*(?:const\s+)?\w[\w\s\*]*?\b(gpk_\w+)\s*\(", text, flags=re.M)
     return sorted(set(names))
 
 
-__all__ = ["lib", "check", "GPKError", "CThermoDesc", "exported_symbols"]
+__all__ = ["lib", "check", "GPKError", "CThermoDesc", "CAlCuParams", "exported_symbols"]

@@ -22,7 +22,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-prec-div=true",
               "-ftz=false", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-ffp-contract=off,-fopenmp,-O2"]
 SOURCES = ["gpk_capi.cu", "gpk_step.cu", "gpk_geometry.cu", "gpk_local.cu", "gpk_topology.cu", "gpk_spectral.cu",
-           "gpk_batch.cu", "gpk_adjoint.cu", "gpk_init_dev.cu", "gpk_init.cpp", "gpk_core_shim.cpp"]
+           "gpk_batch.cu", "gpk_adjoint.cu", "gpk_init_dev.cu", "gpk_alcu.cu", "gpk_init.cpp", "gpk_core_shim.cpp"]
 
 
 def _nvcc() -> str:

@@ -1,0 +1,1201 @@
+// gpk_alcu.cu — Al-Cu per-step Cu transport and Gaussian label remap (FP64, sm_100a).
+//
+// Restates the numpy/scipy functions the reference's Al-Cu driver runs once
+// per step (scripts/run_alcu_gpk_microstructure.py): neighbor_competitor
+// (260-276), precip_fraction (675-676), diffuse_conservative[_subcycled]
+// (679-699), conservative_partition_transfer (702-737),
+// interface_matrix_composition (740-755) and conservative_gaussian_remap
+// (562-594), bit for bit:
+//
+//  * elementwise arithmetic in numpy's operand order, built without FMA
+//    contraction; numpy's maximum/clip keep their own argument on ties;
+//  * np.sum of a float64 field = numpy's pairwise summation of the flattened
+//    array: leaves of at most 128 values, each summed by 8 running partials
+//    (here 8 lanes, combined ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7))), ranges
+//    above 128 split at half the length rounded down to a multiple of 8.  The
+//    tree depends on N only; the host cuts it at sizes 128 * 32^k, and each
+//    level is one launch (a thread per node walks its subtree);
+//  * scipy.ndimage.gaussian_filter(mode="wrap") = three periodic passes (axis
+//    0, 1, 2), each output x[i] w0 + (x[i-j] + x[i+j]) w_j added for
+//    j = r, ..., 1;
+//  * the remap's components (scipy `label`: face connectivity, no wrap,
+//    numbered by first cell) come from a union-find that links to the smaller
+//    root, so a component's root is its first cell.  The reference relabels
+//    components one after the other; a component reads and writes only cells
+//    of its 3^d dilation, so two components interact only when their
+//    dilations meet.  Components are scheduled in waves (the longest chain of
+//    earlier interacting components, relaxed to a fixed point over the cells
+//    where dilations meet); a wave's components run together and the result
+//    is that of the serial order.  Per wave: candidates compacted in cell
+//    order, scores evaluated per candidate from the component's indicator
+//    (the three passes restricted to the (2r+1)^d box, same operations), two
+//    stable radix sorts (score descending, then component), and the first
+//    `size` entries of each component's run take its label.
+//
+// Every kernel is HBM- or latency-bound FP64 work; none is a contraction.
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/gpk_alcu.h"
+#include "gpk_grid.h"
+
+namespace {
+
+#define ALCU_TRY(expr)                                                                 \
+    do {                                                                               \
+        cudaError_t _e = (expr);                                                       \
+        if (_e != cudaSuccess) {                                                       \
+            gpk_set_error(std::string(#expr " failed: ") + cudaGetErrorString(_e));    \
+            return GPK_ERR_CUDA;                                                       \
+        }                                                                              \
+    } while (0)
+
+struct Ext {
+    int e[3];        // extents (e[2] = 1 in 2-D)
+    long long st[3]; // strides of the C-order layout
+    int ndim;
+    long long N;
+};
+
+struct Taps {
+    double w[GPK_ALCU_MAX_RADIUS + 1];  // w[j]: the tap at offsets -j and +j
+    int r;
+};
+
+struct Phys {
+    double dx, D, ceq, ct;
+};
+
+__device__ __forceinline__ int wrapi(int x, int n) {
+    const int r = x % n;
+    return r < 0 ? r + n : r;
+}
+__device__ __forceinline__ void coords(const Ext& d, long long i, int x[3]) {
+    x[2] = (int)(i % d.e[2]);
+    const long long t = i / d.e[2];
+    x[1] = (int)(t % d.e[1]);
+    x[0] = (int)(t / d.e[1]);
+}
+// numpy's float maximum / clip (no NaN reaches these here): the first
+// argument is kept only when strictly beyond the bound
+__device__ __forceinline__ double np_max(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double np_clip(double x, double lo, double hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+#define GRID_STRIDE(i, n) \
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+// ---------------------------------------------------------------- elementwise
+
+__global__ void k_competitor(Ext d, const int8_t* __restrict__ lab, uint8_t* __restrict__ mask,
+                             int8_t* __restrict__ comp) {
+    GRID_STRIDE(i, d.N) {
+        int x[3];
+        coords(d, i, x);
+        const int8_t l = lab[i];
+        bool m = false, mat = false;
+        int s1 = 0, s2 = 0, s3 = 0;
+        for (int a = 0; a < d.ndim; ++a) {
+            for (int sgn = -1; sgn <= 1; sgn += 2) {
+                const int y = wrapi(x[a] + sgn, d.e[a]);
+                const int8_t nb = lab[i + (long long)(y - x[a]) * d.st[a]];
+                m |= nb != l;
+                mat |= nb == 0;
+                s1 += nb == 1;
+                s2 += nb == 2;
+                s3 += nb == 3;
+            }
+        }
+        // argmax over (s1, s2, s3), first maximum
+        int8_t c = 1;
+        int best = s1;
+        if (s2 > best) { c = 2; best = s2; }
+        if (s3 > best) { c = 3; }
+        if (l > 0 && mat) c = 0;
+        if (!m) c = l;
+        mask[i] = m ? 1 : 0;
+        comp[i] = c;
+    }
+}
+
+__global__ void k_precip_fraction(long long N, const int8_t* __restrict__ lab, const double* __restrict__ alpha,
+                                  const int8_t* __restrict__ comp, double* __restrict__ fp) {
+    GRID_STRIDE(i, N) fp[i] = lab[i] > 0 ? alpha[i] : (comp[i] > 0 ? 1.0 - alpha[i] : 0.0);
+}
+
+// matrix fraction max(1 - f, 1e-8) and the clipped lever-rule composition
+__device__ __forceinline__ void lever(double c, double f, const Phys& p, double& m, double& cm) {
+    m = np_max(1.0 - f, 1e-8);
+    const double raw = m > 1e-7 ? (c - f * p.ct) / m : p.ceq;
+    cm = np_clip(raw, 0.0, p.ct);
+}
+
+__global__ void k_matrix_composition(long long N, Phys p, const double* __restrict__ c, const double* __restrict__ f,
+                                     double* __restrict__ cm) {
+    GRID_STRIDE(i, N) {
+        double m, v;
+        lever(c[i], f[i], p, m, v);
+        cm[i] = v;
+    }
+}
+
+// one explicit substep of diffuse_conservative (lines 679-688)
+__global__ void k_diffuse(Ext d, Phys p, double dt, const double* __restrict__ c, const double* __restrict__ f,
+                          double* __restrict__ out, double* __restrict__ cm_out) {
+    GRID_STRIDE(i, d.N) {
+        int x[3];
+        coords(d, i, x);
+        double mc, cmc;
+        lever(c[i], f[i], p, mc, cmc);
+        const double nD = -p.D;
+        double dc = 0.0;
+        for (int a = 0; a < d.ndim; ++a) {
+            const long long ip = i + (long long)(wrapi(x[a] + 1, d.e[a]) - x[a]) * d.st[a];
+            const long long im = i + (long long)(wrapi(x[a] - 1, d.e[a]) - x[a]) * d.st[a];
+            double mp, cmp, mm, cmm;
+            lever(c[ip], f[ip], p, mp, cmp);
+            lever(c[im], f[im], p, mm, cmm);
+            const double mfp = 0.5 * (mc + mp);
+            double fpl = (nD * mfp) * (cmp - cmc);
+            fpl = fpl / p.dx;
+            const double mfm = 0.5 * (mm + mc);
+            double fmi = (nD * mfm) * (cmc - cmm);
+            fmi = fmi / p.dx;
+            dc = dc - (fpl - fmi) / p.dx;
+        }
+        out[i] = c[i] + dt * dc;
+        if (cm_out) cm_out[i] = cmc;
+    }
+}
+
+// ---------------------------------------------------------------- Gaussian
+
+// one periodic pass along `axis` of NF fields
+template <int NF>
+__global__ void k_gauss_pass(Ext d, int axis, Taps t, const double* __restrict__ a0, const double* __restrict__ a1,
+                             double* __restrict__ o0, double* __restrict__ o1) {
+    const int n = d.e[axis];
+    const long long s = d.st[axis];
+    GRID_STRIDE(i, d.N) {
+        int x[3];
+        coords(d, i, x);
+        const long long base = i - (long long)x[axis] * s;
+        double v0 = a0[i] * t.w[0];
+        double v1 = 0.0;
+        if (NF == 2) v1 = a1[i] * t.w[0];
+        for (int j = t.r; j >= 1; --j) {
+            const long long lo = base + (long long)wrapi(x[axis] - j, n) * s;
+            const long long hi = base + (long long)wrapi(x[axis] + j, n) * s;
+            v0 = v0 + (a0[lo] + a0[hi]) * t.w[j];
+            if (NF == 2) v1 = v1 + (a1[lo] + a1[hi]) * t.w[j];
+        }
+        o0[i] = v0;
+        if (NF == 2) o1[i] = v1;
+    }
+}
+
+// ---------------------------------------------------------------- numpy's pairwise sum
+
+// a field value, or (corr * w[i]) / wsum for the correction residue
+struct LoadF {
+    const double* a;
+    __device__ __forceinline__ double operator()(long long i) const { return a[i]; }
+};
+struct CorrF {
+    const double* w;
+    double corr, wsum;
+    __device__ __forceinline__ double operator()(long long i) const { return (corr * w[i]) / wsum; }
+};
+
+// 8 lanes per leaf: lane j holds numpy's running partial r[j]
+template <class F>
+__global__ void k_pw_leaves(F f, const int* __restrict__ start, const int* __restrict__ len, int L,
+                            double* __restrict__ out) {
+    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long leaf = gid >> 3;
+    const int lane = (int)(gid & 7);
+    const bool act = leaf < L;
+    const long long s = act ? start[leaf] : 0;
+    const int n = act ? len[leaf] : 0;
+    double r = 0.0;
+    if (act && n >= 8) {
+        r = f(s + lane);
+        const int end = n - n % 8;
+        for (int i = 8; i < end; i += 8) r = r + f(s + i + lane);
+    }
+    const unsigned full = 0xffffffffu;
+    const double t = r + __shfl_down_sync(full, r, 1);  // r0+r1, r2+r3, r4+r5, r6+r7 on even lanes
+    const double u = t + __shfl_down_sync(full, t, 2);  // (r0+r1)+(r2+r3), (r4+r5)+(r6+r7)
+    const double v = u + __shfl_down_sync(full, u, 4);  // lane 0 of the group: the 8-way total
+    if (act && lane == 0) {
+        double res;
+        if (n < 8) {
+            res = 0.0;
+            for (int i = 0; i < n; ++i) res = res + f(s + i);
+        } else {
+            res = v;
+            for (int i = n - n % 8; i < n; ++i) res = res + f(s + i);
+        }
+        out[leaf] = res;
+    }
+}
+
+// the pairwise tree of a range of n values whose subtrees of size <= t have
+// been summed into lower[k], lower[k + 1], ... (left to right)
+__device__ double pw_walk(long long n, long long t, const double* __restrict__ lower, int k) {
+    long long pend[40];
+    double part[40];
+    unsigned char state[40];
+    int sp = 0;
+    double v;
+    for (;;) {
+        while (n > t && sp < 40) {
+            long long n2 = n / 2;
+            n2 -= n2 % 8;
+            pend[sp] = n - n2;
+            state[sp] = 0;
+            ++sp;
+            n = n2;
+        }
+        v = lower[k++];
+        for (;;) {
+            if (sp == 0) return v;
+            if (state[sp - 1] == 0) {
+                part[sp - 1] = v;
+                state[sp - 1] = 1;
+                n = pend[sp - 1];
+                break;
+            }
+            v = part[sp - 1] + v;
+            --sp;
+        }
+    }
+}
+
+__global__ void k_pw_nodes(const int* __restrict__ node_n, const int* __restrict__ node_first, int M, long long t,
+                           const double* __restrict__ lower, double* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < M) out[k] = pw_walk(node_n[k], t, lower, node_first[k]);
+}
+
+// ---------------------------------------------------------------- partition transfer
+
+__global__ void k_pt_transfer(long long N, double ct, double* __restrict__ c, const double* __restrict__ oldf,
+                              const double* __restrict__ newf, const double* __restrict__ mcomp,
+                              double* __restrict__ tr, double* __restrict__ abs_tr) {
+    GRID_STRIDE(i, N) {
+        const double delta = np_clip(newf[i], 0.0, 1.0) - oldf[i];
+        const double t = delta * (ct - mcomp[i]);
+        tr[i] = t;
+        c[i] = c[i] + t;
+        abs_tr[i] = fabs(t);
+    }
+}
+
+// weight = G|transfer| * matrix (times the capacity above equilibrium when Cu
+// is drawn from the matrix)
+__global__ void k_pt_weight(long long N, double ceq, int draw, const double* __restrict__ g,
+                            const double* __restrict__ newf, const double* __restrict__ c, double* __restrict__ w,
+                            double* __restrict__ cap) {
+    GRID_STRIDE(i, N) {
+        const double m = np_clip(1.0 - newf[i], 0.0, 1.0);
+        double v = g[i] * m;
+        if (draw) {
+            const double k = np_max(c[i] - ceq * m, 0.0);
+            v = v * k;
+            cap[i] = k;
+        }
+        w[i] = v;
+    }
+}
+
+__global__ void k_pt_apply(long long N, double corr, double wsum, const double* __restrict__ w, double* __restrict__ c) {
+    GRID_STRIDE(i, N) c[i] = c[i] + (corr * w[i]) / wsum;
+}
+
+// order-preserving key of a double (larger value, larger key)
+__device__ __forceinline__ unsigned long long okey(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__global__ void k_max_key(long long N, const double* __restrict__ w, unsigned long long* __restrict__ best) {
+    typedef cub::BlockReduce<unsigned long long, 256> BR;
+    __shared__ typename BR::TempStorage tmp;
+    unsigned long long m = 0;
+    GRID_STRIDE(i, N) {
+        const unsigned long long k = okey(w[i]);
+        m = k > m ? k : m;
+    }
+    const unsigned long long agg = BR(tmp).Reduce(m, cub::Max());
+    if (threadIdx.x == 0) atomicMax(best, agg);
+}
+__global__ void k_first_at(long long N, const double* __restrict__ w, const unsigned long long* __restrict__ best,
+                           unsigned long long* __restrict__ idx) {
+    const unsigned long long b = *best;
+    GRID_STRIDE(i, N) if (okey(w[i]) == b) atomicMin(idx, (unsigned long long)i);
+}
+__global__ void k_pt_residue(long long N, double* __restrict__ c, const unsigned long long* __restrict__ idx,
+                             double residue) {
+    const unsigned long long i = *idx;
+    if (i < (unsigned long long)N) c[i] = c[i] - residue;
+}
+
+// ---------------------------------------------------------------- interface composition
+
+__global__ void k_ic_pre(long long N, const double* __restrict__ cm, const double* __restrict__ f,
+                         double* __restrict__ num, double* __restrict__ den) {
+    GRID_STRIDE(i, N) {
+        const double m = np_clip(1.0 - f[i], 0.0, 1.0);
+        num[i] = cm[i] * m;
+        den[i] = m;
+    }
+}
+__global__ void k_ic_post(long long N, double ct, const double* __restrict__ num, const double* __restrict__ den,
+                          double* __restrict__ out) {
+    GRID_STRIDE(i, N) out[i] = np_clip(num[i] / np_max(den[i], 1.0e-12), 0.0, ct);
+}
+
+// ---------------------------------------------------------------- Gaussian remap
+
+// Roots only decrease, so every walk ends; the loops are capped all the same
+// (the cap sets *err).  Reads go to L2: other SMs change parents atomically.
+constexpr int UF_CAP = 1 << 26;
+
+__device__ __forceinline__ int uf_find(int* parent, int i, unsigned* err) {
+    for (int it = 0; it < UF_CAP; ++it) {
+        const int p = __ldcg(&parent[i]);
+        if (p == i) return i;
+        const int gp = __ldcg(&parent[p]);
+        if (gp != p) atomicMin(&parent[i], gp);
+        i = p;
+    }
+    atomicExch(err, 1u);
+    return i;
+}
+__device__ void uf_unite(int* parent, int a, int b, unsigned* err) {
+    for (int it = 0; it < UF_CAP; ++it) {
+        a = uf_find(parent, a, err);
+        b = uf_find(parent, b, err);
+        if (a == b) return;
+        const int lo = a < b ? a : b, hi = a < b ? b : a;
+        const int old = atomicCAS(&parent[hi], hi, lo);
+        if (old == hi) return;
+        a = lo;
+        b = old;
+    }
+    atomicExch(err, 1u);
+}
+
+__global__ void k_cc_init(long long N, int* __restrict__ parent, int* __restrict__ size, int* __restrict__ wave) {
+    GRID_STRIDE(i, N) {
+        parent[i] = (int)i;
+        size[i] = 0;
+        wave[i] = 0;
+    }
+}
+// face neighbours without wrap, equal nonzero labels
+__global__ void k_cc_union(Ext d, const int8_t* __restrict__ lab, int* parent, unsigned* err) {
+    GRID_STRIDE(i, d.N) {
+        const int8_t l = lab[i];
+        if (l == 0) continue;
+        int x[3];
+        coords(d, i, x);
+        for (int a = 0; a < d.ndim; ++a)
+            if (x[a] + 1 < d.e[a] && lab[i + d.st[a]] == l) uf_unite(parent, (int)i, (int)(i + d.st[a]), err);
+    }
+}
+__global__ void k_cc_finish(long long N, const int8_t* __restrict__ lab, int* parent, int* __restrict__ root,
+                            int* __restrict__ size, unsigned* err) {
+    GRID_STRIDE(i, N) {
+        if (lab[i] == 0) {
+            root[i] = -1;
+            continue;
+        }
+        const int r = uf_find(parent, (int)i, err);
+        root[i] = r;
+        atomicAdd(&size[r], 1);
+    }
+}
+
+// the components (of more than one cell) with a cell in the 3^d box of x,
+// without wrap; returns how many (at most 27)
+__device__ __forceinline__ int box_components(const Ext& d, const int x[3], long long i, const int* __restrict__ root,
+                                              const int* __restrict__ size, int S[27]) {
+    int n = 0;
+    const int lo2 = d.ndim == 3 ? -1 : 0, hi2 = d.ndim == 3 ? 1 : 0;
+    for (int o0 = -1; o0 <= 1; ++o0) {
+        if (x[0] + o0 < 0 || x[0] + o0 >= d.e[0]) continue;
+        for (int o1 = -1; o1 <= 1; ++o1) {
+            if (x[1] + o1 < 0 || x[1] + o1 >= d.e[1]) continue;
+            for (int o2 = lo2; o2 <= hi2; ++o2) {
+                if (x[2] + o2 < 0 || x[2] + o2 >= d.e[2]) continue;
+                const int r = root[i + o0 * d.st[0] + o1 * d.st[1] + o2 * d.st[2]];
+                if (r < 0 || size[r] <= 1) continue;
+                bool seen = false;
+                for (int q = 0; q < n; ++q) seen |= S[q] == r;
+                if (!seen) S[n++] = r;
+            }
+        }
+    }
+    return n;
+}
+
+// the reference's processing order: label ascending, then first cell
+__device__ __forceinline__ long long order_key(const int8_t* __restrict__ orig, int r) {
+    return ((long long)((int)orig[r] + 128) << 32) | (long long)r;
+}
+
+__global__ void k_cgr_conflicts(Ext d, const int* __restrict__ root, const int* __restrict__ size,
+                                int* __restrict__ list, int* __restrict__ count, int* __restrict__ n_active) {
+    GRID_STRIDE(i, d.N) {
+        const int r = root[i];
+        if (r == (int)i && size[r] > 1) atomicAdd(n_active, 1);
+        int x[3];
+        coords(d, i, x);
+        int S[27];
+        if (box_components(d, x, i, root, size, S) >= 2) list[atomicAdd(count, 1)] = (int)i;
+    }
+}
+
+__global__ void k_cgr_relax(Ext d, const int* __restrict__ list, int M, const int8_t* __restrict__ orig,
+                            const int* __restrict__ root, const int* __restrict__ size, int* wave,
+                            int* __restrict__ changed) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
+        const long long i = list[q];
+        int x[3];
+        coords(d, i, x);
+        int S[27];
+        const int n = box_components(d, x, i, root, size, S);
+        for (int b = 0; b < n; ++b) {
+            const long long kb = order_key(orig, S[b]);
+            int m = __ldcg(&wave[S[b]]);
+            const int m0 = m;
+            for (int a = 0; a < n; ++a)
+                if (order_key(orig, S[a]) < kb) {
+                    const int wa = __ldcg(&wave[S[a]]) + 1;
+                    m = wa > m ? wa : m;
+                }
+            if (m > m0) {
+                atomicMax(&wave[S[b]], m);
+                *changed = 1;
+            }
+        }
+    }
+}
+
+__global__ void k_cgr_max_wave(long long N, const int* __restrict__ root, const int* __restrict__ size,
+                               const int* __restrict__ wave, int* __restrict__ max_wave) {
+    GRID_STRIDE(i, N) if (root[i] == (int)i && size[i] > 1) atomicMax(max_wave, wave[i]);
+}
+
+// candidates of wave w: cells of the dilation of a wave-w component that are
+// zero or its own
+__global__ void k_cgr_flags(Ext d, int w, const int8_t* __restrict__ lab, const int* __restrict__ root,
+                            const int* __restrict__ size, const int* __restrict__ wave, int* __restrict__ flag,
+                            int* __restrict__ seg) {
+    GRID_STRIDE(i, d.N) {
+        int x[3];
+        coords(d, i, x);
+        int S[27];
+        const int n = box_components(d, x, i, root, size, S);
+        int B = -1;
+        for (int q = 0; q < n; ++q)
+            if (wave[S[q]] == w) B = S[q];
+        const int f = B >= 0 && (root[i] == B || lab[i] == 0);
+        flag[i] = f;
+        seg[i] = B;
+    }
+}
+__global__ void k_cgr_scatter(long long N, const int* __restrict__ flag, const int* __restrict__ pos,
+                              int* __restrict__ cand, int* __restrict__ count) {
+    GRID_STRIDE(i, N) {
+        if (flag[i]) cand[pos[i]] = (int)i;
+        if (i == N - 1) *count = pos[i] + flag[i];
+    }
+}
+
+// the wrapped Gaussian of component B's indicator at cell x: pass 0 along
+// axis 0, pass 1 along axis 1, pass 2 along axis 2, each x0 w0 + sum over
+// j = r..1 of (x-j + x+j) w_j, evaluated only on the (2r+1)^d box
+__device__ __forceinline__ double ind(const int* __restrict__ root, long long i, int B) {
+    return root[i] == B ? 1.0 : 0.0;
+}
+__device__ double pass0(const Ext& d, const Taps& t, const int* __restrict__ root, int B, int y0, int y1, int y2) {
+    const long long rest = (long long)y1 * d.st[1] + y2;
+    double v = ind(root, (long long)y0 * d.st[0] + rest, B) * t.w[0];
+    for (int j = t.r; j >= 1; --j)
+        v = v + (ind(root, (long long)wrapi(y0 - j, d.e[0]) * d.st[0] + rest, B) +
+                 ind(root, (long long)wrapi(y0 + j, d.e[0]) * d.st[0] + rest, B)) * t.w[j];
+    return v;
+}
+__device__ double pass1(const Ext& d, const Taps& t, const int* __restrict__ root, int B, int y0, int y1, int y2) {
+    double v = pass0(d, t, root, B, y0, y1, y2) * t.w[0];
+    for (int j = t.r; j >= 1; --j)
+        v = v + (pass0(d, t, root, B, y0, wrapi(y1 - j, d.e[1]), y2) +
+                 pass0(d, t, root, B, y0, wrapi(y1 + j, d.e[1]), y2)) * t.w[j];
+    return v;
+}
+__device__ double pass2(const Ext& d, const Taps& t, const int* __restrict__ root, int B, int y0, int y1, int y2) {
+    double v = pass1(d, t, root, B, y0, y1, y2) * t.w[0];
+    for (int j = t.r; j >= 1; --j)
+        v = v + (pass1(d, t, root, B, y0, y1, wrapi(y2 - j, d.e[2])) +
+                 pass1(d, t, root, B, y0, y1, wrapi(y2 + j, d.e[2]))) * t.w[j];
+    return v;
+}
+
+__global__ void k_cgr_score(Ext d, Taps t, const int* __restrict__ cand, const int* __restrict__ count,
+                            const int* __restrict__ root, const int* __restrict__ seg,
+                            unsigned long long* __restrict__ key) {
+    const int M = *count;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
+        const long long i = cand[q];
+        int x[3];
+        coords(d, i, x);
+        const int B = seg[i];
+        const double s = d.ndim == 3 ? pass2(d, t, root, B, x[0], x[1], x[2]) : pass1(d, t, root, B, x[0], x[1], 0);
+        key[q] = ~okey(s);  // ascending key = descending score
+    }
+}
+__global__ void k_cgr_segkeys(const int* __restrict__ cells, const int* __restrict__ count, const int* __restrict__ seg,
+                              unsigned* __restrict__ out) {
+    const int M = *count;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) out[q] = (unsigned)seg[cells[q]];
+}
+__global__ void k_cgr_starts(const unsigned* __restrict__ sk, const int* __restrict__ count, int* __restrict__ start) {
+    const int M = *count;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x)
+        if (q == 0 || sk[q - 1] != sk[q]) start[sk[q]] = q;
+}
+__global__ void k_cgr_vacate(long long N, int w, const int* __restrict__ root, const int* __restrict__ size,
+                             const int* __restrict__ wave, int8_t* __restrict__ lab) {
+    GRID_STRIDE(i, N) {
+        const int r = root[i];
+        if (r >= 0 && size[r] > 1 && wave[r] == w) lab[i] = 0;
+    }
+}
+__global__ void k_cgr_select(const unsigned* __restrict__ sk, const int* __restrict__ cells, const int* __restrict__ count,
+                             const int* __restrict__ start, const int* __restrict__ size,
+                             const int8_t* __restrict__ orig, int8_t* __restrict__ lab) {
+    const int M = *count;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
+        const int B = (int)sk[q];
+        if (q - start[B] < size[B]) lab[cells[q]] = orig[B];
+    }
+}
+__global__ void k_cgr_changed(long long N, const int8_t* __restrict__ lab, const int8_t* __restrict__ orig,
+                              double* __restrict__ alpha, unsigned long long* __restrict__ count) {
+    typedef cub::BlockReduce<unsigned long long, 256> BR;
+    __shared__ typename BR::TempStorage tmp;
+    unsigned long long n = 0;
+    GRID_STRIDE(i, N) if (lab[i] != orig[i]) {
+        alpha[i] = 1.0;
+        ++n;
+    }
+    const unsigned long long agg = BR(tmp).Sum(n);
+    if (threadIdx.x == 0 && agg) atomicAdd(count, agg);
+}
+
+}  // namespace
+
+// ============================================================== handle
+
+struct gpk_alcu {
+    Ext d{};
+    Phys p{};
+    int device = 0;
+    int num_sms = 148;
+    int grid = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    long long bytes = 0;
+    // transport scratch
+    double* f[6] = {};  // six N-double fields
+    // pairwise-sum tree: leaves, then upper levels up to the root
+    int* leaf_start = nullptr;
+    int* leaf_len = nullptr;
+    int n_leaves = 0;
+    std::vector<int*> lvl_n, lvl_first;
+    std::vector<int> lvl_count;
+    std::vector<long long> lvl_below;  // threshold of the level under each
+    double* pw_buf[2] = {};
+    // reductions
+    unsigned long long* u64 = nullptr;  // [0] max key, [1] index, [2] changed count
+    int* i32 = nullptr;                 // [0] candidates, [1] conflicts, [2] changed flag, [3] max wave, [4] active
+    unsigned* err = nullptr;
+    // remap scratch
+    int8_t* orig = nullptr;
+    int *parent = nullptr, *root = nullptr, *size = nullptr, *wave = nullptr, *seg = nullptr, *start = nullptr;
+    int *flag = nullptr, *pos = nullptr, *cand = nullptr, *cells1 = nullptr, *cells2 = nullptr, *conflicts = nullptr;
+    unsigned long long *key1 = nullptr, *key2 = nullptr;
+    unsigned *sk1 = nullptr, *sk2 = nullptr;
+    void* cub_tmp = nullptr;
+    size_t cub_bytes = 0;
+    int seg_bits = 1;
+    long long last_components = 0, last_waves = 0;
+};
+
+namespace {
+
+int set_params(gpk_alcu* h, const gpk_alcu_params* p) {
+    if (!p || !(p->dx > 0.0) || !(p->diffusivity > 0.0)) {
+        gpk_set_error("alcu: params must be given with dx > 0 and diffusivity > 0");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    h->p.dx = p->dx;
+    h->p.D = p->diffusivity;
+    h->p.ceq = p->c_matrix_eq;
+    h->p.ct = p->c_theta;
+    return GPK_OK;
+}
+
+// maximal subtrees of numpy's pairwise tree with at most t values, in order
+void cut(long long lo, long long n, long long t, std::vector<long long>& s, std::vector<long long>& len) {
+    if (n <= t) {
+        s.push_back(lo);
+        len.push_back(n);
+        return;
+    }
+    long long n2 = n / 2;
+    n2 -= n2 % 8;
+    cut(lo, n2, t, s, len);
+    cut(lo + n2, n - n2, t, s, len);
+}
+
+void free_all(gpk_alcu* h) {
+    for (double*& q : h->f) cudaFree(q);
+    cudaFree(h->leaf_start); cudaFree(h->leaf_len);
+    for (int* q : h->lvl_n) cudaFree(q);
+    for (int* q : h->lvl_first) cudaFree(q);
+    cudaFree(h->pw_buf[0]); cudaFree(h->pw_buf[1]);
+    cudaFree(h->u64); cudaFree(h->i32); cudaFree(h->err);
+    cudaFree(h->orig); cudaFree(h->parent); cudaFree(h->root); cudaFree(h->size); cudaFree(h->wave);
+    cudaFree(h->seg); cudaFree(h->start); cudaFree(h->flag); cudaFree(h->pos); cudaFree(h->cand);
+    cudaFree(h->cells1); cudaFree(h->cells2); cudaFree(h->conflicts);
+    cudaFree(h->key1); cudaFree(h->key2); cudaFree(h->sk1); cudaFree(h->sk2); cudaFree(h->cub_tmp);
+    if (h->own) cudaStreamDestroy(h->own);
+}
+
+int taps_of(const double* taps, int radius, Taps& t) {
+    if (!taps || radius < 0 || radius > GPK_ALCU_MAX_RADIUS) {
+        gpk_set_error("alcu: taps must be given with 0 <= radius <= " + std::to_string(GPK_ALCU_MAX_RADIUS));
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    t.r = radius;
+    for (int j = 0; j <= radius; ++j) {
+        if (taps[radius - j] != taps[radius + j]) {
+            gpk_set_error("alcu: the taps must be symmetric");
+            return GPK_ERR_INVALID_ARGUMENT;
+        }
+        t.w[j] = taps[radius + j];
+    }
+    return GPK_OK;
+}
+
+// np.sum of the values f(0..N-1); waits for the stream
+template <class F>
+int pw_sum(gpk_alcu* h, F f, double* out) {
+    cudaStream_t st = h->stream;
+    const long long threads = 8ll * h->n_leaves;
+    k_pw_leaves<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(f, h->leaf_start, h->leaf_len, h->n_leaves,
+                                                                     h->pw_buf[0]);
+    ALCU_TRY(cudaGetLastError());
+    int cur = 0;
+    for (size_t k = 0; k < h->lvl_n.size(); ++k) {
+        const int M = h->lvl_count[k];
+        k_pw_nodes<<<(M + 127) / 128, 128, 0, st>>>(h->lvl_n[k], h->lvl_first[k], M, h->lvl_below[k],
+                                                     h->pw_buf[cur], h->pw_buf[cur ^ 1]);
+        ALCU_TRY(cudaGetLastError());
+        cur ^= 1;
+    }
+    ALCU_TRY(cudaMemcpyAsync(out, h->pw_buf[cur], sizeof(double), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaStreamSynchronize(st));
+    return GPK_OK;
+}
+
+// CUB's scratch for the remap's scan and sorts at M items (sized for N at
+// creation; grown here should a smaller problem ever ask for more)
+int cub_reserve(gpk_alcu* h, int M) {
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, b1, h->flag, h->pos, (int)h->d.N);
+    cub::DeviceRadixSort::SortPairs(nullptr, b2, h->key1, h->key2, h->cand, h->cells1, M);
+    cub::DeviceRadixSort::SortPairs(nullptr, b3, h->sk1, h->sk2, h->cells1, h->cells2, M, 0, h->seg_bits);
+    size_t need = b1 > b2 ? b1 : b2;
+    if (b3 > need) need = b3;
+    if (need <= h->cub_bytes) return GPK_OK;
+    ALCU_TRY(cudaStreamSynchronize(h->stream));
+    cudaFree(h->cub_tmp);
+    h->cub_tmp = nullptr;
+    if (cudaMalloc(&h->cub_tmp, need) != cudaSuccess) {
+        cudaGetLastError();
+        h->cub_bytes = 0;
+        gpk_set_error("alcu: cudaMalloc of the sort scratch failed");
+        return GPK_ERR_OUT_OF_MEMORY;
+    }
+    h->bytes += (long long)(need - h->cub_bytes);
+    h->cub_bytes = need;
+    return GPK_OK;
+}
+
+// out = the wrapped Gaussian of in (3 or 2 passes); tmp: one N-double scratch
+int gauss(gpk_alcu* h, const Taps& t, const double* in, double* out, double* tmp) {
+    const Ext& d = h->d;
+    // ping-pong so that the last pass lands in out
+    const double* src = in;
+    for (int a = 0; a < d.ndim; ++a) {
+        double* dst = ((d.ndim - 1 - a) % 2 == 0) ? out : tmp;
+        k_gauss_pass<1><<<h->grid, 256, 0, h->stream>>>(d, a, t, src, nullptr, dst, nullptr);
+        ALCU_TRY(cudaGetLastError());
+        src = dst;
+    }
+    return GPK_OK;
+}
+// two fields smoothed together, results in a and b (ta, tb: scratch)
+int gauss2(gpk_alcu* h, const Taps& t, double* a, double* b, double* ta, double* tb) {
+    const Ext& d = h->d;
+    double *sa = a, *sb = b, *da = ta, *db = tb;
+    for (int ax = 0; ax < d.ndim; ++ax) {
+        k_gauss_pass<2><<<h->grid, 256, 0, h->stream>>>(d, ax, t, sa, sb, da, db);
+        ALCU_TRY(cudaGetLastError());
+        std::swap(sa, da);
+        std::swap(sb, db);
+    }
+    if (sa != a) {
+        ALCU_TRY(cudaMemcpyAsync(a, sa, sizeof(double) * d.N, cudaMemcpyDeviceToDevice, h->stream));
+        ALCU_TRY(cudaMemcpyAsync(b, sb, sizeof(double) * d.N, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    return GPK_OK;
+}
+
+}  // namespace
+
+// ============================================================== C ABI
+
+extern "C" int gpk_alcu_gauss_taps(double sigma, double* taps, int max_taps, int* radius) {
+    if (!(sigma > 0.0) || !taps || !radius) {
+        gpk_set_error("alcu: sigma > 0 with taps and radius pointers");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    const int r = (int)(4.0 * sigma + 0.5);
+    if (r > GPK_ALCU_MAX_RADIUS || max_taps < 2 * r + 1) {
+        gpk_set_error("alcu: radius " + std::to_string(r) + " too large for the taps array or the limit");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    const double s2 = sigma * sigma;
+    const double c = -0.5 / s2;
+    std::vector<double> phi(2 * r + 1);
+    for (int k = 0; k <= 2 * r; ++k) {
+        const long long x = k - r;
+        phi[k] = std::exp(c * (double)(x * x));
+    }
+    // numpy's sum of at most 65 values
+    const int n = 2 * r + 1;
+    double sum;
+    if (n < 8) {
+        sum = 0.0;
+        for (int k = 0; k < n; ++k) sum = sum + phi[k];
+    } else {
+        double acc[8];
+        for (int j = 0; j < 8; ++j) acc[j] = phi[j];
+        int i = 8;
+        for (; i < n - n % 8; i += 8)
+            for (int j = 0; j < 8; ++j) acc[j] = acc[j] + phi[i + j];
+        sum = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+        for (; i < n; ++i) sum = sum + phi[i];
+    }
+    for (int k = 0; k < n; ++k) taps[k] = phi[k] / sum;
+    *radius = r;
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_create(int ndim, const int* shape, const gpk_alcu_params* p, gpk_alcu** out) {
+    if (!out || !shape || (ndim != 2 && ndim != 3)) {
+        gpk_set_error("alcu: ndim must be 2 or 3 with a shape array and an output pointer");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    long long N = 1;
+    for (int a = 0; a < ndim; ++a) {
+        if (shape[a] < 1 || shape[a] > (1 << 20)) {
+            gpk_set_error("alcu: extents must lie in [1, 2^20]");
+            return GPK_ERR_INVALID_ARGUMENT;
+        }
+        N *= shape[a];
+    }
+    if (N >= (1ll << 31) - 1) {
+        gpk_set_error("alcu: fewer than 2^31 - 1 cells");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        gpk_set_error("no CUDA device available");
+        return GPK_ERR_NO_DEVICE;
+    }
+    gpk_alcu* h = new gpk_alcu();
+    int rc = set_params(h, p);
+    if (rc != GPK_OK) { delete h; return rc; }
+    Ext& d = h->d;
+    d.ndim = ndim;
+    d.e[0] = shape[0];
+    d.e[1] = shape[1];
+    d.e[2] = ndim == 3 ? shape[2] : 1;
+    d.st[2] = 1;
+    d.st[1] = d.e[2];
+    d.st[0] = (long long)d.e[1] * d.e[2];
+    d.N = N;
+    auto fail = [&](int code) { free_all(h); delete h; return code; };
+    if (cudaGetDevice(&h->device) != cudaSuccess) return fail(GPK_ERR_CUDA);
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+    long long blocks = (N + 255) / 256;
+    if (blocks > (long long)h->num_sms * 16) blocks = (long long)h->num_sms * 16;
+    h->grid = (int)blocks;
+    if (cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking) != cudaSuccess) {
+        gpk_set_error("alcu: cudaStreamCreate failed");
+        return fail(GPK_ERR_CUDA);
+    }
+    h->stream = h->own;
+    auto alloc = [&](void** q, size_t b) -> bool {
+        if (cudaMalloc(q, b < 16 ? 16 : b) != cudaSuccess) {
+            cudaGetLastError();
+            gpk_set_error("alcu: cudaMalloc of " + std::to_string(b) + " bytes failed");
+            return false;
+        }
+        h->bytes += (long long)b;
+        return true;
+    };
+    for (double*& q : h->f)
+        if (!alloc((void**)&q, sizeof(double) * N)) return fail(GPK_ERR_OUT_OF_MEMORY);
+    // pairwise-sum tree
+    {
+        std::vector<long long> s, len;
+        cut(0, N, 128, s, len);
+        h->n_leaves = (int)s.size();
+        std::vector<int> s32(s.begin(), s.end()), l32(len.begin(), len.end());
+        if (!alloc((void**)&h->leaf_start, sizeof(int) * s32.size()) ||
+            !alloc((void**)&h->leaf_len, sizeof(int) * l32.size()))
+            return fail(GPK_ERR_OUT_OF_MEMORY);
+        if (cudaMemcpy(h->leaf_start, s32.data(), sizeof(int) * s32.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->leaf_len, l32.data(), sizeof(int) * l32.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+            gpk_set_error("alcu: upload of the summation tree failed");
+            return fail(GPK_ERR_CUDA);
+        }
+        std::vector<long long> below_s = s;
+        long long t_below = 128;
+        while (below_s.size() > 1) {
+            const long long t = t_below * 32;
+            std::vector<long long> ns, nl;
+            if (t >= N) {
+                ns.push_back(0);
+                nl.push_back(N);
+            } else {
+                cut(0, N, t, ns, nl);
+            }
+            // first lower-level node of each node: walk both ordered lists
+            std::vector<int> first(ns.size()), n32(ns.size());
+            size_t k = 0;
+            for (size_t q = 0; q < ns.size(); ++q) {
+                while (k < below_s.size() && below_s[k] < ns[q]) ++k;
+                first[q] = (int)k;
+                n32[q] = (int)nl[q];
+            }
+            int *dn = nullptr, *df = nullptr;
+            if (!alloc((void**)&dn, sizeof(int) * ns.size()) || !alloc((void**)&df, sizeof(int) * ns.size()))
+                return fail(GPK_ERR_OUT_OF_MEMORY);
+            h->lvl_n.push_back(dn);
+            h->lvl_first.push_back(df);
+            if (cudaMemcpy(dn, n32.data(), sizeof(int) * ns.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(df, first.data(), sizeof(int) * ns.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+                gpk_set_error("alcu: upload of the summation tree failed");
+                return fail(GPK_ERR_CUDA);
+            }
+            h->lvl_count.push_back((int)ns.size());
+            h->lvl_below.push_back(t_below);
+            below_s = ns;
+            t_below = t;
+        }
+        if (!alloc((void**)&h->pw_buf[0], sizeof(double) * h->n_leaves) ||
+            !alloc((void**)&h->pw_buf[1], sizeof(double) * h->n_leaves))
+            return fail(GPK_ERR_OUT_OF_MEMORY);
+    }
+    if (!alloc((void**)&h->u64, sizeof(unsigned long long) * 4) || !alloc((void**)&h->i32, sizeof(int) * 8) ||
+        !alloc((void**)&h->err, sizeof(unsigned) * 2))
+        return fail(GPK_ERR_OUT_OF_MEMORY);
+    // remap scratch
+    int** ints[] = {&h->parent, &h->root, &h->size, &h->wave, &h->seg, &h->start,
+                    &h->flag, &h->pos, &h->cand, &h->cells1, &h->cells2, &h->conflicts};
+    for (int** q : ints)
+        if (!alloc((void**)q, sizeof(int) * N)) return fail(GPK_ERR_OUT_OF_MEMORY);
+    if (!alloc((void**)&h->orig, N) || !alloc((void**)&h->key1, 8 * N) || !alloc((void**)&h->key2, 8 * N) ||
+        !alloc((void**)&h->sk1, 4 * N) || !alloc((void**)&h->sk2, 4 * N))
+        return fail(GPK_ERR_OUT_OF_MEMORY);
+    while ((1ll << h->seg_bits) < N) ++h->seg_bits;
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, b1, h->flag, h->pos, (int)N);
+    cub::DeviceRadixSort::SortPairs(nullptr, b2, h->key1, h->key2, h->cand, h->cells1, (int)N);
+    cub::DeviceRadixSort::SortPairs(nullptr, b3, h->sk1, h->sk2, h->cells1, h->cells2, (int)N, 0, h->seg_bits);
+    h->cub_bytes = b1 > b2 ? b1 : b2;
+    if (b3 > h->cub_bytes) h->cub_bytes = b3;
+    if (!alloc(&h->cub_tmp, h->cub_bytes)) return fail(GPK_ERR_OUT_OF_MEMORY);
+    *out = h;
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_destroy(gpk_alcu* h) {
+    if (!h) return GPK_OK;
+    cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_set_params(gpk_alcu* h, const gpk_alcu_params* p) {
+    if (!h) { gpk_set_error("alcu: null handle"); return GPK_ERR_INVALID_ARGUMENT; }
+    return set_params(h, p);
+}
+
+extern "C" int gpk_alcu_set_stream(gpk_alcu* h, void* stream) {
+    if (!h) { gpk_set_error("alcu: null handle"); return GPK_ERR_INVALID_ARGUMENT; }
+    h->stream = (cudaStream_t)stream;
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_competitor(gpk_alcu* h, const int8_t* labels, uint8_t* mask, int8_t* competitor) {
+    if (!h || !labels || !mask || !competitor) { gpk_set_error("alcu: null argument"); return GPK_ERR_INVALID_ARGUMENT; }
+    k_competitor<<<h->grid, 256, 0, h->stream>>>(h->d, labels, mask, competitor);
+    ALCU_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_precip_fraction(gpk_alcu* h, const int8_t* labels, const double* alpha,
+                                        const int8_t* competitor, double* fprec) {
+    if (!h || !labels || !alpha || !competitor || !fprec) {
+        gpk_set_error("alcu: null argument");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    k_precip_fraction<<<h->grid, 256, 0, h->stream>>>(h->d.N, labels, alpha, competitor, fprec);
+    ALCU_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_matrix_composition(gpk_alcu* h, const double* ctot, const double* fprec, double* cm) {
+    if (!h || !ctot || !fprec || !cm) { gpk_set_error("alcu: null argument"); return GPK_ERR_INVALID_ARGUMENT; }
+    k_matrix_composition<<<h->grid, 256, 0, h->stream>>>(h->d.N, h->p, ctot, fprec, cm);
+    ALCU_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_diffuse(gpk_alcu* h, double* ctot, const double* fprec, double dt, double* cm, int* substeps) {
+    if (!h || !ctot || !fprec) { gpk_set_error("alcu: null argument"); return GPK_ERR_INVALID_ARGUMENT; }
+    const Phys& p = h->p;
+    const double stable_dt = 0.4 * p.dx * p.dx / (2.0 * h->d.ndim * p.D);
+    const double nsub = std::ceil(dt / stable_dt);
+    if (!(nsub < 1e7) || dt != dt) {
+        gpk_set_error("alcu: dt needs more than 10^7 diffusion substeps");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    const int n = nsub > 1.0 ? (int)nsub : 1;
+    const double sub_dt = dt / n;
+    double* bufs[2] = {ctot, h->f[0]};
+    int cur = 0;
+    for (int s = 0; s < n; ++s) {
+        k_diffuse<<<h->grid, 256, 0, h->stream>>>(h->d, p, sub_dt, bufs[cur], fprec, bufs[cur ^ 1],
+                                                  s == n - 1 ? cm : nullptr);
+        ALCU_TRY(cudaGetLastError());
+        cur ^= 1;
+    }
+    if (cur != 0)
+        ALCU_TRY(cudaMemcpyAsync(ctot, bufs[cur], sizeof(double) * h->d.N, cudaMemcpyDeviceToDevice, h->stream));
+    if (substeps) *substeps = n;
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_sum(gpk_alcu* h, const double* x, double* out) {
+    if (!h || !x || !out) { gpk_set_error("alcu: null argument"); return GPK_ERR_INVALID_ARGUMENT; }
+    return pw_sum(h, LoadF{x}, out);
+}
+
+extern "C" int gpk_alcu_gaussian_filter(gpk_alcu* h, const double* in, double* out, const double* taps, int radius) {
+    if (!h || !in || !out || in == out) {
+        gpk_set_error("alcu: null or aliased arguments");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    Taps t;
+    int rc = taps_of(taps, radius, t);
+    if (rc != GPK_OK) return rc;
+    return gauss(h, t, in, out, h->f[5]);
+}
+
+extern "C" int gpk_alcu_partition_transfer(gpk_alcu* h, double* ctot, const double* old_fraction,
+                                           const double* new_fraction, const double* matrix_composition,
+                                           const double* taps, int radius) {
+    if (!h || !ctot || !old_fraction || !new_fraction || !matrix_composition) {
+        gpk_set_error("alcu: null argument");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    Taps t;
+    int rc = taps_of(taps, radius, t);
+    if (rc != GPK_OK) return rc;
+    const long long N = h->d.N;
+    double *tr = h->f[0], *absd = h->f[1], *g = h->f[2], *w = h->f[3], *cap = h->f[4], *tmp = h->f[5];
+    k_pt_transfer<<<h->grid, 256, 0, h->stream>>>(N, h->p.ct, ctot, old_fraction, new_fraction, matrix_composition, tr,
+                                                  absd);
+    ALCU_TRY(cudaGetLastError());
+    double total = 0.0;
+    if ((rc = pw_sum(h, LoadF{tr}, &total)) != GPK_OK) return rc;
+    if (std::fabs(total) <= 1.0e-30) return GPK_OK;
+    if ((rc = gauss(h, t, absd, g, tmp)) != GPK_OK) return rc;
+    const double correction = -total;
+    const int draw = correction < 0.0;
+    k_pt_weight<<<h->grid, 256, 0, h->stream>>>(N, h->p.ceq, draw, g, new_fraction, ctot, w, cap);
+    ALCU_TRY(cudaGetLastError());
+    if (draw) {
+        double cap_sum = 0.0;
+        if ((rc = pw_sum(h, LoadF{cap}, &cap_sum)) != GPK_OK) return rc;
+        if (cap_sum < -correction * (1.0 - 1.0e-12)) {
+            gpk_set_error("insufficient matrix Cu for partition transfer");
+            return GPK_ERR_INFEASIBLE;
+        }
+    }
+    double wsum = 0.0;
+    if ((rc = pw_sum(h, LoadF{w}, &wsum)) != GPK_OK) return rc;
+    if (wsum <= 0.0) {
+        gpk_set_error("empty matrix neighbourhood for partition transfer");
+        return GPK_ERR_INFEASIBLE;
+    }
+    k_pt_apply<<<h->grid, 256, 0, h->stream>>>(N, correction, wsum, w, ctot);
+    ALCU_TRY(cudaGetLastError());
+    double s = 0.0;
+    if ((rc = pw_sum(h, CorrF{w, correction, wsum}, &s)) != GPK_OK) return rc;
+    const double residue = total + s;
+    ALCU_TRY(cudaMemsetAsync(h->u64, 0, sizeof(unsigned long long), h->stream));
+    ALCU_TRY(cudaMemsetAsync(h->u64 + 1, 0xff, sizeof(unsigned long long), h->stream));
+    k_max_key<<<h->grid, 256, 0, h->stream>>>(N, w, h->u64);
+    k_first_at<<<h->grid, 256, 0, h->stream>>>(N, w, h->u64, h->u64 + 1);
+    k_pt_residue<<<1, 1, 0, h->stream>>>(N, ctot, h->u64 + 1, residue);
+    ALCU_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_interface_composition(gpk_alcu* h, const double* cm, const double* fprec, double* trace,
+                                              const double* taps, int radius) {
+    if (!h || !cm || !fprec || !trace) { gpk_set_error("alcu: null argument"); return GPK_ERR_INVALID_ARGUMENT; }
+    Taps t;
+    int rc = taps_of(taps, radius, t);
+    if (rc != GPK_OK) return rc;
+    const long long N = h->d.N;
+    double *num = h->f[1], *den = h->f[2];
+    k_ic_pre<<<h->grid, 256, 0, h->stream>>>(N, cm, fprec, num, den);
+    ALCU_TRY(cudaGetLastError());
+    if ((rc = gauss2(h, t, num, den, h->f[3], h->f[4])) != GPK_OK) return rc;
+    k_ic_post<<<h->grid, 256, 0, h->stream>>>(N, h->p.ct, num, den, trace);
+    ALCU_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alpha, const double* taps, int radius,
+                                       int64_t* changed) {
+    if (!h || !labels || !alpha) { gpk_set_error("alcu: null argument"); return GPK_ERR_INVALID_ARGUMENT; }
+    Taps t;
+    int rc = taps_of(taps, radius, t);
+    if (rc != GPK_OK) return rc;
+    const Ext& d = h->d;
+    const long long N = d.N;
+    cudaStream_t st = h->stream;
+    const int G = h->grid;
+    ALCU_TRY(cudaMemcpyAsync(h->orig, labels, N, cudaMemcpyDeviceToDevice, st));
+    ALCU_TRY(cudaMemsetAsync(h->i32, 0, sizeof(int) * 8, st));
+    ALCU_TRY(cudaMemsetAsync(h->err, 0, sizeof(unsigned) * 2, st));
+    ALCU_TRY(cudaMemsetAsync(h->u64 + 2, 0, sizeof(unsigned long long), st));
+    k_cc_init<<<G, 256, 0, st>>>(N, h->parent, h->size, h->wave);
+    k_cc_union<<<G, 256, 0, st>>>(d, h->orig, h->parent, h->err);
+    k_cc_finish<<<G, 256, 0, st>>>(N, h->orig, h->parent, h->root, h->size, h->err);
+    k_cgr_conflicts<<<G, 256, 0, st>>>(d, h->root, h->size, h->conflicts, h->i32 + 1, h->i32 + 4);
+    ALCU_TRY(cudaGetLastError());
+    int hv[8];
+    unsigned herr = 0;
+    ALCU_TRY(cudaMemcpyAsync(hv, h->i32, sizeof(hv), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaMemcpyAsync(&herr, h->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaStreamSynchronize(st));
+    if (herr) {
+        gpk_set_error("alcu: component search exceeded its iteration cap");
+        return GPK_ERR_INTERNAL;
+    }
+    const int n_conf = hv[1], n_active = hv[4];
+    h->last_components = n_active;
+    h->last_waves = 0;
+    if (n_active == 0) {
+        if (changed) *changed = 0;
+        return GPK_OK;
+    }
+    // waves: longest chain of earlier interacting components
+    if (n_conf > 0) {
+        for (int it = 0;; ++it) {
+            if (it > n_active + 1) {
+                gpk_set_error("alcu: wave relaxation did not settle");
+                return GPK_ERR_INTERNAL;
+            }
+            int flag = 0;
+            ALCU_TRY(cudaMemsetAsync(h->i32 + 2, 0, sizeof(int), st));
+            const int blocks = (n_conf + 255) / 256 < G ? (n_conf + 255) / 256 : G;
+            k_cgr_relax<<<blocks, 256, 0, st>>>(d, h->conflicts, n_conf, h->orig, h->root, h->size, h->wave,
+                                                 h->i32 + 2);
+            ALCU_TRY(cudaGetLastError());
+            ALCU_TRY(cudaMemcpyAsync(&flag, h->i32 + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+            ALCU_TRY(cudaStreamSynchronize(st));
+            if (!flag) break;
+        }
+    }
+    int max_wave = 0;
+    k_cgr_max_wave<<<G, 256, 0, st>>>(N, h->root, h->size, h->wave, h->i32 + 3);
+    ALCU_TRY(cudaGetLastError());
+    ALCU_TRY(cudaMemcpyAsync(&max_wave, h->i32 + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaStreamSynchronize(st));
+    h->last_waves = max_wave + 1;
+    for (int w = 0; w <= max_wave; ++w) {
+        k_cgr_flags<<<G, 256, 0, st>>>(d, w, labels, h->root, h->size, h->wave, h->flag, h->seg);
+        ALCU_TRY(cudaGetLastError());
+        size_t b = h->cub_bytes;
+        ALCU_TRY(cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, h->flag, h->pos, (int)N, st));
+        k_cgr_scatter<<<G, 256, 0, st>>>(N, h->flag, h->pos, h->cand, h->i32);
+        ALCU_TRY(cudaGetLastError());
+        int M = 0;
+        ALCU_TRY(cudaMemcpyAsync(&M, h->i32, sizeof(int), cudaMemcpyDeviceToHost, st));
+        ALCU_TRY(cudaStreamSynchronize(st));
+        if (M == 0) continue;
+        if ((rc = cub_reserve(h, M)) != GPK_OK) return rc;
+        const int sb = (M + 255) / 256 < G ? (M + 255) / 256 : G;
+        k_cgr_score<<<sb, 256, 0, st>>>(d, t, h->cand, h->i32, h->root, h->seg, h->key1);
+        ALCU_TRY(cudaGetLastError());
+        b = h->cub_bytes;
+        ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->key1, h->key2, h->cand, h->cells1, M, 0, 64, st));
+        k_cgr_segkeys<<<sb, 256, 0, st>>>(h->cells1, h->i32, h->seg, h->sk1);
+        ALCU_TRY(cudaGetLastError());
+        b = h->cub_bytes;
+        ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->sk1, h->sk2, h->cells1, h->cells2, M, 0,
+                                                 h->seg_bits, st));
+        k_cgr_starts<<<sb, 256, 0, st>>>(h->sk2, h->i32, h->start);
+        k_cgr_vacate<<<G, 256, 0, st>>>(N, w, h->root, h->size, h->wave, labels);
+        k_cgr_select<<<sb, 256, 0, st>>>(h->sk2, h->cells2, h->i32, h->start, h->size, h->orig, labels);
+        ALCU_TRY(cudaGetLastError());
+    }
+    k_cgr_changed<<<G, 256, 0, st>>>(N, labels, h->orig, alpha, h->u64 + 2);
+    ALCU_TRY(cudaGetLastError());
+    unsigned long long n_changed = 0;
+    ALCU_TRY(cudaMemcpyAsync(&n_changed, h->u64 + 2, sizeof(n_changed), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaStreamSynchronize(st));
+    if (changed) *changed = (int64_t)n_changed;
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_info(const gpk_alcu* h, int64_t* cells, int64_t* device_bytes, int64_t* last_components,
+                             int64_t* last_waves) {
+    if (!h) { gpk_set_error("alcu: null handle"); return GPK_ERR_INVALID_ARGUMENT; }
+    if (cells) *cells = h->d.N;
+    if (device_bytes) *device_bytes = h->bytes;
+    if (last_components) *last_components = h->last_components;
+    if (last_waves) *last_waves = h->last_waves;
+    return GPK_OK;
+}

@@ -39,6 +39,7 @@ extern "C" {
 #define GPK_ERR_TIMEOUT            6  /* a bounded device wait gave up         */
 #define GPK_ERR_NO_DEVICE          7  /* no CUDA device / wrong architecture   */
 #define GPK_ERR_INTERNAL           8  /* device-side consistency check failed  */
+#define GPK_ERR_INFEASIBLE         9  /* no admissible result (the reference raises) */
 
 /* ---- arithmetic modes ---------------------------------------------------- */
 /* GPK_PREC_F32: the reference's own FP32 arithmetic, operation for operation

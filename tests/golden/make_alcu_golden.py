@@ -144,6 +144,13 @@ def main(root: str) -> None:
             out[f"{tag}_labels"] = lab
             out[f"{tag}_alpha"] = al
             out[f"{tag}_changed"] = np.int64(n)
+    # the taps scipy sampled in this process (numpy's exp), for callers whose
+    # numpy rounds exp differently
+    for sigma in (0.70, 0.75, 1.2):
+        r = int(4.0 * sigma + 0.5)
+        x = np.arange(-r, r + 1)
+        phi = np.exp(-0.5 / (sigma * sigma) * x ** 2)
+        out[f"taps_{int(round(sigma * 100))}"] = phi / phi.sum()
     np.savez_compressed(OUT, **out)
     print("wrote", OUT, {k: v.shape for k, v in out.items() if np.ndim(v)})
 

@@ -1,0 +1,379 @@
+"""The Al-Cu transport and remap kernels against the reference and the oracle.
+
+Bit-exact comparisons throughout (the functions are FP64 elementwise,
+stencil, pairwise-sum and sort work):
+
+* against the reference's own outputs in tests/golden/alcu_transport.npz
+  (make_alcu_golden.py), with the taps recorded beside them;
+* against oracle/alcu_oracle.py on larger seeded states: a 96^3 field with
+  plates of the three variants as in the reference's 3-D case, chains of
+  interacting components (several remap waves), odd extents, extents shorter
+  than the Gaussian's radius, empty and full label fields;
+* at 256^3 through properties: each label's volume is unchanged by the
+  remap, the device sum equals np.sum bit for bit, diffusion and partition
+  transfer keep the summed Cu.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from oracle import alcu_oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "alcu_transport.npz")
+
+
+def same(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return a.shape == b.shape and np.array_equal(np.ascontiguousarray(a).view(np.uint8),
+                                                 np.ascontiguousarray(b).view(np.uint8))
+
+
+def test_host_taps_agree_with_numpy_to_rounding():
+    """gpk_alcu_gauss_taps uses the C library's exp: equal to numpy's taps up
+    to the last bit (numpy's vectorised exp rounds differently at times)."""
+    from gpk_b200._lib import lib
+    from gpk_b200.alcu import gauss_taps
+
+    for s in (0.1, 0.7, 0.75, 0.85, 1.2, 2.0, 8.0 / 3.0, 7.0):
+        t = np.zeros(2 * 32 + 1)
+        r = C.c_int()
+        assert lib().gpk_alcu_gauss_taps(s, t.ctypes.data_as(C.POINTER(C.c_double)), t.size, C.byref(r)) == 0
+        g = gauss_taps(s)
+        assert r.value == (g.size - 1) // 2
+        assert np.allclose(t[:g.size], g, rtol=4e-16, atol=0)
+
+
+# --------------------------------------------------------------------------
+gpu = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    return torch
+
+
+@pytest.fixture(scope="module")
+def z():
+    return np.load(GOLDEN)
+
+
+def dev(torch, x):
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+def params(dx=1.5e-9):
+    return O.AlCuParams(dx=dx)
+
+
+@gpu
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_golden_competitor_fraction_composition(torch_cuda, z, name):
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    h = AlCuTransport(z[f"{name}_labels"].shape, params(float(z[f"{name}_dx"])))
+    lab = dev(torch, z[f"{name}_labels"])
+    mask, comp = h.competitor(lab)
+    assert np.array_equal(host(mask), z[f"{name}_mask"]) and np.array_equal(host(comp), z[f"{name}_competitor"])
+    fp = h.precip_fraction(lab, dev(torch, z[f"{name}_alpha"]), comp)
+    assert same(host(fp), z[f"{name}_fprec"])
+    cm = h.matrix_composition(dev(torch, z[f"{name}_ctot"]), fp)
+    assert same(host(cm), z[f"{name}_cm"])
+    tr = h.interface_composition(cm, fp, z["taps_75"])
+    assert same(host(tr), z[f"{name}_trace"])
+
+
+@gpu
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_golden_diffusion(torch_cuda, z, name):
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    h = AlCuTransport(z[f"{name}_labels"].shape, params(float(z[f"{name}_dx"])))
+    c = dev(torch, z[f"{name}_ctot"])
+    cm, n = h.diffuse(c, dev(torch, z[f"{name}_fprec"]), float(z[f"{name}_dt"]))
+    assert n == int(z[f"{name}_substeps"])
+    assert same(host(c), z[f"{name}_diffused"]) and same(host(cm), z[f"{name}_cm_last"])
+
+
+@gpu
+@pytest.mark.parametrize("kind", ["grow", "shrink", "none"])
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_golden_partition_transfer(torch_cuda, z, name, kind):
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    h = AlCuTransport(z[f"{name}_labels"].shape, params(float(z[f"{name}_dx"])))
+    c = dev(torch, z[f"{name}_ctot"])
+    h.partition_transfer(c, dev(torch, z[f"{name}_fprec"]), dev(torch, z[f"{name}_pt_{kind}_new"]),
+                         dev(torch, z[f"{name}_trace"]), z["taps_75"])
+    assert same(host(c), z[f"{name}_pt_{kind}_out"])
+
+
+@gpu
+@pytest.mark.parametrize("sigma", [70, 120])
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_golden_gaussian_remap(torch_cuda, z, name, sigma):
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    h = AlCuTransport(z[f"{name}_labels"].shape, params())
+    lab = dev(torch, z[f"{name}_labels"])
+    al = dev(torch, z[f"{name}_alpha"])
+    n = h.gaussian_remap(lab, al, z[f"taps_{sigma}"])
+    tag = f"{name}_cgr_{sigma}"
+    assert n == int(z[f"{tag}_changed"])
+    assert np.array_equal(host(lab), z[f"{tag}_labels"]) and same(host(al), z[f"{tag}_alpha"])
+
+
+@gpu
+def test_dropins_on_numpy_match_golden(torch_cuda, z):
+    """The module-level functions take and return numpy like the reference."""
+    from gpk_b200 import alcu
+
+    name = "3d"
+    p = O.AlCuParams(dx=float(z[f"{name}_dx"]))
+    mask, comp = alcu.neighbor_competitor(z[f"{name}_labels"])
+    assert mask.dtype == bool and comp.dtype == np.int8
+    assert np.array_equal(mask, z[f"{name}_mask"]) and np.array_equal(comp, z[f"{name}_competitor"])
+    fp = alcu.precip_fraction(z[f"{name}_labels"], z[f"{name}_alpha"], comp)
+    assert same(fp, z[f"{name}_fprec"])
+    c, cm, n = alcu.diffuse_conservative_subcycled(z[f"{name}_ctot"], fp, p, float(z[f"{name}_dt"]))
+    assert same(c, z[f"{name}_diffused"]) and same(cm, z[f"{name}_cm_last"]) and n == int(z[f"{name}_substeps"])
+    c = z[f"{name}_ctot"].copy()
+    alcu.conservative_partition_transfer(c, fp, z[f"{name}_pt_grow_new"], z[f"{name}_trace"], p)
+    lab = z[f"{name}_labels"].copy()
+    al = z[f"{name}_alpha"].copy()
+    changed = alcu.conservative_gaussian_remap(lab, al, 0.70)
+    # numpy's exp on this host gives the taps; they agree with the recorded
+    # ones wherever the host's numpy rounds exp as the fixture's did
+    if np.array_equal(alcu.gauss_taps(0.70), z["taps_70"]) and np.array_equal(alcu.gauss_taps(0.75), z["taps_75"]):
+        assert same(c, z[f"{name}_pt_grow_out"])
+        assert changed == int(z[f"{name}_cgr_70_changed"]) and np.array_equal(lab, z[f"{name}_cgr_70_labels"])
+
+
+# --------------------------------------------------------------------------
+# larger seeded states against the oracle
+
+
+def plates(shape, n, rng, variants=3):
+    """int8 labels with n thin plates (normal along the variant's axis) and
+    jagged faces."""
+    lab = np.zeros(shape, dtype=np.int8)
+    nd = len(shape)
+    coords = np.indices(shape)
+    for k in range(n):
+        v = 1 + k % variants
+        c = [int(rng.integers(0, s)) for s in shape]
+        r = float(rng.uniform(4.0, 9.0))
+        axes = np.full(nd, r)
+        if v - 1 < nd:
+            axes[v - 1] = r / 5.0
+        d2 = 0.0
+        for a in range(nd):
+            d = np.abs(coords[a] - c[a])
+            d = np.minimum(d, shape[a] - d)
+            d2 = d2 + (d / axes[a]) ** 2
+        lab[(d2 <= 1.0) & (lab == 0)] = v
+    flip = rng.random(shape) < 0.08
+    nb = np.roll(lab, 1, axis=0)
+    grow = flip & (lab == 0) & (nb > 0)
+    lab[grow] = nb[grow]
+    lab[(rng.random(shape) < 0.05) & (lab > 0)] = 0
+    return lab
+
+
+def state(shape, rng, labels=None):
+    lab = plates(shape, 12, rng) if labels is None else labels
+    mask, comp = O.neighbor_competitor(lab)
+    alpha = np.ones(shape)
+    alpha[mask] = rng.uniform(0.05, 1.0, int(mask.sum()))
+    ctot = np.full(shape, 0.012) * (1.0 + 0.05 * rng.standard_normal(shape))
+    ctot[lab > 0] = 1.0 / 3.0
+    return lab, alpha, ctot, mask, comp
+
+
+def chain_labels(shape):
+    """Slabs of label 1, two cells thick, one cell apart along axis 0 (each a
+    component of its own, each interacting with the next: a chain of waves),
+    and a plane of another label two cells from all of them."""
+    lab = np.zeros(shape, dtype=np.int8)
+    for x in range(1, shape[0] - 2, 3):
+        lab[x:x + 2, 2:shape[1] - 2] = 1
+    lab[:, shape[1] - 1] = 3 if len(shape) == 3 else 2
+    return lab
+
+
+CASES = [
+    ("plates_96", (96, 96, 96), None),
+    ("odd_2d", (67, 45), None),
+    ("thin_3d", (5, 40, 33), None),
+    ("chain_3d", (40, 24, 10), "chain"),
+    ("chain_2d", (61, 30), "chain"),
+    ("empty", (20, 18, 16), "empty"),
+    ("full", (12, 14, 10), "full"),
+]
+
+
+def case_state(shape, kind, seed):
+    rng = np.random.default_rng(seed)
+    if kind == "chain":
+        return state(shape, rng, chain_labels(shape))
+    if kind == "empty":
+        return state(shape, rng, np.zeros(shape, dtype=np.int8))
+    if kind == "full":
+        return state(shape, rng, np.full(shape, 2, dtype=np.int8))
+    return state(shape, rng)
+
+
+@gpu
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_transport_against_oracle(torch_cuda, case):
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    name, shape, kind = case
+    lab, alpha, ctot, mask, comp = case_state(shape, kind, 7)
+    p = params(0.5e-9 if len(shape) == 2 else 1.5e-9)
+    h = AlCuTransport(shape, p)
+    dl = dev(torch, lab)
+    m, c = h.competitor(dl)
+    assert np.array_equal(host(m), mask) and np.array_equal(host(c), comp)
+    fp_ref = O.precip_fraction(lab, alpha, comp)
+    fp = h.precip_fraction(dl, dev(torch, alpha), c)
+    assert same(host(fp), fp_ref)
+    cm_ref = O.matrix_composition(ctot, fp_ref, p)
+    cm = h.matrix_composition(dev(torch, ctot), fp)
+    assert same(host(cm), cm_ref)
+    tr_ref = O.interface_matrix_composition(cm_ref, fp_ref, p)
+    tr = h.interface_composition(cm, fp, 0.75)
+    assert same(host(tr), tr_ref)
+    for dt in (10.0, 3.0):
+        c_ref, cml_ref, n_ref = O.diffuse_conservative_subcycled(ctot.copy(), fp_ref, p, dt)
+        cd = dev(torch, ctot)
+        cml, n = h.diffuse(cd, fp, dt)
+        assert n == n_ref and same(host(cd), c_ref) and same(host(cml), cml_ref)
+    rng = np.random.default_rng(11)
+    for sign in (1.0, -1.0):
+        new = np.clip(fp_ref + sign * rng.uniform(0.0, 0.3, shape) * mask, -0.2, 1.2)
+        c_ref = ctot.copy()
+        err_ref = None
+        try:
+            O.conservative_partition_transfer(c_ref, fp_ref, new, tr_ref, p)
+        except RuntimeError as e:
+            err_ref = str(e)
+        cd = dev(torch, ctot)
+        err = None
+        try:
+            h.partition_transfer(cd, fp, dev(torch, new), tr, 0.75)
+        except RuntimeError as e:
+            err = str(e)
+        assert (err is None) == (err_ref is None)
+        if err_ref is not None:
+            assert err_ref in err
+        assert same(host(cd), c_ref)
+    g = h.gaussian_filter(dev(torch, ctot), 2.0)
+    assert same(host(g), O.gaussian_filter_wrap(ctot, 2.0))
+    assert h.sum(dev(torch, ctot)) == float(np.sum(ctot))
+
+
+@gpu
+@pytest.mark.parametrize("sigma", [0.70, 1.2, 2.0])
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_gaussian_remap_against_oracle(torch_cuda, case, sigma):
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    name, shape, kind = case
+    if name == "plates_96" and sigma != 0.70:
+        pytest.skip("the oracle's per-component full-field filters are slow at 96^3")
+    lab, alpha, _, _, _ = case_state(shape, kind, 3)
+    lr, ar = lab.copy(), alpha.copy()
+    n_ref = O.conservative_gaussian_remap(lr, ar, sigma)
+    h = AlCuTransport(shape, params())
+    dl, da = dev(torch, lab), dev(torch, alpha)
+    n = h.gaussian_remap(dl, da, sigma)
+    assert n == n_ref
+    assert np.array_equal(host(dl), lr) and same(host(da), ar)
+    info = h.info()
+    if kind == "chain":
+        assert info["waves"] > 2
+    if kind == "empty":
+        assert info["components"] == 0 and n == 0
+
+
+@gpu
+def test_partition_transfer_errors_match_oracle(torch_cuda):
+    from gpk_b200 import GPKError
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    p = params()
+    shape = (12, 10)
+    h = AlCuTransport(shape, p)
+    old = np.zeros(shape)
+    new = np.zeros(shape)
+    new[5, 5] = 0.5
+    cases = [(np.full(shape, -0.5), old, new, np.full(shape, p.c_matrix_eq), "insufficient matrix Cu"),
+             (np.full(shape, 0.2), np.full(shape, 0.5), np.ones(shape), np.full(shape, 0.01),
+              "empty matrix neighbourhood")]
+    for c0, o, nw, mc, msg in cases:
+        c_ref = c0.copy()
+        with pytest.raises(RuntimeError, match=msg):
+            O.conservative_partition_transfer(c_ref, o, nw, mc, p)
+        cd = dev(torch, c0)
+        with pytest.raises(GPKError, match=msg) as e:
+            h.partition_transfer(cd, dev(torch, o), dev(torch, nw), dev(torch, mc), 0.75)
+        assert e.value.code == 9
+        assert same(host(cd), c_ref)  # the transfer without correction, as the reference leaves it
+
+
+@gpu
+def test_full_size_properties_256(torch_cuda):
+    """256^3: sums bit-equal to np.sum, the remap keeps every label's
+    volume, diffusion and partition transfer keep the summed Cu."""
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    shape = (256, 256, 256)
+    # 400 plates (17 x 17 x 3 boxes, thin along the variant's axis) drawn on the device
+    g = torch.Generator(device="cuda").manual_seed(1)
+    lab_t = torch.zeros(shape, dtype=torch.int8, device="cuda")
+    centres = torch.randint(0, 256, (400, 3), generator=g, device="cuda").tolist()
+    for k, ctr in enumerate(centres):
+        v = 1 + k % 3
+        sl = [slice(max(q - 8, 0), q + 9) for q in ctr]
+        sl[v - 1] = slice(max(ctr[v - 1] - 1, 0), ctr[v - 1] + 2)
+        box = lab_t[tuple(sl)]
+        box[box == 0] = v
+    h = AlCuTransport(shape, params())
+    counts0 = torch.bincount(lab_t.flatten().long(), minlength=4).tolist()
+    alpha = torch.rand(shape, dtype=torch.float64, device="cuda", generator=g)
+    n = h.gaussian_remap(lab_t, alpha, 0.70)
+    counts1 = torch.bincount(lab_t.flatten().long(), minlength=4).tolist()
+    assert counts0 == counts1 and n > 0
+    assert h.info()["components"] >= 300
+    ctot = torch.rand(shape, dtype=torch.float64, device="cuda", generator=g) * 0.02
+    assert h.sum(ctot) == float(np.sum(ctot.cpu().numpy()))
+    mask, comp = h.competitor(lab_t)
+    fp = h.precip_fraction(lab_t, alpha, comp)
+    s0 = h.sum(ctot)
+    c2 = ctot.clone()
+    h.diffuse(c2, fp, 10.0)
+    assert abs(h.sum(c2) - s0) <= 1e-12 * abs(s0)
+    cm = h.matrix_composition(ctot, fp)
+    tr = h.interface_composition(cm, fp, 0.75)
+    new = torch.clamp(fp + 0.2 * torch.rand(shape, dtype=torch.float64, device="cuda", generator=g) * mask, 0.0, 1.0)
+    h.partition_transfer(ctot, fp, new, tr, 0.75)
+    assert abs(h.sum(ctot) - s0) <= 1e-12 * abs(s0)
