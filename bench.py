@@ -242,6 +242,143 @@ def spectral_measurement(with_cpu: bool):
     return res
 
 
+def _alcu_state(shape, plates, rng):
+    """int8 labels with theta-prime plates (thin along the variant's axis,
+    aspect 8 as in the reference's embryos), alpha, and total Cu as the
+    reference's initial_state sets them (matrix at the composition that keeps
+    the mean at c0 = 0.0169, precipitates at c_theta)."""
+    import numpy as np
+    lab = np.zeros(shape, dtype=np.int8)
+    coords = np.indices(shape)
+    for centre, v, scale in plates:
+        axes = np.full(3, 6.0 * scale)
+        axes[v - 1] /= 8.0
+        d2 = 0.0
+        for a in range(3):
+            d = np.abs(coords[a] - centre[a])
+            d = np.minimum(d, shape[a] - d)
+            d2 = d2 + (d / axes[a]) ** 2
+        lab[d2 <= 1.0] = v
+    f0 = float(np.mean(lab > 0))
+    cm0 = (0.0169 - f0 / 3.0) / (1.0 - f0)
+    ctot = np.full(shape, cm0)
+    ctot[lab > 0] = 1.0 / 3.0
+    alpha = np.ones(shape)
+    return lab, alpha, ctot
+
+
+def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
+    """The Al-Cu module's per-step transport and remap (competitor,
+    precipitate fraction, matrix composition, interface composition, sub-cycled
+    diffusion, partition transfer, Gaussian remap), FP64, on the reference's
+    three_dimensional case (96^3, three plates of its layout_3d_96) and on a
+    256^3 field with 400 plates; inputs resident, each stage timed with CUDA
+    events on the launching stream."""
+    import numpy as np
+    import torch
+    from gpk_b200.alcu import AlCuTransport
+    from oracle import alcu_oracle as O
+
+    out = {}
+    cases = {
+        "96^3 reference three_dimensional layout": ((96, 96, 96), [((24, 24, 24), 1, 1.05), ((72, 27, 68), 2, 0.95),
+                                                                    ((29, 72, 69), 3, 1.00)]),
+    }
+    rng = np.random.default_rng(3)
+    many = [(tuple(int(q) for q in rng.integers(0, 256, 3)), 1 + k % 3, float(rng.uniform(1.0, 2.5)))
+            for k in range(400)]
+    cases["256^3, 400 plates"] = ((256, 256, 256), many)
+    p = O.AlCuParams()
+    stages = ["competitor", "fraction", "composition", "interface", "diffuse", "transfer", "remap"]
+    # algorithmic bytes per cell of each stage (each field read or written
+    # once; labels 1 B, fields 8 B): competitor 1 + 2, fraction 10 + 8,
+    # composition 16 + 8, interface composition 16 + 16 in, 3 passes of 2
+    # fields 32 each, 16 + 8 out, diffusion 2 substeps of 16 + 8 and the last
+    # c_m 8, partition transfer (transfer 32 + 24, 4 sums 32, 3 passes 48,
+    # weight 24 + 16, apply 16 + 8, argmax 16), remap (labels copy 2, union-
+    # find 4 x 4, flags / scatter / vacate per wave 10, changed 1 + 8)
+    per_cell = {"competitor": 3, "fraction": 18, "composition": 24, "interface": 152, "diffuse": 56,
+                "transfer": 216, "remap": 37}
+    peak, peak_kind = _peaks()
+    for name, (shape, plates) in cases.items():
+        lab, alpha, ctot = _alcu_state(shape, plates, rng)
+        n = int(np.prod(shape))
+        h = AlCuTransport(shape, p)
+        dl = torch.from_numpy(lab).cuda()
+        da = torch.from_numpy(alpha).cuda()
+        dc = torch.from_numpy(ctot).cuda()
+        # a fixed synthetic growth of the fraction at interface cells
+        m0, _ = h.competitor(dl)
+        grow = (0.05 * m0.double()).contiguous()
+        stream = torch.cuda.current_stream()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(stages) + 1)]
+        acc = {k: 0.0 for k in stages}
+        info = {}
+
+        def step(timed):
+            if timed:
+                ev[0].record(stream)
+            mask, comp = h.competitor(dl)
+            if timed:
+                ev[1].record(stream)
+            fp = h.precip_fraction(dl, da, comp)
+            if timed:
+                ev[2].record(stream)
+            cm = h.matrix_composition(dc, fp)
+            if timed:
+                ev[3].record(stream)
+            trace = h.interface_composition(cm, fp, 0.75)
+            if timed:
+                ev[4].record(stream)
+            h.diffuse(dc, fp, 10.0)
+            if timed:
+                ev[5].record(stream)
+            h.partition_transfer(dc, fp, fp + grow, trace, 0.75)
+            if timed:
+                ev[6].record(stream)
+            info["changed"] = h.gaussian_remap(dl, da, 0.70)
+            if timed:
+                ev[7].record(stream)
+
+        for _ in range(warmup):
+            step(False)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(steps):
+            step(True)
+            ev[-1].synchronize()
+            for k, st in enumerate(stages):
+                acc[st] += ev[k].elapsed_time(ev[k + 1])
+        t1.record(stream)
+        t1.synchronize()
+        ms = t0.elapsed_time(t1) / steps
+        st_ms = {k: v / steps for k, v in acc.items()}
+        res = {"ms_per_step": ms, "cells_per_s": n / (ms / 1e3), "stages_ms": st_ms,
+               "components": h.info()["components"], "remap_waves": h.info()["waves"],
+               "changed_last_step": info["changed"],
+               "stage_GBps": {k: per_cell[k] * n / (st_ms[k] / 1e3) / 1e9 for k in stages if st_ms[k] > 0},
+               "algorithmic_bytes_per_cell": per_cell, "peak": peak, "peak_kind": peak_kind}
+        if with_cpu and shape == (96, 96, 96):
+            lab_h, al_h, c_h = lab.copy(), alpha.copy(), ctot.copy()
+            g_h = grow.cpu().numpy()
+            t_cpu = time.perf_counter()
+            mask_h, comp_h = O.neighbor_competitor(lab_h)
+            fp_h = O.precip_fraction(lab_h, al_h, comp_h)
+            cm_h = O.matrix_composition(c_h, fp_h, p)
+            tr_h = O.interface_matrix_composition(cm_h, fp_h, p)
+            c_h, _, _ = O.diffuse_conservative_subcycled(c_h, fp_h, p, 10.0)
+            O.conservative_partition_transfer(c_h, fp_h, fp_h + g_h, tr_h, p)
+            O.conservative_gaussian_remap(lab_h, al_h, 0.70)
+            cpu_s = time.perf_counter() - t_cpu
+            res["cpu_baseline"] = {"value": n / cpu_s, "unit": "cells/s", "cores": 1, "kind": "port",
+                                   "sample": "one step of the numpy restatement of the same seven functions "
+                                             "(numpy/scipy order, one thread) on the 96^3 state"}
+        out[name] = res
+        h.close()
+    return out
+
+
 def batched_measurement(n_inst: int = 512, steps: int = 10, warmup: int = 3, ws: int = 1, rank: int = 0):
     """The lamellar-precipitate sweep: n_inst 2-D instances of sides
     U{64..512} (FP64, OstwaldThermo), advanced together by the batch engine
@@ -580,12 +717,17 @@ def main():
     ap.add_argument("--adjoint-only", action="store_true", help="time only the 512^2 adjoint gradient")
     ap.add_argument("--coupled-only", action="store_true",
                     help="time only the 128^3 solidification step with a spectral solve per step")
+    ap.add_argument("--alcu-only", action="store_true",
+                    help="time only the Al-Cu transport and remap chain (96^3 and 256^3)")
     ap.add_argument("--spectral-only", action="store_true",
                     help="time only the 128^3 spectral elasticity solve (profiling its kernels)")
     args = ap.parse_args()
     globals()["SIZE"], globals()["GRAINS"] = args.size, args.grains
     if args.spectral_only:
         print(json.dumps({"spectral": spectral_measurement(not args.no_cpu)}))
+        return 0
+    if args.alcu_only:
+        print(json.dumps({"alcu": alcu_measurement(not args.no_cpu)}))
         return 0
     if args.coupled_only:
         print(json.dumps({"coupled": coupled_measurement()}))

@@ -752,8 +752,10 @@ int gauss(gpk_alcu* h, const Taps& t, const double* in, double* out, double* tmp
     }
     return GPK_OK;
 }
-// two fields smoothed together, results in a and b (ta, tb: scratch)
-int gauss2(gpk_alcu* h, const Taps& t, double* a, double* b, double* ta, double* tb) {
+// two fields smoothed together (ta, tb: scratch); *ra, *rb point at the
+// results, which lie in (a, b) or (ta, tb) depending on the pass count
+int gauss2(gpk_alcu* h, const Taps& t, double* a, double* b, double* ta, double* tb, const double** ra,
+           const double** rb) {
     const Ext& d = h->d;
     double *sa = a, *sb = b, *da = ta, *db = tb;
     for (int ax = 0; ax < d.ndim; ++ax) {
@@ -762,10 +764,8 @@ int gauss2(gpk_alcu* h, const Taps& t, double* a, double* b, double* ta, double*
         std::swap(sa, da);
         std::swap(sb, db);
     }
-    if (sa != a) {
-        ALCU_TRY(cudaMemcpyAsync(a, sa, sizeof(double) * d.N, cudaMemcpyDeviceToDevice, h->stream));
-        ALCU_TRY(cudaMemcpyAsync(b, sb, sizeof(double) * d.N, cudaMemcpyDeviceToDevice, h->stream));
-    }
+    *ra = sa;
+    *rb = sb;
     return GPK_OK;
 }
 
@@ -1089,8 +1089,9 @@ extern "C" int gpk_alcu_interface_composition(gpk_alcu* h, const double* cm, con
     double *num = h->f[1], *den = h->f[2];
     k_ic_pre<<<h->grid, 256, 0, h->stream>>>(N, cm, fprec, num, den);
     ALCU_TRY(cudaGetLastError());
-    if ((rc = gauss2(h, t, num, den, h->f[3], h->f[4])) != GPK_OK) return rc;
-    k_ic_post<<<h->grid, 256, 0, h->stream>>>(N, h->p.ct, num, den, trace);
+    const double *rn = nullptr, *rd = nullptr;
+    if ((rc = gauss2(h, t, num, den, h->f[3], h->f[4], &rn, &rd)) != GPK_OK) return rc;
+    k_ic_post<<<h->grid, 256, 0, h->stream>>>(N, h->p.ct, rn, rd, trace);
     ALCU_TRY(cudaGetLastError());
     return GPK_OK;
 }
