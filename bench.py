@@ -244,21 +244,24 @@ def spectral_measurement(with_cpu: bool):
 
 def _alcu_state(shape, plates, rng):
     """int8 labels with theta-prime plates (thin along the variant's axis,
-    aspect 8 as in the reference's embryos), alpha, and total Cu as the
-    reference's initial_state sets them (matrix at the composition that keeps
-    the mean at c0 = 0.0169, precipitates at c_theta)."""
+    aspect 8 as in the reference's embryos, periodic minimum image), alpha,
+    and total Cu as the reference's initial_state sets them (matrix at the
+    composition that keeps the mean at c0 = 0.0169, precipitates at
+    c_theta).  Each plate is drawn in its own periodic window."""
     import numpy as np
     lab = np.zeros(shape, dtype=np.int8)
-    coords = np.indices(shape)
     for centre, v, scale in plates:
         axes = np.full(3, 6.0 * scale)
         axes[v - 1] /= 8.0
-        d2 = 0.0
-        for a in range(3):
-            d = np.abs(coords[a] - centre[a])
-            d = np.minimum(d, shape[a] - d)
-            d2 = d2 + (d / axes[a]) ** 2
-        lab[d2 <= 1.0] = v
+        half = [int(np.ceil(a)) for a in axes]
+        offs = [np.arange(-h, h + 1) for h in half]
+        idx = [(centre[a] + offs[a]) % shape[a] for a in range(3)]
+        d2 = ((offs[0][:, None, None] / axes[0]) ** 2 + (offs[1][None, :, None] / axes[1]) ** 2
+              + (offs[2][None, None, :] / axes[2]) ** 2)
+        win = np.ix_(*idx)
+        sub = lab[win]
+        sub[d2 <= 1.0] = v
+        lab[win] = sub
     f0 = float(np.mean(lab > 0))
     cm0 = (0.0169 - f0 / 3.0) / (1.0 - f0)
     ctot = np.full(shape, cm0)
