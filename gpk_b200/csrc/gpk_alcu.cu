@@ -26,13 +26,18 @@
 //    dilations meet.  Components are scheduled in waves (the longest chain of
 //    earlier interacting components, relaxed to a fixed point over the cells
 //    where dilations meet); a wave's components run together and the result
-//    is that of the serial order.  Per wave: candidates compacted in cell
-//    order, scores evaluated per candidate from the component's indicator
+//    is that of the serial order.  The cells of any component's dilation
+//    (the band: the 3^d box maximum of the active cells, three separable
+//    passes, then an exact test) are compacted once per call; per wave,
+//    candidates are compacted from the band in cell order, scores evaluated
+//    per candidate from the component's indicator
 //    (the three passes restricted to the (2r+1)^d box, same operations), two
 //    stable radix sorts (score descending, then component), and the first
 //    `size` entries of each component's run take its label.
 //
-// Every kernel is HBM- or latency-bound FP64 work; none is a contraction.
+// Cell kernels take their coordinates from a 3-D launch (a 2-D field is held
+// as 1 x n0 x n1); periodic neighbours wrap by a compare.  Every kernel is
+// HBM- or latency-bound FP64 work; none is a contraction.
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 
@@ -55,9 +60,10 @@ namespace {
     } while (0)
 
 struct Ext {
-    int e[3];        // extents (e[2] = 1 in 2-D)
+    int e[3];        // extents; a 2-D field (n0, n1) is held as (1, n0, n1)
     long long st[3]; // strides of the C-order layout
     int ndim;
+    int a0;          // first axis that belongs to the field (3 - ndim)
     long long N;
 };
 
@@ -74,11 +80,10 @@ __device__ __forceinline__ int wrapi(int x, int n) {
     const int r = x % n;
     return r < 0 ? r + n : r;
 }
-__device__ __forceinline__ void coords(const Ext& d, long long i, int x[3]) {
-    x[2] = (int)(i % d.e[2]);
-    const long long t = i / d.e[2];
-    x[1] = (int)(t % d.e[1]);
-    x[0] = (int)(t / d.e[1]);
+// x + off on a periodic axis of n points; `near` when |off| <= n
+__device__ __forceinline__ int wrap_off(int y, int n, bool near) {
+    if (near) return y < 0 ? y + n : (y >= n ? y - n : y);
+    return wrapi(y, n);
 }
 // numpy's float maximum / clip (no NaN reaches these here): the first
 // argument is kept only when strictly beyond the bound
@@ -88,20 +93,34 @@ __device__ __forceinline__ double np_clip(double x, double lo, double hi) { retu
 #define GRID_STRIDE(i, n) \
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
 
+// one thread per cell of a (32 x 4) block tile of axes 2 and 1, looping over
+// axis 0: the coordinates come from the launch, not from divisions
+#define CELLS3(d)                                                                           \
+    for (int x1 = blockIdx.y * 4 + threadIdx.y; x1 < (d).e[1]; x1 += gridDim.y * 4)         \
+        for (int x0 = blockIdx.z; x0 < (d).e[0]; x0 += gridDim.z)                           \
+            if (const int x2 = blockIdx.x * 32 + threadIdx.x; x2 < (d).e[2])
+#define CELL_INDEX(d) (((long long)x0 * (d).e[1] + x1) * (d).e[2] + x2)
+
 // ---------------------------------------------------------------- elementwise
 
-__global__ void k_competitor(Ext d, const int8_t* __restrict__ lab, uint8_t* __restrict__ mask,
-                             int8_t* __restrict__ comp) {
-    GRID_STRIDE(i, d.N) {
-        int x[3];
-        coords(d, i, x);
+__global__ void __launch_bounds__(128) k_competitor(Ext d, const int8_t* __restrict__ lab, uint8_t* __restrict__ mask,
+                                                    int8_t* __restrict__ comp) {
+    CELLS3(d) {
+        const long long i = CELL_INDEX(d);
+        const int x[3] = {x0, x1, x2};
         const int8_t l = lab[i];
         bool m = false, mat = false;
         int s1 = 0, s2 = 0, s3 = 0;
-        for (int a = 0; a < d.ndim; ++a) {
-            for (int sgn = -1; sgn <= 1; sgn += 2) {
-                const int y = wrapi(x[a] + sgn, d.e[a]);
-                const int8_t nb = lab[i + (long long)(y - x[a]) * d.st[a]];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (a < d.a0) continue;
+            const int n = d.e[a];
+            const long long ip = i + (long long)((x[a] + 1 == n ? 0 : x[a] + 1) - x[a]) * d.st[a];
+            const long long im = i + (long long)((x[a] == 0 ? n - 1 : x[a] - 1) - x[a]) * d.st[a];
+            const int8_t nbs[2] = {lab[im], lab[ip]};
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int8_t nb = nbs[q];
                 m |= nb != l;
                 mat |= nb == 0;
                 s1 += nb == 1;
@@ -143,18 +162,22 @@ __global__ void k_matrix_composition(long long N, Phys p, const double* __restri
 }
 
 // one explicit substep of diffuse_conservative (lines 679-688)
-__global__ void k_diffuse(Ext d, Phys p, double dt, const double* __restrict__ c, const double* __restrict__ f,
-                          double* __restrict__ out, double* __restrict__ cm_out) {
-    GRID_STRIDE(i, d.N) {
-        int x[3];
-        coords(d, i, x);
+__global__ void __launch_bounds__(128) k_diffuse(Ext d, Phys p, double dt, const double* __restrict__ c,
+                                                 const double* __restrict__ f, double* __restrict__ out,
+                                                 double* __restrict__ cm_out) {
+    CELLS3(d) {
+        const long long i = CELL_INDEX(d);
+        const int x[3] = {x0, x1, x2};
         double mc, cmc;
         lever(c[i], f[i], p, mc, cmc);
         const double nD = -p.D;
         double dc = 0.0;
-        for (int a = 0; a < d.ndim; ++a) {
-            const long long ip = i + (long long)(wrapi(x[a] + 1, d.e[a]) - x[a]) * d.st[a];
-            const long long im = i + (long long)(wrapi(x[a] - 1, d.e[a]) - x[a]) * d.st[a];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (a < d.a0) continue;
+            const int n = d.e[a];
+            const long long ip = i + (long long)((x[a] + 1 == n ? 0 : x[a] + 1) - x[a]) * d.st[a];
+            const long long im = i + (long long)((x[a] == 0 ? n - 1 : x[a] - 1) - x[a]) * d.st[a];
             double mp, cmp, mm, cmm;
             lever(c[ip], f[ip], p, mp, cmp);
             lever(c[im], f[im], p, mm, cmm);
@@ -173,22 +196,24 @@ __global__ void k_diffuse(Ext d, Phys p, double dt, const double* __restrict__ c
 
 // ---------------------------------------------------------------- Gaussian
 
-// one periodic pass along `axis` of NF fields
-template <int NF>
-__global__ void k_gauss_pass(Ext d, int axis, Taps t, const double* __restrict__ a0, const double* __restrict__ a1,
-                             double* __restrict__ o0, double* __restrict__ o1) {
-    const int n = d.e[axis];
-    const long long s = d.st[axis];
-    GRID_STRIDE(i, d.N) {
-        int x[3];
-        coords(d, i, x);
-        const long long base = i - (long long)x[axis] * s;
+// one periodic pass along axis AX of NF fields
+template <int NF, int AX>
+__global__ void __launch_bounds__(128) k_gauss_pass(Ext d, Taps t, const double* __restrict__ a0,
+                                                    const double* __restrict__ a1, double* __restrict__ o0,
+                                                    double* __restrict__ o1) {
+    const int n = d.e[AX];
+    const long long s = d.st[AX];
+    const bool near = t.r <= n;
+    CELLS3(d) {
+        const long long i = CELL_INDEX(d);
+        const int xa = AX == 0 ? x0 : (AX == 1 ? x1 : x2);
+        const long long base = i - (long long)xa * s;
         double v0 = a0[i] * t.w[0];
         double v1 = 0.0;
         if (NF == 2) v1 = a1[i] * t.w[0];
         for (int j = t.r; j >= 1; --j) {
-            const long long lo = base + (long long)wrapi(x[axis] - j, n) * s;
-            const long long hi = base + (long long)wrapi(x[axis] + j, n) * s;
+            const long long lo = base + (long long)wrap_off(xa - j, n, near) * s;
+            const long long hi = base + (long long)wrap_off(xa + j, n, near) * s;
             v0 = v0 + (a0[lo] + a0[hi]) * t.w[j];
             if (NF == 2) v1 = v1 + (a1[lo] + a1[hi]) * t.w[j];
         }
@@ -398,14 +423,16 @@ __global__ void k_cc_init(long long N, int* __restrict__ parent, int* __restrict
     }
 }
 // face neighbours without wrap, equal nonzero labels
-__global__ void k_cc_union(Ext d, const int8_t* __restrict__ lab, int* parent, unsigned* err) {
-    GRID_STRIDE(i, d.N) {
+__global__ void __launch_bounds__(128) k_cc_union(Ext d, const int8_t* __restrict__ lab, int* parent, unsigned* err) {
+    CELLS3(d) {
+        const long long i = CELL_INDEX(d);
         const int8_t l = lab[i];
         if (l == 0) continue;
-        int x[3];
-        coords(d, i, x);
-        for (int a = 0; a < d.ndim; ++a)
-            if (x[a] + 1 < d.e[a] && lab[i + d.st[a]] == l) uf_unite(parent, (int)i, (int)(i + d.st[a]), err);
+        const int x[3] = {x0, x1, x2};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            if (a >= d.a0 && x[a] + 1 < d.e[a] && lab[i + d.st[a]] == l)
+                uf_unite(parent, (int)i, (int)(i + d.st[a]), err);
     }
 }
 __global__ void k_cc_finish(long long N, const int8_t* __restrict__ lab, int* parent, int* __restrict__ root,
@@ -420,19 +447,40 @@ __global__ void k_cc_finish(long long N, const int8_t* __restrict__ lab, int* pa
         atomicAdd(&size[r], 1);
     }
 }
+// cells of components of more than one cell; their count of components
+__global__ void k_cgr_active(long long N, const int* __restrict__ root, const int* __restrict__ size,
+                             uint8_t* __restrict__ act, int* __restrict__ n_active) {
+    GRID_STRIDE(i, N) {
+        const int r = root[i];
+        const bool a = r >= 0 && size[r] > 1;
+        act[i] = a;
+        if (a && r == (int)i) atomicAdd(n_active, 1);
+    }
+}
+// one axis of the 3^d box maximum (no wrap)
+template <int AX>
+__global__ void __launch_bounds__(128) k_box_pass(Ext d, const uint8_t* __restrict__ in, uint8_t* __restrict__ out) {
+    CELLS3(d) {
+        const long long i = CELL_INDEX(d);
+        const int xa = AX == 0 ? x0 : (AX == 1 ? x1 : x2);
+        uint8_t v = in[i];
+        if (xa > 0) v |= in[i - d.st[AX]];
+        if (xa + 1 < d.e[AX]) v |= in[i + d.st[AX]];
+        out[i] = v;
+    }
+}
 
 // the components (of more than one cell) with a cell in the 3^d box of x,
 // without wrap; returns how many (at most 27)
-__device__ __forceinline__ int box_components(const Ext& d, const int x[3], long long i, const int* __restrict__ root,
-                                              const int* __restrict__ size, int S[27]) {
+__device__ __forceinline__ int box_components(const Ext& d, int x0, int x1, int x2, long long i,
+                                              const int* __restrict__ root, const int* __restrict__ size, int S[27]) {
     int n = 0;
-    const int lo2 = d.ndim == 3 ? -1 : 0, hi2 = d.ndim == 3 ? 1 : 0;
     for (int o0 = -1; o0 <= 1; ++o0) {
-        if (x[0] + o0 < 0 || x[0] + o0 >= d.e[0]) continue;
+        if (x0 + o0 < 0 || x0 + o0 >= d.e[0]) continue;
         for (int o1 = -1; o1 <= 1; ++o1) {
-            if (x[1] + o1 < 0 || x[1] + o1 >= d.e[1]) continue;
-            for (int o2 = lo2; o2 <= hi2; ++o2) {
-                if (x[2] + o2 < 0 || x[2] + o2 >= d.e[2]) continue;
+            if (x1 + o1 < 0 || x1 + o1 >= d.e[1]) continue;
+            for (int o2 = -1; o2 <= 1; ++o2) {
+                if (x2 + o2 < 0 || x2 + o2 >= d.e[2]) continue;
                 const int r = root[i + o0 * d.st[0] + o1 * d.st[1] + o2 * d.st[2]];
                 if (r < 0 || size[r] <= 1) continue;
                 bool seen = false;
@@ -443,21 +491,41 @@ __device__ __forceinline__ int box_components(const Ext& d, const int x[3], long
     }
     return n;
 }
+__device__ __forceinline__ void cell_coords(const Ext& d, long long i, int& x0, int& x1, int& x2) {
+    unsigned u = (unsigned)i;
+    x2 = (int)(u % (unsigned)d.e[2]);
+    u /= (unsigned)d.e[2];
+    x1 = (int)(u % (unsigned)d.e[1]);
+    x0 = (int)(u / (unsigned)d.e[1]);
+}
 
 // the reference's processing order: label ascending, then first cell
 __device__ __forceinline__ long long order_key(const int8_t* __restrict__ orig, int r) {
     return ((long long)((int)orig[r] + 128) << 32) | (long long)r;
 }
 
-__global__ void k_cgr_conflicts(Ext d, const int* __restrict__ root, const int* __restrict__ size,
-                                int* __restrict__ list, int* __restrict__ count, int* __restrict__ n_active) {
-    GRID_STRIDE(i, d.N) {
-        const int r = root[i];
-        if (r == (int)i && size[r] > 1) atomicAdd(n_active, 1);
-        int x[3];
-        coords(d, i, x);
-        int S[27];
-        if (box_components(d, x, i, root, size, S) >= 2) list[atomicAdd(count, 1)] = (int)i;
+// band = cells of some component's dilation; conflicts = cells of two or more
+__global__ void __launch_bounds__(128) k_cgr_band(Ext d, const uint8_t* __restrict__ near, const int* __restrict__ root,
+                                                  const int* __restrict__ size, int* __restrict__ flag,
+                                                  int* __restrict__ list, int* __restrict__ count) {
+    CELLS3(d) {
+        const long long i = CELL_INDEX(d);
+        int f = 0;
+        if (near[i]) {
+            int S[27];
+            const int n = box_components(d, x0, x1, x2, i, root, size, S);
+            f = n >= 1;
+            if (n >= 2) list[atomicAdd(count, 1)] = (int)i;
+        }
+        flag[i] = f;
+    }
+}
+// order-preserving compaction: out[pos[q]] = (idx ? idx[q] : q) where flag[q]
+__global__ void k_compact(long long M, const int* __restrict__ flag, const int* __restrict__ pos,
+                          const int* __restrict__ idx, int* __restrict__ out, int* __restrict__ count) {
+    GRID_STRIDE(q, M) {
+        if (flag[q]) out[pos[q]] = idx ? idx[q] : (int)q;
+        if (q == M - 1) *count = pos[q] + flag[q];
     }
 }
 
@@ -466,10 +534,10 @@ __global__ void k_cgr_relax(Ext d, const int* __restrict__ list, int M, const in
                             int* __restrict__ changed) {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
         const long long i = list[q];
-        int x[3];
-        coords(d, i, x);
+        int x0, x1, x2;
+        cell_coords(d, i, x0, x1, x2);
         int S[27];
-        const int n = box_components(d, x, i, root, size, S);
+        const int n = box_components(d, x0, x1, x2, i, root, size, S);
         for (int b = 0; b < n; ++b) {
             const long long kb = order_key(orig, S[b]);
             int m = __ldcg(&wave[S[b]]);
@@ -492,58 +560,47 @@ __global__ void k_cgr_max_wave(long long N, const int* __restrict__ root, const 
     GRID_STRIDE(i, N) if (root[i] == (int)i && size[i] > 1) atomicMax(max_wave, wave[i]);
 }
 
-// candidates of wave w: cells of the dilation of a wave-w component that are
-// zero or its own
-__global__ void k_cgr_flags(Ext d, int w, const int8_t* __restrict__ lab, const int* __restrict__ root,
-                            const int* __restrict__ size, const int* __restrict__ wave, int* __restrict__ flag,
-                            int* __restrict__ seg) {
-    GRID_STRIDE(i, d.N) {
-        int x[3];
-        coords(d, i, x);
+// candidates of wave w among the band: cells of the dilation of a wave-w
+// component that are zero or its own
+__global__ void k_cgr_flags(Ext d, int w, const int* __restrict__ band, const int* __restrict__ n_band,
+                            const int8_t* __restrict__ lab, const int* __restrict__ root, const int* __restrict__ size,
+                            const int* __restrict__ wave, int* __restrict__ flag, int* __restrict__ seg) {
+    const int M = *n_band;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
+        const long long i = band[q];
+        int x0, x1, x2;
+        cell_coords(d, i, x0, x1, x2);
         int S[27];
-        const int n = box_components(d, x, i, root, size, S);
+        const int n = box_components(d, x0, x1, x2, i, root, size, S);
         int B = -1;
-        for (int q = 0; q < n; ++q)
-            if (wave[S[q]] == w) B = S[q];
-        const int f = B >= 0 && (root[i] == B || lab[i] == 0);
-        flag[i] = f;
+        for (int k = 0; k < n; ++k)
+            if (wave[S[k]] == w) B = S[k];
+        flag[q] = B >= 0 && (root[i] == B || lab[i] == 0);
         seg[i] = B;
     }
 }
-__global__ void k_cgr_scatter(long long N, const int* __restrict__ flag, const int* __restrict__ pos,
-                              int* __restrict__ cand, int* __restrict__ count) {
-    GRID_STRIDE(i, N) {
-        if (flag[i]) cand[pos[i]] = (int)i;
-        if (i == N - 1) *count = pos[i] + flag[i];
-    }
-}
 
-// the wrapped Gaussian of component B's indicator at cell x: pass 0 along
-// axis 0, pass 1 along axis 1, pass 2 along axis 2, each x0 w0 + sum over
-// j = r..1 of (x-j + x+j) w_j, evaluated only on the (2r+1)^d box
+// the wrapped Gaussian of component B's indicator at y: the pass along axis
+// A0 (the first of the field) reads the indicator, each later axis AX reads
+// the pass before it; each is y w0 + sum over j = r..1 of (y-j + y+j) w_j,
+// evaluated on the (2r+1)^d box only
 __device__ __forceinline__ double ind(const int* __restrict__ root, long long i, int B) {
     return root[i] == B ? 1.0 : 0.0;
 }
-__device__ double pass0(const Ext& d, const Taps& t, const int* __restrict__ root, int B, int y0, int y1, int y2) {
-    const long long rest = (long long)y1 * d.st[1] + y2;
-    double v = ind(root, (long long)y0 * d.st[0] + rest, B) * t.w[0];
-    for (int j = t.r; j >= 1; --j)
-        v = v + (ind(root, (long long)wrapi(y0 - j, d.e[0]) * d.st[0] + rest, B) +
-                 ind(root, (long long)wrapi(y0 + j, d.e[0]) * d.st[0] + rest, B)) * t.w[j];
-    return v;
-}
-__device__ double pass1(const Ext& d, const Taps& t, const int* __restrict__ root, int B, int y0, int y1, int y2) {
-    double v = pass0(d, t, root, B, y0, y1, y2) * t.w[0];
-    for (int j = t.r; j >= 1; --j)
-        v = v + (pass0(d, t, root, B, y0, wrapi(y1 - j, d.e[1]), y2) +
-                 pass0(d, t, root, B, y0, wrapi(y1 + j, d.e[1]), y2)) * t.w[j];
-    return v;
-}
-__device__ double pass2(const Ext& d, const Taps& t, const int* __restrict__ root, int B, int y0, int y1, int y2) {
-    double v = pass1(d, t, root, B, y0, y1, y2) * t.w[0];
-    for (int j = t.r; j >= 1; --j)
-        v = v + (pass1(d, t, root, B, y0, y1, wrapi(y2 - j, d.e[2])) +
-                 pass1(d, t, root, B, y0, y1, wrapi(y2 + j, d.e[2]))) * t.w[j];
+template <int AX, int A0>
+__device__ double gpass(const Ext& d, const Taps& t, const int* __restrict__ root, int B, int y0, int y1, int y2) {
+    const int n = d.e[AX];
+    const bool near = t.r <= n;
+    const int ya = AX == 0 ? y0 : (AX == 1 ? y1 : y2);
+    auto at = [&](int v) -> double {
+        const int z0 = AX == 0 ? v : y0, z1 = AX == 1 ? v : y1, z2 = AX == 2 ? v : y2;
+        if constexpr (AX == A0)
+            return ind(root, ((long long)z0 * d.e[1] + z1) * d.e[2] + z2, B);
+        else
+            return gpass<(AX > A0 ? AX - 1 : A0), A0>(d, t, root, B, z0, z1, z2);
+    };
+    double v = at(ya) * t.w[0];
+    for (int j = t.r; j >= 1; --j) v = v + (at(wrap_off(ya - j, n, near)) + at(wrap_off(ya + j, n, near))) * t.w[j];
     return v;
 }
 
@@ -553,10 +610,10 @@ __global__ void k_cgr_score(Ext d, Taps t, const int* __restrict__ cand, const i
     const int M = *count;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
         const long long i = cand[q];
-        int x[3];
-        coords(d, i, x);
+        int x0, x1, x2;
+        cell_coords(d, i, x0, x1, x2);
         const int B = seg[i];
-        const double s = d.ndim == 3 ? pass2(d, t, root, B, x[0], x[1], x[2]) : pass1(d, t, root, B, x[0], x[1], 0);
+        const double s = d.a0 == 0 ? gpass<2, 0>(d, t, root, B, x0, x1, x2) : gpass<2, 1>(d, t, root, B, x0, x1, x2);
         key[q] = ~okey(s);  // ascending key = descending score
     }
 }
@@ -570,9 +627,13 @@ __global__ void k_cgr_starts(const unsigned* __restrict__ sk, const int* __restr
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x)
         if (q == 0 || sk[q - 1] != sk[q]) start[sk[q]] = q;
 }
-__global__ void k_cgr_vacate(long long N, int w, const int* __restrict__ root, const int* __restrict__ size,
-                             const int* __restrict__ wave, int8_t* __restrict__ lab) {
-    GRID_STRIDE(i, N) {
+// the wave's components give up their cells (all of them lie in the band)
+__global__ void k_cgr_vacate(int w, const int* __restrict__ band, const int* __restrict__ n_band,
+                             const int* __restrict__ root, const int* __restrict__ size, const int* __restrict__ wave,
+                             int8_t* __restrict__ lab) {
+    const int M = *n_band;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
+        const int i = band[q];
         const int r = root[i];
         if (r >= 0 && size[r] > 1 && wave[r] == w) lab[i] = 0;
     }
@@ -586,14 +647,20 @@ __global__ void k_cgr_select(const unsigned* __restrict__ sk, const int* __restr
         if (q - start[B] < size[B]) lab[cells[q]] = orig[B];
     }
 }
-__global__ void k_cgr_changed(long long N, const int8_t* __restrict__ lab, const int8_t* __restrict__ orig,
+// labels change only inside the band
+__global__ void k_cgr_changed(const int* __restrict__ band, const int* __restrict__ n_band,
+                              const int8_t* __restrict__ lab, const int8_t* __restrict__ orig,
                               double* __restrict__ alpha, unsigned long long* __restrict__ count) {
     typedef cub::BlockReduce<unsigned long long, 256> BR;
     __shared__ typename BR::TempStorage tmp;
+    const int M = *n_band;
     unsigned long long n = 0;
-    GRID_STRIDE(i, N) if (lab[i] != orig[i]) {
-        alpha[i] = 1.0;
-        ++n;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
+        const int i = band[q];
+        if (lab[i] != orig[i]) {
+            alpha[i] = 1.0;
+            ++n;
+        }
     }
     const unsigned long long agg = BR(tmp).Sum(n);
     if (threadIdx.x == 0 && agg) atomicAdd(count, agg);
@@ -631,6 +698,8 @@ struct gpk_alcu {
     int *flag = nullptr, *pos = nullptr, *cand = nullptr, *cells1 = nullptr, *cells2 = nullptr, *conflicts = nullptr;
     unsigned long long *key1 = nullptr, *key2 = nullptr;
     unsigned *sk1 = nullptr, *sk2 = nullptr;
+    uint8_t *u8a = nullptr, *u8b = nullptr;  // active cells and their 3^d box maximum
+    int* band = nullptr;                     // cells of some component's dilation, in order
     void* cub_tmp = nullptr;
     size_t cub_bytes = 0;
     int seg_bits = 1;
@@ -649,6 +718,13 @@ int set_params(gpk_alcu* h, const gpk_alcu_params* p) {
     h->p.ceq = p->c_matrix_eq;
     h->p.ct = p->c_theta;
     return GPK_OK;
+}
+
+// launch shape of the CELLS3 kernels
+const dim3 B3(32, 4);
+dim3 grid3(const Ext& d) {
+    const int gy = (d.e[1] + 3) / 4;
+    return dim3((d.e[2] + 31) / 32, gy < 65535 ? gy : 65535, d.e[0] < 65535 ? d.e[0] : 65535);
 }
 
 // maximal subtrees of numpy's pairwise tree with at most t values, in order
@@ -675,6 +751,7 @@ void free_all(gpk_alcu* h) {
     cudaFree(h->seg); cudaFree(h->start); cudaFree(h->flag); cudaFree(h->pos); cudaFree(h->cand);
     cudaFree(h->cells1); cudaFree(h->cells2); cudaFree(h->conflicts);
     cudaFree(h->key1); cudaFree(h->key2); cudaFree(h->sk1); cudaFree(h->sk2); cudaFree(h->cub_tmp);
+    cudaFree(h->u8a); cudaFree(h->u8b); cudaFree(h->band);
     if (h->own) cudaStreamDestroy(h->own);
 }
 
@@ -739,14 +816,26 @@ int cub_reserve(gpk_alcu* h, int M) {
     return GPK_OK;
 }
 
-// out = the wrapped Gaussian of in (3 or 2 passes); tmp: one N-double scratch
+template <int NF>
+void gauss_pass(gpk_alcu* h, int ax, const Taps& t, const double* a, const double* b, double* oa, double* ob) {
+    const dim3 g = grid3(h->d);
+    if (ax == 0)
+        k_gauss_pass<NF, 0><<<g, B3, 0, h->stream>>>(h->d, t, a, b, oa, ob);
+    else if (ax == 1)
+        k_gauss_pass<NF, 1><<<g, B3, 0, h->stream>>>(h->d, t, a, b, oa, ob);
+    else
+        k_gauss_pass<NF, 2><<<g, B3, 0, h->stream>>>(h->d, t, a, b, oa, ob);
+}
+
+// out = the wrapped Gaussian of in (a pass per axis of the field, the first
+// axis first); tmp: one N-double scratch
 int gauss(gpk_alcu* h, const Taps& t, const double* in, double* out, double* tmp) {
     const Ext& d = h->d;
     // ping-pong so that the last pass lands in out
     const double* src = in;
-    for (int a = 0; a < d.ndim; ++a) {
-        double* dst = ((d.ndim - 1 - a) % 2 == 0) ? out : tmp;
-        k_gauss_pass<1><<<h->grid, 256, 0, h->stream>>>(d, a, t, src, nullptr, dst, nullptr);
+    for (int a = d.a0; a < 3; ++a) {
+        double* dst = ((2 - a) % 2 == 0) ? out : tmp;
+        gauss_pass<1>(h, a, t, src, nullptr, dst, nullptr);
         ALCU_TRY(cudaGetLastError());
         src = dst;
     }
@@ -756,10 +845,9 @@ int gauss(gpk_alcu* h, const Taps& t, const double* in, double* out, double* tmp
 // results, which lie in (a, b) or (ta, tb) depending on the pass count
 int gauss2(gpk_alcu* h, const Taps& t, double* a, double* b, double* ta, double* tb, const double** ra,
            const double** rb) {
-    const Ext& d = h->d;
     double *sa = a, *sb = b, *da = ta, *db = tb;
-    for (int ax = 0; ax < d.ndim; ++ax) {
-        k_gauss_pass<2><<<h->grid, 256, 0, h->stream>>>(d, ax, t, sa, sb, da, db);
+    for (int ax = h->d.a0; ax < 3; ++ax) {
+        gauss_pass<2>(h, ax, t, sa, sb, da, db);
         ALCU_TRY(cudaGetLastError());
         std::swap(sa, da);
         std::swap(sb, db);
@@ -839,9 +927,10 @@ extern "C" int gpk_alcu_create(int ndim, const int* shape, const gpk_alcu_params
     if (rc != GPK_OK) { delete h; return rc; }
     Ext& d = h->d;
     d.ndim = ndim;
-    d.e[0] = shape[0];
-    d.e[1] = shape[1];
-    d.e[2] = ndim == 3 ? shape[2] : 1;
+    d.a0 = 3 - ndim;
+    d.e[0] = ndim == 3 ? shape[0] : 1;
+    d.e[1] = ndim == 3 ? shape[1] : shape[0];
+    d.e[2] = ndim == 3 ? shape[2] : shape[1];
     d.st[2] = 1;
     d.st[1] = d.e[2];
     d.st[0] = (long long)d.e[1] * d.e[2];
@@ -929,7 +1018,8 @@ extern "C" int gpk_alcu_create(int ndim, const int* shape, const gpk_alcu_params
     for (int** q : ints)
         if (!alloc((void**)q, sizeof(int) * N)) return fail(GPK_ERR_OUT_OF_MEMORY);
     if (!alloc((void**)&h->orig, N) || !alloc((void**)&h->key1, 8 * N) || !alloc((void**)&h->key2, 8 * N) ||
-        !alloc((void**)&h->sk1, 4 * N) || !alloc((void**)&h->sk2, 4 * N))
+        !alloc((void**)&h->sk1, 4 * N) || !alloc((void**)&h->sk2, 4 * N) || !alloc((void**)&h->u8a, N) ||
+        !alloc((void**)&h->u8b, N) || !alloc((void**)&h->band, 4 * N))
         return fail(GPK_ERR_OUT_OF_MEMORY);
     while ((1ll << h->seg_bits) < N) ++h->seg_bits;
     size_t b1 = 0, b2 = 0, b3 = 0;
@@ -964,7 +1054,7 @@ extern "C" int gpk_alcu_set_stream(gpk_alcu* h, void* stream) {
 
 extern "C" int gpk_alcu_competitor(gpk_alcu* h, const int8_t* labels, uint8_t* mask, int8_t* competitor) {
     if (!h || !labels || !mask || !competitor) { gpk_set_error("alcu: null argument"); return GPK_ERR_INVALID_ARGUMENT; }
-    k_competitor<<<h->grid, 256, 0, h->stream>>>(h->d, labels, mask, competitor);
+    k_competitor<<<grid3(h->d), B3, 0, h->stream>>>(h->d, labels, mask, competitor);
     ALCU_TRY(cudaGetLastError());
     return GPK_OK;
 }
@@ -1001,7 +1091,7 @@ extern "C" int gpk_alcu_diffuse(gpk_alcu* h, double* ctot, const double* fprec, 
     double* bufs[2] = {ctot, h->f[0]};
     int cur = 0;
     for (int s = 0; s < n; ++s) {
-        k_diffuse<<<h->grid, 256, 0, h->stream>>>(h->d, p, sub_dt, bufs[cur], fprec, bufs[cur ^ 1],
+        k_diffuse<<<grid3(h->d), B3, 0, h->stream>>>(h->d, p, sub_dt, bufs[cur], fprec, bufs[cur ^ 1],
                                                   s == n - 1 ? cm : nullptr);
         ALCU_TRY(cudaGetLastError());
         cur ^= 1;
@@ -1106,14 +1196,38 @@ extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alph
     const long long N = d.N;
     cudaStream_t st = h->stream;
     const int G = h->grid;
+    const dim3 g3 = grid3(d);
+    // i32: [0] candidates, [1] conflicts, [2] relax flag, [3] max wave,
+    //      [4] active components, [5] band cells
+    int* n_cand = h->i32;
+    int* n_band = h->i32 + 5;
     ALCU_TRY(cudaMemcpyAsync(h->orig, labels, N, cudaMemcpyDeviceToDevice, st));
     ALCU_TRY(cudaMemsetAsync(h->i32, 0, sizeof(int) * 8, st));
     ALCU_TRY(cudaMemsetAsync(h->err, 0, sizeof(unsigned) * 2, st));
     ALCU_TRY(cudaMemsetAsync(h->u64 + 2, 0, sizeof(unsigned long long), st));
     k_cc_init<<<G, 256, 0, st>>>(N, h->parent, h->size, h->wave);
-    k_cc_union<<<G, 256, 0, st>>>(d, h->orig, h->parent, h->err);
+    k_cc_union<<<g3, B3, 0, st>>>(d, h->orig, h->parent, h->err);
     k_cc_finish<<<G, 256, 0, st>>>(N, h->orig, h->parent, h->root, h->size, h->err);
-    k_cgr_conflicts<<<G, 256, 0, st>>>(d, h->root, h->size, h->conflicts, h->i32 + 1, h->i32 + 4);
+    k_cgr_active<<<G, 256, 0, st>>>(N, h->root, h->size, h->u8a, h->i32 + 4);
+    // 3^d box maximum of the active cells: one pass per axis of the field
+    {
+        uint8_t* src = h->u8a;
+        uint8_t* dst = h->u8b;
+        for (int ax = d.a0; ax < 3; ++ax) {
+            if (ax == 0)
+                k_box_pass<0><<<g3, B3, 0, st>>>(d, src, dst);
+            else if (ax == 1)
+                k_box_pass<1><<<g3, B3, 0, st>>>(d, src, dst);
+            else
+                k_box_pass<2><<<g3, B3, 0, st>>>(d, src, dst);
+            std::swap(src, dst);
+        }
+        k_cgr_band<<<g3, B3, 0, st>>>(d, src, h->root, h->size, h->flag, h->conflicts, h->i32 + 1);
+    }
+    ALCU_TRY(cudaGetLastError());
+    size_t b = h->cub_bytes;
+    ALCU_TRY(cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, h->flag, h->pos, (int)N, st));
+    k_compact<<<G, 256, 0, st>>>(N, h->flag, h->pos, nullptr, h->band, n_band);
     ALCU_TRY(cudaGetLastError());
     int hv[8];
     unsigned herr = 0;
@@ -1124,13 +1238,14 @@ extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alph
         gpk_set_error("alcu: component search exceeded its iteration cap");
         return GPK_ERR_INTERNAL;
     }
-    const int n_conf = hv[1], n_active = hv[4];
+    const int n_conf = hv[1], n_active = hv[4], Mb = hv[5];
     h->last_components = n_active;
     h->last_waves = 0;
     if (n_active == 0) {
         if (changed) *changed = 0;
         return GPK_OK;
     }
+    const int gb = (Mb + 255) / 256 < G ? (Mb + 255) / 256 : G;
     // waves: longest chain of earlier interacting components
     if (n_conf > 0) {
         for (int it = 0;; ++it) {
@@ -1156,33 +1271,33 @@ extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alph
     ALCU_TRY(cudaStreamSynchronize(st));
     h->last_waves = max_wave + 1;
     for (int w = 0; w <= max_wave; ++w) {
-        k_cgr_flags<<<G, 256, 0, st>>>(d, w, labels, h->root, h->size, h->wave, h->flag, h->seg);
+        k_cgr_flags<<<gb, 256, 0, st>>>(d, w, h->band, n_band, labels, h->root, h->size, h->wave, h->flag, h->seg);
         ALCU_TRY(cudaGetLastError());
-        size_t b = h->cub_bytes;
-        ALCU_TRY(cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, h->flag, h->pos, (int)N, st));
-        k_cgr_scatter<<<G, 256, 0, st>>>(N, h->flag, h->pos, h->cand, h->i32);
+        b = h->cub_bytes;
+        ALCU_TRY(cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, h->flag, h->pos, Mb, st));
+        k_compact<<<gb, 256, 0, st>>>(Mb, h->flag, h->pos, h->band, h->cand, n_cand);
         ALCU_TRY(cudaGetLastError());
         int M = 0;
-        ALCU_TRY(cudaMemcpyAsync(&M, h->i32, sizeof(int), cudaMemcpyDeviceToHost, st));
+        ALCU_TRY(cudaMemcpyAsync(&M, n_cand, sizeof(int), cudaMemcpyDeviceToHost, st));
         ALCU_TRY(cudaStreamSynchronize(st));
         if (M == 0) continue;
         if ((rc = cub_reserve(h, M)) != GPK_OK) return rc;
         const int sb = (M + 255) / 256 < G ? (M + 255) / 256 : G;
-        k_cgr_score<<<sb, 256, 0, st>>>(d, t, h->cand, h->i32, h->root, h->seg, h->key1);
+        k_cgr_score<<<sb, 256, 0, st>>>(d, t, h->cand, n_cand, h->root, h->seg, h->key1);
         ALCU_TRY(cudaGetLastError());
         b = h->cub_bytes;
         ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->key1, h->key2, h->cand, h->cells1, M, 0, 64, st));
-        k_cgr_segkeys<<<sb, 256, 0, st>>>(h->cells1, h->i32, h->seg, h->sk1);
+        k_cgr_segkeys<<<sb, 256, 0, st>>>(h->cells1, n_cand, h->seg, h->sk1);
         ALCU_TRY(cudaGetLastError());
         b = h->cub_bytes;
         ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->sk1, h->sk2, h->cells1, h->cells2, M, 0,
                                                  h->seg_bits, st));
-        k_cgr_starts<<<sb, 256, 0, st>>>(h->sk2, h->i32, h->start);
-        k_cgr_vacate<<<G, 256, 0, st>>>(N, w, h->root, h->size, h->wave, labels);
-        k_cgr_select<<<sb, 256, 0, st>>>(h->sk2, h->cells2, h->i32, h->start, h->size, h->orig, labels);
+        k_cgr_starts<<<sb, 256, 0, st>>>(h->sk2, n_cand, h->start);
+        k_cgr_vacate<<<gb, 256, 0, st>>>(w, h->band, n_band, h->root, h->size, h->wave, labels);
+        k_cgr_select<<<sb, 256, 0, st>>>(h->sk2, h->cells2, n_cand, h->start, h->size, h->orig, labels);
         ALCU_TRY(cudaGetLastError());
     }
-    k_cgr_changed<<<G, 256, 0, st>>>(N, labels, h->orig, alpha, h->u64 + 2);
+    k_cgr_changed<<<gb, 256, 0, st>>>(h->band, n_band, labels, h->orig, alpha, h->u64 + 2);
     ALCU_TRY(cudaGetLastError());
     unsigned long long n_changed = 0;
     ALCU_TRY(cudaMemcpyAsync(&n_changed, h->u64 + 2, sizeof(n_changed), cudaMemcpyDeviceToHost, st));
