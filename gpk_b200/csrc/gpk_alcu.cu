@@ -194,6 +194,97 @@ __global__ void __launch_bounds__(128) k_diffuse(Ext d, Phys p, double dt, const
     }
 }
 
+// The same substep for a 3-D field, tiled: a (32 x 8) block marches along
+// axis 0 through DZC planes.  The lever rule (one division) is evaluated once
+// per cell and plane (own cells carried in registers from the plane before,
+// the halo ring recomputed), and the flux through each face is evaluated once
+// and read by both of its cells, with the reference's operands: for the face
+// between cell lo and its + neighbour hi, ((-D) (0.5 (m_lo + m_hi)))
+// (cm_hi - cm_lo) / dx.  dc then takes the axes in the reference's order.
+constexpr int DTX = 32, DTY = 8, DZC = 16;
+
+__device__ __forceinline__ double face_flux(double nD, double dx, double m_lo, double cm_lo, double m_hi, double cm_hi) {
+    const double mf = 0.5 * (m_lo + m_hi);
+    const double fl = (nD * mf) * (cm_hi - cm_lo);
+    return fl / dx;
+}
+
+__global__ void __launch_bounds__(DTX * DTY) k_diffuse_tiled(Ext d, Phys p, double dt, const double* __restrict__ c,
+                                                             const double* __restrict__ f, double* __restrict__ out,
+                                                             double* __restrict__ cm_out) {
+    __shared__ double sm[DTY + 2][DTX + 2];   // matrix fraction of the plane, halo included
+    __shared__ double scm[DTY + 2][DTX + 2];  // lever composition of the plane
+    __shared__ double fx[DTY][DTX + 1];       // fx[y][k]: the face between local x = k - 1 and k
+    __shared__ double fy[DTY + 1][DTX];       // fy[k][x]: the face between local y = k - 1 and k
+    const int n0 = d.e[0], n1 = d.e[1], n2 = d.e[2];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * DTX + tx;
+    const int xs = blockIdx.x * DTX, ys = blockIdx.y * DTY;
+    const bool valid = xs + tx < n2 && ys + ty < n1;
+    const int ox = (xs + tx) % n2, oy = (ys + ty) % n1;  // own column (wrapped for idle threads)
+    const long long plane = (long long)n1 * n2;
+    const long long col = (long long)oy * n2 + ox;
+    const double nD = -p.D;
+    const int z0 = blockIdx.z * DZC;
+    const int z1 = z0 + DZC < n0 ? z0 + DZC : n0;
+    // own column at planes z0 - 1 and z0
+    const int zp = z0 == 0 ? n0 - 1 : z0 - 1;
+    double m_prev, cm_prev, m_cur, cm_cur;
+    lever(c[zp * plane + col], f[zp * plane + col], p, m_prev, cm_prev);
+    double c_cur = c[z0 * plane + col];
+    lever(c_cur, f[z0 * plane + col], p, m_cur, cm_cur);
+    double fz_minus = face_flux(nD, p.dx, m_prev, cm_prev, m_cur, cm_cur);
+    for (int z = z0; z < z1; ++z) {
+        const int zn = z + 1 == n0 ? 0 : z + 1;
+        const double c_next = c[zn * plane + col];
+        double m_next, cm_next;
+        lever(c_next, f[zn * plane + col], p, m_next, cm_next);
+        // the plane's tile: own cells from registers, the halo ring evaluated
+        sm[ty + 1][tx + 1] = m_cur;
+        scm[ty + 1][tx + 1] = cm_cur;
+        constexpr int HALO = 2 * (DTX + 2) + 2 * DTY;
+        for (int k = tid; k < HALO; k += DTX * DTY) {
+            int ly, lx;
+            if (k < DTX + 2) { ly = -1; lx = k - 1; }
+            else if (k < 2 * (DTX + 2)) { ly = DTY; lx = k - (DTX + 2) - 1; }
+            else if (k < 2 * (DTX + 2) + DTY) { ly = k - 2 * (DTX + 2); lx = -1; }
+            else { ly = k - 2 * (DTX + 2) - DTY; lx = DTX; }
+            int gy = ys + ly, gx = xs + lx;
+            gy = gy < 0 ? gy + n1 : gy % n1;
+            gx = gx < 0 ? gx + n2 : gx % n2;
+            const long long q = z * plane + (long long)gy * n2 + gx;
+            double mh, cmh;
+            lever(c[q], f[q], p, mh, cmh);
+            sm[ly + 1][lx + 1] = mh;
+            scm[ly + 1][lx + 1] = cmh;
+        }
+        __syncthreads();
+        fx[ty][tx + 1] = face_flux(nD, p.dx, sm[ty + 1][tx + 1], scm[ty + 1][tx + 1], sm[ty + 1][tx + 2],
+                                   scm[ty + 1][tx + 2]);
+        if (tx == 0) fx[ty][0] = face_flux(nD, p.dx, sm[ty + 1][0], scm[ty + 1][0], sm[ty + 1][1], scm[ty + 1][1]);
+        fy[ty + 1][tx] = face_flux(nD, p.dx, sm[ty + 1][tx + 1], scm[ty + 1][tx + 1], sm[ty + 2][tx + 1],
+                                   scm[ty + 2][tx + 1]);
+        if (ty == 0) fy[0][tx] = face_flux(nD, p.dx, sm[0][tx + 1], scm[0][tx + 1], sm[1][tx + 1], scm[1][tx + 1]);
+        const double fz_plus = face_flux(nD, p.dx, m_cur, cm_cur, m_next, cm_next);
+        __syncthreads();
+        if (valid) {
+            double dc = 0.0;
+            dc = dc - (fz_plus - fz_minus) / p.dx;
+            dc = dc - (fy[ty + 1][tx] - fy[ty][tx]) / p.dx;
+            dc = dc - (fx[ty][tx + 1] - fx[ty][tx]) / p.dx;
+            const long long i = z * plane + col;
+            out[i] = c_cur + dt * dc;
+            if (cm_out) cm_out[i] = cm_cur;
+        }
+        fz_minus = fz_plus;
+        m_cur = m_next;
+        cm_cur = cm_next;
+        c_cur = c_next;
+        // the next plane rewrites sm/scm only after every thread has read
+        // them (second barrier above); fx/fy are rewritten after the next
+        // plane's first barrier, which every thread reaches after its update
+    }
+}
+
 // ---------------------------------------------------------------- Gaussian
 
 // one periodic pass along axis AX of NF fields
@@ -415,8 +506,10 @@ __device__ void uf_unite(int* parent, int a, int b, unsigned* err) {
     atomicExch(err, 1u);
 }
 
-__global__ void k_cc_init(long long N, int* __restrict__ parent, int* __restrict__ size, int* __restrict__ wave) {
-    GRID_STRIDE(i, N) {
+// union-find state of the labelled cells (only they are ever read)
+__global__ void k_cc_init(long long N, const int8_t* __restrict__ lab, int* __restrict__ parent,
+                          int* __restrict__ size, int* __restrict__ wave) {
+    GRID_STRIDE(i, N) if (lab[i] != 0) {
         parent[i] = (int)i;
         size[i] = 0;
         wave[i] = 0;
@@ -555,9 +648,15 @@ __global__ void k_cgr_relax(Ext d, const int* __restrict__ list, int M, const in
     }
 }
 
-__global__ void k_cgr_max_wave(long long N, const int* __restrict__ root, const int* __restrict__ size,
+// every active component's root lies in the band
+__global__ void k_cgr_max_wave(const int* __restrict__ band, const int* __restrict__ n_band,
+                               const int* __restrict__ root, const int* __restrict__ size,
                                const int* __restrict__ wave, int* __restrict__ max_wave) {
-    GRID_STRIDE(i, N) if (root[i] == (int)i && size[i] > 1) atomicMax(max_wave, wave[i]);
+    const int M = *n_band;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
+        const int i = band[q];
+        if (root[i] == i && size[i] > 1) atomicMax(max_wave, wave[i]);
+    }
 }
 
 // candidates of wave w among the band: cells of the dilation of a wave-w
@@ -1090,9 +1189,16 @@ extern "C" int gpk_alcu_diffuse(gpk_alcu* h, double* ctot, const double* fprec, 
     const double sub_dt = dt / n;
     double* bufs[2] = {ctot, h->f[0]};
     int cur = 0;
+    const Ext& d = h->d;
+    const long long gy = (d.e[1] + DTY - 1) / DTY, gz = (d.e[0] + DZC - 1) / DZC;
+    const bool tiled = d.ndim == 3 && gy <= 65535 && gz <= 65535;
+    const dim3 tg((d.e[2] + DTX - 1) / DTX, (unsigned)gy, (unsigned)gz);
     for (int s = 0; s < n; ++s) {
-        k_diffuse<<<grid3(h->d), B3, 0, h->stream>>>(h->d, p, sub_dt, bufs[cur], fprec, bufs[cur ^ 1],
-                                                  s == n - 1 ? cm : nullptr);
+        double* cm_s = s == n - 1 ? cm : nullptr;
+        if (tiled)
+            k_diffuse_tiled<<<tg, dim3(DTX, DTY), 0, h->stream>>>(d, p, sub_dt, bufs[cur], fprec, bufs[cur ^ 1], cm_s);
+        else
+            k_diffuse<<<grid3(d), B3, 0, h->stream>>>(d, p, sub_dt, bufs[cur], fprec, bufs[cur ^ 1], cm_s);
         ALCU_TRY(cudaGetLastError());
         cur ^= 1;
     }
@@ -1205,7 +1311,7 @@ extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alph
     ALCU_TRY(cudaMemsetAsync(h->i32, 0, sizeof(int) * 8, st));
     ALCU_TRY(cudaMemsetAsync(h->err, 0, sizeof(unsigned) * 2, st));
     ALCU_TRY(cudaMemsetAsync(h->u64 + 2, 0, sizeof(unsigned long long), st));
-    k_cc_init<<<G, 256, 0, st>>>(N, h->parent, h->size, h->wave);
+    k_cc_init<<<G, 256, 0, st>>>(N, h->orig, h->parent, h->size, h->wave);
     k_cc_union<<<g3, B3, 0, st>>>(d, h->orig, h->parent, h->err);
     k_cc_finish<<<G, 256, 0, st>>>(N, h->orig, h->parent, h->root, h->size, h->err);
     k_cgr_active<<<G, 256, 0, st>>>(N, h->root, h->size, h->u8a, h->i32 + 4);
@@ -1265,7 +1371,7 @@ extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alph
         }
     }
     int max_wave = 0;
-    k_cgr_max_wave<<<G, 256, 0, st>>>(N, h->root, h->size, h->wave, h->i32 + 3);
+    k_cgr_max_wave<<<gb, 256, 0, st>>>(h->band, n_band, h->root, h->size, h->wave, h->i32 + 3);
     ALCU_TRY(cudaGetLastError());
     ALCU_TRY(cudaMemcpyAsync(&max_wave, h->i32 + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
     ALCU_TRY(cudaStreamSynchronize(st));
