@@ -195,21 +195,23 @@ __global__ void __launch_bounds__(128) k_diffuse(Ext d, Phys p, double dt, const
 }
 
 // The same substep for a 3-D field, tiled: a (32 x 8) block marches along
-// axis 0 through DZC planes.  The lever rule (one division) is evaluated once
+// axis 0 through zc planes.  The lever rule (one division) is evaluated once
 // per cell and plane (own cells carried in registers from the plane before,
 // the halo ring recomputed), and the flux through each face is evaluated once
 // and read by both of its cells, with the reference's operands: for the face
 // between cell lo and its + neighbour hi, ((-D) (0.5 (m_lo + m_hi)))
 // (cm_hi - cm_lo) / dx.  dc then takes the axes in the reference's order.
-constexpr int DTX = 32, DTY = 8, DZC = 16;
+constexpr int DTX = 32, DTY = 8;
 
-__device__ __forceinline__ double face_flux(double nD, double dx, double m_lo, double cm_lo, double m_hi, double cm_hi) {
+__device__ __forceinline__ double face_flux(double nD, const Phys& p, double m_lo, double cm_lo, double m_hi,
+                                            double cm_hi) {
     const double mf = 0.5 * (m_lo + m_hi);
     const double fl = (nD * mf) * (cm_hi - cm_lo);
-    return fl / dx;
+    return fl / p.dx;
 }
 
-__global__ void __launch_bounds__(DTX * DTY) k_diffuse_tiled(Ext d, Phys p, double dt, const double* __restrict__ c,
+__global__ void __launch_bounds__(DTX * DTY) k_diffuse_tiled(Ext d, Phys p, double dt, int zc,
+                                                             const double* __restrict__ c,
                                                              const double* __restrict__ f, double* __restrict__ out,
                                                              double* __restrict__ cm_out) {
     __shared__ double sm[DTY + 2][DTX + 2];   // matrix fraction of the plane, halo included
@@ -224,15 +226,15 @@ __global__ void __launch_bounds__(DTX * DTY) k_diffuse_tiled(Ext d, Phys p, doub
     const long long plane = (long long)n1 * n2;
     const long long col = (long long)oy * n2 + ox;
     const double nD = -p.D;
-    const int z0 = blockIdx.z * DZC;
-    const int z1 = z0 + DZC < n0 ? z0 + DZC : n0;
+    const int z0 = blockIdx.z * zc;
+    const int z1 = z0 + zc < n0 ? z0 + zc : n0;
     // own column at planes z0 - 1 and z0
     const int zp = z0 == 0 ? n0 - 1 : z0 - 1;
     double m_prev, cm_prev, m_cur, cm_cur;
     lever(c[zp * plane + col], f[zp * plane + col], p, m_prev, cm_prev);
     double c_cur = c[z0 * plane + col];
     lever(c_cur, f[z0 * plane + col], p, m_cur, cm_cur);
-    double fz_minus = face_flux(nD, p.dx, m_prev, cm_prev, m_cur, cm_cur);
+    double fz_minus = face_flux(nD, p, m_prev, cm_prev, m_cur, cm_cur);
     for (int z = z0; z < z1; ++z) {
         const int zn = z + 1 == n0 ? 0 : z + 1;
         const double c_next = c[zn * plane + col];
@@ -249,8 +251,10 @@ __global__ void __launch_bounds__(DTX * DTY) k_diffuse_tiled(Ext d, Phys p, doub
             else if (k < 2 * (DTX + 2) + DTY) { ly = k - 2 * (DTX + 2); lx = -1; }
             else { ly = k - 2 * (DTX + 2) - DTY; lx = DTX; }
             int gy = ys + ly, gx = xs + lx;
-            gy = gy < 0 ? gy + n1 : gy % n1;
-            gx = gx < 0 ? gx + n2 : gx % n2;
+            if (gy < 0) gy += n1;
+            while (gy >= n1) gy -= n1;  // at most DTY + 1 times
+            if (gx < 0) gx += n2;
+            while (gx >= n2) gx -= n2;  // at most DTX + 1 times
             const long long q = z * plane + (long long)gy * n2 + gx;
             double mh, cmh;
             lever(c[q], f[q], p, mh, cmh);
@@ -258,13 +262,13 @@ __global__ void __launch_bounds__(DTX * DTY) k_diffuse_tiled(Ext d, Phys p, doub
             scm[ly + 1][lx + 1] = cmh;
         }
         __syncthreads();
-        fx[ty][tx + 1] = face_flux(nD, p.dx, sm[ty + 1][tx + 1], scm[ty + 1][tx + 1], sm[ty + 1][tx + 2],
+        fx[ty][tx + 1] = face_flux(nD, p, sm[ty + 1][tx + 1], scm[ty + 1][tx + 1], sm[ty + 1][tx + 2],
                                    scm[ty + 1][tx + 2]);
-        if (tx == 0) fx[ty][0] = face_flux(nD, p.dx, sm[ty + 1][0], scm[ty + 1][0], sm[ty + 1][1], scm[ty + 1][1]);
-        fy[ty + 1][tx] = face_flux(nD, p.dx, sm[ty + 1][tx + 1], scm[ty + 1][tx + 1], sm[ty + 2][tx + 1],
+        if (tx == 0) fx[ty][0] = face_flux(nD, p, sm[ty + 1][0], scm[ty + 1][0], sm[ty + 1][1], scm[ty + 1][1]);
+        fy[ty + 1][tx] = face_flux(nD, p, sm[ty + 1][tx + 1], scm[ty + 1][tx + 1], sm[ty + 2][tx + 1],
                                    scm[ty + 2][tx + 1]);
-        if (ty == 0) fy[0][tx] = face_flux(nD, p.dx, sm[0][tx + 1], scm[0][tx + 1], sm[1][tx + 1], scm[1][tx + 1]);
-        const double fz_plus = face_flux(nD, p.dx, m_cur, cm_cur, m_next, cm_next);
+        if (ty == 0) fy[0][tx] = face_flux(nD, p, sm[0][tx + 1], scm[0][tx + 1], sm[1][tx + 1], scm[1][tx + 1]);
+        const double fz_plus = face_flux(nD, p, m_cur, cm_cur, m_next, cm_next);
         __syncthreads();
         if (valid) {
             double dc = 0.0;
@@ -310,6 +314,58 @@ __global__ void __launch_bounds__(128) k_gauss_pass(Ext d, Taps t, const double*
         }
         o0[i] = v0;
         if (NF == 2) o1[i] = v1;
+    }
+}
+
+// The same pass along axis AX = 0 or 1 for radius R: a thread marches along
+// AX through `chunk` outputs of one line, keeping the 2R + 1 inputs of the
+// current output in registers, so that each input is read once per line
+// chunk instead of 2R + 1 times.  Same operations and order as
+// k_gauss_pass; requires 2R + 1 <= the axis extent.
+template <int NF, int AX, int R>
+__global__ void __launch_bounds__(128) k_gauss_march(Ext d, Taps t, int chunk, const double* __restrict__ a0,
+                                                     const double* __restrict__ a1, double* __restrict__ o0,
+                                                     double* __restrict__ o1) {
+    constexpr int OX = AX == 0 ? 1 : 0;  // the axis across the lines (with axis 2)
+    constexpr int W = 2 * R + 1;
+    const int x2 = blockIdx.x * 32 + threadIdx.x;
+    const int xo = blockIdx.y * 4 + threadIdx.y;
+    if (x2 >= d.e[2] || xo >= d.e[OX]) return;
+    const int n = d.e[AX];
+    const long long s = d.st[AX];
+    const long long base = (long long)xo * d.st[OX] + x2;
+    const int z0 = blockIdx.z * chunk;
+    const int z1 = z0 + chunk < n ? z0 + chunk : n;
+    double u[W], v[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+        int z = z0 - R + k;
+        z = z < 0 ? z + n : (z >= n ? z - n : z);
+        u[k] = a0[base + z * s];
+        if (NF == 2) v[k] = a1[base + z * s];
+    }
+    for (int z = z0; z < z1; ++z) {
+        double r0 = u[R] * t.w[0];
+        double r1 = 0.0;
+        if (NF == 2) r1 = v[R] * t.w[0];
+#pragma unroll
+        for (int j = R; j >= 1; --j) {
+            r0 = r0 + (u[R - j] + u[R + j]) * t.w[j];
+            if (NF == 2) r1 = r1 + (v[R - j] + v[R + j]) * t.w[j];
+        }
+        o0[base + z * s] = r0;
+        if (NF == 2) o1[base + z * s] = r1;
+        if (z + 1 < z1) {
+#pragma unroll
+            for (int k = 0; k < W - 1; ++k) {
+                u[k] = u[k + 1];
+                if (NF == 2) v[k] = v[k + 1];
+            }
+            int zn = z + 1 + R;
+            zn = zn >= n ? zn - n : zn;
+            u[W - 1] = a0[base + zn * s];
+            if (NF == 2) v[W - 1] = a1[base + zn * s];
+        }
     }
 }
 
@@ -917,13 +973,33 @@ int cub_reserve(gpk_alcu* h, int M) {
 
 template <int NF>
 void gauss_pass(gpk_alcu* h, int ax, const Taps& t, const double* a, const double* b, double* oa, double* ob) {
-    const dim3 g = grid3(h->d);
+    const Ext& d = h->d;
+    // lines along axes 0 and 1 marched with a register window when the radius
+    // is 3 (the module's widths 0.70 and 0.75) and the axis holds the window
+    if (ax < 2 && t.r == 3 && d.e[ax] >= 7) {
+        const int ox = ax == 0 ? 1 : 0;
+        const long long gy = (d.e[ox] + 3) / 4;
+        const long long lines = (long long)((d.e[2] + 31) / 32) * gy;
+        const long long want = (32ll * h->num_sms + lines - 1) / lines;  // line chunks for ~32 blocks per SM
+        long long chunk = (d.e[ax] + want - 1) / want;
+        chunk = chunk < 16 ? 16 : chunk;
+        const long long gz = (d.e[ax] + chunk - 1) / chunk;
+        if (gy <= 65535 && gz <= 65535) {
+            const dim3 g((d.e[2] + 31) / 32, (unsigned)gy, (unsigned)gz);
+            if (ax == 0)
+                k_gauss_march<NF, 0, 3><<<g, B3, 0, h->stream>>>(d, t, (int)chunk, a, b, oa, ob);
+            else
+                k_gauss_march<NF, 1, 3><<<g, B3, 0, h->stream>>>(d, t, (int)chunk, a, b, oa, ob);
+            return;
+        }
+    }
+    const dim3 g = grid3(d);
     if (ax == 0)
-        k_gauss_pass<NF, 0><<<g, B3, 0, h->stream>>>(h->d, t, a, b, oa, ob);
+        k_gauss_pass<NF, 0><<<g, B3, 0, h->stream>>>(d, t, a, b, oa, ob);
     else if (ax == 1)
-        k_gauss_pass<NF, 1><<<g, B3, 0, h->stream>>>(h->d, t, a, b, oa, ob);
+        k_gauss_pass<NF, 1><<<g, B3, 0, h->stream>>>(d, t, a, b, oa, ob);
     else
-        k_gauss_pass<NF, 2><<<g, B3, 0, h->stream>>>(h->d, t, a, b, oa, ob);
+        k_gauss_pass<NF, 2><<<g, B3, 0, h->stream>>>(d, t, a, b, oa, ob);
 }
 
 // out = the wrapped Gaussian of in (a pass per axis of the field, the first
@@ -1190,13 +1266,19 @@ extern "C" int gpk_alcu_diffuse(gpk_alcu* h, double* ctot, const double* fprec, 
     double* bufs[2] = {ctot, h->f[0]};
     int cur = 0;
     const Ext& d = h->d;
-    const long long gy = (d.e[1] + DTY - 1) / DTY, gz = (d.e[0] + DZC - 1) / DZC;
+    // planes per block: about 32 blocks per SM, from 4 to 16 planes
+    const long long gx = (d.e[2] + DTX - 1) / DTX, gy = (d.e[1] + DTY - 1) / DTY;
+    const long long chunks = (32ll * h->num_sms + gx * gy - 1) / (gx * gy);
+    long long zc = (d.e[0] + chunks - 1) / chunks;
+    zc = zc < 4 ? 4 : (zc > 16 ? 16 : zc);
+    const long long gz = (d.e[0] + zc - 1) / zc;
     const bool tiled = d.ndim == 3 && gy <= 65535 && gz <= 65535;
-    const dim3 tg((d.e[2] + DTX - 1) / DTX, (unsigned)gy, (unsigned)gz);
+    const dim3 tg((unsigned)gx, (unsigned)gy, (unsigned)gz);
     for (int s = 0; s < n; ++s) {
         double* cm_s = s == n - 1 ? cm : nullptr;
         if (tiled)
-            k_diffuse_tiled<<<tg, dim3(DTX, DTY), 0, h->stream>>>(d, p, sub_dt, bufs[cur], fprec, bufs[cur ^ 1], cm_s);
+            k_diffuse_tiled<<<tg, dim3(DTX, DTY), 0, h->stream>>>(d, p, sub_dt, (int)zc, bufs[cur], fprec,
+                                                                  bufs[cur ^ 1], cm_s);
         else
             k_diffuse<<<grid3(d), B3, 0, h->stream>>>(d, p, sub_dt, bufs[cur], fprec, bufs[cur ^ 1], cm_s);
         ALCU_TRY(cudaGetLastError());

@@ -377,3 +377,26 @@ def test_full_size_properties_256(torch_cuda):
     new = torch.clamp(fp + 0.2 * torch.rand(shape, dtype=torch.float64, device="cuda", generator=g) * mask, 0.0, 1.0)
     h.partition_transfer(ctot, fp, new, tr, 0.75)
     assert abs(h.sum(ctot) - s0) <= 1e-12 * abs(s0)
+
+
+@gpu
+@pytest.mark.parametrize("dx", [1.5e-9, 0.5e-9, 1.0, 3.7, 2.0 ** -20])
+@pytest.mark.parametrize("shape", [(48, 40, 36), (70, 66)])
+def test_diffusion_wide_range_against_oracle(torch_cuda, shape, dx):
+    """Compositions spread over twelve decades and several grid spacings, so
+    that the substep's divisions by dx meet many operand magnitudes; every
+    result is compared bit for bit with numpy's IEEE division."""
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    rng = np.random.default_rng(int(dx * 1e9) % 1000 + len(shape))
+    ctot = 10.0 ** rng.uniform(-12.0, -0.5, shape)
+    fp = np.where(rng.random(shape) < 0.3, rng.random(shape), 0.0)
+    fp[rng.random(shape) < 0.05] = 1.0
+    p = O.AlCuParams(dx=dx, diffusivity=1.66e-20 if dx < 1e-6 else 0.01)
+    h = AlCuTransport(shape, p)
+    for dt in (p.dx * p.dx / p.diffusivity * 0.05, p.dx * p.dx / p.diffusivity * 0.9):
+        c_ref, cm_ref, n_ref = O.diffuse_conservative_subcycled(ctot.copy(), fp, p, dt)
+        cd = dev(torch, ctot)
+        cm, n = h.diffuse(cd, dev(torch, fp), dt)
+        assert n == n_ref and same(host(cd), c_ref) and same(host(cm), cm_ref)
