@@ -665,13 +665,14 @@ def run_gpu_arm(args):
             cpu.pop("seconds", None)
         except Exception as exc:  # the GPU number stands on its own
             cpu = {"error": str(exc)}
-    spectral = batched = adjoint = coupled = None
+    spectral = batched = adjoint = coupled = alcu = None
     # the sweep shards over all ranks (same collective order on every rank)
-    try:
-        batched = batched_measurement(ws=ws, rank=rank)
-    except Exception as exc:
-        batched = {"error": str(exc)}
-    if rank == 0:
+    if not args.headline_only:
+        try:
+            batched = batched_measurement(ws=ws, rank=rank)
+        except Exception as exc:
+            batched = {"error": str(exc)}
+    if rank == 0 and not args.headline_only:
         try:
             spectral = spectral_measurement(not args.no_cpu and ws == 1)
         except Exception as exc:  # reported, never silent
@@ -684,6 +685,10 @@ def run_gpu_arm(args):
             coupled = coupled_measurement()
         except Exception as exc:
             coupled = {"error": str(exc)}
+        try:
+            alcu = alcu_measurement(not args.no_cpu and ws == 1)
+        except Exception as exc:
+            alcu = {"error": str(exc)}
     if rank == 0:
         line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -693,7 +698,7 @@ def run_gpu_arm(args):
                 "stages_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in stages.items()},
                 "interface_fraction": iface, "counters_last_step": list(grid.counters()),
                 "per_step_topology": waves,
-                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "spectral": spectral, "batched": batched, "adjoint": adjoint, "coupled": coupled, "init": init,
+                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "spectral": spectral, "batched": batched, "adjoint": adjoint, "coupled": coupled, "alcu": alcu, "init": init,
                 "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": io,
                         "d2h_bytes_per_step": io, "steps": e2e_steps,
                         "path": "GPKGrid drop-in semantics: upload phi/alpha/g, step, download phi/alpha/g"}}
@@ -720,6 +725,8 @@ def main():
     ap.add_argument("--adjoint-only", action="store_true", help="time only the 512^2 adjoint gradient")
     ap.add_argument("--coupled-only", action="store_true",
                     help="time only the 128^3 solidification step with a spectral solve per step")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="only the grain-growth step and its e2e (profiling the headline kernels)")
     ap.add_argument("--alcu-only", action="store_true",
                     help="time only the Al-Cu transport and remap chain (96^3 and 256^3)")
     ap.add_argument("--spectral-only", action="store_true",
