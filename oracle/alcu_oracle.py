@@ -16,6 +16,12 @@ per step:
   conservative_partition_transfer  lines 702-737
   interface_matrix_composition     lines 740-755
   conservative_gaussian_remap      lines 562-594
+  balanced_gaussian_remap          lines 597-672
+  commit_topology_transactions     lines 526-559
+  topology_simple_relabel          lines 464-523, with local_only=True (the
+                                   form both callers above use), and its
+                                   helpers _periodic_patch / _topological_number
+                                   (lines 383-428)
 
 with the reference's operand order, so that the results are bit-identical.
 The reference calls two third-party pieces, both restated here from their
@@ -270,4 +276,153 @@ def conservative_gaussian_remap(labels: np.ndarray, alpha: np.ndarray, sigma_cel
     changed = remapped != labels
     labels[:] = remapped
     alpha[changed] = 1.0
+    return int(np.count_nonzero(changed))
+
+
+# --------------------------------------------------------------------------
+# topology transactions and the balanced remap
+
+
+def _periodic_patch(labels: np.ndarray, index: tuple) -> np.ndarray:
+    axes = [np.asarray([(i - 1) % n, i, (i + 1) % n]) for i, n in zip(index, labels.shape)]
+    return labels[np.ix_(*axes)]
+
+
+def _topological_number(mask: np.ndarray) -> int:
+    """Face-connected components of the 3^d patch (centre cleared) that touch
+    a face neighbour of the centre."""
+    nd = mask.ndim
+    occupied = {tuple(int(v) for v in c) for c in np.argwhere(mask)}
+    if not occupied:
+        return 0
+    offsets, incident = [], set()
+    centre = (1,) * nd
+    for axis in range(nd):
+        for shift in (-1, 1):
+            off = [0] * nd
+            off[axis] = shift
+            offsets.append(tuple(off))
+            pos = list(centre)
+            pos[axis] += shift
+            incident.add(tuple(pos))
+    count = 0
+    unseen = set(occupied)
+    while unseen:
+        seed = unseen.pop()
+        stack = [seed]
+        touches = seed in incident
+        while stack:
+            pt = stack.pop()
+            for off in offsets:
+                nb = tuple(a + b for a, b in zip(pt, off))
+                if nb in unseen:
+                    unseen.remove(nb)
+                    stack.append(nb)
+                    touches |= nb in incident
+        count += int(touches)
+    return count
+
+
+def simple_relabel_local(labels, index, old_label, new_label, label_counts) -> bool:
+    """The local certificate of topology_simple_relabel(..., local_only=True)."""
+    if old_label == new_label:
+        return False
+    patch = _periodic_patch(labels, index)
+    centre = (1,) * labels.ndim
+    old_object = patch == old_label
+    old_object[centre] = False
+    oc = _topological_number(old_object)
+    extinction = label_counts.get(old_label, 0) <= 1
+    if oc == 0 and not extinction:
+        return False
+    if oc > 1:
+        return False
+    new_object = patch == new_label
+    new_object[centre] = False
+    nc = _topological_number(new_object)
+    if nc == 0 or nc > 1:
+        return False
+    return True
+
+
+def commit_topology_transactions(labels, alpha, competitor, crossing) -> int:
+    """Serial relabel of the crossing cells in C order (lines 526-559);
+    labels and alpha in place; returns the deferred count."""
+    if not np.any(crossing):
+        return 0
+    label_counts = {int(v): int(np.count_nonzero(labels == v)) for v in np.unique(labels)}
+    deferred = 0
+    for coordinate in np.argwhere(crossing):
+        index = tuple(int(x) for x in coordinate)
+        old_label = int(labels[index])
+        new_label = int(competitor[index])
+        if simple_relabel_local(labels, index, old_label, new_label, label_counts):
+            labels[index] = new_label
+            alpha[index] = 1.0
+            label_counts[old_label] = label_counts.get(old_label, 0) - 1
+            label_counts[new_label] = label_counts.get(new_label, 0) + 1
+        else:
+            deferred += 1
+            alpha[index] = max(float(alpha[index]), 1.0e-6)
+    return deferred
+
+
+def balanced_gaussian_remap(labels: np.ndarray, alpha: np.ndarray, sigma_cells: float) -> int:
+    """Volume-balanced exchange of the strongest opposite proposals per label
+    pair of one phase class (lines 597-672); in place; changed-cell count."""
+    values = np.unique(labels)
+    scores = {int(v): gaussian_filter_wrap((labels == v).astype(float), sigma_cells) for v in values}
+    interface = np.zeros(labels.shape, dtype=bool)
+    candidates = {int(v): np.zeros(labels.shape, dtype=bool) for v in values}
+    for axis in range(labels.ndim):
+        for shift in (-1, 1):
+            nb = np.roll(labels, shift, axis=axis)
+            interface |= nb != labels
+            for v in values:
+                candidates[int(v)] |= nb == v
+    proposals = {}
+    flat_labels = labels.ravel()
+    for flat in np.flatnonzero(interface):
+        old = int(flat_labels[flat])
+        old_score = float(scores[old].ravel()[flat])
+        best, best_gain = old, 0.0
+        for v in values:
+            v = int(v)
+            if v == old or not candidates[v].ravel()[flat]:
+                continue
+            gain = float(scores[v].ravel()[flat]) - old_score
+            if gain > best_gain:
+                best, best_gain = v, gain
+        if best != old:
+            proposals.setdefault((old, best), []).append((best_gain, int(flat)))
+    changed = np.zeros(labels.size, dtype=bool)
+    label_counts = {int(v): int(np.count_nonzero(labels == v)) for v in values}
+    for ia, first in enumerate(values):
+        for second in values[ia + 1:]:
+            first, second = int(first), int(second)
+            if (first == 0) != (second == 0):
+                continue
+            forward = sorted(proposals.get((first, second), ()), reverse=True)
+            reverse = sorted(proposals.get((second, first), ()), reverse=True)
+            for (_, ff), (_, fr) in zip(forward, reverse):
+                index_f = np.unravel_index(ff, labels.shape)
+                index_r = np.unravel_index(fr, labels.shape)
+                if int(flat_labels[ff]) != first or int(flat_labels[fr]) != second:
+                    continue
+                if not simple_relabel_local(labels, index_f, first, second, label_counts):
+                    continue
+                flat_labels[ff] = second
+                label_counts[first] -= 1
+                label_counts[second] += 1
+                if not simple_relabel_local(labels, index_r, second, first, label_counts):
+                    flat_labels[ff] = first
+                    label_counts[first] += 1
+                    label_counts[second] -= 1
+                    continue
+                flat_labels[fr] = first
+                label_counts[second] -= 1
+                label_counts[first] += 1
+                changed[ff] = True
+                changed[fr] = True
+    alpha.ravel()[changed] = 1.0
     return int(np.count_nonzero(changed))

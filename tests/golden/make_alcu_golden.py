@@ -7,7 +7,8 @@ material module, scripts/run_alcu_gpk_microstructure.py:
   diffuse_conservative_subcycled (679-699),
   conservative_partition_transfer (702-737),
   interface_matrix_composition (740-755),
-  conservative_gaussian_remap (562-594),
+  conservative_gaussian_remap (562-594), balanced_gaussian_remap (597-672),
+  commit_topology_transactions (526-559), topology_simple_relabel (464-523),
 
 and runs them on seeded states shaped like the module's own: int8 labels
 0..3 (alpha-Al and three theta-prime variants) with plates and spheres, one
@@ -144,6 +145,74 @@ def main(root: str) -> None:
             out[f"{tag}_labels"] = lab
             out[f"{tag}_alpha"] = al
             out[f"{tag}_changed"] = np.int64(n)
+            lab = labels.copy()
+            al = alpha.copy()
+            n = ref.balanced_gaussian_remap(lab, al, sigma)
+            tag = f"{name}_bgr_{int(round(sigma * 100))}"
+            out[f"{tag}_labels"] = lab
+            out[f"{tag}_alpha"] = al
+            out[f"{tag}_changed"] = np.int64(n)
+        # crossing commits on a random 40% of the interface cells
+        crossing = mask & (rng.random(shape) < 0.4)
+        lab = labels.copy()
+        al = alpha.copy()
+        al[crossing] = -rng.uniform(0.0, 0.2, int(crossing.sum()))
+        al_in = al.copy()
+        deferred = ref.commit_topology_transactions(lab, al, comp, crossing)
+        out.update({f"{name}_tx_crossing": crossing, f"{name}_tx_alpha_in": al_in, f"{name}_tx_labels": lab,
+                    f"{name}_tx_alpha": al, f"{name}_tx_deferred": np.int64(deferred)})
+    # balanced remap on rough boundaries between variants (proposals both ways)
+    for name, shape in (("rough_2d", (48, 50)), ("rough_3d", (20, 22, 18))):
+        nd = len(shape)
+        coords = np.indices(shape)
+        wobble = rng.integers(-2, 3, size=shape[1:])
+        lab = np.where(coords[0] < shape[0] // 2 + wobble[None], 1, 2).astype(np.int8)
+        if nd == 3:
+            lab[(coords[2] > shape[2] * 2 // 3 + rng.integers(-1, 2, size=shape))] = 3
+        flip = rng.random(shape) < 0.06
+        lab[flip] = rng.integers(1, 4 if nd == 3 else 3, size=int(flip.sum()))
+        lab[:, :2] = 0  # a matrix strip: its pairs with the variants are not exchanged
+        alpha = rng.uniform(0.1, 1.0, shape)
+        out[f"{name}_labels"] = lab
+        out[f"{name}_alpha"] = alpha
+        for sigma in (0.70, 1.2):
+            l2 = lab.copy()
+            a2 = alpha.copy()
+            n = ref.balanced_gaussian_remap(l2, a2, sigma)
+            tag = f"{name}_bgr_{int(round(sigma * 100))}"
+            out[f"{tag}_labels"] = l2
+            out[f"{tag}_alpha"] = a2
+            out[f"{tag}_changed"] = np.int64(n)
+    # canonical certificate configurations, with the reference's verdicts in
+    # its local form (used by both callers) and its global form
+    topo = []
+    a = np.zeros((9, 9), np.int8); a[:, :5] = 1
+    topo.append(("smooth_2d", a, (4, 4), 0))
+    a = np.zeros((11, 11), np.int8); a[3:8, 2:5] = 1; a[3:8, 6:9] = 1; a[5, 5] = 1
+    topo.append(("split_2d", a, (5, 5), 0))
+    a = np.zeros((9, 9), np.int8); a[4, 3] = 1; a[4, 5] = 1
+    topo.append(("merge_2d", a, (4, 4), 1))
+    a = np.zeros((9, 9), np.int8); a[4, 4] = 1
+    topo.append(("extinct_2d", a, (4, 4), 0))
+    a = np.zeros((9, 9), np.int8); a[2:7, 2] = 1; a[2:7, 6] = 1; a[2, 2:7] = 1; a[6, 2:7] = 1
+    topo.append(("ring_2d", a, (2, 4), 0))
+    a = np.zeros((9, 9, 9), np.int8); a[3:6, 3:6, 1:4] = 2; a[3:6, 3:6, 5:8] = 2; a[4, 4, 4] = 2
+    topo.append(("split_3d", a, (4, 4, 4), 0))
+    a = np.zeros((7, 7, 7), np.int8); a[3, 3, 3] = 3
+    topo.append(("extinct_3d", a, (3, 3, 3), 0))
+    a = np.zeros((8, 8, 8), np.int8); a[2:6, 2:6, 2:6] = 1
+    topo.append(("corner_3d", a, (2, 2, 2), 0))
+    a = np.zeros((2, 5), np.int8); a[:, 2:] = 2
+    topo.append(("narrow_2d", a, (0, 2), 0))
+    for tname, lab, index, new in topo:
+        counts = {int(v): int(np.count_nonzero(lab == v)) for v in np.unique(lab)}
+        local = ref.topology_simple_relabel(lab.copy(), index, int(lab[index]), new, counts, local_only=True)
+        glob = ref.topology_simple_relabel(lab.copy(), index, int(lab[index]), new, counts, local_only=False)
+        out[f"topo_{tname}_labels"] = lab
+        out[f"topo_{tname}_index"] = np.asarray(index, dtype=np.int64)
+        out[f"topo_{tname}_new"] = np.int64(new)
+        out[f"topo_{tname}_local"] = np.bool_(local)
+        out[f"topo_{tname}_global"] = np.bool_(glob)
     # the taps scipy sampled in this process (numpy's exp), for callers whose
     # numpy rounds exp differently
     for sigma in (0.70, 0.75, 1.2):

@@ -113,3 +113,34 @@ def test_oracle_gaussian_remap(z, name, sigma):
     tag = f"{name}_cgr_{int(round(sigma * 100))}"
     assert n == int(z[f"{tag}_changed"])
     assert np.array_equal(lab, z[f"{tag}_labels"]) and same(al, z[f"{tag}_alpha"])
+
+
+@pytest.mark.parametrize("sigma", [0.70, 1.2])
+@pytest.mark.parametrize("name", ["2d", "3d", "rough_2d", "rough_3d"])
+def test_oracle_balanced_remap(z, name, sigma):
+    lab = z[f"{name}_labels"].copy()
+    al = z[f"{name}_alpha"].copy()
+    n = O.balanced_gaussian_remap(lab, al, sigma)
+    tag = f"{name}_bgr_{int(round(sigma * 100))}"
+    assert n == int(z[f"{tag}_changed"])
+    assert np.array_equal(lab, z[f"{tag}_labels"]) and same(al, z[f"{tag}_alpha"])
+
+
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_oracle_topology_transactions(z, name):
+    lab = z[f"{name}_labels"].copy()
+    al = z[f"{name}_tx_alpha_in"].copy()
+    d = O.commit_topology_transactions(lab, al, z[f"{name}_competitor"], z[f"{name}_tx_crossing"])
+    assert d == int(z[f"{name}_tx_deferred"])
+    assert np.array_equal(lab, z[f"{name}_tx_labels"]) and same(al, z[f"{name}_tx_alpha"])
+
+
+def test_oracle_certificate_known_answers(z):
+    names = sorted({k[5:-7] for k in z.files if k.startswith("topo_") and k.endswith("_labels")})
+    assert len(names) >= 9
+    for n in names:
+        lab = z[f"topo_{n}_labels"]
+        index = tuple(int(v) for v in z[f"topo_{n}_index"])
+        counts = {int(v): int(np.count_nonzero(lab == v)) for v in np.unique(lab)}
+        got = O.simple_relabel_local(lab.copy(), index, int(lab[index]), int(z[f"topo_{n}_new"]), counts)
+        assert got == bool(z[f"topo_{n}_local"]), n
