@@ -273,7 +273,7 @@ def _alcu_state(shape, plates, rng):
 def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
     """The Al-Cu module's per-step transport and remap (competitor,
     precipitate fraction, matrix composition, interface composition, sub-cycled
-    diffusion, partition transfer, Gaussian remap), FP64, on the reference's
+    diffusion, partition transfer, crossing transactions, Gaussian remap), FP64, on the reference's
     three_dimensional case (96^3, three plates of its layout_3d_96) and on a
     256^3 field with 400 plates; inputs resident, each stage timed with CUDA
     events on the launching stream."""
@@ -292,16 +292,17 @@ def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
             for k in range(400)]
     cases["256^3, 400 plates"] = ((256, 256, 256), many)
     p = O.AlCuParams()
-    stages = ["competitor", "fraction", "composition", "interface", "diffuse", "transfer", "remap"]
+    stages = ["competitor", "fraction", "composition", "interface", "diffuse", "transfer", "transactions", "remap"]
     # algorithmic bytes per cell of each stage (each field read or written
-    # once; labels 1 B, fields 8 B): competitor 1 + 2, fraction 10 + 8,
+    # once; labels 1 B, fields 8 B): transactions (histogram 1, crossing
+    # flags 1 + 4, ordered compaction 8), competitor 1 + 2, fraction 10 + 8,
     # composition 16 + 8, interface composition 16 + 16 in, 3 passes of 2
     # fields 32 each, 16 + 8 out, diffusion 2 substeps of 16 + 8 and the last
     # c_m 8, partition transfer (transfer 32 + 24, 4 sums 32, 3 passes 48,
     # weight 24 + 16, apply 16 + 8, argmax 16), remap (labels copy 2, union-
     # find 4 x 4, flags / scatter / vacate per wave 10, changed 1 + 8)
     per_cell = {"competitor": 3, "fraction": 18, "composition": 24, "interface": 152, "diffuse": 56,
-                "transfer": 216, "remap": 37}
+                "transfer": 216, "transactions": 14, "remap": 37}
     peak, peak_kind = _peaks()
     for name, (shape, plates) in cases.items():
         lab, alpha, ctot = _alcu_state(shape, plates, rng)
@@ -313,6 +314,8 @@ def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
         # a fixed synthetic growth of the fraction at interface cells
         m0, _ = h.competitor(dl)
         grow = (0.05 * m0.double()).contiguous()
+        # a fixed tenth of the initial interface cells cross in every step
+        cross = (m0 & (torch.rand(shape, device="cuda") < 0.1)).to(torch.uint8).contiguous()
         stream = torch.cuda.current_stream()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(stages) + 1)]
         acc = {k: 0.0 for k in stages}
@@ -339,9 +342,12 @@ def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
             h.partition_transfer(dc, fp, fp + grow, trace, 0.75)
             if timed:
                 ev[6].record(stream)
-            info["changed"] = h.gaussian_remap(dl, da, 0.70)
+            info["deferred"] = h.commit_transactions(dl, da, comp, cross)
             if timed:
                 ev[7].record(stream)
+            info["changed"] = h.gaussian_remap(dl, da, 0.70)
+            if timed:
+                ev[8].record(stream)
 
         for _ in range(warmup):
             step(False)
@@ -359,7 +365,8 @@ def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
         st_ms = {k: v / steps for k, v in acc.items()}
         res = {"ms_per_step": ms, "cells_per_s": n / (ms / 1e3), "stages_ms": st_ms,
                "components": h.info()["components"], "remap_waves": h.info()["waves"],
-               "changed_last_step": info["changed"],
+               "changed_last_step": info["changed"], "deferred_last_step": info["deferred"],
+               "crossing_cells": int(cross.sum().item()),
                "stage_GBps": {k: per_cell[k] * n / (st_ms[k] / 1e3) / 1e9 for k in stages if st_ms[k] > 0},
                "algorithmic_bytes_per_cell": per_cell, "peak": peak, "peak_kind": peak_kind}
         if with_cpu and shape == (96, 96, 96):
@@ -372,10 +379,11 @@ def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
             tr_h = O.interface_matrix_composition(cm_h, fp_h, p)
             c_h, _, _ = O.diffuse_conservative_subcycled(c_h, fp_h, p, 10.0)
             O.conservative_partition_transfer(c_h, fp_h, fp_h + g_h, tr_h, p)
+            O.commit_topology_transactions(lab_h, al_h, comp_h, cross.cpu().numpy().astype(bool))
             O.conservative_gaussian_remap(lab_h, al_h, 0.70)
             cpu_s = time.perf_counter() - t_cpu
             res["cpu_baseline"] = {"value": n / cpu_s, "unit": "cells/s", "cores": 1, "kind": "port",
-                                   "sample": "one step of the numpy restatement of the same seven functions "
+                                   "sample": "one step of the numpy restatement of the same eight functions "
                                              "(numpy/scipy order, one thread) on the 96^3 state"}
         out[name] = res
         h.close()

@@ -120,6 +120,8 @@ def lib() -> C.CDLL:
         "gpk_alcu_interface_composition": ([vp, vp, vp, vp, C.POINTER(dbl), i32], i32),
         "gpk_alcu_gaussian_remap": ([vp, vp, vp, C.POINTER(dbl), i32, C.POINTER(i64)], i32),
         "gpk_alcu_sum": ([vp, vp, C.POINTER(dbl)], i32),
+        "gpk_alcu_commit_transactions": ([vp, vp, vp, vp, vp, C.POINTER(i64)], i32),
+        "gpk_alcu_balanced_remap": ([vp, vp, vp, C.POINTER(dbl), i32, C.POINTER(i64)], i32),
         "gpk_alcu_gaussian_filter": ([vp, vp, vp, C.POINTER(dbl), i32], i32),
         "gpk_alcu_info": ([vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)], i32),
     }

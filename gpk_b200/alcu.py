@@ -10,6 +10,8 @@ in-place behaviour of the reference's Al-Cu material module
   conservative_partition_transfer(ctot, old, new, c_m, p)         702-737
   interface_matrix_composition(cm, fprec, p)                      740-755
   conservative_gaussian_remap(labels, alpha, sigma_cells)         562-594
+  balanced_gaussian_remap(labels, alpha, sigma_cells)             597-672
+  commit_topology_transactions(labels, alpha, competitor, crossing) 526-559
 
 `p` is any object with the reference's `Parameters` fields (dx, diffusivity,
 c_matrix_eq, c_theta, composition_extension_sigma_cells).  NumPy inputs give
@@ -30,7 +32,7 @@ from ._lib import CAlCuParams, check, lib
 
 __all__ = ["AlCuTransport", "gauss_taps", "neighbor_competitor", "precip_fraction", "matrix_composition",
            "diffuse_conservative_subcycled", "conservative_partition_transfer", "interface_matrix_composition",
-           "conservative_gaussian_remap", "field_sum"]
+           "conservative_gaussian_remap", "balanced_gaussian_remap", "commit_topology_transactions", "field_sum"]
 
 
 def gauss_taps(sigma: float, truncate: float = 4.0) -> np.ndarray:
@@ -184,6 +186,25 @@ class AlCuTransport:
         check(lib().gpk_alcu_gaussian_remap(self._h, self._i8(labels), self._f64(alpha), tp, r, C.byref(n)))
         return int(n.value)
 
+    def balanced_remap(self, labels, alpha, sigma) -> int:
+        self._bind(labels, alpha)
+        t, tp, r = _taps_arg(sigma)
+        n = C.c_int64(0)
+        check(lib().gpk_alcu_balanced_remap(self._h, self._i8(labels), self._f64(alpha), tp, r, C.byref(n)))
+        return int(n.value)
+
+    def commit_transactions(self, labels, alpha, competitor, crossing) -> int:
+        """crossing: a CUDA bool or uint8 tensor; returns the deferred count."""
+        import torch
+
+        self._bind(labels, alpha, competitor, crossing)
+        if crossing.dtype not in (torch.bool, torch.uint8):
+            raise ValueError("crossing must be a bool or uint8 tensor")
+        n = C.c_int64(0)
+        check(lib().gpk_alcu_commit_transactions(self._h, self._i8(labels), self._f64(alpha), self._i8(competitor),
+                                                 crossing.data_ptr(), C.byref(n)))
+        return int(n.value)
+
     def sum(self, x) -> float:
         self._bind(x)
         out = C.c_double(0.0)
@@ -309,6 +330,36 @@ def conservative_gaussian_remap(labels, alpha, sigma_cells) -> int:
         alpha[...] = al.cpu().numpy()
         return n
     return h.gaussian_remap(labels, alpha, sigma_cells)
+
+
+def balanced_gaussian_remap(labels, alpha, sigma_cells) -> int:
+    """labels and alpha updated in place; returns the changed-cell count."""
+    h = _handle(labels.shape)
+    if _is_np(labels, alpha):
+        if labels.dtype != np.int8:
+            raise ValueError("labels must be int8, as in the reference")
+        lab = _dev(labels, np.int8)
+        al = _dev(alpha, np.float64)
+        n = h.balanced_remap(lab, al, sigma_cells)
+        labels[...] = lab.cpu().numpy()
+        alpha[...] = al.cpu().numpy()
+        return n
+    return h.balanced_remap(labels, alpha, sigma_cells)
+
+
+def commit_topology_transactions(labels, alpha, competitor, crossing) -> int:
+    """labels and alpha updated in place; returns the deferred-cell count."""
+    h = _handle(labels.shape)
+    if _is_np(labels, alpha, competitor, crossing):
+        if labels.dtype != np.int8:
+            raise ValueError("labels must be int8, as in the reference")
+        lab = _dev(labels, np.int8)
+        al = _dev(alpha, np.float64)
+        n = h.commit_transactions(lab, al, _dev(competitor, np.int8), _dev(crossing, np.uint8))
+        labels[...] = lab.cpu().numpy()
+        alpha[...] = al.cpu().numpy()
+        return n
+    return h.commit_transactions(labels, alpha, competitor, crossing)
 
 
 def field_sum(x) -> float:

@@ -821,6 +821,255 @@ __global__ void k_cgr_changed(const int* __restrict__ band, const int* __restric
     if (threadIdx.x == 0 && agg) atomicAdd(count, agg);
 }
 
+// ---------------------------------------------------------------- topology transactions, balanced remap
+
+// The local certificate of topology_simple_relabel(..., local_only=True)
+// (lines 464-523) on bitmasks of the periodic 3^d patch (3^2 in 2-D):
+// position p = 9 a + 3 b + c in 3-D, 3 b + c in 2-D, centre 13 or 4.
+__device__ __forceinline__ unsigned face_nbr(int b, int nd) {
+    unsigned m = 0;
+    if (nd == 3) {
+        const int a = b / 9, r = b % 9, y = r / 3, x = r % 3;
+        if (a > 0) m |= 1u << (b - 9);
+        if (a < 2) m |= 1u << (b + 9);
+        if (y > 0) m |= 1u << (b - 3);
+        if (y < 2) m |= 1u << (b + 3);
+        if (x > 0) m |= 1u << (b - 1);
+        if (x < 2) m |= 1u << (b + 1);
+    } else {
+        const int y = b / 3, x = b % 3;
+        if (y > 0) m |= 1u << (b - 3);
+        if (y < 2) m |= 1u << (b + 3);
+        if (x > 0) m |= 1u << (b - 1);
+        if (x < 2) m |= 1u << (b + 1);
+    }
+    return m;
+}
+// face-connected components of mask that touch a face neighbour of the centre
+__device__ int topo_number(unsigned mask, int nd) {
+    const unsigned incident = nd == 3 ? ((1u << 4) | (1u << 10) | (1u << 12) | (1u << 14) | (1u << 16) | (1u << 22))
+                                      : ((1u << 1) | (1u << 3) | (1u << 5) | (1u << 7));
+    int count = 0;
+    unsigned unseen = mask;
+    while (unseen) {
+        unsigned comp = unseen & (~unseen + 1u);
+        unsigned frontier = comp;
+        while (frontier) {
+            unsigned grow = 0;
+            for (unsigned f = frontier; f; f &= f - 1u) grow |= face_nbr(__ffs(f) - 1, nd);
+            grow &= unseen & ~comp;
+            comp |= grow;
+            frontier = grow;
+        }
+        unseen &= ~comp;
+        if (comp & incident) ++count;
+    }
+    return count;
+}
+// positions of the periodic patch around cell i holding label a / b (centre excluded)
+__device__ void patch_masks(const Ext& d, const int8_t* lab, long long i, int a, int b, unsigned& ma, unsigned& mb) {
+    int x0, x1, x2;
+    cell_coords(d, i, x0, x1, x2);
+    const int y1[3] = {x1 == 0 ? d.e[1] - 1 : x1 - 1, x1, x1 + 1 == d.e[1] ? 0 : x1 + 1};
+    const int y2[3] = {x2 == 0 ? d.e[2] - 1 : x2 - 1, x2, x2 + 1 == d.e[2] ? 0 : x2 + 1};
+    const int y0[3] = {x0 == 0 ? d.e[0] - 1 : x0 - 1, x0, x0 + 1 == d.e[0] ? 0 : x0 + 1};
+    ma = mb = 0;
+    const int n0 = d.ndim == 3 ? 3 : 1;
+    for (int p0 = 0; p0 < n0; ++p0)
+        for (int p1 = 0; p1 < 3; ++p1)
+            for (int p2 = 0; p2 < 3; ++p2) {
+                const int bit = d.ndim == 3 ? 9 * p0 + 3 * p1 + p2 : 3 * p1 + p2;
+                if (bit == (d.ndim == 3 ? 13 : 4)) continue;
+                const int z0 = d.ndim == 3 ? y0[p0] : 0;
+                const int v = lab[((long long)z0 * d.e[1] + y1[p1]) * d.e[2] + y2[p2]];
+                if (v == a) ma |= 1u << bit;
+                if (v == b) mb |= 1u << bit;
+            }
+}
+// counts: label value + 128 -> cells holding it
+__device__ bool cert_local(const Ext& d, const int8_t* lab, long long i, int old_label, int new_label,
+                           const int* counts) {
+    if (old_label == new_label) return false;
+    unsigned mo, mn;
+    patch_masks(d, lab, i, old_label, new_label, mo, mn);
+    const int oc = topo_number(mo, d.ndim);
+    const bool extinction = counts[old_label + 128] <= 1;
+    if (oc == 0 && !extinction) return false;
+    if (oc > 1) return false;
+    const int nc = topo_number(mn, d.ndim);
+    if (nc == 0 || nc > 1) return false;
+    return true;
+}
+
+__global__ void k_label_hist(long long N, const int8_t* __restrict__ lab, int* __restrict__ counts) {
+    __shared__ int h[256];
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) h[k] = 0;
+    __syncthreads();
+    GRID_STRIDE(i, N) atomicAdd(&h[(int)lab[i] + 128], 1);
+    __syncthreads();
+    for (int k = threadIdx.x; k < 256; k += blockDim.x)
+        if (h[k]) atomicAdd(&counts[k], h[k]);
+}
+__global__ void k_u8_flags(long long N, const uint8_t* __restrict__ m, int* __restrict__ flag) {
+    GRID_STRIDE(i, N) flag[i] = m[i] != 0;
+}
+
+// commit_topology_transactions (lines 526-559): the crossing cells in C
+// order, each certificate against the state the earlier ones left
+__global__ void k_tx_commit(Ext d, const int* __restrict__ list, const int* __restrict__ n_list, int8_t* lab,
+                            double* alpha, const int8_t* __restrict__ comp, int* counts,
+                            unsigned long long* __restrict__ deferred) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int M = *n_list;
+    unsigned long long nd = 0;
+    for (int q = 0; q < M; ++q) {
+        const long long i = list[q];
+        const int old_label = lab[i], new_label = comp[i];
+        if (cert_local(d, lab, i, old_label, new_label, counts)) {
+            lab[i] = (int8_t)new_label;
+            alpha[i] = 1.0;
+            counts[old_label + 128] -= 1;
+            counts[new_label + 128] += 1;
+        } else {
+            ++nd;
+            const double a = alpha[i];
+            alpha[i] = 1.0e-6 > a ? 1.0e-6 : a;  // Python max(a, 1e-6)
+        }
+    }
+    *deferred = nd;
+}
+
+// the labels present, ascending (np.unique), at most 8
+struct Vals {
+    int n;
+    int v[8];
+};
+
+__global__ void k_indicator(long long N, const int8_t* __restrict__ lab, int v, double* __restrict__ out) {
+    GRID_STRIDE(i, N) out[i] = lab[i] == v ? 1.0 : 0.0;
+}
+
+// proposals of balanced_gaussian_remap (lines 611-636): an interface cell
+// proposes the face-neighbour label of largest score gain over its own
+// (labels in ascending order, strictly larger gains only)
+__global__ void __launch_bounds__(128) k_bgr_propose(Ext d, Vals vals, const int8_t* __restrict__ lab,
+                                                     const double* __restrict__ scores, int* __restrict__ flag,
+                                                     int* __restrict__ pair, double* __restrict__ gain) {
+    CELLS3(d) {
+        const long long i = CELL_INDEX(d);
+        const int x[3] = {x0, x1, x2};
+        const int l = lab[i];
+        unsigned near = 0;  // bit k: a face neighbour holds vals.v[k]
+        bool iface = false;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (a < d.a0) continue;
+            const int n = d.e[a];
+            const long long ip = i + (long long)((x[a] + 1 == n ? 0 : x[a] + 1) - x[a]) * d.st[a];
+            const long long im = i + (long long)((x[a] == 0 ? n - 1 : x[a] - 1) - x[a]) * d.st[a];
+            const int nbs[2] = {lab[im], lab[ip]};
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                iface |= nbs[q] != l;
+                for (int k = 0; k < vals.n; ++k)
+                    if (nbs[q] == vals.v[k]) near |= 1u << k;
+            }
+        }
+        int f = 0;
+        if (iface) {
+            int oi = 0;
+            for (int k = 0; k < vals.n; ++k)
+                if (vals.v[k] == l) oi = k;
+            const double old_score = scores[(long long)oi * d.N + i];
+            int best = oi;
+            double best_gain = 0.0;
+            for (int k = 0; k < vals.n; ++k) {
+                if (k == oi || !((near >> k) & 1u)) continue;
+                const double g = scores[(long long)k * d.N + i] - old_score;
+                if (g > best_gain) {
+                    best = k;
+                    best_gain = g;
+                }
+            }
+            if (best != oi) {
+                f = 1;
+                pair[i] = oi * 8 + best;
+                gain[i] = best_gain;
+            }
+        }
+        flag[i] = f;
+    }
+}
+// records in descending cell order: key = descending gain
+__global__ void k_bgr_records(long long N, const int* __restrict__ flag, const int* __restrict__ pos,
+                              const int* __restrict__ count, const double* __restrict__ gain,
+                              int* __restrict__ cells, unsigned long long* __restrict__ key) {
+    const int M = *count;
+    GRID_STRIDE(i, N) if (flag[i]) {
+        const int q = M - 1 - pos[i];
+        cells[q] = (int)i;
+        key[q] = ~okey(gain[i]);
+    }
+}
+__global__ void k_pair_hist(const unsigned* __restrict__ pk, const int* __restrict__ count, int* __restrict__ hist) {
+    const int M = *count;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) atomicAdd(&hist[pk[q]], 1);
+}
+
+struct PairSegs {
+    int start[64], len[64];
+};
+
+// the exchanges (lines 640-671), serially in the reference's order
+__global__ void k_bgr_exchange(Ext d, Vals vals, PairSegs segs, const int* __restrict__ cells, int8_t* lab,
+                               int* counts, uint8_t* __restrict__ changed) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (int ia = 0; ia < vals.n; ++ia)
+        for (int ib = ia + 1; ib < vals.n; ++ib) {
+            const int first = vals.v[ia], second = vals.v[ib];
+            if ((first == 0) != (second == 0)) continue;
+            const int sf = ia * 8 + ib, sr = ib * 8 + ia;
+            const int cnt = segs.len[sf] < segs.len[sr] ? segs.len[sf] : segs.len[sr];
+            for (int k = 0; k < cnt; ++k) {
+                const long long f = cells[segs.start[sf] + k];
+                const long long r = cells[segs.start[sr] + k];
+                if (lab[f] != first || lab[r] != second) continue;
+                if (!cert_local(d, lab, f, first, second, counts)) continue;
+                lab[f] = (int8_t)second;
+                counts[first + 128] -= 1;
+                counts[second + 128] += 1;
+                if (!cert_local(d, lab, r, second, first, counts)) {
+                    lab[f] = (int8_t)first;
+                    counts[first + 128] += 1;
+                    counts[second + 128] -= 1;
+                    continue;
+                }
+                lab[r] = (int8_t)first;
+                counts[second + 128] -= 1;
+                counts[first + 128] += 1;
+                changed[f] = 1;
+                changed[r] = 1;
+            }
+        }
+}
+__global__ void k_bgr_finish(const int* __restrict__ cells, const int* __restrict__ count,
+                             const uint8_t* __restrict__ changed, double* __restrict__ alpha,
+                             unsigned long long* __restrict__ n_changed) {
+    typedef cub::BlockReduce<unsigned long long, 256> BR;
+    __shared__ typename BR::TempStorage tmp;
+    const int M = *count;
+    unsigned long long n = 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
+        const int i = cells[q];
+        if (changed[i]) {
+            alpha[i] = 1.0;
+            ++n;
+        }
+    }
+    const unsigned long long agg = BR(tmp).Sum(n);
+    if (threadIdx.x == 0 && agg) atomicAdd(n_changed, agg);
+}
+
 }  // namespace
 
 // ============================================================== handle
@@ -855,6 +1104,9 @@ struct gpk_alcu {
     unsigned *sk1 = nullptr, *sk2 = nullptr;
     uint8_t *u8a = nullptr, *u8b = nullptr;  // active cells and their 3^d box maximum
     int* band = nullptr;                     // cells of some component's dilation, in order
+    int* cnt256 = nullptr;                   // cells per label value (value + 128)
+    double* scores = nullptr;                // the balanced remap's per-label Gaussians
+    int n_scores = 0;
     void* cub_tmp = nullptr;
     size_t cub_bytes = 0;
     int seg_bits = 1;
@@ -906,7 +1158,7 @@ void free_all(gpk_alcu* h) {
     cudaFree(h->seg); cudaFree(h->start); cudaFree(h->flag); cudaFree(h->pos); cudaFree(h->cand);
     cudaFree(h->cells1); cudaFree(h->cells2); cudaFree(h->conflicts);
     cudaFree(h->key1); cudaFree(h->key2); cudaFree(h->sk1); cudaFree(h->sk2); cudaFree(h->cub_tmp);
-    cudaFree(h->u8a); cudaFree(h->u8b); cudaFree(h->band);
+    cudaFree(h->u8a); cudaFree(h->u8b); cudaFree(h->band); cudaFree(h->cnt256); cudaFree(h->scores);
     if (h->own) cudaStreamDestroy(h->own);
 }
 
@@ -1194,7 +1446,7 @@ extern "C" int gpk_alcu_create(int ndim, const int* shape, const gpk_alcu_params
         if (!alloc((void**)q, sizeof(int) * N)) return fail(GPK_ERR_OUT_OF_MEMORY);
     if (!alloc((void**)&h->orig, N) || !alloc((void**)&h->key1, 8 * N) || !alloc((void**)&h->key2, 8 * N) ||
         !alloc((void**)&h->sk1, 4 * N) || !alloc((void**)&h->sk2, 4 * N) || !alloc((void**)&h->u8a, N) ||
-        !alloc((void**)&h->u8b, N) || !alloc((void**)&h->band, 4 * N))
+        !alloc((void**)&h->u8b, N) || !alloc((void**)&h->band, 4 * N) || !alloc((void**)&h->cnt256, 4 * 256))
         return fail(GPK_ERR_OUT_OF_MEMORY);
     while ((1ll << h->seg_bits) < N) ++h->seg_bits;
     size_t b1 = 0, b2 = 0, b3 = 0;
@@ -1491,6 +1743,124 @@ extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alph
     ALCU_TRY(cudaMemcpyAsync(&n_changed, h->u64 + 2, sizeof(n_changed), cudaMemcpyDeviceToHost, st));
     ALCU_TRY(cudaStreamSynchronize(st));
     if (changed) *changed = (int64_t)n_changed;
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_commit_transactions(gpk_alcu* h, int8_t* labels, double* alpha, const int8_t* competitor,
+                                            const uint8_t* crossing, int64_t* deferred) {
+    if (!h || !labels || !alpha || !competitor || !crossing) {
+        gpk_set_error("alcu: null argument");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    const Ext& d = h->d;
+    const long long N = d.N;
+    cudaStream_t st = h->stream;
+    const int G = h->grid;
+    ALCU_TRY(cudaMemsetAsync(h->cnt256, 0, sizeof(int) * 256, st));
+    ALCU_TRY(cudaMemsetAsync(h->u64 + 3, 0, sizeof(unsigned long long), st));
+    k_label_hist<<<G, 256, 0, st>>>(N, labels, h->cnt256);
+    k_u8_flags<<<G, 256, 0, st>>>(N, crossing, h->flag);
+    ALCU_TRY(cudaGetLastError());
+    size_t b = h->cub_bytes;
+    ALCU_TRY(cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, h->flag, h->pos, (int)N, st));
+    k_compact<<<G, 256, 0, st>>>(N, h->flag, h->pos, nullptr, h->cand, h->i32 + 6);
+    k_tx_commit<<<1, 32, 0, st>>>(d, h->cand, h->i32 + 6, labels, alpha, competitor, h->cnt256, h->u64 + 3);
+    ALCU_TRY(cudaGetLastError());
+    unsigned long long nd = 0;
+    ALCU_TRY(cudaMemcpyAsync(&nd, h->u64 + 3, sizeof(nd), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaStreamSynchronize(st));
+    if (deferred) *deferred = (int64_t)nd;
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_balanced_remap(gpk_alcu* h, int8_t* labels, double* alpha, const double* taps, int radius,
+                                       int64_t* changed) {
+    if (!h || !labels || !alpha) { gpk_set_error("alcu: null argument"); return GPK_ERR_INVALID_ARGUMENT; }
+    Taps t;
+    int rc = taps_of(taps, radius, t);
+    if (rc != GPK_OK) return rc;
+    const Ext& d = h->d;
+    const long long N = d.N;
+    cudaStream_t st = h->stream;
+    const int G = h->grid;
+    // the labels present (np.unique)
+    ALCU_TRY(cudaMemsetAsync(h->cnt256, 0, sizeof(int) * 256, st));
+    k_label_hist<<<G, 256, 0, st>>>(N, labels, h->cnt256);
+    ALCU_TRY(cudaGetLastError());
+    int hc[256];
+    ALCU_TRY(cudaMemcpyAsync(hc, h->cnt256, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaStreamSynchronize(st));
+    Vals vals{};
+    for (int k = 0; k < 256; ++k)
+        if (hc[k]) {
+            if (vals.n == 8) {
+                gpk_set_error("alcu: the balanced remap takes at most 8 distinct labels");
+                return GPK_ERR_INVALID_ARGUMENT;
+            }
+            vals.v[vals.n++] = k - 128;
+        }
+    if (h->n_scores < vals.n) {
+        ALCU_TRY(cudaStreamSynchronize(st));
+        cudaFree(h->scores);
+        h->scores = nullptr;
+        h->n_scores = 0;
+        if (cudaMalloc((void**)&h->scores, sizeof(double) * N * vals.n) != cudaSuccess) {
+            cudaGetLastError();
+            gpk_set_error("alcu: cudaMalloc of the balanced remap's score fields failed");
+            return GPK_ERR_OUT_OF_MEMORY;
+        }
+        h->n_scores = vals.n;
+        h->bytes += (long long)sizeof(double) * N * vals.n;
+    }
+    for (int k = 0; k < vals.n; ++k) {
+        k_indicator<<<G, 256, 0, st>>>(N, labels, vals.v[k], h->f[1]);
+        ALCU_TRY(cudaGetLastError());
+        if ((rc = gauss(h, t, h->f[1], h->scores + (long long)k * N, h->f[5])) != GPK_OK) return rc;
+    }
+    k_bgr_propose<<<grid3(d), B3, 0, st>>>(d, vals, labels, h->scores, h->flag, h->seg, h->f[2]);
+    ALCU_TRY(cudaGetLastError());
+    size_t b = h->cub_bytes;
+    ALCU_TRY(cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, h->flag, h->pos, (int)N, st));
+    int* n_rec = h->i32 + 7;
+    k_compact<<<G, 256, 0, st>>>(N, h->flag, h->pos, nullptr, h->cells2, n_rec);  // count only
+    k_bgr_records<<<G, 256, 0, st>>>(N, h->flag, h->pos, n_rec, h->f[2], h->cand, h->key1);
+    ALCU_TRY(cudaGetLastError());
+    int M = 0;
+    ALCU_TRY(cudaMemcpyAsync(&M, n_rec, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaStreamSynchronize(st));
+    if (changed) *changed = 0;
+    if (M == 0) return GPK_OK;
+    if ((rc = cub_reserve(h, M)) != GPK_OK) return rc;
+    const int sb = (M + 255) / 256 < G ? (M + 255) / 256 : G;
+    // descending gain, ties in descending cell order (the records' order);
+    // then grouped by (old, best) pair, stable
+    b = h->cub_bytes;
+    ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->key1, h->key2, h->cand, h->cells1, M, 0, 64, st));
+    k_cgr_segkeys<<<sb, 256, 0, st>>>(h->cells1, n_rec, h->seg, h->sk1);
+    ALCU_TRY(cudaGetLastError());
+    b = h->cub_bytes;
+    ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->sk1, h->sk2, h->cells1, h->cells2, M, 0, 6, st));
+    ALCU_TRY(cudaMemsetAsync(h->start, 0, sizeof(int) * 64, st));
+    k_pair_hist<<<sb, 256, 0, st>>>(h->sk2, n_rec, h->start);
+    ALCU_TRY(cudaGetLastError());
+    int hist[64];
+    ALCU_TRY(cudaMemcpyAsync(hist, h->start, sizeof(hist), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaStreamSynchronize(st));
+    PairSegs segs{};
+    for (int k = 0, acc = 0; k < 64; ++k) {
+        segs.start[k] = acc;
+        segs.len[k] = hist[k];
+        acc += hist[k];
+    }
+    ALCU_TRY(cudaMemsetAsync(h->u8a, 0, N, st));
+    ALCU_TRY(cudaMemsetAsync(h->u64 + 3, 0, sizeof(unsigned long long), st));
+    k_bgr_exchange<<<1, 32, 0, st>>>(d, vals, segs, h->cells2, labels, h->cnt256, h->u8a);
+    k_bgr_finish<<<sb, 256, 0, st>>>(h->cells2, n_rec, h->u8a, alpha, h->u64 + 3);
+    ALCU_TRY(cudaGetLastError());
+    unsigned long long nc = 0;
+    ALCU_TRY(cudaMemcpyAsync(&nc, h->u64 + 3, sizeof(nc), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaStreamSynchronize(st));
+    if (changed) *changed = (int64_t)nc;
     return GPK_OK;
 }
 

@@ -13,6 +13,8 @@
  *   gpk_alcu_partition_transfer     conservative_partition_transfer (702-737)
  *   gpk_alcu_interface_composition  interface_matrix_composition    (740-755)
  *   gpk_alcu_gaussian_remap         conservative_gaussian_remap     (562-594)
+ *   gpk_alcu_balanced_remap         balanced_gaussian_remap         (597-672)
+ *   gpk_alcu_commit_transactions    commit_topology_transactions    (526-559)
  *   gpk_alcu_sum                    np.sum of a float64 field
  *
  * Arrays keep the reference's layout: C order over the shape (n0, n1[, n2]),
@@ -104,6 +106,27 @@ int gpk_alcu_interface_composition(gpk_alcu* h, const double* cm, const double* 
  * (host, may be NULL) gets the count.  Components whose dilations are
  * disjoint are processed together: the result is that of the serial order. */
 int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alpha, const double* taps, int radius,
+                            int64_t* changed);
+/* The crossing cells (crossing != 0) relabelled to their competitor in C
+ * order, each only if the local certificate of topology_simple_relabel
+ * (lines 464-523, local_only=True: one face-connected component of the old
+ * label and of the new one around the cell within its periodic 3^d patch, or
+ * the old label's last cell) holds against the labels left by the earlier
+ * ones; accepted cells get alpha = 1, deferred ones alpha = max(alpha, 1e-6).
+ * The certificates run in that order on one device thread; deferred (host,
+ * may be NULL) gets the deferred count.                                    */
+int gpk_alcu_commit_transactions(gpk_alcu* h, int8_t* labels, double* alpha, const int8_t* competitor,
+                                 const uint8_t* crossing, int64_t* deferred);
+/* Every interface cell proposes the face-neighbour label of largest wrapped-
+ * Gaussian score gain over its own; for each pair of labels of one phase
+ * class (both nonzero, or both zero) the k-th strongest proposals of the two
+ * directions (gain descending, then cell descending) are exchanged when both
+ * pass the local certificate, so every label keeps its volume.  labels in
+ * place, alpha = 1 where a label changed, changed (host, may be NULL) the
+ * count.  At most 8 distinct label values; the proposals and their ordering
+ * run in parallel, the exchanges in the reference's order on one device
+ * thread.                                                                  */
+int gpk_alcu_balanced_remap(gpk_alcu* h, int8_t* labels, double* alpha, const double* taps, int radius,
                             int64_t* changed);
 /* out (host) = np.sum(x) of an N-cell field, same bits.                   */
 int gpk_alcu_sum(gpk_alcu* h, const double* x, double* out);

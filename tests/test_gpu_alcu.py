@@ -400,3 +400,126 @@ def test_diffusion_wide_range_against_oracle(torch_cuda, shape, dx):
         cd = dev(torch, ctot)
         cm, n = h.diffuse(cd, dev(torch, fp), dt)
         assert n == n_ref and same(host(cd), c_ref) and same(host(cm), cm_ref)
+
+
+# --------------------------------------------------------------------------
+# topology transactions and the balanced remap
+
+
+@gpu
+@pytest.mark.parametrize("sigma", [70, 120])
+@pytest.mark.parametrize("name", ["2d", "3d", "rough_2d", "rough_3d"])
+def test_golden_balanced_remap(torch_cuda, z, name, sigma):
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    h = AlCuTransport(z[f"{name}_labels"].shape, params())
+    lab = dev(torch, z[f"{name}_labels"])
+    al = dev(torch, z[f"{name}_alpha"])
+    n = h.balanced_remap(lab, al, z[f"taps_{sigma}"])
+    tag = f"{name}_bgr_{sigma}"
+    assert n == int(z[f"{tag}_changed"])
+    assert np.array_equal(host(lab), z[f"{tag}_labels"]) and same(host(al), z[f"{tag}_alpha"])
+
+
+@gpu
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_golden_topology_transactions(torch_cuda, z, name):
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    h = AlCuTransport(z[f"{name}_labels"].shape, params())
+    lab = dev(torch, z[f"{name}_labels"])
+    al = dev(torch, z[f"{name}_tx_alpha_in"])
+    d = h.commit_transactions(lab, al, dev(torch, z[f"{name}_competitor"]), dev(torch, z[f"{name}_tx_crossing"]))
+    assert d == int(z[f"{name}_tx_deferred"])
+    assert np.array_equal(host(lab), z[f"{name}_tx_labels"]) and same(host(al), z[f"{name}_tx_alpha"])
+
+
+@gpu
+def test_certificate_known_answers(torch_cuda, z):
+    """The reference's verdicts (local form) on canonical configurations,
+    each as a single-cell transaction."""
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    names = sorted({k[5:-7] for k in z.files if k.startswith("topo_") and k.endswith("_labels")})
+    for n in names:
+        lab = z[f"topo_{n}_labels"]
+        index = tuple(int(v) for v in z[f"topo_{n}_index"])
+        comp = lab.copy()
+        comp[index] = int(z[f"topo_{n}_new"])
+        crossing = np.zeros(lab.shape, dtype=np.uint8)
+        crossing[index] = 1
+        h = AlCuTransport(lab.shape, params())
+        dl = dev(torch, lab)
+        deferred = h.commit_transactions(dl, dev(torch, np.ones(lab.shape)), dev(torch, comp), dev(torch, crossing))
+        accepted = bool(z[f"topo_{n}_local"])
+        assert deferred == (0 if accepted else 1), n
+        assert int(host(dl)[index]) == (int(comp[index]) if accepted else int(lab[index])), n
+
+
+def rough_labels(shape, rng, variants):
+    coords = np.indices(shape)
+    wob = rng.integers(-2, 3, size=shape[1:])
+    lab = np.where(coords[0] < shape[0] // 2 + wob[None], 1, 2).astype(np.int8)
+    if variants == 3 and len(shape) == 3:
+        lab[coords[2] > shape[2] * 2 // 3 + rng.integers(-1, 2, size=shape)] = 3
+    flip = rng.random(shape) < 0.06
+    lab[flip] = rng.integers(1, variants + 1, size=int(flip.sum()))
+    lab[:, :2] = 0
+    return lab
+
+
+TX_CASES = [("plates_96", (96, 96, 96)), ("odd_2d", (67, 45)), ("thin_3d", (5, 40, 33)), ("narrow_2d", (2, 31))]
+
+
+@gpu
+@pytest.mark.parametrize("case", TX_CASES, ids=[c[0] for c in TX_CASES])
+def test_topology_transactions_against_oracle(torch_cuda, case):
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    name, shape = case
+    rng = np.random.default_rng(21)
+    lab, alpha, _, mask, comp = state(shape, rng)
+    crossing = mask & (rng.random(shape) < 0.5)
+    alpha[crossing] = -rng.uniform(0.0, 0.3, int(crossing.sum()))
+    lr, ar = lab.copy(), alpha.copy()
+    d_ref = O.commit_topology_transactions(lr, ar, comp, crossing)
+    h = AlCuTransport(shape, params())
+    dl, da = dev(torch, lab), dev(torch, alpha)
+    d = h.commit_transactions(dl, da, dev(torch, comp), dev(torch, crossing.astype(np.uint8)))
+    assert d == d_ref
+    assert np.array_equal(host(dl), lr) and same(host(da), ar)
+
+
+BGR_CASES = [("rough_128_2d", (128, 120), 2), ("rough_40_3d", (40, 36, 30), 3), ("plates_64", (64, 64, 64), 0),
+             ("chain_3d", (40, 24, 10), 0)]
+
+
+@gpu
+@pytest.mark.parametrize("sigma", [0.70, 1.2])
+@pytest.mark.parametrize("case", BGR_CASES, ids=[c[0] for c in BGR_CASES])
+def test_balanced_remap_against_oracle(torch_cuda, case, sigma):
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    name, shape, variants = case
+    rng = np.random.default_rng(5)
+    if variants:
+        lab = rough_labels(shape, rng, variants)
+    elif name.startswith("chain"):
+        lab = chain_labels(shape)
+    else:
+        lab = plates(shape, 10, rng)
+    alpha = rng.uniform(0.1, 1.0, shape)
+    lr, ar = lab.copy(), alpha.copy()
+    n_ref = O.balanced_gaussian_remap(lr, ar, sigma)
+    h = AlCuTransport(shape, params())
+    dl, da = dev(torch, lab), dev(torch, alpha)
+    n = h.balanced_remap(dl, da, sigma)
+    assert n == n_ref
+    assert np.array_equal(host(dl), lr) and same(host(da), ar)
+    if variants:
+        assert n > 0
