@@ -886,14 +886,15 @@ __device__ void patch_masks(const Ext& d, const int8_t* lab, long long i, int a,
                 if (v == b) mb |= 1u << bit;
             }
 }
-// counts: label value + 128 -> cells holding it
+// counts: label value + 128 -> cells holding it; null when no label can
+// fall to one cell (extinction never applies)
 __device__ bool cert_local(const Ext& d, const int8_t* lab, long long i, int old_label, int new_label,
                            const int* counts) {
     if (old_label == new_label) return false;
     unsigned mo, mn;
     patch_masks(d, lab, i, old_label, new_label, mo, mn);
     const int oc = topo_number(mo, d.ndim);
-    const bool extinction = counts[old_label + 128] <= 1;
+    const bool extinction = counts ? counts[old_label + 128] <= 1 : false;
     if (oc == 0 && !extinction) return false;
     if (oc > 1) return false;
     const int nc = topo_number(mn, d.ndim);
@@ -937,6 +938,65 @@ __global__ void k_tx_commit(Ext d, const int* __restrict__ list, const int* __re
         }
     }
     *deferred = nd;
+}
+
+// The same commits in rounds.  A transaction reads only its periodic 3^d
+// patch, so it may run once every earlier (lower cell index) crossing cell in
+// that patch has run in an earlier round; transactions ready in one round
+// are never neighbours of one another, and their later neighbours have not
+// run yet, so each sees exactly the state of the serial order.  Used when no
+// label can fall to one cell during the sweep (then the extinction test is
+// false throughout); done[i] = round of the commit, INT_MAX while pending.
+constexpr int TX_PENDING = 0x7fffffff;
+
+__global__ void k_tx_init(const int* __restrict__ list, const int* __restrict__ n_list, int* __restrict__ done,
+                          int* __restrict__ crossing_hist, const int8_t* __restrict__ lab) {
+    const int M = *n_list;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
+        done[list[q]] = TX_PENDING;
+        atomicAdd(&crossing_hist[(int)lab[list[q]] + 128], 1);
+    }
+}
+__global__ void k_tx_round(Ext d, int round, const int* __restrict__ list, const int* __restrict__ n_list,
+                           const uint8_t* __restrict__ crossing, int* done, int8_t* lab, double* alpha,
+                           const int8_t* __restrict__ comp, unsigned long long* __restrict__ counters) {
+    const int M = *n_list;
+    unsigned long long ran = 0, nd = 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
+        const int j = list[q];
+        if (__ldcg(&done[j]) != TX_PENDING) continue;
+        int x0, x1, x2;
+        cell_coords(d, j, x0, x1, x2);
+        const int y1[3] = {x1 == 0 ? d.e[1] - 1 : x1 - 1, x1, x1 + 1 == d.e[1] ? 0 : x1 + 1};
+        const int y2[3] = {x2 == 0 ? d.e[2] - 1 : x2 - 1, x2, x2 + 1 == d.e[2] ? 0 : x2 + 1};
+        const int y0[3] = {x0 == 0 ? d.e[0] - 1 : x0 - 1, x0, x0 + 1 == d.e[0] ? 0 : x0 + 1};
+        bool ready = true;
+        const int n0 = d.ndim == 3 ? 3 : 1;
+        for (int p0 = 0; p0 < n0 && ready; ++p0)
+            for (int p1 = 0; p1 < 3 && ready; ++p1)
+                for (int p2 = 0; p2 < 3; ++p2) {
+                    const int z0 = d.ndim == 3 ? y0[p0] : 0;
+                    const int nb = (int)(((long long)z0 * d.e[1] + y1[p1]) * d.e[2] + y2[p2]);
+                    if (nb < j && crossing[nb] && __ldcg(&done[nb]) >= round) {
+                        ready = false;
+                        break;
+                    }
+                }
+        if (!ready) continue;
+        const int old_label = lab[j], new_label = comp[j];
+        if (cert_local(d, lab, j, old_label, new_label, nullptr)) {
+            lab[j] = (int8_t)new_label;
+            alpha[j] = 1.0;
+        } else {
+            ++nd;
+            const double a = alpha[j];
+            alpha[j] = 1.0e-6 > a ? 1.0e-6 : a;  // Python max(a, 1e-6)
+        }
+        done[j] = round;
+        ++ran;
+    }
+    if (ran) atomicAdd(&counters[0], ran);
+    if (nd) atomicAdd(&counters[1], nd);
 }
 
 // the labels present, ascending (np.unique), at most 8
@@ -1105,6 +1165,7 @@ struct gpk_alcu {
     uint8_t *u8a = nullptr, *u8b = nullptr;  // active cells and their 3^d box maximum
     int* band = nullptr;                     // cells of some component's dilation, in order
     int* cnt256 = nullptr;                   // cells per label value (value + 128)
+    int* aux = nullptr;                      // 512 ints: small histograms
     double* scores = nullptr;                // the balanced remap's per-label Gaussians
     int n_scores = 0;
     void* cub_tmp = nullptr;
@@ -1158,7 +1219,7 @@ void free_all(gpk_alcu* h) {
     cudaFree(h->seg); cudaFree(h->start); cudaFree(h->flag); cudaFree(h->pos); cudaFree(h->cand);
     cudaFree(h->cells1); cudaFree(h->cells2); cudaFree(h->conflicts);
     cudaFree(h->key1); cudaFree(h->key2); cudaFree(h->sk1); cudaFree(h->sk2); cudaFree(h->cub_tmp);
-    cudaFree(h->u8a); cudaFree(h->u8b); cudaFree(h->band); cudaFree(h->cnt256); cudaFree(h->scores);
+    cudaFree(h->u8a); cudaFree(h->u8b); cudaFree(h->band); cudaFree(h->cnt256); cudaFree(h->aux); cudaFree(h->scores);
     if (h->own) cudaStreamDestroy(h->own);
 }
 
@@ -1446,7 +1507,8 @@ extern "C" int gpk_alcu_create(int ndim, const int* shape, const gpk_alcu_params
         if (!alloc((void**)q, sizeof(int) * N)) return fail(GPK_ERR_OUT_OF_MEMORY);
     if (!alloc((void**)&h->orig, N) || !alloc((void**)&h->key1, 8 * N) || !alloc((void**)&h->key2, 8 * N) ||
         !alloc((void**)&h->sk1, 4 * N) || !alloc((void**)&h->sk2, 4 * N) || !alloc((void**)&h->u8a, N) ||
-        !alloc((void**)&h->u8b, N) || !alloc((void**)&h->band, 4 * N) || !alloc((void**)&h->cnt256, 4 * 256))
+        !alloc((void**)&h->u8b, N) || !alloc((void**)&h->band, 4 * N) || !alloc((void**)&h->cnt256, 4 * 256) ||
+        !alloc((void**)&h->aux, 4 * 512))
         return fail(GPK_ERR_OUT_OF_MEMORY);
     while ((1ll << h->seg_bits) < N) ++h->seg_bits;
     size_t b1 = 0, b2 = 0, b3 = 0;
@@ -1756,19 +1818,56 @@ extern "C" int gpk_alcu_commit_transactions(gpk_alcu* h, int8_t* labels, double*
     const long long N = d.N;
     cudaStream_t st = h->stream;
     const int G = h->grid;
+    int* n_list = h->i32 + 6;
+    int* xhist = h->aux;  // 256 ints: crossing cells per label
     ALCU_TRY(cudaMemsetAsync(h->cnt256, 0, sizeof(int) * 256, st));
-    ALCU_TRY(cudaMemsetAsync(h->u64 + 3, 0, sizeof(unsigned long long), st));
+    ALCU_TRY(cudaMemsetAsync(xhist, 0, sizeof(int) * 256, st));
+    ALCU_TRY(cudaMemsetAsync(h->u64, 0, sizeof(unsigned long long) * 4, st));
     k_label_hist<<<G, 256, 0, st>>>(N, labels, h->cnt256);
     k_u8_flags<<<G, 256, 0, st>>>(N, crossing, h->flag);
     ALCU_TRY(cudaGetLastError());
     size_t b = h->cub_bytes;
     ALCU_TRY(cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, h->flag, h->pos, (int)N, st));
-    k_compact<<<G, 256, 0, st>>>(N, h->flag, h->pos, nullptr, h->cand, h->i32 + 6);
-    k_tx_commit<<<1, 32, 0, st>>>(d, h->cand, h->i32 + 6, labels, alpha, competitor, h->cnt256, h->u64 + 3);
+    k_compact<<<G, 256, 0, st>>>(N, h->flag, h->pos, nullptr, h->cand, n_list);
+    k_tx_init<<<G, 256, 0, st>>>(h->cand, n_list, h->wave, xhist, labels);
     ALCU_TRY(cudaGetLastError());
-    unsigned long long nd = 0;
-    ALCU_TRY(cudaMemcpyAsync(&nd, h->u64 + 3, sizeof(nd), cudaMemcpyDeviceToHost, st));
+    int M = 0;
+    int hc[256], hx[256];
+    ALCU_TRY(cudaMemcpyAsync(&M, n_list, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaMemcpyAsync(hc, h->cnt256, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaMemcpyAsync(hx, xhist, sizeof(hx), cudaMemcpyDeviceToHost, st));
     ALCU_TRY(cudaStreamSynchronize(st));
+    if (deferred) *deferred = 0;
+    if (M == 0) return GPK_OK;
+    // the extinction test can only fire for a label that the sweep may
+    // reduce to one cell; then the serial order runs on one thread
+    bool extinction_possible = false;
+    for (int k = 0; k < 256; ++k)
+        if (hx[k] && hc[k] - hx[k] < 2) extinction_possible = true;
+    unsigned long long nd = 0;
+    if (extinction_possible) {
+        k_tx_commit<<<1, 32, 0, st>>>(d, h->cand, n_list, labels, alpha, competitor, h->cnt256, h->u64 + 1);
+        ALCU_TRY(cudaGetLastError());
+        ALCU_TRY(cudaMemcpyAsync(&nd, h->u64 + 1, sizeof(nd), cudaMemcpyDeviceToHost, st));
+        ALCU_TRY(cudaStreamSynchronize(st));
+    } else {
+        const int gb = (M + 255) / 256 < G ? (M + 255) / 256 : G;
+        unsigned long long hcnt[2] = {0, 0};
+        // the earliest pending transaction is always ready: at most M rounds
+        for (int round = 0; hcnt[0] < (unsigned long long)M;) {
+            if (round > M) {
+                gpk_set_error("alcu: transaction rounds did not finish");
+                return GPK_ERR_INTERNAL;
+            }
+            for (int k = 0; k < 8; ++k, ++round)
+                k_tx_round<<<gb, 256, 0, st>>>(d, round, h->cand, n_list, crossing, h->wave, labels, alpha,
+                                                competitor, h->u64);
+            ALCU_TRY(cudaGetLastError());
+            ALCU_TRY(cudaMemcpyAsync(hcnt, h->u64, sizeof(hcnt), cudaMemcpyDeviceToHost, st));
+            ALCU_TRY(cudaStreamSynchronize(st));
+        }
+        nd = hcnt[1];
+    }
     if (deferred) *deferred = (int64_t)nd;
     return GPK_OK;
 }
@@ -1840,11 +1939,11 @@ extern "C" int gpk_alcu_balanced_remap(gpk_alcu* h, int8_t* labels, double* alph
     ALCU_TRY(cudaGetLastError());
     b = h->cub_bytes;
     ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->sk1, h->sk2, h->cells1, h->cells2, M, 0, 6, st));
-    ALCU_TRY(cudaMemsetAsync(h->start, 0, sizeof(int) * 64, st));
-    k_pair_hist<<<sb, 256, 0, st>>>(h->sk2, n_rec, h->start);
+    ALCU_TRY(cudaMemsetAsync(h->aux, 0, sizeof(int) * 64, st));
+    k_pair_hist<<<sb, 256, 0, st>>>(h->sk2, n_rec, h->aux);
     ALCU_TRY(cudaGetLastError());
     int hist[64];
-    ALCU_TRY(cudaMemcpyAsync(hist, h->start, sizeof(hist), cudaMemcpyDeviceToHost, st));
+    ALCU_TRY(cudaMemcpyAsync(hist, h->aux, sizeof(hist), cudaMemcpyDeviceToHost, st));
     ALCU_TRY(cudaStreamSynchronize(st));
     PairSegs segs{};
     for (int k = 0, acc = 0; k < 64; ++k) {
