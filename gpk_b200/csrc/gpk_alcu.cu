@@ -1112,6 +1112,84 @@ __global__ void k_bgr_exchange(Ext d, Vals vals, PairSegs segs, const int* __res
             }
         }
 }
+// The same exchanges in rounds.  Exchange m (its place in the serial order)
+// writes its cells f and r and reads their periodic 3^d patches, so it may
+// run once every earlier exchange writing a cell of those patches has run in
+// an earlier round.  Used when every label holds at least 3 cells: an
+// exchange leaves the counts unchanged and moves them by one in between, so
+// the extinction test is false throughout.  xid[c] = the exchange writing
+// record cell c (TX_PENDING for proposals that take part in none).
+struct PairList {
+    int n;
+    int sf[28], sr[28], cnt[28], base[28], first[28], second[28];
+};
+
+__global__ void k_bgr_xinit(const int* __restrict__ cells, const int* __restrict__ count, int* __restrict__ xid) {
+    const int M = *count;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) xid[cells[q]] = TX_PENDING;
+}
+__global__ void k_bgr_xindex(PairList pl, PairSegs segs, const int* __restrict__ cells, int* __restrict__ xf,
+                             int* __restrict__ xr, int* __restrict__ xp, int* __restrict__ xid, int* __restrict__ done,
+                             int total) {
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < total; m += gridDim.x * blockDim.x) {
+        int t = 0;
+        while (t + 1 < pl.n && pl.base[t + 1] <= m) ++t;
+        const int k = m - pl.base[t];
+        const int f = cells[segs.start[pl.sf[t]] + k], r = cells[segs.start[pl.sr[t]] + k];
+        xf[m] = f;
+        xr[m] = r;
+        xp[m] = t;
+        xid[f] = m;
+        xid[r] = m;
+        done[m] = TX_PENDING;
+    }
+}
+// no earlier exchange still pending writes a cell of the patch around i
+__device__ bool patch_free(const Ext& d, long long i, int m, int round, const int* __restrict__ flag,
+                           const int* xid, const int* done) {
+    int x0, x1, x2;
+    cell_coords(d, i, x0, x1, x2);
+    const int y1[3] = {x1 == 0 ? d.e[1] - 1 : x1 - 1, x1, x1 + 1 == d.e[1] ? 0 : x1 + 1};
+    const int y2[3] = {x2 == 0 ? d.e[2] - 1 : x2 - 1, x2, x2 + 1 == d.e[2] ? 0 : x2 + 1};
+    const int y0[3] = {x0 == 0 ? d.e[0] - 1 : x0 - 1, x0, x0 + 1 == d.e[0] ? 0 : x0 + 1};
+    const int n0 = d.ndim == 3 ? 3 : 1;
+    for (int p0 = 0; p0 < n0; ++p0)
+        for (int p1 = 0; p1 < 3; ++p1)
+            for (int p2 = 0; p2 < 3; ++p2) {
+                const int z0 = d.ndim == 3 ? y0[p0] : 0;
+                const long long c = ((long long)z0 * d.e[1] + y1[p1]) * d.e[2] + y2[p2];
+                if (!flag[c]) continue;
+                const int w = __ldcg(&xid[c]);
+                if (w < m && __ldcg(&done[w]) >= round) return false;
+            }
+    return true;
+}
+__global__ void k_bgr_round(Ext d, PairList pl, int round, int total, const int* __restrict__ xf,
+                            const int* __restrict__ xr, const int* __restrict__ xp, const int* __restrict__ flag,
+                            const int* xid, int* done, int8_t* lab, uint8_t* __restrict__ changed,
+                            unsigned long long* __restrict__ ran_count) {
+    unsigned long long ran = 0;
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < total; m += gridDim.x * blockDim.x) {
+        if (__ldcg(&done[m]) != TX_PENDING) continue;
+        const long long f = xf[m], r = xr[m];
+        if (!patch_free(d, f, m, round, flag, xid, done) || !patch_free(d, r, m, round, flag, xid, done)) continue;
+        const int first = pl.first[xp[m]], second = pl.second[xp[m]];
+        if (lab[f] == first && lab[r] == second && cert_local(d, lab, f, first, second, nullptr)) {
+            lab[f] = (int8_t)second;
+            if (cert_local(d, lab, r, second, first, nullptr)) {
+                lab[r] = (int8_t)first;
+                changed[f] = 1;
+                changed[r] = 1;
+            } else {
+                lab[f] = (int8_t)first;
+            }
+        }
+        done[m] = round;
+        ++ran;
+    }
+    if (ran) atomicAdd(ran_count, ran);
+}
+
 __global__ void k_bgr_finish(const int* __restrict__ cells, const int* __restrict__ count,
                              const uint8_t* __restrict__ changed, double* __restrict__ alpha,
                              unsigned long long* __restrict__ n_changed) {
@@ -1952,8 +2030,56 @@ extern "C" int gpk_alcu_balanced_remap(gpk_alcu* h, int8_t* labels, double* alph
         acc += hist[k];
     }
     ALCU_TRY(cudaMemsetAsync(h->u8a, 0, N, st));
-    ALCU_TRY(cudaMemsetAsync(h->u64 + 3, 0, sizeof(unsigned long long), st));
-    k_bgr_exchange<<<1, 32, 0, st>>>(d, vals, segs, h->cells2, labels, h->cnt256, h->u8a);
+    ALCU_TRY(cudaMemsetAsync(h->u64 + 2, 0, sizeof(unsigned long long) * 2, st));
+    // the exchanges of each pair, in the serial order
+    PairList pl{};
+    int total = 0;
+    for (int ia = 0; ia < vals.n; ++ia)
+        for (int ib = ia + 1; ib < vals.n; ++ib) {
+            const int first = vals.v[ia], second = vals.v[ib];
+            if ((first == 0) != (second == 0)) continue;
+            const int sf = ia * 8 + ib, sr = ib * 8 + ia;
+            const int cnt = segs.len[sf] < segs.len[sr] ? segs.len[sf] : segs.len[sr];
+            if (cnt == 0) continue;
+            pl.sf[pl.n] = sf;
+            pl.sr[pl.n] = sr;
+            pl.cnt[pl.n] = cnt;
+            pl.base[pl.n] = total;
+            pl.first[pl.n] = first;
+            pl.second[pl.n] = second;
+            ++pl.n;
+            total += cnt;
+        }
+    bool few = false;  // a label of at most 2 cells: the extinction test may apply
+    for (int k = 0; k < vals.n; ++k)
+        if (hc[vals.v[k] + 128] <= 2) few = true;
+    if (total > 0 && few) {
+        k_bgr_exchange<<<1, 32, 0, st>>>(d, vals, segs, h->cells2, labels, h->cnt256, h->u8a);
+        ALCU_TRY(cudaGetLastError());
+    } else if (total > 0) {
+        // exchange arrays: f, r, pair, done in key2 (as ints), xid in wave
+        int* xf = reinterpret_cast<int*>(h->key2);
+        int* xr = xf + total;
+        int* xp = xr + total;
+        int* done = h->pos;
+        const int gx = (total + 255) / 256 < G ? (total + 255) / 256 : G;
+        k_bgr_xinit<<<sb, 256, 0, st>>>(h->cells2, n_rec, h->wave);
+        k_bgr_xindex<<<gx, 256, 0, st>>>(pl, segs, h->cells2, xf, xr, xp, h->wave, done, total);
+        ALCU_TRY(cudaGetLastError());
+        unsigned long long ran = 0;
+        for (int round = 0; ran < (unsigned long long)total;) {
+            if (round > total) {
+                gpk_set_error("alcu: exchange rounds did not finish");
+                return GPK_ERR_INTERNAL;
+            }
+            for (int k = 0; k < 8; ++k, ++round)
+                k_bgr_round<<<gx, 256, 0, st>>>(d, pl, round, total, xf, xr, xp, h->flag, h->wave, done, labels,
+                                                 h->u8a, h->u64 + 2);
+            ALCU_TRY(cudaGetLastError());
+            ALCU_TRY(cudaMemcpyAsync(&ran, h->u64 + 2, sizeof(ran), cudaMemcpyDeviceToHost, st));
+            ALCU_TRY(cudaStreamSynchronize(st));
+        }
+    }
     k_bgr_finish<<<sb, 256, 0, st>>>(h->cells2, n_rec, h->u8a, alpha, h->u64 + 3);
     ALCU_TRY(cudaGetLastError());
     unsigned long long nc = 0;

@@ -506,7 +506,7 @@ def test_topology_transactions_against_oracle(torch_cuda, case):
 
 
 BGR_CASES = [("rough_128_2d", (128, 120), 2), ("rough_40_3d", (40, 36, 30), 3), ("plates_64", (64, 64, 64), 0),
-             ("chain_3d", (40, 24, 10), 0)]
+             ("chain_3d", (40, 24, 10), 0), ("rough_96_3d", (96, 96, 96), 3), ("few_2d", (64, 60), 2)]
 
 
 @gpu
@@ -517,9 +517,15 @@ def test_balanced_remap_against_oracle(torch_cuda, case, sigma):
 
     torch = torch_cuda
     name, shape, variants = case
+    if name == "rough_96_3d" and sigma != 0.70:
+        pytest.skip("one width at 96^3 keeps the oracle's loop short")
     rng = np.random.default_rng(5)
     if variants:
         lab = rough_labels(shape, rng, variants)
+        if name.startswith("few"):
+            # a label of two cells on the boundary: exchanges run serially
+            lab[shape[0] // 2, 10] = 3
+            lab[shape[0] // 2, 11] = 3
     elif name.startswith("chain"):
         lab = chain_labels(shape)
     else:
