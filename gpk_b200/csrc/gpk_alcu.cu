@@ -619,10 +619,48 @@ __global__ void __launch_bounds__(128) k_box_pass(Ext d, const uint8_t* __restri
     }
 }
 
+// The whole 3^d box maximum (no wrap) in one pass: a (32 x 8) block marches
+// along axis 0 through a chunk of BOX_ZC planes (and the plane on either
+// side), ORs each plane's 3 x 3 box from a shared tile with a 1-cell halo, and
+// keeps the last three plane results of its cell in registers.
+constexpr int BOX_ZC = 8;
+__global__ void __launch_bounds__(256) k_box_max3(Ext d, const uint8_t* __restrict__ in, uint8_t* __restrict__ out) {
+    __shared__ uint8_t t[10][34];
+    const int n0 = d.e[0], n1 = d.e[1], n2 = d.e[2];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
+    const int xs = blockIdx.x * 32, ys = blockIdx.y * 8;
+    const int x = xs + tx, y = ys + ty;
+    const long long plane = (long long)n1 * n2;
+    const int z0 = blockIdx.z * BOX_ZC;
+    const int z1 = z0 + BOX_ZC < n0 ? z0 + BOX_ZC : n0;
+    uint8_t prev = 0, cur = 0;
+    for (int z = z0 - 1; z <= z1; ++z) {
+        uint8_t next = 0;
+        if (z >= 0 && z < n0) {
+            for (int k = tid; k < 340; k += 256) {
+                const int ly = k / 34 - 1, lx = k % 34 - 1;
+                const int gy = ys + ly, gx = xs + lx;
+                t[ly + 1][lx + 1] = (gy >= 0 && gy < n1 && gx >= 0 && gx < n2) ? in[z * plane + (long long)gy * n2 + gx]
+                                                                            : (uint8_t)0;
+            }
+            __syncthreads();
+            next = t[ty][tx] | t[ty][tx + 1] | t[ty][tx + 2] | t[ty + 1][tx] | t[ty + 1][tx + 1] | t[ty + 1][tx + 2] |
+                   t[ty + 2][tx] | t[ty + 2][tx + 1] | t[ty + 2][tx + 2];
+            __syncthreads();
+        }
+        // plane z - 1 is complete: its neighbours z - 2 (prev) and z (next)
+        if (z - 1 >= z0 && x < n2 && y < n1) out[(z - 1) * plane + (long long)y * n2 + x] = prev | cur | next;
+        prev = cur;
+        cur = next;
+    }
+}
+
 // the components (of more than one cell) with a cell in the 3^d box of x,
 // without wrap; returns how many (at most 27)
+// (act[c]: cell c belongs to such a component)
 __device__ __forceinline__ int box_components(const Ext& d, int x0, int x1, int x2, long long i,
-                                              const int* __restrict__ root, const int* __restrict__ size, int S[27]) {
+                                              const int* __restrict__ root, const uint8_t* __restrict__ act,
+                                              int S[27]) {
     int n = 0;
     for (int o0 = -1; o0 <= 1; ++o0) {
         if (x0 + o0 < 0 || x0 + o0 >= d.e[0]) continue;
@@ -630,8 +668,9 @@ __device__ __forceinline__ int box_components(const Ext& d, int x0, int x1, int 
             if (x1 + o1 < 0 || x1 + o1 >= d.e[1]) continue;
             for (int o2 = -1; o2 <= 1; ++o2) {
                 if (x2 + o2 < 0 || x2 + o2 >= d.e[2]) continue;
-                const int r = root[i + o0 * d.st[0] + o1 * d.st[1] + o2 * d.st[2]];
-                if (r < 0 || size[r] <= 1) continue;
+                const long long c = i + o0 * d.st[0] + o1 * d.st[1] + o2 * d.st[2];
+                if (!act[c]) continue;
+                const int r = root[c];
                 bool seen = false;
                 for (int q = 0; q < n; ++q) seen |= S[q] == r;
                 if (!seen) S[n++] = r;
@@ -655,14 +694,14 @@ __device__ __forceinline__ long long order_key(const int8_t* __restrict__ orig, 
 
 // band = cells of some component's dilation; conflicts = cells of two or more
 __global__ void __launch_bounds__(128) k_cgr_band(Ext d, const uint8_t* __restrict__ near, const int* __restrict__ root,
-                                                  const int* __restrict__ size, int* __restrict__ flag,
+                                                  const uint8_t* __restrict__ act, int* __restrict__ flag,
                                                   int* __restrict__ list, int* __restrict__ count) {
     CELLS3(d) {
         const long long i = CELL_INDEX(d);
         int f = 0;
         if (near[i]) {
             int S[27];
-            const int n = box_components(d, x0, x1, x2, i, root, size, S);
+            const int n = box_components(d, x0, x1, x2, i, root, act, S);
             f = n >= 1;
             if (n >= 2) list[atomicAdd(count, 1)] = (int)i;
         }
@@ -679,14 +718,14 @@ __global__ void k_compact(long long M, const int* __restrict__ flag, const int* 
 }
 
 __global__ void k_cgr_relax(Ext d, const int* __restrict__ list, int M, const int8_t* __restrict__ orig,
-                            const int* __restrict__ root, const int* __restrict__ size, int* wave,
+                            const int* __restrict__ root, const uint8_t* __restrict__ act, int* wave,
                             int* __restrict__ changed) {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
         const long long i = list[q];
         int x0, x1, x2;
         cell_coords(d, i, x0, x1, x2);
         int S[27];
-        const int n = box_components(d, x0, x1, x2, i, root, size, S);
+        const int n = box_components(d, x0, x1, x2, i, root, act, S);
         for (int b = 0; b < n; ++b) {
             const long long kb = order_key(orig, S[b]);
             int m = __ldcg(&wave[S[b]]);
@@ -718,15 +757,16 @@ __global__ void k_cgr_max_wave(const int* __restrict__ band, const int* __restri
 // candidates of wave w among the band: cells of the dilation of a wave-w
 // component that are zero or its own
 __global__ void k_cgr_flags(Ext d, int w, const int* __restrict__ band, const int* __restrict__ n_band,
-                            const int8_t* __restrict__ lab, const int* __restrict__ root, const int* __restrict__ size,
-                            const int* __restrict__ wave, int* __restrict__ flag, int* __restrict__ seg) {
+                            const int8_t* __restrict__ lab, const int* __restrict__ root,
+                            const uint8_t* __restrict__ act, const int* __restrict__ wave, int* __restrict__ flag,
+                            int* __restrict__ seg) {
     const int M = *n_band;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
         const long long i = band[q];
         int x0, x1, x2;
         cell_coords(d, i, x0, x1, x2);
         int S[27];
-        const int n = box_components(d, x0, x1, x2, i, root, size, S);
+        const int n = box_components(d, x0, x1, x2, i, root, act, S);
         int B = -1;
         for (int k = 0; k < n; ++k)
             if (wave[S[k]] == w) B = S[k];
@@ -1789,20 +1829,29 @@ extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alph
     k_cc_union<<<g3, B3, 0, st>>>(d, h->orig, h->parent, h->err);
     k_cc_finish<<<G, 256, 0, st>>>(N, h->orig, h->parent, h->root, h->size, h->err);
     k_cgr_active<<<G, 256, 0, st>>>(N, h->root, h->size, h->u8a, h->i32 + 4);
-    // 3^d box maximum of the active cells: one pass per axis of the field
+    // 3^d box maximum of the active cells (u8a) into u8b: one marching pass,
+    // or one pass per axis where the tile grid would be too tall
     {
-        uint8_t* src = h->u8a;
-        uint8_t* dst = h->u8b;
-        for (int ax = d.a0; ax < 3; ++ax) {
-            if (ax == 0)
-                k_box_pass<0><<<g3, B3, 0, st>>>(d, src, dst);
-            else if (ax == 1)
-                k_box_pass<1><<<g3, B3, 0, st>>>(d, src, dst);
-            else
-                k_box_pass<2><<<g3, B3, 0, st>>>(d, src, dst);
-            std::swap(src, dst);
+        const long long gyb = (d.e[1] + 7) / 8, gzb = (d.e[0] + BOX_ZC - 1) / BOX_ZC;
+        if (gyb <= 65535 && gzb <= 65535) {
+            k_box_max3<<<dim3((d.e[2] + 31) / 32, (unsigned)gyb, (unsigned)gzb), dim3(32, 8), 0, st>>>(d, h->u8a,
+                                                                                                     h->u8b);
+        } else {
+            // passes ping-pong through u8b and band (as bytes); the result in u8b
+            uint8_t* tmp = reinterpret_cast<uint8_t*>(h->band);
+            const uint8_t* src = h->u8a;
+            for (int ax = d.a0; ax < 3; ++ax) {
+                uint8_t* dst = ((2 - ax) % 2 == 0) ? h->u8b : tmp;
+                if (ax == 0)
+                    k_box_pass<0><<<g3, B3, 0, st>>>(d, src, dst);
+                else if (ax == 1)
+                    k_box_pass<1><<<g3, B3, 0, st>>>(d, src, dst);
+                else
+                    k_box_pass<2><<<g3, B3, 0, st>>>(d, src, dst);
+                src = dst;
+            }
         }
-        k_cgr_band<<<g3, B3, 0, st>>>(d, src, h->root, h->size, h->flag, h->conflicts, h->i32 + 1);
+        k_cgr_band<<<g3, B3, 0, st>>>(d, h->u8b, h->root, h->u8a, h->flag, h->conflicts, h->i32 + 1);
     }
     ALCU_TRY(cudaGetLastError());
     size_t b = h->cub_bytes;
@@ -1836,7 +1885,7 @@ extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alph
             int flag = 0;
             ALCU_TRY(cudaMemsetAsync(h->i32 + 2, 0, sizeof(int), st));
             const int blocks = (n_conf + 255) / 256 < G ? (n_conf + 255) / 256 : G;
-            k_cgr_relax<<<blocks, 256, 0, st>>>(d, h->conflicts, n_conf, h->orig, h->root, h->size, h->wave,
+            k_cgr_relax<<<blocks, 256, 0, st>>>(d, h->conflicts, n_conf, h->orig, h->root, h->u8a, h->wave,
                                                  h->i32 + 2);
             ALCU_TRY(cudaGetLastError());
             ALCU_TRY(cudaMemcpyAsync(&flag, h->i32 + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1851,7 +1900,7 @@ extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alph
     ALCU_TRY(cudaStreamSynchronize(st));
     h->last_waves = max_wave + 1;
     for (int w = 0; w <= max_wave; ++w) {
-        k_cgr_flags<<<gb, 256, 0, st>>>(d, w, h->band, n_band, labels, h->root, h->size, h->wave, h->flag, h->seg);
+        k_cgr_flags<<<gb, 256, 0, st>>>(d, w, h->band, n_band, labels, h->root, h->u8a, h->wave, h->flag, h->seg);
         ALCU_TRY(cudaGetLastError());
         b = h->cub_bytes;
         ALCU_TRY(cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, h->flag, h->pos, Mb, st));
