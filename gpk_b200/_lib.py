@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
         "gpk_alcu_competitor": ([vp, vp, vp, vp], i32),
         "gpk_alcu_precip_fraction": ([vp, vp, vp, vp, vp], i32),
         "gpk_alcu_matrix_composition": ([vp, vp, vp, vp], i32),
+        "gpk_alcu_variant_fractions": ([vp, vp, vp, vp, vp], i32),
         "gpk_alcu_diffuse": ([vp, vp, vp, dbl, vp, C.POINTER(i32)], i32),
         "gpk_alcu_partition_transfer": ([vp, vp, vp, vp, vp, C.POINTER(dbl), i32], i32),
         "gpk_alcu_interface_composition": ([vp, vp, vp, vp, C.POINTER(dbl), i32], i32),

@@ -6,6 +6,7 @@ in-place behaviour of the reference's Al-Cu material module
 
   neighbor_competitor(labels)                                     260-276
   precip_fraction(labels, alpha, competitor)                      675-676
+  variant_fraction_fields(labels, alpha, competitor)              278-283
   diffuse_conservative_subcycled(ctot, fprec, p, dt)              691-699
   conservative_partition_transfer(ctot, old, new, c_m, p)         702-737
   interface_matrix_composition(cm, fprec, p)                      740-755
@@ -30,7 +31,8 @@ import numpy as np
 
 from ._lib import CAlCuParams, check, lib
 
-__all__ = ["AlCuTransport", "gauss_taps", "neighbor_competitor", "precip_fraction", "matrix_composition",
+__all__ = ["AlCuTransport", "gauss_taps", "neighbor_competitor", "precip_fraction", "variant_fraction_fields",
+           "matrix_composition",
            "diffuse_conservative_subcycled", "conservative_partition_transfer", "interface_matrix_composition",
            "conservative_gaussian_remap", "balanced_gaussian_remap", "commit_topology_transactions", "field_sum"]
 
@@ -144,6 +146,16 @@ class AlCuTransport:
         check(lib().gpk_alcu_precip_fraction(self._h, self._i8(labels), self._f64(alpha), self._i8(competitor),
                                              fp.data_ptr()))
         return fp
+
+    def variant_fractions(self, labels, alpha, competitor):
+        """(3, *shape) float64: the spectral solve's input."""
+        import torch
+
+        self._bind(labels, alpha, competitor)
+        out = torch.empty((3,) + self.shape, dtype=torch.float64, device=alpha.device)
+        check(lib().gpk_alcu_variant_fractions(self._h, self._i8(labels), self._f64(alpha), self._i8(competitor),
+                                               out.data_ptr()))
+        return out
 
     def matrix_composition(self, ctot, fprec):
         import torch
@@ -270,6 +282,15 @@ def precip_fraction(labels, alpha, competitor):
         return h.precip_fraction(_dev(labels, np.int8), _dev(alpha, np.float64),
                                  _dev(competitor, np.int8)).cpu().numpy()
     return _handle(labels.shape).precip_fraction(labels, alpha, competitor)
+
+
+def variant_fraction_fields(labels, alpha, competitor):
+    """One precipitate-fraction field per variant, stacked (3, *shape)."""
+    if _is_np(labels, alpha, competitor):
+        h = _handle(labels.shape)
+        return h.variant_fractions(_dev(labels, np.int8), _dev(alpha, np.float64),
+                                   _dev(competitor, np.int8)).cpu().numpy()
+    return _handle(labels.shape).variant_fractions(labels, alpha, competitor)
 
 
 def matrix_composition(ctot, fprec, p):

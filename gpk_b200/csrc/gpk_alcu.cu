@@ -145,6 +145,20 @@ __global__ void k_precip_fraction(long long N, const int8_t* __restrict__ lab, c
     GRID_STRIDE(i, N) fp[i] = lab[i] > 0 ? alpha[i] : (comp[i] > 0 ? 1.0 - alpha[i] : 0.0);
 }
 
+// variant_fraction_fields (lines 278-283): fraction * (variant == v), the
+// product taken as numpy takes it (times 1.0 or 0.0, so a negative fraction
+// gives -0.0 off its variant)
+__global__ void k_variant_fractions(long long N, const int8_t* __restrict__ lab, const double* __restrict__ alpha,
+                                    const int8_t* __restrict__ comp, double* __restrict__ out) {
+    GRID_STRIDE(i, N) {
+        const int l = lab[i], c = comp[i];
+        const double f = l > 0 ? alpha[i] : (c > 0 ? 1.0 - alpha[i] : 0.0);
+        const int v = l > 0 ? l : c;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) out[k * N + i] = f * (v == k + 1 ? 1.0 : 0.0);
+    }
+}
+
 // matrix fraction max(1 - f, 1e-8) and the clipped lever-rule composition
 __device__ __forceinline__ void lever(double c, double f, const Phys& p, double& m, double& cm) {
     m = np_max(1.0 - f, 1e-8);
@@ -1673,6 +1687,17 @@ extern "C" int gpk_alcu_precip_fraction(gpk_alcu* h, const int8_t* labels, const
         return GPK_ERR_INVALID_ARGUMENT;
     }
     k_precip_fraction<<<h->grid, 256, 0, h->stream>>>(h->d.N, labels, alpha, competitor, fprec);
+    ALCU_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
+extern "C" int gpk_alcu_variant_fractions(gpk_alcu* h, const int8_t* labels, const double* alpha,
+                                          const int8_t* competitor, double* fractions) {
+    if (!h || !labels || !alpha || !competitor || !fractions) {
+        gpk_set_error("alcu: null argument");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    k_variant_fractions<<<h->grid, 256, 0, h->stream>>>(h->d.N, labels, alpha, competitor, fractions);
     ALCU_TRY(cudaGetLastError());
     return GPK_OK;
 }

@@ -8,6 +8,7 @@
  *
  *   gpk_alcu_competitor             neighbor_competitor             (260-276)
  *   gpk_alcu_precip_fraction        precip_fraction                 (675-676)
+ *   gpk_alcu_variant_fractions      variant_fraction_fields         (278-283)
  *   gpk_alcu_matrix_composition     c_m of the lever rule           (917-919)
  *   gpk_alcu_diffuse                diffuse_conservative_subcycled  (679-699)
  *   gpk_alcu_partition_transfer     conservative_partition_transfer (702-737)
@@ -78,6 +79,11 @@ int gpk_alcu_competitor(gpk_alcu* h, const int8_t* labels, uint8_t* mask, int8_t
 /* fprec = labels > 0 ? alpha : (competitor > 0 ? 1 - alpha : 0)           */
 int gpk_alcu_precip_fraction(gpk_alcu* h, const int8_t* labels, const double* alpha, const int8_t* competitor,
                              double* fprec);
+/* fractions (3 N doubles, variant-major, the input of gpk_spectral_solve):
+ * fractions[v - 1] = fprec * (variant == v), variant = labels > 0 ? labels
+ * : competitor, v = 1, 2, 3.                                              */
+int gpk_alcu_variant_fractions(gpk_alcu* h, const int8_t* labels, const double* alpha, const int8_t* competitor,
+                               double* fractions);
 /* cm = clip((ctot - fprec c_theta) / max(1 - fprec, 1e-8), 0, c_theta),
  * c_matrix_eq where the matrix fraction is below 1e-7.                    */
 int gpk_alcu_matrix_composition(gpk_alcu* h, const double* ctot, const double* fprec, double* cm);

@@ -10,6 +10,7 @@ per step:
 
   neighbor_competitor              lines 260-276
   precip_fraction                  lines 675-676
+  variant_fraction_fields          lines 278-283
   matrix composition c_m           lines 680-682 (also 917-919)
   diffuse_conservative             lines 679-688
   diffuse_conservative_subcycled   lines 691-699
@@ -185,6 +186,13 @@ def neighbor_competitor(labels: np.ndarray):
 def precip_fraction(labels, alpha, competitor):
     """Local theta-prime fraction (lines 675-676)."""
     return np.where(labels > 0, alpha, np.where(competitor > 0, 1.0 - alpha, 0.0))
+
+
+def variant_fraction_fields(labels, alpha, competitor):
+    """One precipitate-fraction field per habit variant (lines 278-283)."""
+    fraction = precip_fraction(labels, alpha, competitor)
+    variant = np.where(labels > 0, labels, competitor)
+    return np.asarray([fraction * (variant == v) for v in (1, 2, 3)])
 
 
 def matrix_composition(ctot, fprec, p: AlCuParams):

@@ -3,7 +3,8 @@
 Imports the per-step transport and remap functions of the reference's Al-Cu
 material module, scripts/run_alcu_gpk_microstructure.py:
 
-  neighbor_competitor (260-276), precip_fraction (675-676),
+  neighbor_competitor (260-276), variant_fraction_fields (278-283),
+  precip_fraction (675-676),
   diffuse_conservative_subcycled (679-699),
   conservative_partition_transfer (702-737),
   interface_matrix_composition (740-755),
@@ -113,6 +114,10 @@ def main(root: str) -> None:
         labels, alpha, ctot = make_state(shape, rng, ref, p)
         mask, comp = ref.neighbor_competitor(labels)
         fp = ref.precip_fraction(labels, alpha, comp)
+        al_neg = alpha.copy()
+        al_neg[mask & (rng.random(shape) < 0.2)] *= -1.0  # crossing cells carry alpha < 0
+        out[f"{name}_vf_alpha"] = al_neg
+        out[f"{name}_vf"] = ref.variant_fraction_fields(labels, al_neg, comp)
         matrix = np.maximum(1.0 - fp, 1e-8)
         cm = np.where(matrix > 1e-7, (ctot - fp * p.c_theta) / matrix, p.c_matrix_eq)
         cm = np.clip(cm, 0.0, p.c_theta)

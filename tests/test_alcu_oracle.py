@@ -144,3 +144,9 @@ def test_oracle_certificate_known_answers(z):
         counts = {int(v): int(np.count_nonzero(lab == v)) for v in np.unique(lab)}
         got = O.simple_relabel_local(lab.copy(), index, int(lab[index]), int(z[f"topo_{n}_new"]), counts)
         assert got == bool(z[f"topo_{n}_local"]), n
+
+
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_oracle_variant_fractions(z, name):
+    got = O.variant_fraction_fields(z[f"{name}_labels"], z[f"{name}_vf_alpha"], z[f"{name}_competitor"])
+    assert same(got, z[f"{name}_vf"])

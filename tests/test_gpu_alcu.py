@@ -540,3 +540,19 @@ def test_balanced_remap_against_oracle(torch_cuda, case, sigma):
     assert np.array_equal(host(dl), lr) and same(host(da), ar)
     if variants:
         assert n > 0
+
+
+@gpu
+@pytest.mark.parametrize("name", ["2d", "3d"])
+def test_golden_variant_fractions(torch_cuda, z, name):
+    """The spectral solve's input, negative fractions (alpha < 0) included:
+    their products with 0.0 keep numpy's -0.0."""
+    from gpk_b200 import alcu
+
+    torch = torch_cuda
+    h = alcu.AlCuTransport(z[f"{name}_labels"].shape, params())
+    got = h.variant_fractions(dev(torch, z[f"{name}_labels"]), dev(torch, z[f"{name}_vf_alpha"]),
+                              dev(torch, z[f"{name}_competitor"]))
+    assert same(host(got), z[f"{name}_vf"])
+    assert same(alcu.variant_fraction_fields(z[f"{name}_labels"], z[f"{name}_vf_alpha"], z[f"{name}_competitor"]),
+                z[f"{name}_vf"])
