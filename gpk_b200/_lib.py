@@ -124,7 +124,7 @@ def lib() -> C.CDLL:
         "gpk_alcu_commit_transactions": ([vp, vp, vp, vp, vp, C.POINTER(i64)], i32),
         "gpk_alcu_balanced_remap": ([vp, vp, vp, C.POINTER(dbl), i32, C.POINTER(i64)], i32),
         "gpk_alcu_gaussian_filter": ([vp, vp, vp, C.POINTER(dbl), i32], i32),
-        "gpk_alcu_info": ([vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)], i32),
+        "gpk_alcu_info": ([vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)], i32),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)

@@ -95,9 +95,10 @@ class AlCuTransport:
             pass
 
     def info(self) -> dict:
-        v = [C.c_int64() for _ in range(4)]
+        v = [C.c_int64() for _ in range(5)]
         check(lib().gpk_alcu_info(self._h, *[C.byref(x) for x in v]))
-        return dict(cells=v[0].value, device_bytes=v[1].value, components=v[2].value, waves=v[3].value)
+        return dict(cells=v[0].value, device_bytes=v[1].value, components=v[2].value, waves=v[3].value,
+                    pairs=v[4].value)
 
     # ---- helpers
     def _bind(self, *tensors) -> None:

@@ -789,6 +789,33 @@ __global__ void k_cgr_flags(Ext d, int w, const int* __restrict__ band, const in
     }
 }
 
+// Pairs (cell, component B) of the band that can be admissible at B's wave:
+// the cell is B's own, or zero, or a cell of a component processed in an
+// earlier wave (which may vacate it).  Cells of later-wave components, and
+// of components of one cell, are never zero when B runs.
+__device__ __forceinline__ bool pair_possible(int cell, int B, const int8_t* __restrict__ orig,
+                                              const int* __restrict__ root, const uint8_t* __restrict__ act,
+                                              const int* __restrict__ wave) {
+    if (orig[cell] == 0) return true;
+    const int r = root[cell];
+    if (r == B) return true;
+    return act[cell] && wave[r] < wave[B];
+}
+__global__ void k_cgr_paircount(Ext d, const int* __restrict__ band, int Mb, const int8_t* __restrict__ orig,
+                                const int* __restrict__ root, const uint8_t* __restrict__ act,
+                                const int* __restrict__ wave, int* __restrict__ cnt) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < Mb; q += gridDim.x * blockDim.x) {
+        const int i = band[q];
+        int x0, x1, x2;
+        cell_coords(d, i, x0, x1, x2);
+        int S[27];
+        const int n = box_components(d, x0, x1, x2, i, root, act, S);
+        int c = 0;
+        for (int k = 0; k < n; ++k) c += pair_possible(i, S[k], orig, root, act, wave);
+        cnt[q] = c;
+    }
+}
+
 // the wrapped Gaussian of component B's indicator at y: the pass along axis
 // A0 (the first of the field) reads the indicator, each later axis AX reads
 // the pass before it; each is y w0 + sum over j = r..1 of (y-j + y+j) w_j,
@@ -826,6 +853,63 @@ __global__ void k_cgr_score(Ext d, Taps t, const int* __restrict__ cand, const i
         key[q] = ~okey(s);  // ascending key = descending score
     }
 }
+// the pairs of band cell q at pos[q]..: cell, component, descending-score key
+__global__ void k_cgr_pairs(Ext d, Taps t, const int* __restrict__ band, int Mb, const int* __restrict__ pos,
+                            const int8_t* __restrict__ orig, const int* __restrict__ root,
+                            const uint8_t* __restrict__ act, const int* __restrict__ wave, int* __restrict__ pcell,
+                            int* __restrict__ pseg, unsigned long long* __restrict__ pkey, int* __restrict__ iota) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < Mb; q += gridDim.x * blockDim.x) {
+        const int i = band[q];
+        int x0, x1, x2;
+        cell_coords(d, i, x0, x1, x2);
+        int S[27];
+        const int n = box_components(d, x0, x1, x2, i, root, act, S);
+        int o = pos[q];
+        for (int k = 0; k < n; ++k) {
+            const int B = S[k];
+            if (!pair_possible(i, B, orig, root, act, wave)) continue;
+            const double sc = d.a0 == 0 ? gpass<2, 0>(d, t, root, B, x0, x1, x2) : gpass<2, 1>(d, t, root, B, x0, x1, x2);
+            pcell[o] = i;
+            pseg[o] = B;
+            pkey[o] = ~okey(sc);  // ascending key = descending score
+            iota[o] = o;
+            ++o;
+        }
+    }
+}
+__global__ void k_total(int M, const int* __restrict__ cnt, const int* __restrict__ pos, int* __restrict__ out) {
+    *out = M > 0 ? pos[M - 1] + cnt[M - 1] : 0;
+}
+// per sorted position: the pair's component (for the stable second sort)
+__global__ void k_cgr_pairseg(int P, const int* __restrict__ perm, const int* __restrict__ pseg,
+                              unsigned* __restrict__ out) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < P; q += gridDim.x * blockDim.x) out[q] = (unsigned)pseg[perm[q]];
+}
+// admissible now: wave-w pairs whose cell is B's own or zero
+__global__ void k_cgr_adm(int P, int w, const int* __restrict__ perm, const unsigned* __restrict__ sk,
+                          const int* __restrict__ pcell, const int* __restrict__ root, const int* __restrict__ wave,
+                          const int8_t* __restrict__ lab, int* __restrict__ adm) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < P; q += gridDim.x * blockDim.x) {
+        const int B = (int)sk[q];
+        int a = 0;
+        if (wave[B] == w) {
+            const int c = pcell[perm[q]];
+            a = root[c] == B || lab[c] == 0;
+        }
+        adm[q] = a;
+    }
+}
+// the first size[B] admissible entries of B's run take its label
+__global__ void k_cgr_take(int P, int w, const int* __restrict__ perm, const unsigned* __restrict__ sk,
+                           const int* __restrict__ pcell, const int* __restrict__ adm, const int* __restrict__ rank,
+                           const int* __restrict__ size, const int* __restrict__ wave, const int8_t* __restrict__ orig,
+                           int8_t* __restrict__ lab) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < P; q += gridDim.x * blockDim.x) {
+        const int B = (int)sk[q];
+        if (adm[q] && wave[B] == w && rank[q] < size[B]) lab[pcell[perm[q]]] = orig[B];
+    }
+}
+
 __global__ void k_cgr_segkeys(const int* __restrict__ cells, const int* __restrict__ count, const int* __restrict__ seg,
                               unsigned* __restrict__ out) {
     const int M = *count;
@@ -1015,6 +1099,11 @@ __global__ void k_tx_round(Ext d, int round, const int* __restrict__ list, const
                            const uint8_t* __restrict__ crossing, int* done, int8_t* lab, double* alpha,
                            const int8_t* __restrict__ comp, unsigned long long* __restrict__ counters) {
     const int M = *n_list;
+    // rounds launched after the last transaction ran return at once
+    __shared__ int finished;
+    if (threadIdx.x == 0) finished = __ldcg(&counters[0]) >= (unsigned long long)M;
+    __syncthreads();
+    if (finished) return;
     unsigned long long ran = 0, nd = 0;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < M; q += gridDim.x * blockDim.x) {
         const int j = list[q];
@@ -1222,6 +1311,10 @@ __global__ void k_bgr_round(Ext d, PairList pl, int round, int total, const int*
                             const int* __restrict__ xr, const int* __restrict__ xp, const int* __restrict__ flag,
                             const int* xid, int* done, int8_t* lab, uint8_t* __restrict__ changed,
                             unsigned long long* __restrict__ ran_count) {
+    __shared__ int finished;
+    if (threadIdx.x == 0) finished = __ldcg(ran_count) >= (unsigned long long)total;
+    __syncthreads();
+    if (finished) return;
     unsigned long long ran = 0;
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < total; m += gridDim.x * blockDim.x) {
         if (__ldcg(&done[m]) != TX_PENDING) continue;
@@ -1303,7 +1396,7 @@ struct gpk_alcu {
     void* cub_tmp = nullptr;
     size_t cub_bytes = 0;
     int seg_bits = 1;
-    long long last_components = 0, last_waves = 0;
+    long long last_components = 0, last_waves = 0, last_pairs = 0;
 };
 
 namespace {
@@ -1395,12 +1488,14 @@ int pw_sum(gpk_alcu* h, F f, double* out) {
 // CUB's scratch for the remap's scan and sorts at M items (sized for N at
 // creation; grown here should a smaller problem ever ask for more)
 int cub_reserve(gpk_alcu* h, int M) {
-    size_t b1 = 0, b2 = 0, b3 = 0;
+    size_t b1 = 0, b2 = 0, b3 = 0, b4 = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, b1, h->flag, h->pos, (int)h->d.N);
     cub::DeviceRadixSort::SortPairs(nullptr, b2, h->key1, h->key2, h->cand, h->cells1, M);
     cub::DeviceRadixSort::SortPairs(nullptr, b3, h->sk1, h->sk2, h->cells1, h->cells2, M, 0, h->seg_bits);
+    cub::DeviceScan::ExclusiveSumByKey(nullptr, b4, h->sk2, h->flag, h->pos, M);
     size_t need = b1 > b2 ? b1 : b2;
     if (b3 > need) need = b3;
+    if (b4 > need) need = b4;
     if (need <= h->cub_bytes) return GPK_OK;
     ALCU_TRY(cudaStreamSynchronize(h->stream));
     cudaFree(h->cub_tmp);
@@ -1895,6 +1990,7 @@ extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alph
     const int n_conf = hv[1], n_active = hv[4], Mb = hv[5];
     h->last_components = n_active;
     h->last_waves = 0;
+    h->last_pairs = 0;
     if (n_active == 0) {
         if (changed) *changed = 0;
         return GPK_OK;
@@ -1918,38 +2014,81 @@ extern "C" int gpk_alcu_gaussian_remap(gpk_alcu* h, int8_t* labels, double* alph
             if (!flag) break;
         }
     }
-    int max_wave = 0;
+    // the wave count, and the (cell, component) pairs that can be admissible
     k_cgr_max_wave<<<gb, 256, 0, st>>>(h->band, n_band, h->root, h->size, h->wave, h->i32 + 3);
+    k_cgr_paircount<<<gb, 256, 0, st>>>(d, h->band, Mb, h->orig, h->root, h->u8a, h->wave, h->flag);
     ALCU_TRY(cudaGetLastError());
-    ALCU_TRY(cudaMemcpyAsync(&max_wave, h->i32 + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
+    b = h->cub_bytes;
+    ALCU_TRY(cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, h->flag, h->pos, Mb, st));
+    k_total<<<1, 1, 0, st>>>(Mb, h->flag, h->pos, h->i32 + 7);
+    ALCU_TRY(cudaGetLastError());
+    int mw_p[5];
+    ALCU_TRY(cudaMemcpyAsync(mw_p, h->i32 + 3, sizeof(mw_p), cudaMemcpyDeviceToHost, st));
     ALCU_TRY(cudaStreamSynchronize(st));
+    const int max_wave = mw_p[0];
+    const long long P = mw_p[4];
     h->last_waves = max_wave + 1;
-    for (int w = 0; w <= max_wave; ++w) {
-        k_cgr_flags<<<gb, 256, 0, st>>>(d, w, h->band, n_band, labels, h->root, h->u8a, h->wave, h->flag, h->seg);
+    h->last_pairs = P;
+    if (P > 0 && P <= N) {
+        // every pair scored once and put in the reference's candidate order
+        // (component, score descending, cell ascending) by two stable sorts;
+        // a wave then takes, per component, the first `size` pairs that are
+        // admissible on the labels the earlier waves left
+        const int Pi = (int)P;
+        const int sp = (Pi + 255) / 256 < G ? (Pi + 255) / 256 : G;
+        k_cgr_pairs<<<gb, 256, 0, st>>>(d, t, h->band, Mb, h->pos, h->orig, h->root, h->u8a, h->wave, h->cand,
+                                         h->seg, h->key1, h->start);
+        ALCU_TRY(cudaGetLastError());
+        if ((rc = cub_reserve(h, Pi)) != GPK_OK) return rc;
+        b = h->cub_bytes;
+        ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->key1, h->key2, h->start, h->cells1, Pi, 0, 64, st));
+        k_cgr_pairseg<<<sp, 256, 0, st>>>(Pi, h->cells1, h->seg, h->sk1);
         ALCU_TRY(cudaGetLastError());
         b = h->cub_bytes;
-        ALCU_TRY(cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, h->flag, h->pos, Mb, st));
-        k_compact<<<gb, 256, 0, st>>>(Mb, h->flag, h->pos, h->band, h->cand, n_cand);
-        ALCU_TRY(cudaGetLastError());
-        int M = 0;
-        ALCU_TRY(cudaMemcpyAsync(&M, n_cand, sizeof(int), cudaMemcpyDeviceToHost, st));
-        ALCU_TRY(cudaStreamSynchronize(st));
-        if (M == 0) continue;
-        if ((rc = cub_reserve(h, M)) != GPK_OK) return rc;
-        const int sb = (M + 255) / 256 < G ? (M + 255) / 256 : G;
-        k_cgr_score<<<sb, 256, 0, st>>>(d, t, h->cand, n_cand, h->root, h->seg, h->key1);
-        ALCU_TRY(cudaGetLastError());
-        b = h->cub_bytes;
-        ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->key1, h->key2, h->cand, h->cells1, M, 0, 64, st));
-        k_cgr_segkeys<<<sb, 256, 0, st>>>(h->cells1, n_cand, h->seg, h->sk1);
-        ALCU_TRY(cudaGetLastError());
-        b = h->cub_bytes;
-        ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->sk1, h->sk2, h->cells1, h->cells2, M, 0,
+        ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->sk1, h->sk2, h->cells1, h->cells2, Pi, 0,
                                                  h->seg_bits, st));
-        k_cgr_starts<<<sb, 256, 0, st>>>(h->sk2, n_cand, h->start);
-        k_cgr_vacate<<<gb, 256, 0, st>>>(w, h->band, n_band, h->root, h->size, h->wave, labels);
-        k_cgr_select<<<sb, 256, 0, st>>>(h->sk2, h->cells2, n_cand, h->start, h->size, h->orig, labels);
-        ALCU_TRY(cudaGetLastError());
+        for (int w = 0; w <= max_wave; ++w) {
+            k_cgr_adm<<<sp, 256, 0, st>>>(Pi, w, h->cells2, h->sk2, h->cand, h->root, h->wave, labels, h->flag);
+            ALCU_TRY(cudaGetLastError());
+            b = h->cub_bytes;
+            ALCU_TRY(cub::DeviceScan::ExclusiveSumByKey(h->cub_tmp, b, h->sk2, h->flag, h->pos, Pi,
+                                                        ::cuda::std::equal_to<>(), st));
+            k_cgr_vacate<<<gb, 256, 0, st>>>(w, h->band, n_band, h->root, h->size, h->wave, labels);
+            k_cgr_take<<<sp, 256, 0, st>>>(Pi, w, h->cells2, h->sk2, h->cand, h->flag, h->pos, h->size, h->wave,
+                                           h->orig, labels);
+            ALCU_TRY(cudaGetLastError());
+        }
+    } else {
+        // more pairs than cells (dilations stacked many deep): wave by wave
+        for (int w = 0; w <= max_wave; ++w) {
+            k_cgr_flags<<<gb, 256, 0, st>>>(d, w, h->band, n_band, labels, h->root, h->u8a, h->wave, h->flag,
+                                            h->seg);
+            ALCU_TRY(cudaGetLastError());
+            b = h->cub_bytes;
+            ALCU_TRY(cub::DeviceScan::ExclusiveSum(h->cub_tmp, b, h->flag, h->pos, Mb, st));
+            k_compact<<<gb, 256, 0, st>>>(Mb, h->flag, h->pos, h->band, h->cand, n_cand);
+            ALCU_TRY(cudaGetLastError());
+            int M = 0;
+            ALCU_TRY(cudaMemcpyAsync(&M, n_cand, sizeof(int), cudaMemcpyDeviceToHost, st));
+            ALCU_TRY(cudaStreamSynchronize(st));
+            if (M == 0) continue;
+            if ((rc = cub_reserve(h, M)) != GPK_OK) return rc;
+            const int sb = (M + 255) / 256 < G ? (M + 255) / 256 : G;
+            k_cgr_score<<<sb, 256, 0, st>>>(d, t, h->cand, n_cand, h->root, h->seg, h->key1);
+            ALCU_TRY(cudaGetLastError());
+            b = h->cub_bytes;
+            ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->key1, h->key2, h->cand, h->cells1, M, 0, 64,
+                                                     st));
+            k_cgr_segkeys<<<sb, 256, 0, st>>>(h->cells1, n_cand, h->seg, h->sk1);
+            ALCU_TRY(cudaGetLastError());
+            b = h->cub_bytes;
+            ALCU_TRY(cub::DeviceRadixSort::SortPairs(h->cub_tmp, b, h->sk1, h->sk2, h->cells1, h->cells2, M, 0,
+                                                     h->seg_bits, st));
+            k_cgr_starts<<<sb, 256, 0, st>>>(h->sk2, n_cand, h->start);
+            k_cgr_vacate<<<gb, 256, 0, st>>>(w, h->band, n_band, h->root, h->size, h->wave, labels);
+            k_cgr_select<<<sb, 256, 0, st>>>(h->sk2, h->cells2, n_cand, h->start, h->size, h->orig, labels);
+            ALCU_TRY(cudaGetLastError());
+        }
     }
     k_cgr_changed<<<gb, 256, 0, st>>>(h->band, n_band, labels, h->orig, alpha, h->u64 + 2);
     ALCU_TRY(cudaGetLastError());
@@ -2164,8 +2303,9 @@ extern "C" int gpk_alcu_balanced_remap(gpk_alcu* h, int8_t* labels, double* alph
 }
 
 extern "C" int gpk_alcu_info(const gpk_alcu* h, int64_t* cells, int64_t* device_bytes, int64_t* last_components,
-                             int64_t* last_waves) {
+                             int64_t* last_waves, int64_t* last_pairs) {
     if (!h) { gpk_set_error("alcu: null handle"); return GPK_ERR_INVALID_ARGUMENT; }
+    if (last_pairs) *last_pairs = h->last_pairs;
     if (cells) *cells = h->d.N;
     if (device_bytes) *device_bytes = h->bytes;
     if (last_components) *last_components = h->last_components;

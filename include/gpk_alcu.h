@@ -139,9 +139,11 @@ int gpk_alcu_sum(gpk_alcu* h, const double* x, double* out);
 /* out = scipy.ndimage.gaussian_filter(in, sigma, mode="wrap") for the taps;
  * in and out may not alias.                                                */
 int gpk_alcu_gaussian_filter(gpk_alcu* h, const double* in, double* out, const double* taps, int radius);
-/* Cells; device bytes held; components and waves of the last remap.      */
+/* Cells; device bytes held; components, waves and scored (cell, component)
+ * pairs of the last Gaussian remap (pairs above the cell count are handled
+ * wave by wave instead).  Any output may be NULL.                         */
 int gpk_alcu_info(const gpk_alcu* h, int64_t* cells, int64_t* device_bytes, int64_t* last_components,
-                  int64_t* last_waves);
+                  int64_t* last_waves, int64_t* last_pairs);
 
 #ifdef __cplusplus
 }

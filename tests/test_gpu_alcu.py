@@ -216,6 +216,8 @@ def chain_labels(shape):
 
 
 CASES = [
+    ("dense_2d", (40, 44), "dense"),
+    ("dense_3d", (14, 16, 12), "dense"),
     ("plates_96", (96, 96, 96), None),
     ("odd_2d", (67, 45), None),
     ("thin_3d", (5, 40, 33), None),
@@ -234,6 +236,10 @@ def case_state(shape, kind, seed):
         return state(shape, rng, np.zeros(shape, dtype=np.int8))
     if kind == "full":
         return state(shape, rng, np.full(shape, 2, dtype=np.int8))
+    if kind == "dense":
+        # tiny components packed tightly: dilations stacked many deep
+        lab = np.where(rng.random(shape) < 0.55, rng.integers(1, 4, size=shape), 0).astype(np.int8)
+        return state(shape, rng, lab)
     return state(shape, rng)
 
 
@@ -307,6 +313,10 @@ def test_gaussian_remap_against_oracle(torch_cuda, case, sigma):
     assert n == n_ref
     assert np.array_equal(host(dl), lr) and same(host(da), ar)
     info = h.info()
+    if kind == "dense":
+        assert info["pairs"] > int(np.prod(shape))  # handled wave by wave
+    elif kind is None:
+        assert 0 < info["pairs"] <= int(np.prod(shape))  # scored once, one pair order
     if kind == "chain":
         assert info["waves"] > 2
     if kind == "empty":
