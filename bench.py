@@ -315,7 +315,8 @@ def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
         m0, _ = h.competitor(dl)
         grow = (0.05 * m0.double()).contiguous()
         # a fixed tenth of the initial interface cells cross in every step
-        cross = (m0 & (torch.rand(shape, device="cuda") < 0.1)).to(torch.uint8).contiguous()
+        gen = torch.Generator(device="cuda").manual_seed(7)
+        cross = (m0 & (torch.rand(shape, device="cuda", generator=gen) < 0.1)).to(torch.uint8).contiguous()
         stream = torch.cuda.current_stream()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(stages) + 1)]
         acc = {k: 0.0 for k in stages}

@@ -161,6 +161,12 @@ __global__ void k_variant_fractions(long long N, const int8_t* __restrict__ lab,
 
 // matrix fraction max(1 - f, 1e-8) and the clipped lever-rule composition
 __device__ __forceinline__ void lever(double c, double f, const Phys& p, double& m, double& cm) {
+    if (f == 0.0) {
+        // matrix cell: m = 1 exactly, and x / 1 = x for every x
+        m = 1.0;
+        cm = np_clip(c - f * p.ct, 0.0, p.ct);
+        return;
+    }
     m = np_max(1.0 - f, 1e-8);
     const double raw = m > 1e-7 ? (c - f * p.ct) / m : p.ceq;
     cm = np_clip(raw, 0.0, p.ct);
@@ -383,17 +389,50 @@ __global__ void __launch_bounds__(128) k_gauss_march(Ext d, Taps t, int chunk, c
     }
 }
 
+// The last pass (axis 2) of the partition transfer's smoothing with the
+// weight computed in its epilogue, as the reference computes it from the
+// smoothed field (lines 721-729): w = G|transfer| * matrix, times the
+// capacity max(ctot - c_eq matrix, 0) when Cu is drawn from the matrix
+__global__ void __launch_bounds__(128) k_gauss_last_weight(Ext d, Taps t, const double* __restrict__ a0,
+                                                           double* __restrict__ w, double* __restrict__ cap,
+                                                           const double* __restrict__ newf,
+                                                           const double* __restrict__ c, double ceq, int draw) {
+    const int n = d.e[2];
+    const bool near = t.r <= n;
+    CELLS3(d) {
+        const long long i = CELL_INDEX(d);
+        const long long base = i - x2;
+        double v0 = a0[i] * t.w[0];
+        for (int j = t.r; j >= 1; --j)
+            v0 = v0 + (a0[base + wrap_off(x2 - j, n, near)] + a0[base + wrap_off(x2 + j, n, near)]) * t.w[j];
+        const double m = np_clip(1.0 - newf[i], 0.0, 1.0);
+        double v = v0 * m;
+        if (draw) {
+            const double k = np_max(c[i] - ceq * m, 0.0);
+            v = v * k;
+            cap[i] = k;
+        }
+        w[i] = v;
+    }
+}
+
 // ---------------------------------------------------------------- numpy's pairwise sum
 
-// a field value, or (corr * w[i]) / wsum for the correction residue
+// a field value, or (corr * w[i]) / wsum for the correction (added to c as it is summed)
 struct LoadF {
     const double* a;
     __device__ __forceinline__ double operator()(long long i) const { return a[i]; }
 };
-struct CorrF {
+// the same value, also added to c[i] (the leaf pass visits every i once)
+struct CorrApplyF {
     const double* w;
+    double* c;
     double corr, wsum;
-    __device__ __forceinline__ double operator()(long long i) const { return (corr * w[i]) / wsum; }
+    __device__ __forceinline__ double operator()(long long i) const {
+        const double v = (corr * w[i]) / wsum;
+        c[i] = c[i] + v;
+        return v;
+    }
 };
 
 // 8 lanes per leaf: lane j holds numpy's running partial r[j]
@@ -466,6 +505,25 @@ __global__ void k_pw_nodes(const int* __restrict__ node_n, const int* __restrict
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < M) out[k] = pw_walk(node_n[k], t, lower, node_first[k]);
 }
+// the small upper levels (at most 1024 nodes each) in one block, a barrier
+// between levels; buffers alternate as in the per-level launches
+struct PwTop {
+    const int* n[12];
+    const int* first[12];
+    int count[12];
+    long long below[12];
+    int levels;
+};
+__global__ void __launch_bounds__(1024) k_pw_top(PwTop lv, double* b0, double* b1, int cur) {
+    for (int l = 0; l < lv.levels; ++l) {
+        const double* lower = cur ? b1 : b0;
+        double* out = cur ? b0 : b1;
+        for (int k = threadIdx.x; k < lv.count[l]; k += blockDim.x)
+            out[k] = pw_walk(lv.n[l][k], lv.below[l], lower, lv.first[l][k]);
+        __syncthreads();
+        cur ^= 1;
+    }
+}
 
 // ---------------------------------------------------------------- partition transfer
 
@@ -479,27 +537,6 @@ __global__ void k_pt_transfer(long long N, double ct, double* __restrict__ c, co
         c[i] = c[i] + t;
         abs_tr[i] = fabs(t);
     }
-}
-
-// weight = G|transfer| * matrix (times the capacity above equilibrium when Cu
-// is drawn from the matrix)
-__global__ void k_pt_weight(long long N, double ceq, int draw, const double* __restrict__ g,
-                            const double* __restrict__ newf, const double* __restrict__ c, double* __restrict__ w,
-                            double* __restrict__ cap) {
-    GRID_STRIDE(i, N) {
-        const double m = np_clip(1.0 - newf[i], 0.0, 1.0);
-        double v = g[i] * m;
-        if (draw) {
-            const double k = np_max(c[i] - ceq * m, 0.0);
-            v = v * k;
-            cap[i] = k;
-        }
-        w[i] = v;
-    }
-}
-
-__global__ void k_pt_apply(long long N, double corr, double wsum, const double* __restrict__ w, double* __restrict__ c) {
-    GRID_STRIDE(i, N) c[i] = c[i] + (corr * w[i]) / wsum;
 }
 
 // order-preserving key of a double (larger value, larger key)
@@ -1473,12 +1510,29 @@ int pw_sum(gpk_alcu* h, F f, double* out) {
                                                                      h->pw_buf[0]);
     ALCU_TRY(cudaGetLastError());
     int cur = 0;
-    for (size_t k = 0; k < h->lvl_n.size(); ++k) {
+    size_t k = 0;
+    for (; k < h->lvl_n.size() && h->lvl_count[k] > 1024; ++k) {
         const int M = h->lvl_count[k];
         k_pw_nodes<<<(M + 127) / 128, 128, 0, st>>>(h->lvl_n[k], h->lvl_first[k], M, h->lvl_below[k],
                                                      h->pw_buf[cur], h->pw_buf[cur ^ 1]);
         ALCU_TRY(cudaGetLastError());
         cur ^= 1;
+    }
+    if (k < h->lvl_n.size()) {
+        PwTop lv{};
+        for (; k < h->lvl_n.size() && lv.levels < 12; ++k, ++lv.levels) {
+            lv.n[lv.levels] = h->lvl_n[k];
+            lv.first[lv.levels] = h->lvl_first[k];
+            lv.count[lv.levels] = h->lvl_count[k];
+            lv.below[lv.levels] = h->lvl_below[k];
+        }
+        if (k < h->lvl_n.size()) {
+            gpk_set_error("alcu: summation tree deeper than expected");
+            return GPK_ERR_INTERNAL;
+        }
+        k_pw_top<<<1, 1024, 0, st>>>(lv, h->pw_buf[0], h->pw_buf[1], cur);
+        ALCU_TRY(cudaGetLastError());
+        cur ^= lv.levels & 1;
     }
     ALCU_TRY(cudaMemcpyAsync(out, h->pw_buf[cur], sizeof(double), cudaMemcpyDeviceToHost, st));
     ALCU_TRY(cudaStreamSynchronize(st));
@@ -1876,11 +1930,22 @@ extern "C" int gpk_alcu_partition_transfer(gpk_alcu* h, double* ctot, const doub
     double total = 0.0;
     if ((rc = pw_sum(h, LoadF{tr}, &total)) != GPK_OK) return rc;
     if (std::fabs(total) <= 1.0e-30) return GPK_OK;
-    if ((rc = gauss(h, t, absd, g, tmp)) != GPK_OK) return rc;
     const double correction = -total;
     const int draw = correction < 0.0;
-    k_pt_weight<<<h->grid, 256, 0, h->stream>>>(N, h->p.ceq, draw, g, new_fraction, ctot, w, cap);
-    ALCU_TRY(cudaGetLastError());
+    {
+        // passes along the field's axes; the last one (axis 2) computes the weight
+        const double* src = absd;
+        double* dst = g;
+        for (int a = h->d.a0; a < 2; ++a) {
+            gauss_pass<1>(h, a, t, src, nullptr, dst, nullptr);
+            ALCU_TRY(cudaGetLastError());
+            src = dst;
+            dst = dst == g ? tmp : g;
+        }
+        k_gauss_last_weight<<<grid3(h->d), B3, 0, h->stream>>>(h->d, t, src, w, cap, new_fraction, ctot, h->p.ceq,
+                                                              draw);
+        ALCU_TRY(cudaGetLastError());
+    }
     if (draw) {
         double cap_sum = 0.0;
         if ((rc = pw_sum(h, LoadF{cap}, &cap_sum)) != GPK_OK) return rc;
@@ -1895,10 +1960,9 @@ extern "C" int gpk_alcu_partition_transfer(gpk_alcu* h, double* ctot, const doub
         gpk_set_error("empty matrix neighbourhood for partition transfer");
         return GPK_ERR_INFEASIBLE;
     }
-    k_pt_apply<<<h->grid, 256, 0, h->stream>>>(N, correction, wsum, w, ctot);
-    ALCU_TRY(cudaGetLastError());
+    // ctot += (correction w) / wsum, summed as it is added
     double s = 0.0;
-    if ((rc = pw_sum(h, CorrF{w, correction, wsum}, &s)) != GPK_OK) return rc;
+    if ((rc = pw_sum(h, CorrApplyF{w, ctot, correction, wsum}, &s)) != GPK_OK) return rc;
     const double residue = total + s;
     ALCU_TRY(cudaMemsetAsync(h->u64, 0, sizeof(unsigned long long), h->stream));
     ALCU_TRY(cudaMemsetAsync(h->u64 + 1, 0xff, sizeof(unsigned long long), h->stream));
