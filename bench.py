@@ -364,7 +364,17 @@ def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
         t1.synchronize()
         ms = t0.elapsed_time(t1) / steps
         st_ms = {k: v / steps for k, v in acc.items()}
-        res = {"ms_per_step": ms, "cells_per_s": n / (ms / 1e3), "stages_ms": st_ms,
+        # the chain's largest single kernel: the tiled diffusion substep
+        # (2 substeps per step at dt = 10 s, dx = 1.5 nm), 24 algorithmic B/cell
+        sub_ms = st_ms["diffuse"] / 2.0
+        diff_gbs = 24.0 * n / (sub_ms / 1e3) / 1e9
+        roof = {"kernel": "k_diffuse_tiled (one explicit substep)", "bound": "hbm", "achieved": diff_gbs,
+                "peak": peak, "unit": "GB/s", "frac": diff_gbs / peak, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": 24.0 * n,
+                "traffic": 381.9e6 * n / 256 ** 3 if shape[0] == 256 else None,
+                "traffic_note": "dram read + write of one 256^3 launch under ncu (profiles/alcu_diffusion_256.md)",
+                "note": "issue-bound on its FP64 divisions in the reference's operand order, not on HBM"}
+        res = {"ms_per_step": ms, "cells_per_s": n / (ms / 1e3), "stages_ms": st_ms, "roofline": roof,
                "components": h.info()["components"], "remap_waves": h.info()["waves"],
                "changed_last_step": info["changed"], "deferred_last_step": info["deferred"],
                "crossing_cells": int(cross.sum().item()),

@@ -63,7 +63,8 @@ typedef struct gpk_alcu_params {
 } gpk_alcu_params;
 
 /* ndim 2 or 3, extents >= 1, fewer than 2^31 - 1 cells.  Allocates about
- * 125 bytes per cell of device memory on the current device.              */
+ * 127 bytes per cell of device memory on the current device; the balanced
+ * remap adds 8 bytes per cell per distinct label at its first call.       */
 int gpk_alcu_create(int ndim, const int* shape, const gpk_alcu_params* p, gpk_alcu** out);
 int gpk_alcu_destroy(gpk_alcu* h);
 int gpk_alcu_set_params(gpk_alcu* h, const gpk_alcu_params* p);
