@@ -342,7 +342,10 @@ __global__ void __launch_bounds__(128) k_gauss_pass(Ext d, Taps t, const double*
 // current output in registers, so that each input is read once per line
 // chunk instead of 2R + 1 times.  Same operations and order as
 // k_gauss_pass; requires 2R + 1 <= the axis extent.
-template <int NF, int AX, int R>
+// With PRE (NF = 2), the inputs are c_m and f of the interface composition
+// and the window holds the reference's operands: c_m * m and m, with
+// m = clip(1 - f, 0, 1).
+template <int NF, int AX, int R, bool PRE = false>
 __global__ void __launch_bounds__(128) k_gauss_march(Ext d, Taps t, int chunk, const double* __restrict__ a0,
                                                      const double* __restrict__ a1, double* __restrict__ o0,
                                                      double* __restrict__ o1) {
@@ -361,8 +364,14 @@ __global__ void __launch_bounds__(128) k_gauss_march(Ext d, Taps t, int chunk, c
     for (int k = 0; k < W; ++k) {
         int z = z0 - R + k;
         z = z < 0 ? z + n : (z >= n ? z - n : z);
-        u[k] = a0[base + z * s];
-        if (NF == 2) v[k] = a1[base + z * s];
+        if (PRE) {
+            const double m = np_clip(1.0 - a1[base + z * s], 0.0, 1.0);
+            u[k] = a0[base + z * s] * m;
+            v[k] = m;
+        } else {
+            u[k] = a0[base + z * s];
+            if (NF == 2) v[k] = a1[base + z * s];
+        }
     }
     for (int z = z0; z < z1; ++z) {
         double r0 = u[R] * t.w[0];
@@ -383,8 +392,14 @@ __global__ void __launch_bounds__(128) k_gauss_march(Ext d, Taps t, int chunk, c
             }
             int zn = z + 1 + R;
             zn = zn >= n ? zn - n : zn;
-            u[W - 1] = a0[base + zn * s];
-            if (NF == 2) v[W - 1] = a1[base + zn * s];
+            if (PRE) {
+                const double m = np_clip(1.0 - a1[base + zn * s], 0.0, 1.0);
+                u[W - 1] = a0[base + zn * s] * m;
+                v[W - 1] = m;
+            } else {
+                u[W - 1] = a0[base + zn * s];
+                if (NF == 2) v[W - 1] = a1[base + zn * s];
+            }
         }
     }
 }
@@ -413,6 +428,27 @@ __global__ void __launch_bounds__(128) k_gauss_last_weight(Ext d, Taps t, const 
             cap[i] = k;
         }
         w[i] = v;
+    }
+}
+
+// The last pass (axis 2) of the interface composition's two smoothed fields
+// with its epilogue: trace = clip(G(c_m m) / max(G(m), 1e-12), 0, c_theta)
+__global__ void __launch_bounds__(128) k_gauss_last_trace(Ext d, Taps t, const double* __restrict__ a0,
+                                                          const double* __restrict__ a1, double ct,
+                                                          double* __restrict__ out) {
+    const int n = d.e[2];
+    const bool near = t.r <= n;
+    CELLS3(d) {
+        const long long i = CELL_INDEX(d);
+        const long long base = i - x2;
+        double v0 = a0[i] * t.w[0];
+        double v1 = a1[i] * t.w[0];
+        for (int j = t.r; j >= 1; --j) {
+            const long long lo = base + wrap_off(x2 - j, n, near), hi = base + wrap_off(x2 + j, n, near);
+            v0 = v0 + (a0[lo] + a0[hi]) * t.w[j];
+            v1 = v1 + (a1[lo] + a1[hi]) * t.w[j];
+        }
+        out[i] = np_clip(v0 / np_max(v1, 1.0e-12), 0.0, ct);
     }
 }
 
@@ -576,10 +612,6 @@ __global__ void k_ic_pre(long long N, const double* __restrict__ cm, const doubl
         num[i] = cm[i] * m;
         den[i] = m;
     }
-}
-__global__ void k_ic_post(long long N, double ct, const double* __restrict__ num, const double* __restrict__ den,
-                          double* __restrict__ out) {
-    GRID_STRIDE(i, N) out[i] = np_clip(num[i] / np_max(den[i], 1.0e-12), 0.0, ct);
 }
 
 // ---------------------------------------------------------------- Gaussian remap
@@ -1610,21 +1642,6 @@ int gauss(gpk_alcu* h, const Taps& t, const double* in, double* out, double* tmp
     }
     return GPK_OK;
 }
-// two fields smoothed together (ta, tb: scratch); *ra, *rb point at the
-// results, which lie in (a, b) or (ta, tb) depending on the pass count
-int gauss2(gpk_alcu* h, const Taps& t, double* a, double* b, double* ta, double* tb, const double** ra,
-           const double** rb) {
-    double *sa = a, *sb = b, *da = ta, *db = tb;
-    for (int ax = h->d.a0; ax < 3; ++ax) {
-        gauss_pass<2>(h, ax, t, sa, sb, da, db);
-        ALCU_TRY(cudaGetLastError());
-        std::swap(sa, da);
-        std::swap(sb, db);
-    }
-    *ra = sa;
-    *rb = sb;
-    return GPK_OK;
-}
 
 }  // namespace
 
@@ -1979,13 +1996,52 @@ extern "C" int gpk_alcu_interface_composition(gpk_alcu* h, const double* cm, con
     Taps t;
     int rc = taps_of(taps, radius, t);
     if (rc != GPK_OK) return rc;
-    const long long N = h->d.N;
-    double *num = h->f[1], *den = h->f[2];
-    k_ic_pre<<<h->grid, 256, 0, h->stream>>>(N, cm, fprec, num, den);
-    ALCU_TRY(cudaGetLastError());
-    const double *rn = nullptr, *rd = nullptr;
-    if ((rc = gauss2(h, t, num, den, h->f[3], h->f[4], &rn, &rd)) != GPK_OK) return rc;
-    k_ic_post<<<h->grid, 256, 0, h->stream>>>(N, h->p.ct, rn, rd, trace);
+    const Ext& d = h->d;
+    const long long N = d.N;
+    double *num = h->f[1], *den = h->f[2], *tn = h->f[3], *td = h->f[4];
+    // passes along the field's axes, the first reading c_m and f (the
+    // product and matrix fraction formed on load when it marches), the last
+    // (axis 2) computing the trace
+    double* sa = nullptr;
+    double* sb = nullptr;
+    const int ax0 = d.a0;
+    const int ox = ax0 == 0 ? 1 : 0;
+    const long long gy = (d.e[ox] + 3) / 4;
+    const long long lines = (long long)((d.e[2] + 31) / 32) * gy;
+    const long long want = (32ll * h->num_sms + lines - 1) / lines;
+    long long chunk = (d.e[ax0] + want - 1) / want;
+    chunk = chunk < 16 ? 16 : chunk;
+    const long long gz = (d.e[ax0] + chunk - 1) / chunk;
+    const bool march_first = t.r == 3 && d.e[ax0] >= 7 && gy <= 65535 && gz <= 65535;
+    if (march_first) {
+        const dim3 g((d.e[2] + 31) / 32, (unsigned)gy, (unsigned)gz);
+        if (ax0 == 0)
+            k_gauss_march<2, 0, 3, true><<<g, B3, 0, h->stream>>>(d, t, (int)chunk, cm, fprec, num, den);
+        else
+            k_gauss_march<2, 1, 3, true><<<g, B3, 0, h->stream>>>(d, t, (int)chunk, cm, fprec, num, den);
+        ALCU_TRY(cudaGetLastError());
+        sa = num;
+        sb = den;
+        if (ax0 == 0) {
+            gauss_pass<2>(h, 1, t, num, den, tn, td);
+            ALCU_TRY(cudaGetLastError());
+            sa = tn;
+            sb = td;
+        }
+    } else {
+        k_ic_pre<<<h->grid, 256, 0, h->stream>>>(N, cm, fprec, num, den);
+        ALCU_TRY(cudaGetLastError());
+        sa = num;
+        sb = den;
+        double *da = tn, *db = td;
+        for (int ax = ax0; ax < 2; ++ax) {
+            gauss_pass<2>(h, ax, t, sa, sb, da, db);
+            ALCU_TRY(cudaGetLastError());
+            std::swap(sa, da);
+            std::swap(sb, db);
+        }
+    }
+    k_gauss_last_trace<<<grid3(d), B3, 0, h->stream>>>(d, t, sa, sb, h->p.ct, trace);
     ALCU_TRY(cudaGetLastError());
     return GPK_OK;
 }
