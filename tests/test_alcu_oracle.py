@@ -9,6 +9,9 @@ pairwise sum against `np.sum`, the wrapped Gaussian against
 `scipy.ndimage.gaussian_filter`, the components against `scipy.ndimage.label`.
 """
 import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 import numpy as np
 import pytest
@@ -150,3 +153,29 @@ def test_oracle_certificate_known_answers(z):
 def test_oracle_variant_fractions(z, name):
     got = O.variant_fraction_fields(z[f"{name}_labels"], z[f"{name}_vf_alpha"], z[f"{name}_competitor"])
     assert same(got, z[f"{name}_vf"])
+
+
+def test_oracle_replays_the_reference_trajectory():
+    """Every recorded call of the reference's driver, through the oracle."""
+    import alcu_replay as R
+
+    def p_of(params):
+        return O.AlCuParams(dx=params["dx"], diffusivity=params["diffusivity"], c_matrix_eq=params["c_matrix_eq"],
+                            c_theta=params["c_theta"], remap_sigma_cells=params["remap_sigma_cells"],
+                            composition_extension_sigma_cells=params["composition_extension_sigma_cells"])
+
+    impl = {
+        "neighbor_competitor": lambda a, pr, z: (O.neighbor_competitor(a[0]), {}),
+        "precip_fraction": lambda a, pr, z: ((O.precip_fraction(a[0], a[1], a[2]),), {}),
+        "variant_fraction_fields": lambda a, pr, z: ((O.variant_fraction_fields(a[0], a[1], a[2]),), {}),
+        "interface_matrix_composition": lambda a, pr, z: ((O.interface_matrix_composition(a[0], a[1], p_of(pr)),), {}),
+        "diffuse_conservative_subcycled": lambda a, pr, z: (O.diffuse_conservative_subcycled(a[0], a[1], p_of(pr),
+                                                                                              a[3]), {}),
+        "conservative_partition_transfer": lambda a, pr, z: (
+            (O.conservative_partition_transfer(a[0], a[1], a[2], a[3], p_of(pr)),), {0: a[0]}),
+        "commit_topology_transactions": lambda a, pr, z: (
+            (O.commit_topology_transactions(a[0], a[1], a[2], a[3]),), {0: a[0], 1: a[1]}),
+        "conservative_gaussian_remap": lambda a, pr, z: (
+            (O.conservative_gaussian_remap(a[0], a[1], a[2]),), {0: a[0], 1: a[1]}),
+    }
+    assert R.replay(impl) == 97

@@ -566,3 +566,72 @@ def test_golden_variant_fractions(torch_cuda, z, name):
     assert same(host(got), z[f"{name}_vf"])
     assert same(alcu.variant_fraction_fields(z[f"{name}_labels"], z[f"{name}_vf_alpha"], z[f"{name}_competitor"]),
                 z[f"{name}_vf"])
+
+
+@gpu
+def test_replays_the_reference_trajectory(torch_cuda):
+    """Every recorded call of the reference's own driver on a 64^2 Al-Cu run
+    (tests/golden/alcu_trajectory.npz: the first steps and four crossing
+    events with their remaps), through the device functions with the taps
+    recorded beside them; bit for bit."""
+    import sys
+
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import alcu_replay as R
+    from gpk_b200.alcu import AlCuTransport
+
+    torch = torch_cuda
+    handles = {}
+
+    def h_of(shape, pr):
+        if shape not in handles:
+            handles[shape] = AlCuTransport(shape, O.AlCuParams(dx=pr["dx"], diffusivity=pr["diffusivity"],
+                                                               c_matrix_eq=pr["c_matrix_eq"], c_theta=pr["c_theta"]))
+        return handles[shape]
+
+    def taps(z, sigma):
+        return z[f"taps_{int(round(sigma * 100))}"]
+
+    def d(x):
+        return dev(torch, x)
+
+    def competitor(a, pr, z):
+        m, c = h_of(a[0].shape, pr).competitor(d(a[0]))
+        return (host(m), host(c)), {}
+
+    def fraction(a, pr, z):
+        return (host(h_of(a[0].shape, pr).precip_fraction(d(a[0]), d(a[1]), d(a[2]))),), {}
+
+    def variants(a, pr, z):
+        return (host(h_of(a[0].shape, pr).variant_fractions(d(a[0]), d(a[1]), d(a[2]))),), {}
+
+    def interface(a, pr, z):
+        sig = pr["composition_extension_sigma_cells"]
+        return (host(h_of(a[0].shape, pr).interface_composition(d(a[0]), d(a[1]), taps(z, sig))),), {}
+
+    def diffuse(a, pr, z):
+        c = d(a[0])
+        cm, n = h_of(a[0].shape, pr).diffuse(c, d(a[1]), a[3])
+        return (host(c), host(cm), n), {}
+
+    def transfer(a, pr, z):
+        c = d(a[0])
+        h_of(a[0].shape, pr).partition_transfer(c, d(a[1]), d(a[2]), d(a[3]),
+                                                taps(z, pr["composition_extension_sigma_cells"]))
+        return (None,), {0: host(c)}
+
+    def transactions(a, pr, z):
+        lab, al = d(a[0]), d(a[1])
+        n = h_of(a[0].shape, pr).commit_transactions(lab, al, d(a[2]), d(a[3].astype(np.uint8)))
+        return (n,), {0: host(lab), 1: host(al)}
+
+    def remap(a, pr, z):
+        lab, al = d(a[0]), d(a[1])
+        n = h_of(a[0].shape, pr).gaussian_remap(lab, al, taps(z, a[2]))
+        return (n,), {0: host(lab), 1: host(al)}
+
+    impl = {"neighbor_competitor": competitor, "precip_fraction": fraction, "variant_fraction_fields": variants,
+            "interface_matrix_composition": interface, "diffuse_conservative_subcycled": diffuse,
+            "conservative_partition_transfer": transfer, "commit_topology_transactions": transactions,
+            "conservative_gaussian_remap": remap}
+    assert R.replay(impl) == 97
