@@ -54,3 +54,23 @@ def replay(impl, check_taps=None):
             assert same(inplace[int(k)], z["arr_" + e["a"]]), (c["name"], c["step"], "argument", k)
         checked += 1
     return checked
+
+
+def spectral_cases():
+    """(variant fractions, p, reference results) of every spectral solve the
+    driver made in the recorded run."""
+    import types
+
+    z, _, params = load()
+    el = z["elastic"]
+    p = types.SimpleNamespace(dx=params["dx"], c11=el[0], c12=el[1], c44=el[2], eigen_small=el[3],
+                              eigen_large=el[4])
+    out = []
+    for c in json.loads(bytes(z["spectral"]).decode()):
+        out.append((z["arr_" + c["vf"]], p, {k: z["arr_" + c[k]] for k in ("driving", "energy", "hydro")},
+                    c["residual"]))
+    return out
+
+
+def rel_err(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300))

@@ -13,9 +13,10 @@ arguments and results of every call of
 
 in the first two steps and in the steps around the first crossing events, so
 that the device functions can be replayed on states the simulation itself
-produces.  Arrays are stored once each (deduplicated by content).  The
-driver's own output files go to a temporary folder.  Run it where the
-reference tree is present:
+produces; and every call of spectral_elasticity (99-190) in the whole run,
+with its variant fractions and results.  Arrays are stored once each
+(deduplicated by content).  The driver's own output files go to a
+temporary folder.  Run it where the reference tree is present:
 
     python tests/golden/make_alcu_trajectory.py [path/to/reference]
 """
@@ -96,6 +97,16 @@ def main(root: str) -> None:
             return result
 
         setattr(ref, name, wrap)
+    spectral = []
+    f_spec = ref.spectral_elasticity
+
+    def spec_wrap(vf, p):
+        r = f_spec(vf, p)
+        spectral.append({"vf": key(vf), "driving": key(r[0]), "energy": key(r[1]), "hydro": key(r[2]),
+                         "residual": float(r[3])})
+        return r
+
+    ref.spectral_elasticity = spec_wrap
     ref.run_case("trajectory", (64, 64), 2, 4.0, 200.0, [0.0], 7, dx=0.5e-9,
                  seed_layout=[((18, 20), 1, 1.0), ((44, 42), 2, 1.0)], initial_shape="sphere")
     # steps kept: the first two, and each crossing step with the next
@@ -108,6 +119,8 @@ def main(root: str) -> None:
             events += 1
     kept = [c for c in calls if c["step"] in keep]
     used = set()
+    for c in spectral:
+        used |= {c["vf"], c["driving"], c["energy"], c["hydro"]}
     for c in kept:
         for e in c["args"] + c["out"] + list(c["inplace"].values()):
             if "a" in e:
@@ -120,9 +133,13 @@ def main(root: str) -> None:
         phi = np.exp(-0.5 / (sigma * sigma) * x ** 2)
         out[f"taps_{int(round(sigma * 100))}"] = phi / phi.sum()
     out["calls"] = np.frombuffer(json.dumps(kept).encode(), dtype=np.uint8)
+    out["spectral"] = np.frombuffer(json.dumps(spectral).encode(), dtype=np.uint8)
+    out["elastic"] = np.asarray([float(getattr(ref.Parameters(), k)) for k in
+                                 ("c11", "c12", "c44", "eigen_small", "eigen_large")])
     out["params"] = np.frombuffer(json.dumps(state["params"]).encode(), dtype=np.uint8)
     np.savez_compressed(OUT, **out)
-    print("wrote", OUT, len(kept), "calls,", len(used), "arrays,", events, "crossing events")
+    print("wrote", OUT, len(kept), "calls,", len(spectral), "spectral solves,", len(used), "arrays,", events,
+          "crossing events")
 
 
 if __name__ == "__main__":

@@ -105,3 +105,21 @@ def test_invalid_arguments():
     s = SpectralElasticity((8, 8), 1.0, 1.0, 0.5, 0.3, np.eye(3))
     with pytest.raises(ValueError):
         s.solve(np.zeros((3, 8, 9)))
+
+
+@pytest.mark.gpu
+def test_gpu_on_the_reference_trajectory():
+    """The driver's own spectral solves of a 64^2 Al-Cu run (variant
+    fractions of the evolving precipitates, tests/golden/alcu_trajectory.npz),
+    through the device solve, every field within 1e-10."""
+    import os
+    import sys
+
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import alcu_replay as R
+    from gpk_b200 import spectral_elasticity as gpu_spectral
+
+    for vf, p, ref, res in R.spectral_cases():
+        d, e, h, r = gpu_spectral(vf, p)
+        assert R.rel_err(d, ref["driving"]) < TOL and R.rel_err(e, ref["energy"]) < TOL
+        assert R.rel_err(h, ref["hydro"]) < TOL and abs(r - res) < 1e-12

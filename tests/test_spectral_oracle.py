@@ -58,3 +58,19 @@ def test_oracle_dilatational_sphere_is_hydrostatic_inside():
     assert r < 1e-12
     assert np.all(h[inside] < 0)
     assert np.all(e >= -1e-9 * e.max())
+
+
+def test_oracle_on_the_reference_trajectory():
+    """The driver's own spectral solves of a 64^2 Al-Cu run (recorded in
+    tests/golden/alcu_trajectory.npz), through the oracle, within 1e-10."""
+    import sys
+
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import alcu_replay as R
+
+    cases = R.spectral_cases()
+    assert len(cases) >= 5
+    for vf, p, ref, res in cases:
+        d, e, h, r = spectral_elasticity(vf, p)
+        assert R.rel_err(d, ref["driving"]) < 1e-10 and R.rel_err(e, ref["energy"]) < 1e-10
+        assert R.rel_err(h, ref["hydro"]) < 1e-10 and abs(r - res) < 1e-12
