@@ -514,27 +514,30 @@ def adjoint_measurement(with_cpu: bool, evals: int = 20):
     return res
 
 
-def coupled_measurement(steps: int = 20, warmup: int = 3):
+def coupled_measurement(steps: int = 20, warmup: int = 3, n: int = 128, elastic: bool = True):
     """3-D solidification with solute partitioning and a spectral elastic
-    solve every step: 128^3, FP64, nucleus of radius 4 at the centre, 5 K
-    undercooling, c0 = 0.02, k = 0.14, cubic 108/62/28 GPa, 0.5% dilatational
-    misfit of the solid (parameters of the reference's solidification deck
-    otherwise)."""
+    solve every step: n^3 (128 by default), FP64, nucleus of radius 4 at the
+    centre, 5 K undercooling, c0 = 0.02, k = 0.14, cubic 108/62/28 GPa, 0.5%
+    dilatational misfit of the solid (parameters of the reference's
+    solidification deck otherwise).  Without elastic, the same step with no
+    elastic solve: the solute transport alone on a field larger than L2."""
     import torch
     from gpk_b200 import GPKGrid, SpectralElasticity, thermo
     from gpk_b200.spectral import variant_eigenstrains
-    n = 128
     th = thermo.solidification(M0=5e-8, sigma0=0.2, eps4=0.04, m_liq=-500.0, k_part=0.14, T_melt=933.0, L=1e8)
-    th.solute_rejection = True
+    th.solute_rejection, th.k_partition = True, 0.14  # as the reference's driver sets both from k_part
     g = GPKGrid(n, n, n, 0.5e-6, th, 3e-9, 1.5, precision="f64")
     z, y, x = np.indices((n, n, n)) - n // 2
     g.set("phi", ((x * x + y * y + z * z) <= 16).astype(np.int32))
     g.set("c", 0.02)
     g.set("T", 933.0 - 5.0)
-    g.set_external_elastic(True)
-    s = SpectralElasticity((n, n, n), 0.5e-6, 108e9, 62e9, 28e9, variant_eigenstrains(0.005, 0.005))
+    s = None
+    if elastic:
+        g.set_external_elastic(True)
+        s = SpectralElasticity((n, n, n), 0.5e-6, 108e9, 62e9, 28e9, variant_eigenstrains(0.005, 0.005))
     for _ in range(warmup):
-        s.couple(g)
+        if s:
+            s.couple(g)
         g.step()
     stream = torch.cuda.ExternalStream(g.stream_ptr())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -542,17 +545,20 @@ def coupled_measurement(steps: int = 20, warmup: int = 3):
     l0 = g.launch_count()
     e0.record(stream)
     for _ in range(steps):
-        s.couple(g)
+        if s:
+            s.couple(g)
         g.step()
     e1.record(stream)
     e1.synchronize()
     ms = e0.elapsed_time(e1) / steps
-    res = {"workload": "3-D solidification 128^3 FP64 with solute partitioning (k 0.14) and a spectral elastic "
-                       "solve every step (cubic 108/62/28 GPa, 0.5% dilatational misfit)",
+    res = {"workload": f"3-D solidification {n}^3 FP64 with solute partitioning (k 0.14)" +
+                       (" and a spectral elastic solve every step (cubic 108/62/28 GPa, 0.5% dilatational misfit)"
+                        if elastic else ", no elastic solve"),
            "steps": steps, "warmup": warmup, "ms_per_step": ms, "value": n ** 3 / (ms / 1e3),
            "unit": "cell-updates/s", "gpu_launches_per_step": (g.launch_count() - l0) / steps,
            "solid_cells": int((g.get("phi") != 0).sum()), "interface_fraction": g.interface_fraction()}
-    s.close()
+    if s:
+        s.close()
     g.close()
     return res
 
@@ -634,6 +640,13 @@ def run_gpu_arm(args):
                 traffic = float(line.split(":")[1])
     clocks = clk.summary()
     tap_adds = n_active * W ** 3 * 9 / (geo_ms / 1e3)
+    separable = (W - 1) // 2 > 18
+    if separable:
+        # per interface label: x pass (labels in, 4 B; t1 out, 4 B), y and z
+        # passes (8 B each), evaluation (labels, mask, S: 9 B); the interface
+        # cells' normals and curvature (16 B) once
+        geo_bytes = GRAINS * cells * 33.0 + n_active * 16
+        achieved = geo_bytes / (geo_ms / 1e3) / 1e9
     roofline = {"kernel": "k_geometry_tiled (label-bitmap Gaussian-Hessian tensor stencil + competitor)",
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic,
@@ -645,6 +658,11 @@ def run_gpu_arm(args):
                 "compute": {"tap_adds_per_s": tap_adds,
                             "peak_fp32_adds_per_s": _fp32_add_peak(clocks["sm_mhz"] or 1965.0),
                             "frac": tap_adds / _fp32_add_peak(clocks["sm_mhz"] or 1965.0)}}
+    if separable:
+        roofline = {"kernel": "k_sep_pass x3 + k_separable_eval per interface label (separable geometry)",
+                    "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": geo_bytes,
+                    "ms_per_launch": geo_ms}
     step_bytes = 16.0 * cells
     step_roofline = {"algorithmic_bytes_per_step": step_bytes,
                      "achieved_GBps": step_bytes / (ms / args.steps / 1e3) / 1e9, "peak": peak,
@@ -744,6 +762,10 @@ def main():
     ap.add_argument("--adjoint-only", action="store_true", help="time only the 512^2 adjoint gradient")
     ap.add_argument("--coupled-only", action="store_true",
                     help="time only the 128^3 solidification step with a spectral solve per step")
+    ap.add_argument("--transport-only", action="store_true",
+                    help="time only the solidification step without the elastic solve, on a --size cube")
+    ap.add_argument("--sigma", type=float, default=SIGMA,
+                    help="Gaussian width in cells (5 selects the per-label separable geometry)")
     ap.add_argument("--headline-only", action="store_true",
                     help="only the grain-growth step and its e2e (profiling the headline kernels)")
     ap.add_argument("--alcu-only", action="store_true",
@@ -751,7 +773,7 @@ def main():
     ap.add_argument("--spectral-only", action="store_true",
                     help="time only the 128^3 spectral elasticity solve (profiling its kernels)")
     args = ap.parse_args()
-    globals()["SIZE"], globals()["GRAINS"] = args.size, args.grains
+    globals()["SIZE"], globals()["GRAINS"], globals()["SIGMA"] = args.size, args.grains, args.sigma
     if args.spectral_only:
         print(json.dumps({"spectral": spectral_measurement(not args.no_cpu)}))
         return 0
@@ -760,6 +782,9 @@ def main():
         return 0
     if args.coupled_only:
         print(json.dumps({"coupled": coupled_measurement()}))
+        return 0
+    if args.transport_only:
+        print(json.dumps({"transport": coupled_measurement(args.steps, args.warmup, args.size, elastic=False)}))
         return 0
     if args.adjoint_only:
         print(json.dumps({"adjoint": adjoint_measurement(not args.no_cpu)}))

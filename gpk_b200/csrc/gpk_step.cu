@@ -244,13 +244,272 @@ __global__ void __launch_bounds__(128) k_geometry_direct(Dims D, const int32_t* 
 }
 
 // ---- separable path (broad 3-D kernels) -----------------------------------
-template <typename real>
-__global__ void k_indicator(int N, const int32_t* __restrict__ phi, int32_t p, real* __restrict__ I) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
-        I[i] = (phi[i] == p) ? (real)1 : (real)0;
+//
+// One periodic 1-D Gaussian pass (src/gpk_gaussian.cpp:9-72): every output is
+// acc = 0; acc += w[k] * in[wrap(q + k - R)] for k = 0 .. 2R, a multiply and
+// an add per tap in tap order (no contraction).  The tiled kernel stages a
+// tile of 32 lines x SEP_TL outputs plus the 2R halo in shared memory; each
+// thread then produces SEP_M consecutive outputs of one line from a ring of
+// SEP_M values in registers, so a tap costs one shared load per SEP_M
+// outputs.  Lines are the cells sharing the other two coordinates; the 32
+// lanes of a warp take 32 lines, so for the y and z passes every global load
+// and store is a 128-byte row of consecutive x.  For the x pass the lines are
+// rows of x: warps load and store whole rows (int4 label loads for the
+// indicator when the rows are whole tiles) and the shared rows are padded to
+// an odd length so that the 32 lanes, each walking its own row, hit 32 banks.
+// With IND the input is the indicator phi == p, formed as the labels load.
+static constexpr int SEP_TL = 64;       // outputs per line per tile
+static constexpr int SEP_M = 8;         // outputs per thread
+static constexpr int SEP_WARPS = SEP_TL / SEP_M;
+static constexpr int SEP_TPB = 32 * SEP_WARPS;
+
+__host__ __device__ __forceinline__ int sep_pitch(int axis, int R) {
+    // positions staged per line: the tile, its halo, and SEP_M of slack for
+    // the ring's last (unused) refill
+    const int p = SEP_TL + 2 * R + SEP_M;
+    return axis == 0 ? (p | 1) : p;
 }
 
-// one periodic 1-D pass along axis (0 = x, 1 = y, 2 = z)
+template <typename real, int AX, bool IND>
+__global__ void __launch_bounds__(SEP_TPB) k_sep_pass(Dims D, const real* __restrict__ in,
+                                                      const int32_t* __restrict__ phi, int32_t p,
+                                                      real* __restrict__ out, const real* __restrict__ kw, int R) {
+    extern __shared__ __align__(16) unsigned char sep_smem[];
+    real* tw = (real*)sep_smem;
+    const int K = 2 * R + 1;
+    const int Kp = (K + 1) & ~1;
+    real* s = tw + Kp;
+    const int n = AX == 0 ? D.Nx : (AX == 1 ? D.Ny : D.Nz);
+    const int nlines = AX == 0 ? D.Nz * D.Ny : (AX == 1 ? D.Nz * D.Nx : D.Ny * D.Nx);
+    const int stride = AX == 0 ? 1 : (AX == 1 ? D.Nx : D.Ny * D.Nx);
+    const int P = sep_pitch(AX, R);
+    const int segs = (n + SEP_TL - 1) / SEP_TL;
+    const int seg = blockIdx.x % segs;
+    const int lb = blockIdx.x / segs;
+    const int a0 = seg * SEP_TL;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    auto line_base = [&](int l) -> int {
+        if (AX == 0) return l * D.Nx;
+        if (AX == 1) return (l / D.Nx) * D.Ny * D.Nx + l % D.Nx;
+        return l;
+    };
+    auto load = [&](int gi) -> real {
+        if (IND) return phi[gi] == p ? (real)1 : (real)0;
+        return in[gi];
+    };
+    for (int k = threadIdx.x; k < K; k += SEP_TPB) tw[k] = kw[k];
+    const int span = SEP_TL + 2 * R;
+    if (AX == 0) {
+        // rows: warp w stages rows w, w + SEP_WARPS, ...; a lane's wrapped
+        // x for pos = lane + 32 i advances by 32 (mod n)
+        const bool vec = IND && (D.Nx % SEP_TL) == 0;
+        const int gw0 = wrap_any(a0 - R + lane, n);
+        for (int r = warp; r < 32; r += SEP_WARPS) {
+            const int l = lb * 32 + r;
+            if (l >= nlines) break;
+            const int b = line_base(l);
+            real* row = s + r * P;
+            if (vec) {
+                for (int c4 = lane; c4 < SEP_TL / 4; c4 += 32) {
+                    const int4 q = *reinterpret_cast<const int4*>(phi + b + a0 + 4 * c4);
+                    row[R + 4 * c4 + 0] = q.x == p ? (real)1 : (real)0;
+                    row[R + 4 * c4 + 1] = q.y == p ? (real)1 : (real)0;
+                    row[R + 4 * c4 + 2] = q.z == p ? (real)1 : (real)0;
+                    row[R + 4 * c4 + 3] = q.w == p ? (real)1 : (real)0;
+                }
+                for (int h = lane; h < 2 * R; h += 32) {
+                    const int pos = h < R ? h : SEP_TL + h;
+                    row[pos] = load(b + wrap_any(a0 - R + pos, n));
+                }
+            } else {
+                int gw = gw0;
+                for (int pos = lane; pos < span; pos += 32) {
+                    row[pos] = load(b + gw);
+                    for (gw += 32; gw >= n;) gw -= n;
+                }
+            }
+        }
+    } else {
+        const int l = lb * 32 + lane;
+        if (l < nlines) {
+            const int b = line_base(l);
+            int gw = wrap_any(a0 - R + warp, n);
+            for (int pos = warp; pos < span; pos += SEP_WARPS) {
+                s[pos * 32 + lane] = load(b + gw * stride);
+                for (gw += SEP_WARPS; gw >= n;) gw -= n;
+            }
+        }
+    }
+    __syncthreads();
+    const int o0 = warp * SEP_M;
+    auto S = [&](int j) -> real { return AX == 0 ? s[lane * P + j] : s[j * 32 + lane]; };
+    real v[SEP_M], acc[SEP_M];
+#pragma unroll
+    for (int m = 0; m < SEP_M; ++m) {
+        v[m] = S(o0 + m);
+        acc[m] = 0;
+    }
+    // ring: slot i holds position o0 + j with j == i (mod SEP_M); after tap
+    // kb + kk the value at o0 + kb + kk is dead and its slot takes the value
+    // SEP_M further on
+    for (int kb = 0; kb < K; kb += SEP_M) {
+#pragma unroll
+        for (int kk = 0; kk < SEP_M; ++kk) {
+            if (kb + kk < K) {
+                const real wk = tw[kb + kk];
+#pragma unroll
+                for (int m = 0; m < SEP_M; ++m) acc[m] += wk * v[(m + kk) % SEP_M];
+                v[kk] = S(o0 + kb + kk + SEP_M);
+            }
+        }
+    }
+    const int l = lb * 32 + lane;
+    if (AX == 0) {
+        // stage the outputs in the (now free) rows, then store whole rows
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < SEP_M; ++m) s[lane * P + o0 + m] = acc[m];
+        __syncthreads();
+        for (int r = warp; r < 32; r += SEP_WARPS) {
+            const int lr = lb * 32 + r;
+            if (lr >= nlines) break;
+            const int b = line_base(lr);
+            for (int pos = lane; pos < SEP_TL; pos += 32)
+                if (a0 + pos < n) out[b + a0 + pos] = s[r * P + pos];
+        }
+    } else if (l < nlines) {
+        const int b = line_base(l);
+#pragma unroll
+        for (int m = 0; m < SEP_M; ++m)
+            if (a0 + o0 + m < n) out[b + (a0 + o0 + m) * stride] = acc[m];
+    }
+}
+
+// Float x pass of an indicator with paired arithmetic.  The input is 0 or 1,
+// so every product w * v is exact and round(acc + w * v) is also what one
+// fused multiply-add gives: the pass may use fma.rn.f32x2 (two outputs per
+// instruction, a quarter of the scalar multiply + add issue count) and still
+// round exactly as the reference's multiply and add.  (For general inputs
+// the products are inexact; those passes keep the scalar k_sep_pass, whose
+// mul.rn / add.rn are not contracted.)  Each lane takes two rows, so a
+// block covers 64 rows x SEP_TL outputs; shared memory and registers hold
+// (row 2i, row 2i + 1) pairs as 64-bit words, row pitch odd in words so that
+// the lanes' 64-bit reads fall in distinct banks.
+typedef unsigned long long sep_u64;
+__device__ __forceinline__ sep_u64 f2_pack(float a, float b) {
+    return ((sep_u64)__float_as_uint(b) << 32) | (sep_u64)__float_as_uint(a);
+}
+__device__ __forceinline__ float f2_lo(sep_u64 v) { return __uint_as_float((unsigned)(v & 0xffffffffu)); }
+__device__ __forceinline__ float f2_hi(sep_u64 v) { return __uint_as_float((unsigned)(v >> 32)); }
+__device__ __forceinline__ sep_u64 f2_fma(sep_u64 w, sep_u64 v, sep_u64 acc) {
+    sep_u64 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(w), "l"(v), "l"(acc));
+    return r;
+}
+
+__global__ void __launch_bounds__(SEP_TPB) k_sep_x_indicator_f2(Dims D, const int32_t* __restrict__ phi, int32_t p,
+                                                                float* __restrict__ out,
+                                                                const float* __restrict__ kw, int R) {
+    extern __shared__ __align__(16) unsigned char sep_smem[];
+    sep_u64* tw = (sep_u64*)sep_smem;
+    const int K = 2 * R + 1;
+    sep_u64* s = tw + K;
+    const int n = D.Nx;
+    const int nlines = D.Nz * D.Ny;
+    const int P = sep_pitch(0, R);
+    const int segs = (n + SEP_TL - 1) / SEP_TL;
+    const int seg = blockIdx.x % segs;
+    const int lb = blockIdx.x / segs;
+    const int a0 = seg * SEP_TL;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    auto ind = [&](int v) -> float { return v == p ? 1.f : 0.f; };
+    for (int k = threadIdx.x; k < K; k += SEP_TPB) {
+        const float w = kw[k];
+        tw[k] = f2_pack(w, w);
+    }
+    const int span = SEP_TL + 2 * R;
+    // pair q holds rows 2q and 2q + 1 of the block's 64
+    if (n % SEP_TL == 0) {
+        // body: half a warp per pair, one int4 of labels per row and lane
+        const int c4 = lane & 15;
+        for (int q = warp * 2 + (lane >> 4); q < 32; q += SEP_WARPS * 2) {
+            const int l0 = lb * 64 + 2 * q;
+            if (l0 >= nlines) continue;
+            const int b0 = l0 * n;
+            const int4 x = *reinterpret_cast<const int4*>(phi + b0 + a0 + 4 * c4);
+            int4 y = make_int4(p + 1, p + 1, p + 1, p + 1);
+            if (l0 + 1 < nlines) y = *reinterpret_cast<const int4*>(phi + b0 + n + a0 + 4 * c4);
+            sep_u64* row = s + q * P + R + 4 * c4;
+            row[0] = f2_pack(ind(x.x), ind(y.x));
+            row[1] = f2_pack(ind(x.y), ind(y.y));
+            row[2] = f2_pack(ind(x.z), ind(y.z));
+            row[3] = f2_pack(ind(x.w), ind(y.w));
+        }
+        for (int q = warp; q < 32; q += SEP_WARPS) {
+            const int l0 = lb * 64 + 2 * q;
+            if (l0 >= nlines) break;
+            const int b0 = l0 * n;
+            const bool v1 = l0 + 1 < nlines;
+            for (int h = lane; h < 2 * R; h += 32) {
+                const int pos = h < R ? h : SEP_TL + h;
+                const int g = wrap_any(a0 - R + pos, n);
+                s[q * P + pos] = f2_pack(ind(phi[b0 + g]), v1 ? ind(phi[b0 + n + g]) : 0.f);
+            }
+        }
+    } else {
+        const int gw0 = wrap_any(a0 - R + lane, n);
+        for (int q = warp; q < 32; q += SEP_WARPS) {
+            const int l0 = lb * 64 + 2 * q;
+            if (l0 >= nlines) break;
+            const int b0 = l0 * n;
+            const bool v1 = l0 + 1 < nlines;
+            int gw = gw0;
+            for (int pos = lane; pos < span; pos += 32) {
+                s[q * P + pos] = f2_pack(ind(phi[b0 + gw]), v1 ? ind(phi[b0 + n + gw]) : 0.f);
+                for (gw += 32; gw >= n;) gw -= n;
+            }
+        }
+    }
+    __syncthreads();
+    const int o0 = warp * SEP_M;
+    sep_u64 v[SEP_M], acc[SEP_M];
+#pragma unroll
+    for (int m = 0; m < SEP_M; ++m) {
+        v[m] = s[lane * P + o0 + m];
+        acc[m] = 0ull;  // (+0, +0)
+    }
+    for (int kb = 0; kb < K; kb += SEP_M) {
+#pragma unroll
+        for (int kk = 0; kk < SEP_M; ++kk) {
+            if (kb + kk < K) {
+                const sep_u64 wk = tw[kb + kk];
+#pragma unroll
+                for (int m = 0; m < SEP_M; ++m) acc[m] = f2_fma(wk, v[(m + kk) % SEP_M], acc[m]);
+                v[kk] = s[lane * P + o0 + kb + kk + SEP_M];
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < SEP_M; ++m) s[lane * P + o0 + m] = acc[m];
+    __syncthreads();
+    for (int q = warp; q < 32; q += SEP_WARPS) {
+        const int l0 = lb * 64 + 2 * q;
+        if (l0 >= nlines) break;
+        const int b0 = l0 * n;
+        const bool v1 = l0 + 1 < nlines;
+        for (int pos = lane; pos < SEP_TL; pos += 32) {
+            if (a0 + pos >= n) break;
+            const sep_u64 r = s[q * P + pos];
+            out[b0 + a0 + pos] = f2_lo(r);
+            if (v1) out[b0 + n + a0 + pos] = f2_hi(r);
+        }
+    }
+}
+
+// one periodic 1-D pass along axis (0 = x, 1 = y, 2 = z), one thread per
+// output, taps from global memory: the form for radii whose tile does not fit
+// in shared memory
 template <typename real>
 __global__ void k_gauss_pass(Dims D, const real* __restrict__ in, real* __restrict__ out, const real* __restrict__ kw,
                              int krad, int axis) {
@@ -270,16 +529,20 @@ __global__ void k_gauss_pass(Dims D, const real* __restrict__ in, real* __restri
 }
 
 template <typename real>
-__global__ void k_separable_eval(Dims D, const int32_t* __restrict__ phi, const uint8_t* __restrict__ mask, int32_t p,
-                                 const real* __restrict__ S, real dx, real kappa_limit, real* __restrict__ nxo,
-                                 real* __restrict__ nyo, real* __restrict__ nzo, real* __restrict__ ko) {
+__global__ void k_separable_eval(Dims D, const int32_t* __restrict__ active, const unsigned* __restrict__ n_active,
+                                 const int32_t* __restrict__ phi, int32_t p, const real* __restrict__ S, real dx,
+                                 real kappa_limit, real* __restrict__ nxo, real* __restrict__ nyo,
+                                 real* __restrict__ nzo, real* __restrict__ ko) {
     const int Nx = D.Nx, Ny = D.Ny, Nz = D.Nz;
     const real idx12 = (real)1 / ((real)12 * dx);
     const real idx_sq = (real)1 / (dx * dx);
     const real idx12_sq = idx_sq / (real)12;
     const real idx144_sq = idx_sq / (real)144;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.N; i += gridDim.x * blockDim.x) {
-        if (!mask[i] || phi[i] != p) continue;
+    // the interface cells of label p, from the ordered interface list
+    const int na = (int)*n_active;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
+        const int i = active[a];
+        if (phi[i] != p) continue;
         int z, y, x;
         D.decode(i, z, y, x);
         const int xm = (x == 0 ? Nx - 1 : x - 1), xp = (x == Nx - 1 ? 0 : x + 1);
@@ -797,45 +1060,52 @@ __device__ __forceinline__ int faces_transport(const Dims& D, int i, int nb[6]) 
     return nn;
 }
 
-// per-source rejected solute q and liquid weight sum (0 when it rejects nothing)
+// The rejection of source i (src/gpk_transport.cpp:64-88) with the
+// reference's tests in its own form (a NaN passes them as it does there):
+// false when i rejects nothing, else its solute q and liquid weight sum.
 template <typename real>
-__global__ void k_rejection_source(Dims D, const int32_t* __restrict__ phi, const real* __restrict__ c,
-                                   const real* __restrict__ s_old, const real* __restrict__ s_new, real k,
-                                   real* __restrict__ q_out, real* __restrict__ wsum_out) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.N; i += gridDim.x * blockDim.x) {
-        real qv = 0, wsum = 0;
-        const real ds = s_new[i] - s_old[i];
-        if (ds > (real)0) {
-            const real s0 = dclamp(s_old[i], (real)0, (real)1);
-            const real cL = c[i] / dmax((real)1 - s0 * ((real)1 - k), (real)1e-6);
-            real q = ((real)1 - k) * cL * dmin(ds, (real)1);
-            q = dmin(q, c[i]);
-            if (q > (real)0) {
-                int nb[6];
-                const int nn = faces_transport(D, i, nb);
-                for (int a = 0; a < nn; ++a) {
-                    const int j = nb[a];
-                    const real w = (phi[j] == 0) ? dmax((real)1 - s_new[j], (real)0) : (real)0;
-                    wsum += w;
-                }
-                if (wsum > (real)0) qv = q;
-            }
-        }
-        q_out[i] = qv;
-        wsum_out[i] = wsum;
+__device__ __forceinline__ bool rejection_at(const Dims& D, const int32_t* __restrict__ phi,
+                                             const real* __restrict__ c, const real* __restrict__ s_old,
+                                             const real* __restrict__ s_new, real k, int i, real& q, real& wsum) {
+    const real ds = s_new[i] - s_old[i];
+    if (ds <= (real)0) return false;
+    const real s0 = dclamp(s_old[i], (real)0, (real)1);
+    const real cL = c[i] / dmax((real)1 - s0 * ((real)1 - k), (real)1e-6);
+    q = ((real)1 - k) * cL * dmin(ds, (real)1);
+    q = dmin(q, c[i]);
+    if (q <= (real)0) return false;
+    int nb[6];
+    const int nn = faces_transport(D, i, nb);
+    wsum = 0;
+    for (int a = 0; a < nn; ++a) {
+        const int j = nb[a];
+        const real w = (phi[j] == 0) ? dmax((real)1 - s_new[j], (real)0) : (real)0;
+        wsum += w;
     }
+    return !(wsum <= (real)0);
 }
 
-// gathers delta[j] in the reference's scatter order (increasing source index,
-// then neighbour slot) and applies c += delta
+// c_out = c + delta, delta gathered per cell in the reference's scatter
+// order (increasing source index, then neighbour slot; src/gpk_transport.cpp:
+// 89-96).  The sources of cell j are j and its face neighbours; a cell none
+// of which grew (the common case) only copies c (c + 0).  Out of place: the
+// sources' q reads the pre-rejection c of cells that other threads update.
 template <typename real>
-__global__ void k_rejection_gather(Dims D, const int32_t* __restrict__ phi, const real* __restrict__ s_new,
-                                   const real* __restrict__ q, const real* __restrict__ wsum, real* __restrict__ c) {
+__global__ void k_rejection(Dims D, const int32_t* __restrict__ phi, const real* __restrict__ s_old,
+                            const real* __restrict__ s_new, real k, const real* __restrict__ c,
+                            real* __restrict__ c_out) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < D.N; j += gridDim.x * blockDim.x) {
-        int src[7];
-        int ns = 0;
         int nbj[6];
         const int nn = faces_transport(D, j, nbj);
+        bool any = !(s_new[j] - s_old[j] <= (real)0);
+        for (int a = 0; a < nn; ++a) any |= !(s_new[nbj[a]] - s_old[nbj[a]] <= (real)0);
+        const real cj = c[j];
+        if (!any) {
+            c_out[j] = cj + (real)0;
+            continue;
+        }
+        int src[7];
+        int ns = 0;
         src[ns++] = j;
         for (int a = 0; a < nn; ++a) {
             bool dup = false;
@@ -848,47 +1118,108 @@ __global__ void k_rejection_gather(Dims D, const int32_t* __restrict__ phi, cons
             while (b >= 0 && src[b] > v) { src[b + 1] = src[b]; --b; }
             src[b + 1] = v;
         }
+        const real wj = (phi[j] == 0) ? dmax((real)1 - s_new[j], (real)0) : (real)0;
         real delta = 0;
         for (int t = 0; t < ns; ++t) {
             const int sidx = src[t];
-            const real qs = q[sidx];
-            if (!(qs > (real)0)) continue;
-            if (sidx == j) delta -= qs;
+            real q, wsum;
+            if (!rejection_at<real>(D, phi, c, s_old, s_new, k, sidx, q, wsum)) continue;
+            if (sidx == j) delta -= q;
             int nbs[6];
             const int ms = faces_transport(D, sidx, nbs);
-            for (int a = 0; a < ms; ++a) {
-                if (nbs[a] != j) continue;
-                const real w = (phi[j] == 0) ? dmax((real)1 - s_new[j], (real)0) : (real)0;
-                if (w > (real)0) delta += qs * w / wsum[sidx];
-            }
+            for (int a = 0; a < ms; ++a)
+                if (nbs[a] == j && wj > (real)0) delta += q * wj / wsum;
         }
-        c[j] += delta;
+        c_out[j] = cj + delta;
     }
 }
 
-template <typename real>
-__global__ void k_liquid_comp(int N, const real* __restrict__ c, const real* __restrict__ s, real k, real* __restrict__ cL) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
-        cL[i] = c[i] / dmax((real)1 - s[i] * ((real)1 - k), (real)1e-6);
-}
+// Partitioned diffusion (src/gpk_transport.cpp:101-135) with the liquid
+// composition cL = c / max(1 - s (1 - k), 1e-6) formed as the tile loads c
+// and s (each cell once, plus a one-cell ring per plane) instead of being
+// stored and re-read.  A 32 x 8 block marches zc planes along z with the
+// column's s and cL at z - 1, z, z + 1 in registers and the plane's tile in
+// shared memory; each cell's flux sums its faces in the reference's order
+// x+, x-, y+, y-, z+, z-.
+static constexpr int PDX = 32, PDY = 8;
 
 template <typename real>
-__global__ void k_diffusion_partitioned(Dims D, const real* __restrict__ c, const real* __restrict__ s,
-                                        const real* __restrict__ cL, real* __restrict__ c_new, real Dc,
-                                        const StepScalars* st, real dx) {
+__global__ void __launch_bounds__(PDX * PDY) k_diffusion_partitioned_tiled(Dims D, const real* __restrict__ c,
+                                                                           const real* __restrict__ s,
+                                                                           real* __restrict__ c_new, real Dc, real k,
+                                                                           const StepScalars* st, real dx, int zc) {
+    __shared__ real ts[PDY + 2][PDX + 2];
+    __shared__ real tl[PDY + 2][PDX + 2];
+    const int Nx = D.Nx, Ny = D.Ny, Nz = D.Nz;
     const real dt = (real)st->dt;
     const real coef = dt * Dc / (dx * dx);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < D.N; i += gridDim.x * blockDim.x) {
-        int nb[6];
-        const int nn = faces_transport(D, i, nb);
-        const real li = (real)1 - s[i];
-        real flux = 0;
-        for (int a = 0; a < nn; ++a) {
-            const int j = nb[a];
-            const real lf = dmin(li, (real)1 - s[j]);
-            if (lf > (real)0) flux += lf * (cL[j] - cL[i]);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * PDX + tx;
+    const int xs = blockIdx.x * PDX, ys = blockIdx.y * PDY;
+    const bool valid = xs + tx < Nx && ys + ty < Ny;
+    const int ox = (xs + tx) % Nx, oy = (ys + ty) % Ny;  // own column (wrapped for idle threads)
+    const int plane = Ny * Nx;
+    const int col = oy * Nx + ox;
+    const bool is3 = Nz > 1;
+    auto liquid = [&](real cv, real sv) -> real { return cv / dmax((real)1 - sv * ((real)1 - k), (real)1e-6); };
+    const int z0 = blockIdx.z * zc;
+    const int z1 = z0 + zc < Nz ? z0 + zc : Nz;
+    real s_prev = 0, l_prev = 0, s_next = 0, l_next = 0, c_next = 0;
+    if (is3) {
+        const int zp = z0 == 0 ? Nz - 1 : z0 - 1;
+        s_prev = s[zp * plane + col];
+        l_prev = liquid(c[zp * plane + col], s_prev);
+    }
+    real c_cur = c[z0 * plane + col];
+    real s_cur = s[z0 * plane + col];
+    real l_cur = liquid(c_cur, s_cur);
+    for (int z = z0; z < z1; ++z) {
+        if (is3) {
+            const int zn = z + 1 == Nz ? 0 : z + 1;
+            c_next = c[zn * plane + col];
+            s_next = s[zn * plane + col];
+            l_next = liquid(c_next, s_next);
         }
-        c_new[i] = c[i] + coef * flux;
+        ts[ty + 1][tx + 1] = s_cur;
+        tl[ty + 1][tx + 1] = l_cur;
+        constexpr int HALO = 2 * (PDX + 2) + 2 * PDY;
+        for (int h = tid; h < HALO; h += PDX * PDY) {
+            int ly, lx;
+            if (h < PDX + 2) { ly = -1; lx = h - 1; }
+            else if (h < 2 * (PDX + 2)) { ly = PDY; lx = h - (PDX + 2) - 1; }
+            else if (h < 2 * (PDX + 2) + PDY) { ly = h - 2 * (PDX + 2); lx = -1; }
+            else { ly = h - 2 * (PDX + 2) - PDY; lx = PDX; }
+            int gy = ys + ly, gx = xs + lx;
+            if (gy < 0) gy += Ny;
+            while (gy >= Ny) gy -= Ny;  // at most PDY + 1 times
+            if (gx < 0) gx += Nx;
+            while (gx >= Nx) gx -= Nx;  // at most PDX + 1 times
+            const int q = z * plane + gy * Nx + gx;
+            const real sh = s[q];
+            ts[ly + 1][lx + 1] = sh;
+            tl[ly + 1][lx + 1] = liquid(c[q], sh);
+        }
+        __syncthreads();
+        const real li = (real)1 - s_cur;
+        real flux = 0;
+        auto face = [&](real sj, real lj) {
+            const real lf = dmin(li, (real)1 - sj);
+            if (lf > (real)0) flux += lf * (lj - l_cur);
+        };
+        face(ts[ty + 1][tx + 2], tl[ty + 1][tx + 2]);  // x+
+        face(ts[ty + 1][tx], tl[ty + 1][tx]);          // x-
+        face(ts[ty + 2][tx + 1], tl[ty + 2][tx + 1]);  // y+
+        face(ts[ty][tx + 1], tl[ty][tx + 1]);          // y-
+        if (is3) {
+            face(s_next, l_next);  // z+
+            face(s_prev, l_prev);  // z-
+        }
+        if (valid) c_new[z * plane + col] = c_cur + coef * flux;
+        __syncthreads();  // the next plane rewrites the tile
+        s_prev = s_cur;
+        l_prev = l_cur;
+        s_cur = s_next;
+        l_cur = l_next;
+        c_cur = c_next;
     }
 }
 
@@ -918,6 +1249,94 @@ static inline int grid_for(gpk_grid* G, long long n, int block = 256) {
     if (b > cap) b = cap;
     if (b < 1) b = 1;
     return (int)b;
+}
+
+template <typename real>
+__global__ void k_indicator(int N, const int32_t* __restrict__ phi, int32_t p, real* __restrict__ I) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        I[i] = (phi[i] == p) ? (real)1 : (real)0;
+}
+
+// Shared memory of one tiled pass (word: bytes per staged value), or 0 when
+// its tile does not fit.
+static size_t sep_smem_bytes(size_t word, int axis, int R) {
+    static int optin = -1;
+    if (optin < 0) {
+        int dev = 0, v = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+            v = 48 * 1024;
+        optin = v;
+    }
+    const size_t b = word * ((size_t)(2 * R + 2) + 32 * (size_t)sep_pitch(axis, R));
+    return b <= (size_t)optin ? b : 0;
+}
+
+template <typename real, int AX, bool IND>
+static cudaError_t sep_launch(const Dims& D, const real* in, const int32_t* phi, int32_t p, real* out, const real* taps,
+                              int R, size_t bytes, cudaStream_t st) {
+    const int n = AX == 0 ? D.Nx : (AX == 1 ? D.Ny : D.Nz);
+    const int segs = (n + SEP_TL - 1) / SEP_TL;
+    if constexpr (sizeof(real) == 4 && AX == 0 && IND) {
+        if (bytes > 48 * 1024) {
+            const cudaError_t e = cudaFuncSetAttribute(k_sep_x_indicator_f2,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+            if (e != cudaSuccess) return e;
+        }
+        const long long blocks = (long long)((D.N / n + 63) / 64) * segs;
+        k_sep_x_indicator_f2<<<(unsigned)blocks, SEP_TPB, bytes, st>>>(D, phi, p, (float*)out, (const float*)taps, R);
+    } else {
+        if (bytes > 48 * 1024) {
+            const cudaError_t e = cudaFuncSetAttribute(k_sep_pass<real, AX, IND>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+            if (e != cudaSuccess) return e;
+        }
+        const long long blocks = (long long)((D.N / n + 31) / 32) * segs;
+        k_sep_pass<real, AX, IND><<<(unsigned)blocks, SEP_TPB, bytes, st>>>(D, in, phi, p, out, taps, R);
+    }
+    return cudaGetLastError();
+}
+
+// The periodic Gaussian of in (or, with phi, of the indicator phi == p)
+// along x (into t1), y (into t2, or out when 2-D) and, in 3-D, z (into out);
+// in may serve as t2, out may not be t1.  Tiled passes where their tiles fit in shared memory, else
+// the one-thread-per-output form.  Returns the number of launches, or -1
+// with the CUDA error in *err.
+template <typename real>
+static int sep_gauss3(const Dims& D, const real* in, const int32_t* phi, int32_t p, real* t1, real* t2, real* out,
+                      real* ind_scratch, const real* taps, int R, int fallback_grid, cudaStream_t st,
+                      cudaError_t* err) {
+    // the float indicator pass stages 8-byte row pairs
+    const size_t b0 = sep_smem_bytes(phi && sizeof(real) == 4 ? 8 : sizeof(real), 0, R);
+    const size_t b1 = sep_smem_bytes(sizeof(real), 1, R), b2 = sep_smem_bytes(sizeof(real), 2, R);
+    int launches = 0;
+    cudaError_t e = cudaSuccess;
+    if (b0 && b1 && b2) {
+        e = phi ? sep_launch<real, 0, true>(D, nullptr, phi, p, t1, taps, R, b0, st)
+                : sep_launch<real, 0, false>(D, in, nullptr, 0, t1, taps, R, b0, st);
+        if (e == cudaSuccess) e = sep_launch<real, 1, false>(D, t1, nullptr, 0, D.Nz > 1 ? t2 : out, taps, R, b1, st);
+        launches = 2;
+        if (e == cudaSuccess && D.Nz > 1) {
+            e = sep_launch<real, 2, false>(D, t2, nullptr, 0, out, taps, R, b2, st);
+            ++launches;
+        }
+    } else {
+        if (phi) {
+            k_indicator<real><<<fallback_grid, 256, 0, st>>>(D.N, phi, p, ind_scratch);
+            in = ind_scratch;
+            ++launches;
+        }
+        k_gauss_pass<real><<<fallback_grid, 256, 0, st>>>(D, in, t1, taps, R, 0);
+        k_gauss_pass<real><<<fallback_grid, 256, 0, st>>>(D, t1, D.Nz > 1 ? t2 : out, taps, R, 1);
+        launches += 2;
+        if (D.Nz > 1) {
+            k_gauss_pass<real><<<fallback_grid, 256, 0, st>>>(D, t2, out, taps, R, 2);
+            ++launches;
+        }
+        e = cudaGetLastError();
+    }
+    *err = e;
+    return e == cudaSuccess ? launches : -1;
 }
 
 // mask + sorted interface list (src/gpk_geometry.cpp:42-82)
@@ -977,16 +1396,13 @@ static int geometry(gpk_grid* G) {
     const int gN = grid_for(G, D.N);
     for (int p = 0; p < G->label_cap; ++p) {
         if (!hp[p]) continue;
-        k_indicator<real><<<gN, 256, 0, G->stream>>>(D.N, G->phi, p, (real*)G->sep_I);
-        k_gauss_pass<real><<<gN, 256, 0, G->stream>>>(D, (const real*)G->sep_I, (real*)G->sep_t1, (const real*)G->d_gauss,
-                                                      hk->gauss_radius, 0);
-        k_gauss_pass<real><<<gN, 256, 0, G->stream>>>(D, (const real*)G->sep_t1, (real*)G->sep_t2,
-                                                      (const real*)G->d_gauss, hk->gauss_radius, 1);
-        k_gauss_pass<real><<<gN, 256, 0, G->stream>>>(D, (const real*)G->sep_t2, (real*)G->sep_S, (const real*)G->d_gauss,
-                                                      hk->gauss_radius, 2);
-        k_separable_eval<real><<<gN, 256, 0, G->stream>>>(D, G->phi, G->mask, p, (const real*)G->sep_S, dx, kappa_limit,
-                                                          nx, ny, nz, kp);
-        G->launches += 5;
+        cudaError_t ce = cudaSuccess;
+        const int nl = sep_gauss3<real>(D, nullptr, G->phi, p, (real*)G->sep_t1, (real*)G->sep_t2, (real*)G->sep_S,
+                                        (real*)G->sep_I, (const real*)G->d_gauss, hk->gauss_radius, gN, G->stream, &ce);
+        GPK_CUDA_TRY(ce);
+        k_separable_eval<real><<<gN, 256, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, p,
+                                                          (const real*)G->sep_S, dx, kappa_limit, nx, ny, nz, kp);
+        G->launches += nl + 1;
     }
     k_competitor_all<real><<<grid_for(G, D.N), 256, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, nx, ny,
                                                                      nz, G->phi_comp);
@@ -1044,26 +1460,28 @@ static int transport(gpk_grid* G) {
     const int gN = grid_for(G, D.N);
     if (th.solute_rejection) {
         const real k = (real)th.k_partition;
-        if (k < (real)1 && G->have_solid_old) {
-            k_solid_fraction<real><<<gN, 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
-                                                              (real*)G->s_new);
-            k_rejection_source<real><<<gN, 256, 0, G->stream>>>(D, G->phi, (const real*)G->f[GPK_FIELD_C],
-                                                                 (const real*)G->solid_old, (const real*)G->s_new, k,
-                                                                 (real*)G->delta, (real*)G->cL);
-            k_rejection_gather<real><<<gN, 256, 0, G->stream>>>(D, G->phi, (const real*)G->s_new, (const real*)G->delta,
-                                                                (const real*)G->cL, (real*)G->f[GPK_FIELD_C]);
-            G->launches += 3;
+        const bool rejected = k < (real)1 && G->have_solid_old;
+        if (!rejected && !(Dc > (real)0)) return GPK_OK;
+        k_solid_fraction<real><<<gN, 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
+                                                          (real*)G->s_new);
+        G->launches++;
+        if (rejected) {
+            k_rejection<real><<<gN, 256, 0, G->stream>>>(D, G->phi, (const real*)G->solid_old, (const real*)G->s_new,
+                                                         k, (const real*)G->f[GPK_FIELD_C], (real*)G->c_new);
+            std::swap(G->f[GPK_FIELD_C], G->c_new);
+            G->launches++;
         }
         if (Dc > (real)0) {
-            k_solid_fraction<real><<<gN, 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
-                                                              (real*)G->s_new);
-            k_liquid_comp<real><<<gN, 256, 0, G->stream>>>(D.N, (const real*)G->f[GPK_FIELD_C], (const real*)G->s_new,
-                                                           (real)th.k_partition, (real*)G->cL);
-            k_diffusion_partitioned<real><<<gN, 256, 0, G->stream>>>(D, (const real*)G->f[GPK_FIELD_C],
-                                                                     (const real*)G->s_new, (const real*)G->cL,
-                                                                     (real*)G->c_new, Dc, G->scal, dx);
+            // about 16 blocks per SM over the z chunks, at most 16 planes each
+            const int bx = (D.Nx + PDX - 1) / PDX, by = (D.Ny + PDY - 1) / PDY;
+            long long zc = ((long long)D.Nz * bx * by + G->num_sms * 16 - 1) / ((long long)G->num_sms * 16);
+            zc = std::max(1LL, std::min(zc, 16LL));
+            const dim3 tg(bx, by, (unsigned)((D.Nz + zc - 1) / zc));
+            k_diffusion_partitioned_tiled<real><<<tg, dim3(PDX, PDY), 0, G->stream>>>(
+                D, (const real*)G->f[GPK_FIELD_C], (const real*)G->s_new, (real*)G->c_new, Dc, k, G->scal, dx,
+                (int)zc);
             std::swap(G->f[GPK_FIELD_C], G->c_new);
-            G->launches += 3;
+            G->launches++;
         }
     } else if (Dc > (real)0) {
         k_diffusion<real><<<gN, 256, 0, G->stream>>>(D, (const real*)G->f[GPK_FIELD_C], (real*)G->c_new, G->mask,
@@ -1175,8 +1593,6 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
         if (!G->solid_old) {
             GPK_TRY(gpk_alloc(G, &G->solid_old, G->rsz * D.N));
             GPK_TRY(gpk_alloc(G, &G->s_new, G->rsz * D.N));
-            GPK_TRY(gpk_alloc(G, &G->delta, G->rsz * D.N));
-            GPK_TRY(gpk_alloc(G, &G->cL, G->rsz * D.N));
         }
         k_solid_fraction<real><<<grid_for(G, D.N), 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
                                                                          (real*)G->solid_old);
@@ -1319,14 +1735,10 @@ extern "C" int gpk_gaussian_filter_3d(const float* in, float* out, int Nz, int N
     if (cudaMemcpyAsync(a, in, nb, cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(w, taps, sizeof(float) * (2 * radius + 1), cudaMemcpyHostToDevice, st) != cudaSuccess)
         return done(GPK_ERR_CUDA);
-    k_gauss_pass<float><<<grid, 256, 0, st>>>(D, a, b, w, radius, 0);
-    k_gauss_pass<float><<<grid, 256, 0, st>>>(D, b, a, w, radius, 1);
-    float* res = a;
-    if (Nz > 1) {
-        k_gauss_pass<float><<<grid, 256, 0, st>>>(D, a, b, w, radius, 2);
-        res = b;
-    }
-    if (cudaGetLastError() != cudaSuccess || cudaMemcpyAsync(out, res, nb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    float* res = Nz > 1 ? b : a;
+    cudaError_t ce = cudaSuccess;
+    sep_gauss3<float>(D, a, nullptr, 0, b, a, res, nullptr, w, radius, grid, st, &ce);
+    if (ce != cudaSuccess || cudaMemcpyAsync(out, res, nb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
         gpk_set_error("gpk_gaussian_filter_3d: CUDA failure");
         rc = GPK_ERR_CUDA;
@@ -1425,14 +1837,10 @@ extern "C" int gpk_gaussian_filter_3d_noalloc(const float* in, float* out, int N
     GPK_CUDA_TRY(cudaMemcpy(w, taps, sizeof(float) * (2 * radius + 1), cudaMemcpyHostToDevice));
     GPK_CUDA_TRY(cudaMemcpy(a, in, nb, cudaMemcpyHostToDevice));
     const int grid = std::min((D.N + 255) / 256, 148 * 8);
-    k_gauss_pass<float><<<grid, 256>>>(D, a, b, w, radius, 0);
-    k_gauss_pass<float><<<grid, 256>>>(D, b, a, w, radius, 1);
-    float* res = a;
-    if (Nz > 1) {
-        k_gauss_pass<float><<<grid, 256>>>(D, a, b, w, radius, 2);
-        res = b;
-    }
-    GPK_CUDA_TRY(cudaGetLastError());
+    float* res = Nz > 1 ? b : a;
+    cudaError_t ce = cudaSuccess;
+    sep_gauss3<float>(D, a, nullptr, 0, b, a, res, nullptr, w, radius, grid, 0, &ce);
+    GPK_CUDA_TRY(ce);
     GPK_CUDA_TRY(cudaMemcpy(out, res, nb, cudaMemcpyDeviceToHost));
     return GPK_OK;
 }
