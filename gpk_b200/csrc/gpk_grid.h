@@ -66,7 +66,7 @@ struct gpk_grid {
     void* vn2 = nullptr;                   // projection output before swap
     void* c_new = nullptr;
     void* eps_star = nullptr; void* eps_smooth = nullptr; void* eps_tmp = nullptr;
-    void* solid_old = nullptr; void* s_new = nullptr;
+    void* solid_old = nullptr; void* s_new = nullptr; uint8_t* grew = nullptr;
     int have_solid_old = 0;
     int32_t* active = nullptr;             // sorted interface cells
     int32_t* tile_off = nullptr;           // compaction tile offsets

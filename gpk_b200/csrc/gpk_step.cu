@@ -351,18 +351,25 @@ __global__ void __launch_bounds__(SEP_TPB) k_sep_pass(Dims D, const real* __rest
     }
     // ring: slot i holds position o0 + j with j == i (mod SEP_M); after tap
     // kb + kk the value at o0 + kb + kk is dead and its slot takes the value
-    // SEP_M further on
-    for (int kb = 0; kb < K; kb += SEP_M) {
-#pragma unroll
-        for (int kk = 0; kk < SEP_M; ++kk) {
-            if (kb + kk < K) {
-                const real wk = tw[kb + kk];
-#pragma unroll
-                for (int m = 0; m < SEP_M; ++m) acc[m] += wk * v[(m + kk) % SEP_M];
-                v[kk] = S(o0 + kb + kk + SEP_M);
-            }
-        }
+    // SEP_M further on.  Whole chunks of SEP_M taps run without guards, the
+    // last partial chunk with them.
+#define SEP_TAP(kk)                                                              \
+    {                                                                            \
+        const real wk = tw[kb + (kk)];                                           \
+        _Pragma("unroll") for (int m = 0; m < SEP_M; ++m) acc[m] += wk * v[(m + (kk)) % SEP_M]; \
+        v[(kk)] = S(o0 + kb + (kk) + SEP_M);                                     \
     }
+    int kb = 0;
+    for (; kb + SEP_M <= K; kb += SEP_M) {
+#pragma unroll
+        for (int kk = 0; kk < SEP_M; ++kk) SEP_TAP(kk)
+    }
+    if (kb < K) {
+#pragma unroll
+        for (int kk = 0; kk < SEP_M; ++kk)
+            if (kb + kk < K) SEP_TAP(kk)
+    }
+#undef SEP_TAP
     const int l = lb * 32 + lane;
     if (AX == 0) {
         // stage the outputs in the (now free) rows, then store whole rows
@@ -478,17 +485,24 @@ __global__ void __launch_bounds__(SEP_TPB) k_sep_x_indicator_f2(Dims D, const in
         v[m] = s[lane * P + o0 + m];
         acc[m] = 0ull;  // (+0, +0)
     }
-    for (int kb = 0; kb < K; kb += SEP_M) {
-#pragma unroll
-        for (int kk = 0; kk < SEP_M; ++kk) {
-            if (kb + kk < K) {
-                const sep_u64 wk = tw[kb + kk];
-#pragma unroll
-                for (int m = 0; m < SEP_M; ++m) acc[m] = f2_fma(wk, v[(m + kk) % SEP_M], acc[m]);
-                v[kk] = s[lane * P + o0 + kb + kk + SEP_M];
-            }
-        }
+    const sep_u64* sl = s + lane * P + o0;
+#define SEP_TAP2(kk)                                                                            \
+    {                                                                                           \
+        const sep_u64 wk = tw[kb + (kk)];                                                       \
+        _Pragma("unroll") for (int m = 0; m < SEP_M; ++m) acc[m] = f2_fma(wk, v[(m + (kk)) % SEP_M], acc[m]); \
+        v[(kk)] = sl[kb + (kk) + SEP_M];                                                        \
     }
+    int kb = 0;
+    for (; kb + SEP_M <= K; kb += SEP_M) {
+#pragma unroll
+        for (int kk = 0; kk < SEP_M; ++kk) SEP_TAP2(kk)
+    }
+    if (kb < K) {
+#pragma unroll
+        for (int kk = 0; kk < SEP_M; ++kk)
+            if (kb + kk < K) SEP_TAP2(kk)
+    }
+#undef SEP_TAP2
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < SEP_M; ++m) s[lane * P + o0 + m] = acc[m];
@@ -1090,20 +1104,39 @@ __device__ __forceinline__ bool rejection_at(const Dims& D, const int32_t* __res
 // 89-96).  The sources of cell j are j and its face neighbours; a cell none
 // of which grew (the common case) only copies c (c + 0).  Out of place: the
 // sources' q reads the pre-rejection c of cells that other threads update.
+// One block row of 128 x per (y, z): grid (ceil(Nx / 128) * Ny, Nz).
+static constexpr int REJ_TPB = 128;
+
 template <typename real>
-__global__ void k_rejection(Dims D, const int32_t* __restrict__ phi, const real* __restrict__ s_old,
-                            const real* __restrict__ s_new, real k, const real* __restrict__ c,
-                            real* __restrict__ c_out) {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < D.N; j += gridDim.x * blockDim.x) {
-        int nbj[6];
-        const int nn = faces_transport(D, j, nbj);
-        bool any = !(s_new[j] - s_old[j] <= (real)0);
-        for (int a = 0; a < nn; ++a) any |= !(s_new[nbj[a]] - s_old[nbj[a]] <= (real)0);
+__global__ void __launch_bounds__(REJ_TPB) k_rejection(Dims D, const int32_t* __restrict__ phi,
+                                                       const real* __restrict__ s_old, const real* __restrict__ s_new,
+                                                       const uint8_t* __restrict__ grew, real k,
+                                                       const real* __restrict__ c, real* __restrict__ c_out) {
+    const int Nx = D.Nx, Ny = D.Ny, Nz = D.Nz;
+    const int nxb = (Nx + REJ_TPB - 1) / REJ_TPB;
+    const int y = blockIdx.x / nxb;
+    const int x = (blockIdx.x - y * nxb) * REJ_TPB + threadIdx.x;
+    const int z = blockIdx.y;
+    if (x >= Nx) return;
+    const int j = (z * Ny + y) * Nx + x;
+    {
+        const int row = j - x, pl = z * Ny * Nx;
+        int any = grew[j] | grew[row + (x == Nx - 1 ? 0 : x + 1)] | grew[row + (x == 0 ? Nx - 1 : x - 1)] |
+                  grew[pl + (y == Ny - 1 ? 0 : y + 1) * Nx + x] | grew[pl + (y == 0 ? Ny - 1 : y - 1) * Nx + x];
+        if (Nz > 1) {
+            const int col = y * Nx + x, plane = Ny * Nx;
+            any |= grew[(z == Nz - 1 ? 0 : z + 1) * plane + col] | grew[(z == 0 ? Nz - 1 : z - 1) * plane + col];
+        }
         const real cj = c[j];
         if (!any) {
             c_out[j] = cj + (real)0;
-            continue;
+            return;
         }
+    }
+    {
+        int nbj[6];
+        const int nn = faces_transport(D, j, nbj);
+        const real cj = c[j];
         int src[7];
         int ns = 0;
         src[ns++] = j;
@@ -1131,6 +1164,19 @@ __global__ void k_rejection(Dims D, const int32_t* __restrict__ phi, const real*
                 if (nbs[a] == j && wj > (real)0) delta += q * wj / wsum;
         }
         c_out[j] = cj + delta;
+    }
+}
+
+// s = the solid fraction of the labels; grew = s - s_old passes the
+// reference's "ds <= 0 rejects nothing" test (a NaN passes it)
+template <typename real>
+__global__ void k_solid_fraction_grew(int N, const int32_t* __restrict__ phi, const real* __restrict__ alpha,
+                                      const real* __restrict__ s_old, real* __restrict__ s,
+                                      uint8_t* __restrict__ grew) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const real sv = (phi[i] != 0) ? alpha[i] : (real)1 - alpha[i];
+        s[i] = sv;
+        grew[i] = !(sv - s_old[i] <= (real)0);
     }
 }
 
@@ -1462,12 +1508,19 @@ static int transport(gpk_grid* G) {
         const real k = (real)th.k_partition;
         const bool rejected = k < (real)1 && G->have_solid_old;
         if (!rejected && !(Dc > (real)0)) return GPK_OK;
-        k_solid_fraction<real><<<gN, 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
-                                                          (real*)G->s_new);
+        if (rejected)
+            k_solid_fraction_grew<real><<<gN, 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
+                                                                   (const real*)G->solid_old, (real*)G->s_new,
+                                                                   G->grew);
+        else
+            k_solid_fraction<real><<<gN, 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
+                                                              (real*)G->s_new);
         G->launches++;
         if (rejected) {
-            k_rejection<real><<<gN, 256, 0, G->stream>>>(D, G->phi, (const real*)G->solid_old, (const real*)G->s_new,
-                                                         k, (const real*)G->f[GPK_FIELD_C], (real*)G->c_new);
+            const dim3 rg((unsigned)(((D.Nx + REJ_TPB - 1) / REJ_TPB) * D.Ny), (unsigned)D.Nz);
+            k_rejection<real><<<rg, REJ_TPB, 0, G->stream>>>(D, G->phi, (const real*)G->solid_old,
+                                                             (const real*)G->s_new, G->grew, k,
+                                                             (const real*)G->f[GPK_FIELD_C], (real*)G->c_new);
             std::swap(G->f[GPK_FIELD_C], G->c_new);
             G->launches++;
         }
@@ -1593,6 +1646,7 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
         if (!G->solid_old) {
             GPK_TRY(gpk_alloc(G, &G->solid_old, G->rsz * D.N));
             GPK_TRY(gpk_alloc(G, &G->s_new, G->rsz * D.N));
+            GPK_TRY(gpk_alloc(G, (void**)&G->grew, D.N));
         }
         k_solid_fraction<real><<<grid_for(G, D.N), 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
                                                                          (real*)G->solid_old);
