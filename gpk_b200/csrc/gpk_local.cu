@@ -266,19 +266,43 @@ static int launch_projection(gpk_grid* G) {
 
 using namespace gpk_dev;
 
-// Tiled remap scores / projection for radius 3 (the radius at every sigma up
-// to 8 cells for the projection and at every sigma for the remap); -1 when
-// no tiled instantiation applies.
+// Tiled remap scores for radius 3 (the remap radius ceil(3 s) at every sigma:
+// s = clamp(sigma / 8, 0.7, 1)); -1 when no tiled instantiation applies.
 template <typename real>
 int gpk_bgr_scores_tiled(gpk_grid* G, int radius, real* res, real* best) {
     if (radius != 3) return -1;
     return G->d.is3d() ? launch_scores<real, 3, true>(G, res, best) : launch_scores<real, 3, false>(G, res, best);
 }
 
+// Tiled projection for the radii ceil(3 s) of the velocity kernel (s =
+// clamp(0.375 sigma, 0.85, 3) in 3-D: radii 3 to 9) whose 3-D halo tile fits
+// in the 227 KB of shared memory: 3 to 8 in FP32, 3 to 6 in FP64 (2-D: 3 to
+// 9).  -1 otherwise (the per-cell kernel runs).
+template <typename real, int R>
+static constexpr bool proj_fits() {
+    // dynamic halo arrays plus 8 KB for the static cell list, weights and scan
+    return (size_t)LocShape<R, true>::NH * (sizeof(int2) + sizeof(real)) + 8 * 1024 <= 227 * 1024;
+}
+
+template <typename real, int R>
+static int projection_r(gpk_grid* G) {
+    if (!G->d.is3d()) return launch_projection<real, R, false>(G);
+    if constexpr (proj_fits<real, R>()) return launch_projection<real, R, true>(G);
+    return -1;
+}
+
 template <typename real>
 int gpk_projection_tiled(gpk_grid* G, int radius) {
-    if (radius != 3) return -1;
-    return G->d.is3d() ? launch_projection<real, 3, true>(G) : launch_projection<real, 3, false>(G);
+    switch (radius) {
+        case 3: return projection_r<real, 3>(G);
+        case 4: return projection_r<real, 4>(G);
+        case 5: return projection_r<real, 5>(G);
+        case 6: return projection_r<real, 6>(G);
+        case 7: return projection_r<real, 7>(G);
+        case 8: return projection_r<real, 8>(G);
+        case 9: return projection_r<real, 9>(G);
+        default: return -1;
+    }
 }
 
 template int gpk_bgr_scores_tiled<float>(gpk_grid*, int, float*, float*);

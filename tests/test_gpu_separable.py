@@ -101,3 +101,22 @@ def test_separable_geometry_polycrystal_f64(oracle_mod):
         assert np.array_equal(gpu.get("phi"), ora.get("phi")), s
         for f in ("kappa_f", "nx_f", "vn_f"):
             assert rel_close(gpu.get(f), ora.get(f), 1e-10), (s, f)
+
+
+# velocity-projection radius ceil(3 clamp(0.375 sigma, 0.85, 3)): 4, 5, 8 — the
+# tiled projection kernels beyond radius 3 (sigma 7 also takes the separable
+# geometry).  Every extent is at least the Gaussian radius ceil(3.5 sigma):
+# beyond it the reference's one-step wrap (src/gpk_gaussian.cpp:27, 42, 59)
+# indexes outside the field, so it has no defined result to match.
+@pytest.mark.parametrize("sigma,shape", [(3.0, (20, 22, 24)), (4.2, (20, 22, 24)), (7.0, (26, 28, 30))])
+def test_projection_radii_f32(oracle_mod, sigma, shape):
+    phi, g = polycrystal(*shape, 8, 5)
+    gpu, ora = _pair(oracle_mod, shape, sigma, "f32")
+    for G in (gpu, ora):
+        G.set("phi", phi)
+        G.set("g", g)
+        G.set("alpha", 1.0)
+    for s in range(3):
+        assert gpu.step() == ora.step(), s
+        bad = compare_all(gpu, ora)
+        assert not bad, (s, bad)
