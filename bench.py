@@ -563,6 +563,54 @@ def coupled_measurement(steps: int = 20, warmup: int = 3, n: int = 128, elastic:
     return res
 
 
+def separable_measurement(n: int = 256, grains: int = 32, sigma: float = 5.0, settle: int = 8, steps: int = 3,
+                          warmup: int = 2):
+    """3-D grain growth with the separable geometry: n^3, `grains` Voronoi
+    grains, sigma 5 cells (Gaussian radius 18, geometry radius 20 > 18), FP32
+    reference arithmetic.  Per step and interface label: the x pass of the
+    indicator, the y and z passes, the evaluation on the label's interface
+    cells; algorithmic bytes of the geometry stage: labels in and the
+    smoothed field out per pass (8 B per cell), the evaluation's labels,
+    mask and smoothed field (9 B per cell), per label."""
+    import torch
+    from gpk_b200 import GPKGrid, thermo
+    g = GPKGrid(n, n, n, 1.0, thermo.isotropic(1.0, 1.0), 0.0, sigma)
+    g.voronoi(grains, SEED)
+    g.set("alpha", 1.0)
+    g.step_n(settle)
+    for _ in range(warmup):
+        g.step()
+    g.sync()
+    g.profile(True)
+    g.stage_times()
+    stream = torch.cuda.ExternalStream(g.stream_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        g.step()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    st = g.stage_times()
+    g.profile(False)
+    geo_ms = st["geometry"][0] / max(1, st["geometry"][1])
+    cells = n ** 3
+    geo_bytes = grains * cells * 33.0
+    peak, peak_kind = _peaks()
+    res = {"workload": f"3-D isotropic grain growth {n}^3, {grains} Voronoi grains, sigma {sigma} cells "
+                       "(separable geometry: per-label x/y/z Gaussian passes + interface evaluation), FP32",
+           "steps": steps, "warmup": warmup, "ms_per_step": ms, "value": cells / (ms / 1e3),
+           "unit": "cell-updates/s", "geometry_ms_per_step": geo_ms,
+           "stages_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in st.items()},
+           "roofline": {"kernels": "k_sep_x_indicator_f2, k_sep_pass (y, z), k_separable_eval per label",
+                        "bound": "fp32 issue (the reference's unfused multiply + add per tap)",
+                        "algorithmic_bytes_per_step": geo_bytes,
+                        "achieved": geo_bytes / (geo_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": geo_bytes / (geo_ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind}}
+    g.close()
+    return res
+
+
 def run_gpu_arm(args):
     ws, rank, local = _dist()
     import torch
@@ -702,7 +750,7 @@ def run_gpu_arm(args):
             cpu.pop("seconds", None)
         except Exception as exc:  # the GPU number stands on its own
             cpu = {"error": str(exc)}
-    spectral = batched = adjoint = coupled = alcu = None
+    spectral = batched = adjoint = coupled = alcu = separable = transport = None
     # the sweep shards over all ranks (same collective order on every rank)
     if not args.headline_only:
         try:
@@ -726,6 +774,14 @@ def run_gpu_arm(args):
             alcu = alcu_measurement(not args.no_cpu and ws == 1)
         except Exception as exc:
             alcu = {"error": str(exc)}
+        try:
+            separable = separable_measurement()
+        except Exception as exc:
+            separable = {"error": str(exc)}
+        try:
+            transport = coupled_measurement(5, 3, 256, elastic=False)
+        except Exception as exc:
+            transport = {"error": str(exc)}
     if rank == 0:
         line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -735,7 +791,7 @@ def run_gpu_arm(args):
                 "stages_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in stages.items()},
                 "interface_fraction": iface, "counters_last_step": list(grid.counters()),
                 "per_step_topology": waves,
-                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "spectral": spectral, "batched": batched, "adjoint": adjoint, "coupled": coupled, "alcu": alcu, "init": init,
+                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "spectral": spectral, "batched": batched, "adjoint": adjoint, "coupled": coupled, "alcu": alcu, "separable": separable, "transport": transport, "init": init,
                 "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": io,
                         "d2h_bytes_per_step": io, "steps": e2e_steps,
                         "path": "GPKGrid drop-in semantics: upload phi/alpha/g, step, download phi/alpha/g"}}
@@ -762,6 +818,8 @@ def main():
     ap.add_argument("--adjoint-only", action="store_true", help="time only the 512^2 adjoint gradient")
     ap.add_argument("--coupled-only", action="store_true",
                     help="time only the 128^3 solidification step with a spectral solve per step")
+    ap.add_argument("--separable-only", action="store_true",
+                    help="time only the 256^3 sigma-5 grain-growth step (separable geometry)")
     ap.add_argument("--transport-only", action="store_true",
                     help="time only the solidification step without the elastic solve, on a --size cube")
     ap.add_argument("--sigma", type=float, default=SIGMA,
@@ -782,6 +840,9 @@ def main():
         return 0
     if args.coupled_only:
         print(json.dumps({"coupled": coupled_measurement()}))
+        return 0
+    if args.separable_only:
+        print(json.dumps({"separable": separable_measurement()}))
         return 0
     if args.transport_only:
         print(json.dumps({"transport": coupled_measurement(args.steps, args.warmup, args.size, elastic=False)}))
