@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(128) k_geometry_direct(Dims D, const int32_t* 
 // indicator when the rows are whole tiles) and the shared rows are padded to
 // an odd length so that the 32 lanes, each walking its own row, hit 32 banks.
 // With IND the input is the indicator phi == p, formed as the labels load.
-static constexpr int SEP_TL = 64;       // outputs per line per tile
+static constexpr int SEP_TL = 128;      // outputs per line per tile
 static constexpr int SEP_M = 8;         // outputs per thread
 static constexpr int SEP_WARPS = SEP_TL / SEP_M;
 static constexpr int SEP_TPB = 32 * SEP_WARPS;
@@ -437,9 +437,10 @@ __global__ void __launch_bounds__(SEP_TPB) k_sep_x_indicator_f2(Dims D, const in
     const int span = SEP_TL + 2 * R;
     // pair q holds rows 2q and 2q + 1 of the block's 64
     if (n % SEP_TL == 0) {
-        // body: half a warp per pair, one int4 of labels per row and lane
-        const int c4 = lane & 15;
-        for (int q = warp * 2 + (lane >> 4); q < 32; q += SEP_WARPS * 2) {
+        // body: one int4 of labels per row of a pair and thread
+        constexpr int C4 = SEP_TL / 4;
+        for (int it = threadIdx.x; it < 32 * C4; it += SEP_TPB) {
+            const int q = it / C4, c4 = it % C4;
             const int l0 = lb * 64 + 2 * q;
             if (l0 >= nlines) continue;
             const int b0 = l0 * n;
