@@ -270,6 +270,15 @@ __host__ __device__ __forceinline__ int sep_pitch(int axis, int R) {
     return axis == 0 ? (p | 1) : p;
 }
 
+// One tap of the ring (KK = the tap's index within its chunk of SEP_M, so
+// every register index is a compile-time constant): each output adds the
+// product of the tap weight with its own ring value, in tap order.
+template <int KK, typename real>
+__device__ __forceinline__ void sep_tap(real (&acc)[SEP_M], const real (&v)[SEP_M], real wk) {
+#pragma unroll
+    for (int m = 0; m < SEP_M; ++m) acc[m] += wk * v[(m + KK) % SEP_M];
+}
+
 template <typename real, int AX, bool IND>
 __global__ void __launch_bounds__(SEP_TPB) k_sep_pass(Dims D, const real* __restrict__ in,
                                                       const int32_t* __restrict__ phi, int32_t p,
@@ -351,25 +360,31 @@ __global__ void __launch_bounds__(SEP_TPB) k_sep_pass(Dims D, const real* __rest
     }
     // ring: slot i holds position o0 + j with j == i (mod SEP_M); after tap
     // kb + kk the value at o0 + kb + kk is dead and its slot takes the value
-    // SEP_M further on.  Whole chunks of SEP_M taps run without guards, the
-    // last partial chunk with them.
-#define SEP_TAP(kk)                                                              \
-    {                                                                            \
-        const real wk = tw[kb + (kk)];                                           \
-        _Pragma("unroll") for (int m = 0; m < SEP_M; ++m) acc[m] += wk * v[(m + (kk)) % SEP_M]; \
-        v[(kk)] = S(o0 + kb + (kk) + SEP_M);                                     \
+    // SEP_M further on.  Whole chunks of SEP_M taps run without guards, with
+    // the tap and ring pointers advanced once per chunk; the last partial
+    // chunk with guards.
+    constexpr int SS = AX == 0 ? 1 : 32;  // shared-memory stride along the line
+    const real* sp = AX == 0 ? &s[lane * P + o0 + SEP_M] : &s[(o0 + SEP_M) * 32 + lane];
+    const real* tp = tw;
+#define SEP_STEP(kk)                          \
+    {                                         \
+        sep_tap<kk>(acc, v, tp[kk]);          \
+        v[kk] = sp[(kk) * SS];                \
     }
     int kb = 0;
-    for (; kb + SEP_M <= K; kb += SEP_M) {
-#pragma unroll
-        for (int kk = 0; kk < SEP_M; ++kk) SEP_TAP(kk)
+    for (; kb + SEP_M <= K; kb += SEP_M, tp += SEP_M, sp += SEP_M * SS) {
+        SEP_STEP(0) SEP_STEP(1) SEP_STEP(2) SEP_STEP(3) SEP_STEP(4) SEP_STEP(5) SEP_STEP(6) SEP_STEP(7)
     }
-    if (kb < K) {
-#pragma unroll
-        for (int kk = 0; kk < SEP_M; ++kk)
-            if (kb + kk < K) SEP_TAP(kk)
-    }
-#undef SEP_TAP
+    static_assert(SEP_M == 8, "the chunk bodies list eight steps");
+    const int rem = K - kb;
+    if (rem > 0) SEP_STEP(0)
+    if (rem > 1) SEP_STEP(1)
+    if (rem > 2) SEP_STEP(2)
+    if (rem > 3) SEP_STEP(3)
+    if (rem > 4) SEP_STEP(4)
+    if (rem > 5) SEP_STEP(5)
+    if (rem > 6) SEP_STEP(6)
+#undef SEP_STEP
     const int l = lb * 32 + lane;
     if (AX == 0) {
         // stage the outputs in the (now free) rows, then store whole rows
@@ -412,6 +427,12 @@ __device__ __forceinline__ sep_u64 f2_fma(sep_u64 w, sep_u64 v, sep_u64 acc) {
     sep_u64 r;
     asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(w), "l"(v), "l"(acc));
     return r;
+}
+
+template <int KK>
+__device__ __forceinline__ void sep_tap_f2(sep_u64 (&acc)[SEP_M], const sep_u64 (&v)[SEP_M], sep_u64 wk) {
+#pragma unroll
+    for (int m = 0; m < SEP_M; ++m) acc[m] = f2_fma(wk, v[(m + KK) % SEP_M], acc[m]);
 }
 
 __global__ void __launch_bounds__(SEP_TPB) k_sep_x_indicator_f2(Dims D, const int32_t* __restrict__ phi, int32_t p,
@@ -486,24 +507,26 @@ __global__ void __launch_bounds__(SEP_TPB) k_sep_x_indicator_f2(Dims D, const in
         v[m] = s[lane * P + o0 + m];
         acc[m] = 0ull;  // (+0, +0)
     }
-    const sep_u64* sl = s + lane * P + o0;
-#define SEP_TAP2(kk)                                                                            \
-    {                                                                                           \
-        const sep_u64 wk = tw[kb + (kk)];                                                       \
-        _Pragma("unroll") for (int m = 0; m < SEP_M; ++m) acc[m] = f2_fma(wk, v[(m + (kk)) % SEP_M], acc[m]); \
-        v[(kk)] = sl[kb + (kk) + SEP_M];                                                        \
+    const sep_u64* sp = &s[lane * P + o0 + SEP_M];
+    const sep_u64* tp = tw;
+#define SEP_STEP2(kk)                        \
+    {                                        \
+        sep_tap_f2<kk>(acc, v, tp[kk]);      \
+        v[kk] = sp[kk];                      \
     }
     int kb = 0;
-    for (; kb + SEP_M <= K; kb += SEP_M) {
-#pragma unroll
-        for (int kk = 0; kk < SEP_M; ++kk) SEP_TAP2(kk)
+    for (; kb + SEP_M <= K; kb += SEP_M, tp += SEP_M, sp += SEP_M) {
+        SEP_STEP2(0) SEP_STEP2(1) SEP_STEP2(2) SEP_STEP2(3) SEP_STEP2(4) SEP_STEP2(5) SEP_STEP2(6) SEP_STEP2(7)
     }
-    if (kb < K) {
-#pragma unroll
-        for (int kk = 0; kk < SEP_M; ++kk)
-            if (kb + kk < K) SEP_TAP2(kk)
-    }
-#undef SEP_TAP2
+    const int rem = K - kb;
+    if (rem > 0) SEP_STEP2(0)
+    if (rem > 1) SEP_STEP2(1)
+    if (rem > 2) SEP_STEP2(2)
+    if (rem > 3) SEP_STEP2(3)
+    if (rem > 4) SEP_STEP2(4)
+    if (rem > 5) SEP_STEP2(5)
+    if (rem > 6) SEP_STEP2(6)
+#undef SEP_STEP2
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < SEP_M; ++m) s[lane * P + o0 + m] = acc[m];
