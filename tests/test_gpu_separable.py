@@ -5,8 +5,8 @@ pass per axis (x, then y, then z); every output is acc = 0; acc += w[k] *
 in[wrap(q + k - R)] for k = 0 .. 2R, a float multiply and a float add per
 tap.  The restatement below does exactly that in numpy float32, so the device
 result must match it bit for bit: on grids whose axes are shorter than the
-radius (several wraps), on axes that are and are not multiples of the 64-cell
-tile, and for radii whose tiles need more than the default 48 KB of shared
+radius (several wraps), on axes that are and are not multiples of the
+128-cell tile, and for radii whose tiles need more than the default 48 KB of shared
 memory or do not fit at all (the one-thread-per-output form).
 """
 import numpy as np
