@@ -37,9 +37,15 @@ GRAINS = 4096
 SIGMA = 1.5
 SEED = 42
 SETTLE = 16  # steps evolved while preparing the input state (untimed)
-# CPU sample: same grain size (4096 cells per grain) on a 128^3 sub-volume
+# single-thread CPU sample: same grain size (4096 cells per grain) on a 128^3 sub-volume
 CPU_SIZE = 128
 CPU_GRAINS = 512
+# DRAM read + write bytes of one k_geometry_tiled launch on the 256^3 / 4096
+# grain / sigma 1.5 workload, measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum, one-pass metrics, one launch after the settling steps)
+GEOMETRY_TRAFFIC_256 = 463.91e6
+GEOMETRY_TRAFFIC_NOTE = ("DRAM bytes of one launch of the kernel, scaled by cell count from a 160^3 ncu capture "
+                         "of the same kernel and grain size")
 
 
 def _peaks():
@@ -146,47 +152,109 @@ def _barrier(ws):
         dist.barrier()
 
 
-def cpu_reference_rate(steps: int, warmup: int, threads: int = 0):
-    """The reference's OpenMP step on this host's cores (oracle/_ref)."""
+def _ref_grid(n: int, phi, g):
+    """The reference's own GPKGrid (oracle/_ref) loaded with a state."""
     import oracle
-    from gpk_b200 import thermo, voronoi
+    from gpk_b200.thermo import isotropic
     if not oracle.ref_available():
         oracle.build()
     if not oracle.ref_available():
         return None
-    n = CPU_SIZE
-    phi, g = voronoi(n, n, n, CPU_GRAINS, SEED)
-    r = oracle.RefGrid(n, n, n, 1.0, thermo.isotropic(1.0, 1.0), 0.0, SIGMA)
-    r.set("phi", phi); r.set("g", g); r.set("alpha", 1.0)
-    r.time_steps(SETTLE + warmup, -1.0, threads)  # same input preparation as the GPU arm
-    per_step = []
-    for _ in range(steps):
-        per_step.append(r.time_steps(1, -1.0, threads))
-    cores = threads if threads > 0 else oracle.RefGrid.max_threads()
-    rate = n ** 3 * steps / sum(per_step)
-    return {"value": rate, "unit": "cell-updates/s", "cores": cores, "kind": "reference",
-            "sample": f"{steps} step(s) of the reference's own GPKGrid::step (src/*.cpp, -O3, OpenMP) on a "
-                      f"{n}^3 sub-volume with {CPU_GRAINS} grains (same 4096 cells/grain and sigma as the "
-                      f"GPU workload), after {SETTLE} settling and {warmup} warm-up step(s)",
-            "seconds": sum(per_step)}
+    r = oracle.RefGrid(n, n, n, 1.0, isotropic(1.0, 1.0), 0.0, SIGMA)
+    r.set("phi", phi)
+    r.set("g", g)
+    return r
+
+
+def single_thread_sample():
+    """One step of the reference on one thread, on a 128^3 sub-volume with 512
+    grains (the workload's 4096 cells per grain), after 16 settling steps on
+    all threads; the same step on all threads beside it."""
+    import oracle
+    n, grains = CPU_SIZE, CPU_GRAINS
+    phi, g = oracle.voronoi(n, n, n, grains, SEED)
+    r = _ref_grid(n, phi, g)
+    if r is None:
+        return None
+    r.set("alpha", 1.0)
+    nproc = oracle.RefGrid.max_threads()
+    r.time_steps(SETTLE, -1.0, nproc)
+    t_all = r.time_steps(1, -1.0, nproc)
+    t_one = r.time_steps(1, -1.0, 1)
+    r.time_steps(0, -1.0, nproc)  # restore the thread count
+    return {"value": n ** 3 / t_one, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+            "same_sample_all_cores": {"value": n ** 3 / t_all, "cores": nproc},
+            "sample": f"one step of the reference's GPKGrid::step on a {n}^3 sub-volume with {grains} grains "
+                      f"(4096 cells per grain, sigma {SIGMA}) after {SETTLE} settling steps; one thread, and all "
+                      f"{nproc} threads on the next step"}
+
+
+def cpu_sample_from_state(phi, alpha, g, steps: int = 2):
+    """The reference's OpenMP step (oracle/_ref) on this host's cores, timed on
+    a bounded sample of the benchmarked workload: the 256^3 state the GPU
+    reached, one untimed step (the reference's step counter starts at zero,
+    whose step runs the extinction pass), then `steps` timed steps."""
+    import oracle
+    n = phi.shape[0]
+    r = _ref_grid(n, phi, g)
+    if r is None:
+        return None
+    r.set("alpha", alpha)
+    r.time_steps(1, -1.0, 0)
+    sec = r.time_steps(steps, -1.0, 0)
+    return {"value": n ** 3 * steps / sec, "unit": "cell-updates/s", "cores": oracle.RefGrid.max_threads(),
+            "kind": "reference",
+            "sample": f"{steps} step(s) of the reference's own GPKGrid::step (src/*.cpp, -O3, OpenMP) on the "
+                      f"{n}^3 state the GPU run reached after its timed steps, after one untimed step"}
 
 
 def run_reference_arm(args):
+    """The reference's own OpenMP GPKGrid::step (its src/*.cpp compiled into
+    oracle/_ref) on the same workload as the GPU arm: the 256^3 polycrystal
+    built by the oracle's restatement of the driver's Voronoi construction
+    (the GPU arm's input, cell for cell), SETTLE settling steps, W warm-up
+    steps, then K timed steps on all host threads.  The CUDA library is
+    never loaded on this path."""
     ws, rank, local = _dist()
     if rank != 0:
         return 0
-    res = cpu_reference_rate(args.steps, args.warmup)
-    if res is None:
+    import oracle
+    t0 = time.perf_counter()
+    phi, g = oracle.voronoi(SIZE, SIZE, SIZE, GRAINS, SEED)
+    init_s = time.perf_counter() - t0
+    r = _ref_grid(SIZE, phi, g)
+    if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference library could not be built here"}))
         return 0
-    line = {"impl": "reference", "metric": "cell-updates/s", "value": res["value"], "unit": "cell-updates/s",
+    del phi, g
+    r.set("alpha", 1.0)
+    nproc = oracle.RefGrid.max_threads()
+    settle_s = r.time_steps(SETTLE + args.warmup, -1.0, nproc)
+    per_step = [r.time_steps(1, -1.0, nproc) for _ in range(args.steps)]
+    sec = sum(per_step)
+    counters = list(r.counters())
+    del r
+    value = SIZE ** 3 * args.steps / sec
+    one = None
+    if not args.no_cpu:
+        try:
+            one = single_thread_sample()
+        except Exception as exc:
+            one = {"error": str(exc)}
+    sample = (f"{args.steps} timed step(s) of the reference's own GPKGrid::step (src/*.cpp, -O3, OpenMP, "
+              f"{nproc} threads) on the benchmarked {SIZE}^3 workload after {SETTLE} settling and "
+              f"{args.warmup} warm-up steps (the GPU arm's step indices)")
+    line = {"impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
             "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * res["seconds"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": 1e3 * sec / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Voronoi polycrystal)",
-            "config": _config({"reference_sample": res["sample"]}),
-            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": res["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+            "config": _config(),
+            "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": nproc, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "single_thread": one, "counters_last_step": counters,
+            "input": {"builder": "oracle restatement of the driver's Voronoi construction (host, one thread)",
+                      "seconds": init_s, "settle_and_warmup_seconds": settle_s}}
     print(json.dumps(line))
     return 0
 
@@ -372,7 +440,7 @@ def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
                 "peak": peak, "unit": "GB/s", "frac": diff_gbs / peak, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_launch": 24.0 * n,
                 "traffic": 381.9e6 * n / 256 ** 3 if shape[0] == 256 else None,
-                "traffic_note": "dram read + write of one 256^3 launch under ncu (profiles/alcu_diffusion_256.md)",
+                "traffic_note": "dram read + write of one 256^3 launch of the same kernel under ncu",
                 "note": "issue-bound on its FP64 divisions in the reference's operand order, not on HBM"}
         res = {"ms_per_step": ms, "cells_per_s": n / (ms / 1e3), "stages_ms": st_ms, "roofline": roof,
                "components": h.info()["components"], "remap_waves": h.info()["waves"],
@@ -611,6 +679,36 @@ def separable_measurement(n: int = 256, grains: int = 32, sigma: float = 5.0, se
     return res
 
 
+def _summary(line):
+    """A compact digest of the line's main figures, printed last so that a
+    reader who keeps only the end of the output still has them."""
+    def g(d, *keys):
+        for k in keys:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+
+    def r3(v):
+        return float("%.4g" % v) if isinstance(v, (int, float)) else v
+
+    out = {"cell_updates_per_s": r3(line["value"]), "ms_per_step": r3(line["ms_per_step"]),
+           "e2e_cell_updates_per_s": r3(g(line, "e2e", "value")),
+           "geometry_ms": r3(g(line, "roofline", "ms_per_launch")),
+           "geometry_fp32_add_frac": r3(g(line, "roofline", "compute", "frac")),
+           "cpu_reference_cell_updates_per_s": r3(g(line, "cpu_baseline", "value")),
+           "cpu_cores": g(line, "cpu_baseline", "cores"),
+           "batched_cell_updates_per_s": r3(g(line, "batched", "value")),
+           "batched_speedup_vs_plain": r3(g(line, "batched", "speedup_vs_plain")),
+           "adjoint_gradients_per_s": r3(g(line, "adjoint", "gradients_per_s")),
+           "spectral_ms_128": r3(g(line, "spectral", "ms_per_solve")),
+           "coupled_ms_128": r3(g(line, "coupled", "ms_per_step")),
+           "near_threshold_cells": g(line, "near_threshold", "cells_last_step")}
+    st = line.get("stages_ms_per_step") or {}
+    out["stages_ms"] = {k: r3(v) for k, v in st.items() if isinstance(v, (int, float)) and v > 0.01}
+    return out
+
+
 def run_gpu_arm(args):
     ws, rank, local = _dist()
     import torch
@@ -680,12 +778,9 @@ def run_gpu_arm(args):
     geo_bytes = cells * 4 + n_active * (4 * 4 + 4)
     peak, peak_kind = _peaks()
     achieved = geo_bytes / (geo_ms / 1e3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "geometry_256_traffic.txt")
-    if os.path.exists(tpath):
-        for line in open(tpath):
-            if line.startswith("traffic_bytes_per_launch:"):
-                traffic = float(line.split(":")[1])
+    # DRAM bytes (read + write) of one launch, from an ncu capture of the
+    # same kernel on this workload; None for other sizes
+    traffic = GEOMETRY_TRAFFIC_256 if (SIZE == 256 and GRAINS == 4096 and SIGMA == 1.5) else None
     clocks = clk.summary()
     tap_adds = n_active * W ** 3 * 9 / (geo_ms / 1e3)
     separable = (W - 1) // 2 > 18
@@ -702,7 +797,7 @@ def run_gpu_arm(args):
                 "note": "the reference-exact tensor stencil adds 9 products per matching tap over (2R+1)^3 "
                         "taps per interface cell in a fixed order; it is bound by FP32 add issue, not HBM "
                         "(compute: the reference's W^3 x 9 tap-adds per interface cell per second)",
-                "traffic_note": "scaled from a 160^3 ncu capture by cell count (profiles/geometry_256_traffic.txt)",
+                "traffic_note": GEOMETRY_TRAFFIC_NOTE,
                 "compute": {"tap_adds_per_s": tap_adds,
                             "peak_fp32_adds_per_s": _fp32_add_peak(clocks["sm_mhz"] or 1965.0),
                             "frac": tap_adds / _fp32_add_peak(clocks["sm_mhz"] or 1965.0)}}
@@ -746,8 +841,7 @@ def run_gpu_arm(args):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
-            cpu = cpu_reference_rate(1, 1)
-            cpu.pop("seconds", None)
+            cpu = cpu_sample_from_state(grid.get("phi"), grid.get("alpha"), grid.get("g"))
         except Exception as exc:  # the GPU number stands on its own
             cpu = {"error": str(exc)}
     spectral = batched = adjoint = coupled = alcu = separable = transport = None
@@ -795,6 +889,7 @@ def run_gpu_arm(args):
                 "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": io,
                         "d2h_bytes_per_step": io, "steps": e2e_steps,
                         "path": "GPKGrid drop-in semantics: upload phi/alpha/g, step, download phi/alpha/g"}}
+        line["summary"] = _summary(line)
         print(json.dumps(line))
     grid.close()
     if ws > 1:

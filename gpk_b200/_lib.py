@@ -85,6 +85,7 @@ def lib() -> C.CDLL:
         "gpk_grid_stage_times": ([vp, C.POINTER(dbl), C.POINTER(u64)], i32),
         "gpk_voronoi_init": ([i32, i32, i32, i32, u64, vp, vp, C.POINTER(i32)], i32),
         "gpk_grid_voronoi": ([vp, i32, u64, C.POINTER(i32)], i32),
+        "gpk_grid_voronoi_seeds": ([vp, i32, vp, vp, vp, vp, C.POINTER(i32)], i32),
         "gpk_spectral_create": ([i32, C.POINTER(i32), dbl, dbl, dbl, dbl, C.POINTER(dbl), C.POINTER(vp)], i32),
         "gpk_spectral_destroy": ([vp], i32),
         "gpk_spectral_set_constants": ([vp, dbl, dbl, dbl, dbl, C.POINTER(dbl)], i32),

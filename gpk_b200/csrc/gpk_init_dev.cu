@@ -230,31 +230,12 @@ __global__ void k_f2d(long long N, const float* __restrict__ a, double* __restri
 
 }  // namespace
 
-extern "C" int gpk_grid_voronoi(gpk_grid* G, int n_seeds, uint64_t seed, int* reassigned) {
-    if (!G) return GPK_ERR_INVALID_ARGUMENT;
+// The construction for a given seed list (cells distinct and in range).
+static int voronoi_build(gpk_grid* G, int n_seeds, const std::vector<int>& sz, const std::vector<int>& sy,
+                         const std::vector<int>& sx, const std::vector<float>& sg, int* reassigned) {
     const gpk_dev::Dims D = G->d;
     const int Nz = D.Nz, Ny = D.Ny, Nx = D.Nx;
     const long long N = D.N;
-    if (n_seeds <= 0 || n_seeds > N || n_seeds >= (1 << 26)) {
-        gpk_set_error("voronoi: need 0 < seeds <= cells and seeds < 2^26");
-        return GPK_ERR_INVALID_ARGUMENT;
-    }
-    // 1. seeds, as gpk_voronoi_init draws them
-    Split rng{seed};
-    std::vector<int> sz(n_seeds), sy(n_seeds), sx(n_seeds);
-    std::vector<float> sg(n_seeds);
-    std::unordered_set<long long> used;
-    used.reserve(2 * (size_t)n_seeds);
-    for (int k = 0; k < n_seeds; ++k) {
-        long long lin;
-        do {
-            sz[k] = (int)rng.below((uint32_t)Nz);
-            sy[k] = (int)rng.below((uint32_t)Ny);
-            sx[k] = (int)rng.below((uint32_t)Nx);
-            lin = ((long long)sz[k] * Ny + sy[k]) * Nx + sx[k];
-        } while (!used.insert(lin).second);
-        sg[k] = rng.unit_float() * (float)(M_PI * 0.5);
-    }
     const double cell_vol = (double)N / n_seeds;
     const int bs = std::max(1, (int)std::ceil(std::cbrt(cell_vol) * (Nz > 1 ? 1.0 : 0.0) +
                                               std::sqrt(cell_vol) * (Nz > 1 ? 0.0 : 1.0)));
@@ -376,4 +357,57 @@ extern "C" int gpk_grid_voronoi(gpk_grid* G, int n_seeds, uint64_t seed, int* re
     GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
     if (reassigned) *reassigned = (int)((unsigned)N - n_initial);
     return GPK_OK;
+}
+
+extern "C" int gpk_grid_voronoi(gpk_grid* G, int n_seeds, uint64_t seed, int* reassigned) {
+    if (!G) return GPK_ERR_INVALID_ARGUMENT;
+    const int Nz = G->d.Nz, Ny = G->d.Ny, Nx = G->d.Nx;
+    const long long N = G->d.N;
+    if (n_seeds <= 0 || n_seeds > N || n_seeds >= (1 << 26)) {
+        gpk_set_error("voronoi: need 0 < seeds <= cells and seeds < 2^26");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    // seeds, as gpk_voronoi_init draws them
+    Split rng{seed};
+    std::vector<int> sz(n_seeds), sy(n_seeds), sx(n_seeds);
+    std::vector<float> sg(n_seeds);
+    std::unordered_set<long long> used;
+    used.reserve(2 * (size_t)n_seeds);
+    for (int k = 0; k < n_seeds; ++k) {
+        long long lin;
+        do {
+            sz[k] = (int)rng.below((uint32_t)Nz);
+            sy[k] = (int)rng.below((uint32_t)Ny);
+            sx[k] = (int)rng.below((uint32_t)Nx);
+            lin = ((long long)sz[k] * Ny + sy[k]) * Nx + sx[k];
+        } while (!used.insert(lin).second);
+        sg[k] = rng.unit_float() * (float)(M_PI * 0.5);
+    }
+    return voronoi_build(G, n_seeds, sz, sy, sx, sg, reassigned);
+}
+
+extern "C" int gpk_grid_voronoi_seeds(gpk_grid* G, int n_seeds, const int* seed_z, const int* seed_y,
+                                      const int* seed_x, const float* seed_g, int* reassigned) {
+    if (!G || !seed_z || !seed_y || !seed_x || !seed_g) return GPK_ERR_INVALID_ARGUMENT;
+    const int Nz = G->d.Nz, Ny = G->d.Ny, Nx = G->d.Nx;
+    const long long N = G->d.N;
+    if (n_seeds <= 0 || n_seeds > N || n_seeds >= (1 << 26)) {
+        gpk_set_error("voronoi: need 0 < seeds <= cells and seeds < 2^26");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    std::vector<int> sz(seed_z, seed_z + n_seeds), sy(seed_y, seed_y + n_seeds), sx(seed_x, seed_x + n_seeds);
+    std::vector<float> sg(seed_g, seed_g + n_seeds);
+    std::unordered_set<long long> used;
+    used.reserve(2 * (size_t)n_seeds);
+    for (int k = 0; k < n_seeds; ++k) {
+        if (sz[k] < 0 || sz[k] >= Nz || sy[k] < 0 || sy[k] >= Ny || sx[k] < 0 || sx[k] >= Nx) {
+            gpk_set_error("voronoi: a seed lies outside the grid");
+            return GPK_ERR_INVALID_ARGUMENT;
+        }
+        if (!used.insert(((long long)sz[k] * Ny + sy[k]) * Nx + sx[k]).second) {
+            gpk_set_error("voronoi: two seeds share a cell");
+            return GPK_ERR_INVALID_ARGUMENT;
+        }
+    }
+    return voronoi_build(G, n_seeds, sz, sy, sx, sg, reassigned);
 }

@@ -225,6 +225,20 @@ class GPKGrid:
         check(lib().gpk_grid_voronoi(self._h, int(n_grains), int(seed), C.byref(moved)))
         return moved.value
 
+    def voronoi_seeds(self, seeds, orientations) -> int:
+        """The same construction on the device for an explicit seed list:
+        ``seeds`` is (3, n) int (z, y, x rows), ``orientations`` (n,) float;
+        seed k labels its Voronoi cell k + 1.  Returns the number of tie
+        cells the connectivity step moved."""
+        s = np.ascontiguousarray(seeds, dtype=np.int32)
+        sg = np.ascontiguousarray(orientations, dtype=np.float32)
+        if s.ndim != 2 or s.shape[0] != 3 or sg.shape != (s.shape[1],):
+            raise ValueError("seeds must be (3, n) and orientations (n,)")
+        moved = C.c_int()
+        check(lib().gpk_grid_voronoi_seeds(self._h, int(s.shape[1]), s[0].ctypes.data, s[1].ctypes.data,
+                                           s[2].ctypes.data, sg.ctypes.data, C.byref(moved)))
+        return moved.value
+
     def geometry(self) -> None:
         """Mask and geometry of the current labels, without stepping."""
         check(lib().gpk_grid_geometry(self._h))

@@ -187,7 +187,9 @@ int gpk_grid_counters(gpk_grid* grid, uint64_t counters[3]);
 /* GPKGrid::topology_simple_move (src/gpk_connectivity.cpp:198-208).        */
 int gpk_grid_topology_simple_move(gpk_grid* grid, int cell, int32_t new_label,
                                   int* result);
-/* Device bytes held by the grid (the analogue of allocated_array_bytes).   */
+/* Device bytes held by the grid (the analogue of allocated_array_bytes).
+ * Not counted: the 16 MiB static array of gpk_gaussian_filter_3d_noalloc,
+ * resident on every GPU that loads the library.                           */
 int gpk_grid_device_bytes(gpk_grid* grid, size_t* out);
 /* Cumulative kernel-launch count issued by this grid (instrumentation).   */
 int gpk_grid_launch_count(gpk_grid* grid, uint64_t* out);
@@ -208,9 +210,12 @@ int gpk_gaussian_filter_3d(const float* in, float* out, int Nz, int Ny, int Nx,
  * cudaMalloc, and no stream of its own.  Larger grids return
  * GPK_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
  * address (cudaGetSymbolAddress) with that device current: make it before
- * any stream capture.  Calls share the array and keep the last call's
- * contents; calls in one process are serialised, calls overlapping on the GPU
- * by any other route race.                                                 */
+ * any stream capture.  Every call copies with synchronous cudaMemcpy on the
+ * legacy default stream, which CUDA refuses while any stream of the process
+ * is capturing in global mode: no call, first or later, may overlap such a
+ * capture.  Calls share the array and keep the last call's contents; calls
+ * in one process are serialised, calls overlapping on the GPU by any other
+ * route race.                                                              */
 #define GPK_NOALLOC_MAX_CELLS (1 << 21)
 int gpk_gaussian_filter_3d_noalloc(const float* in, float* out, int Nz, int Ny, int Nx,
                                    const float* taps, int radius);

@@ -30,6 +30,16 @@ int gpk_voronoi_init(int Nz, int Ny, int Nx, int n_seeds, uint64_t seed, int32_t
 typedef struct gpk_grid gpk_grid;
 int gpk_grid_voronoi(gpk_grid* grid, int n_seeds, uint64_t seed, int* reassigned);
 
+/* The same construction on the device for an explicit seed list: seed k sits
+ * at cell (seed_z[k], seed_y[k], seed_x[k]) with orientation seed_g[k] and
+ * labels its Voronoi cell k + 1.  This is the reference driver's
+ * voronoi_init (demos/gpk.cpp:73-189 of albert-hzbn/GPK) after its seed
+ * draws, so that handing it the seeds the reference draws for a seed value
+ * gives the reference's polycrystal.  Seeds must be distinct cells of the
+ * grid (GPK_ERR_INVALID_ARGUMENT otherwise).                               */
+int gpk_grid_voronoi_seeds(gpk_grid* grid, int n_seeds, const int* seed_z, const int* seed_y, const int* seed_x,
+                           const float* seed_g, int* reassigned);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,9 +29,12 @@ _ORACLE_SO = os.path.join(_HERE, "liboracle.so")
 _REF_SO = os.path.join(_HERE, "_ref", "libgpk_ref.so")
 
 
-def build(quiet: bool = True) -> None:
-    """Compile the oracle (and the reference harness where its sources exist)."""
-    out = subprocess.run(["make", "-f", os.path.join(_HERE, "Makefile")],
+def build(quiet: bool = True, demos: bool = False) -> None:
+    """Compile the oracle (and the reference harness where its sources exist;
+    with demos, also the reference's validation programs in their CPU and
+    drop-in builds).  The reference checkout is named by GPK_REFERENCE."""
+    targets = ["all"] + (["demos"] if demos else [])
+    out = subprocess.run(["make", "-j8", "-f", os.path.join(_HERE, "Makefile")] + targets,
                          capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
@@ -55,6 +58,75 @@ def _load(path: str) -> C.CDLL:
 
 def ref_available() -> bool:
     return os.path.exists(_REF_SO)
+
+
+def _int_ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def voronoi_seeds(Nz, Ny, Nx, n, seed):
+    """Seed cells (z, y, x) and orientations in the draw order of the
+    library's splitmix64 stream (oracle/voronoi_oracle.c)."""
+    L = _load(_ORACLE_SO)
+    s = np.empty((3, n), dtype=np.int32)
+    g = np.empty(n, dtype=np.float32)
+    rc = L.or_voronoi_seeds(C.c_int(Nz), C.c_int(Ny), C.c_int(Nx), C.c_int(n), C.c_uint64(seed),
+                            _int_ptr(s[0]), _int_ptr(s[1]), _int_ptr(s[2]), _int_ptr(g))
+    if rc:
+        raise ValueError(f"or_voronoi_seeds failed ({rc})")
+    return s, g
+
+
+def voronoi_from_seeds(shape, seeds, orientations):
+    """The reference driver's Voronoi construction (demos/gpk.cpp:51-189) for
+    an explicit seed list: labels 1..n, orientations, reassigned tie cells."""
+    L = _load(_ORACLE_SO)
+    Nz, Ny, Nx = shape
+    s = np.ascontiguousarray(seeds, dtype=np.int32)
+    sg = np.ascontiguousarray(orientations, dtype=np.float32)
+    n = s.shape[1]
+    phi = np.empty(shape, dtype=np.int32)
+    g = np.empty(shape, dtype=np.float32)
+    re = C.c_int(0)
+    rc = L.or_voronoi_from_seeds(C.c_int(Nz), C.c_int(Ny), C.c_int(Nx), C.c_int(n), _int_ptr(s[0]),
+                                 _int_ptr(s[1]), _int_ptr(s[2]), _int_ptr(sg), _int_ptr(phi), _int_ptr(g),
+                                 C.byref(re))
+    if rc:
+        raise ValueError(f"or_voronoi_from_seeds failed ({rc})")
+    return phi, g, re.value
+
+
+def voronoi(Nz, Ny, Nx, n, seed):
+    """The polycrystal gpk_voronoi_init builds (seeds from the library's
+    stream, the reference's construction), built without the library."""
+    s, sg = voronoi_seeds(Nz, Ny, Nx, n, seed)
+    phi, g, _ = voronoi_from_seeds((Nz, Ny, Nx), s, sg)
+    return phi, g
+
+
+def ref_voronoi_seeds(Nz, Ny, Nx, n, seed):
+    """The seeds the reference's voronoi_init draws (std::mt19937 + libstdc++
+    distributions, demos/gpk.cpp:56-71)."""
+    L = _load(_REF_SO)
+    s = np.empty((3, n), dtype=np.int32)
+    g = np.empty(n, dtype=np.float32)
+    rc = L.ref_voronoi_seeds(C.c_int(Nz), C.c_int(Ny), C.c_int(Nx), C.c_int(n), C.c_uint32(seed),
+                             _int_ptr(s[0]), _int_ptr(s[1]), _int_ptr(s[2]), _int_ptr(g))
+    if rc:
+        raise ValueError("ref_voronoi_seeds failed")
+    return s, g
+
+
+def ref_voronoi(Nz, Ny, Nx, n, seed):
+    """The reference driver's own voronoi_init (compiled from its source)."""
+    L = _load(_REF_SO)
+    phi = np.empty((Nz, Ny, Nx), dtype=np.int32)
+    g = np.empty((Nz, Ny, Nx), dtype=np.float32)
+    rc = L.ref_voronoi_init(C.c_int(Nz), C.c_int(Ny), C.c_int(Nx), C.c_int(n), C.c_uint32(seed),
+                            _int_ptr(phi), _int_ptr(g))
+    if rc:
+        raise ValueError("ref_voronoi_init rejected its arguments")
+    return phi, g
 
 
 class _GridBase:

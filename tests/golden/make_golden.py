@@ -1,6 +1,6 @@
 """Converts the reference's committed golden data into compact test fixtures.
 
-Run in a container where the reference is mounted (default /root/reference);
+Run with the path of a reference checkout (argument or GPK_REFERENCE);
 writes tests/golden/*.npz.  The sources are the reference's own outputs,
 committed in its repository:
 
@@ -77,4 +77,7 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    _ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GPK_REFERENCE")
+    if not _ref:
+        sys.exit("usage: python %s <path to the reference checkout> (or set GPK_REFERENCE)" % sys.argv[0])
+    main(_ref)

@@ -57,3 +57,38 @@ def test_noalloc_filter_rejects_grids_beyond_its_scratch():
                                           taps.ctypes.data, r)
     assert rc == 1
     assert b"static scratch" in L.gpk_last_error()
+
+
+def test_noalloc_filter_after_a_larger_call():
+    """A small 3-D grid and a 2-D grid (whose result lands in the other half
+    of the array) right after a 128^3 call has filled both field regions:
+    stale data from the larger call must not reach the result."""
+    L = lib()
+    check(L.gpk_device_init(0))
+    rng = np.random.default_rng(11)
+    for shape, sigma in [((128, 128, 128), 5.0), ((1, 70, 90), 2.0), ((12, 18, 10), 1.5), ((1, 33, 17), 0.8)]:
+        taps, r = _taps(sigma)
+        field = rng.random(shape, dtype=np.float32)
+        want = _call(L.gpk_gaussian_filter_3d, field, taps, r)
+        got = _call(L.gpk_gaussian_filter_3d_noalloc, field, taps, r)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), shape
+
+
+def test_noalloc_filter_tap_limit():
+    """511 taps (radius 255, the largest accepted; its passes are too wide
+    for a shared-memory tile and run one thread per output) equal the
+    allocating filter; 513 taps are rejected."""
+    L = lib()
+    check(L.gpk_device_init(0))
+    rng = np.random.default_rng(12)
+    field = rng.random((8, 8, 8), dtype=np.float32)
+    w = rng.random(511, dtype=np.float32)
+    taps = (w / w.sum(dtype=np.float32)).astype(np.float32)
+    want = _call(L.gpk_gaussian_filter_3d, field, taps, 255)
+    got = _call(L.gpk_gaussian_filter_3d_noalloc, field, taps, 255)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    big = np.ones(513, dtype=np.float32) / 513
+    out = np.empty_like(field)
+    rc = L.gpk_gaussian_filter_3d_noalloc(field.ctypes.data, out.ctypes.data, 8, 8, 8, big.ctypes.data, 256)
+    assert rc == 1
+    assert b"static scratch" in L.gpk_last_error()
