@@ -31,6 +31,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "python"))
 
 SIZE = 256
 GRAINS = 4096
@@ -264,7 +265,7 @@ def spectral_measurement(with_cpu: bool):
     (cubic 108/62/28 GPa, 0.5% dilatational misfit, nucleus radius 4), inputs
     resident on the device, 10 timed solves after 3 warm-up solves."""
     import torch
-    from gpk_b200.spectral import SpectralElasticity, variant_eigenstrains
+    from gpk.spectral import SpectralElasticity, variant_eigenstrains
     n = 128
     g = torch.arange(n, device="cuda", dtype=torch.int32) - n // 2
     r2 = g[:, None, None] ** 2 + g[None, :, None] ** 2 + g[None, None, :] ** 2
@@ -347,7 +348,7 @@ def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
     events on the launching stream."""
     import numpy as np
     import torch
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
     from oracle import alcu_oracle as O
 
     out = {}
@@ -531,7 +532,7 @@ def adjoint_measurement(with_cpu: bool, evals: int = 20):
     mobility derivatives per gradient, FP64."""
     import torch
     from gpk_b200 import GPKGrid, thermo
-    from gpk_b200.adjoint import AdjointProblem, calibration_case
+    from gpk.adjoint import AdjointProblem, calibration_case
     n, grains = 512, 256
     phi, g, mob_index = calibration_case(n, grains, 64, 11, (6, 20))
     grid = GPKGrid(1, n, n, 1.0, thermo.isotropic(1.0, 1.0), 0.0, 1.5, precision="f64")
@@ -590,8 +591,8 @@ def coupled_measurement(steps: int = 20, warmup: int = 3, n: int = 128, elastic:
     solidification deck otherwise).  Without elastic, the same step with no
     elastic solve: the solute transport alone on a field larger than L2."""
     import torch
-    from gpk_b200 import GPKGrid, SpectralElasticity, thermo
-    from gpk_b200.spectral import variant_eigenstrains
+    from gpk import GPKGrid, SpectralElasticity, thermo
+    from gpk.spectral import variant_eigenstrains
     th = thermo.solidification(M0=5e-8, sigma0=0.2, eps4=0.04, m_liq=-500.0, k_part=0.14, T_melt=933.0, L=1e8)
     th.solute_rejection, th.k_partition = True, 0.14  # as the reference's driver sets both from k_part
     g = GPKGrid(n, n, n, 0.5e-6, th, 3e-9, 1.5, precision="f64")

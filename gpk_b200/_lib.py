@@ -86,6 +86,10 @@ def lib() -> C.CDLL:
         "gpk_voronoi_init": ([i32, i32, i32, i32, u64, vp, vp, C.POINTER(i32)], i32),
         "gpk_grid_voronoi": ([vp, i32, u64, C.POINTER(i32)], i32),
         "gpk_grid_voronoi_seeds": ([vp, i32, vp, vp, vp, vp, C.POINTER(i32)], i32),
+        "gpk_grid_set_near_threshold": ([vp, dbl], i32),
+        "gpk_grid_near_threshold": ([vp, vp, i32, C.POINTER(i32)], i32),
+        "gpk_grid_set_solid_diffusivity_ratio": ([vp, dbl], i32),
+        "gpk_grid_inject_wait_timeout": ([vp, C.c_longlong], i32),
         "gpk_spectral_create": ([i32, C.POINTER(i32), dbl, dbl, dbl, dbl, C.POINTER(dbl), C.POINTER(vp)], i32),
         "gpk_spectral_destroy": ([vp], i32),
         "gpk_spectral_set_constants": ([vp, dbl, dbl, dbl, dbl, C.POINTER(dbl)], i32),

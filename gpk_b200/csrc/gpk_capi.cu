@@ -348,6 +348,7 @@ extern "C" int gpk_grid_create(int Nz, int Ny, int Nx, double dx, const gpk_ther
     ALLOC(G->stamp, 4 * N);
     ALLOC(G->stamp_rev, 4 * N);
     ALLOC(G->ff_stack, 4 * (5 * N + 64));  // flood-fill queues: cells + search ids
+    ALLOC(G->near_list, 4 * (size_t)N);    // near-threshold cells of the last step
     ALLOC(G->bgr_res, rb);
     ALLOC(G->bgr_best, rb);
     ALLOC(G->key_a, 8 * N);
@@ -693,6 +694,49 @@ extern "C" int gpk_grid_wave_stats(gpk_grid* G, uint64_t out[8]) {
 extern "C" int gpk_grid_set_external_elastic(gpk_grid* G, int on) {
     if (!G) return GPK_ERR_INVALID_ARGUMENT;
     G->external_elastic = on ? 1 : 0;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_set_near_threshold(gpk_grid* G, double tol) {
+    if (!G || !(tol >= 0.0)) {
+        gpk_set_error("near-threshold tolerance must be a number >= 0");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    G->near_tol = tol;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_near_threshold(gpk_grid* G, int32_t* cells, int cap, int* n) {
+    if (!G || !n || cap < 0 || (cap > 0 && !cells)) return GPK_ERR_INVALID_ARGUMENT;
+    GPK_TRY(gpk_sync_scalars(G));
+    const unsigned total = G->h_scal->n_near;
+    *n = (int)total;
+    if (cap == 0 || total == 0) return GPK_OK;
+    // every listed cell is stored (capacity N); restore increasing cell order
+    std::vector<int32_t> all(total);
+    GPK_CUDA_TRY(cudaMemcpyAsync(all.data(), G->near_list, sizeof(int32_t) * total, cudaMemcpyDeviceToHost,
+                                 G->stream));
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    std::sort(all.begin(), all.end());
+    std::copy(all.begin(), all.begin() + std::min<size_t>((size_t)cap, all.size()), cells);
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_set_solid_diffusivity_ratio(gpk_grid* G, double ratio) {
+    if (!G || !(ratio >= 0.0 && ratio <= 1.0)) {
+        gpk_set_error("solid/liquid diffusivity ratio must lie in [0, 1]");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    G->solid_ratio = ratio;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_inject_wait_timeout(gpk_grid* G, long long spin_limit) {
+    if (!G || spin_limit < 1 || spin_limit > (1LL << 24)) {
+        gpk_set_error("inject_wait_timeout: spin limit must lie in [1, 2^24]");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    G->inject_spin_limit = spin_limit;
     return GPK_OK;
 }
 

@@ -109,6 +109,15 @@ struct gpk_grid {
     int geometry_kernel = 0;
     // E_el supplied by the caller (gpk_grid_set_external_elastic)
     int external_elastic = 0;
+    // near-threshold listing of the last step (gpk_grid_near_threshold):
+    // cells appended by k_alpha, sorted when read; capacity N
+    int32_t* near_list = nullptr;
+    double near_tol = 1e-12;
+    // solid/liquid diffusivity ratio of the partitioned transport (0: the reference)
+    double solid_ratio = 0;
+    // gpk_grid_inject_wait_timeout: spin limit for the next cooperative
+    // launch, whose grid barrier then also awaits one block that never comes
+    long long inject_spin_limit = 0;
     // stage timing (gpk_grid_profile)
     int profile = 0;
     cudaEvent_t ev[GPK_NUM_STAGES][2] = {};

@@ -80,7 +80,13 @@ struct StepScalars {
     unsigned wave_rem[3];   // rotating "items left" counters of a wave loop
     unsigned present_labels;  // labels with at least one cell (extinction)
     unsigned n_tasks;       // crossing candidates queued for warp-wide work
-    unsigned pad;
+    unsigned n_near;        // near-threshold cells of the step (may exceed the list)
+    // wait limits of grid_barrier: spin iterations before GPK_ERR_TIMEOUT
+    // (0: the default) and phantom arrivals awaited besides the real blocks
+    // (0 in normal use; gpk_grid_inject_wait_timeout sets them for one launch)
+    long long spin_limit;
+    unsigned bar_extra;
+    unsigned pad2;
     // instrumentation of the label-wide work (summed until read)
     unsigned long long flood_tasks, flood_cells, count_tasks, count_scanned;
 };
@@ -96,14 +102,15 @@ __device__ __forceinline__ bool grid_barrier(StepScalars* s, unsigned nblocks) {
         volatile unsigned* gen = &s->bar_gen;
         const unsigned g = *gen;
         __threadfence();
-        if (atomicAdd(&s->bar_count, 1u) == nblocks - 1) {
+        const long long limit = s->spin_limit > 0 ? s->spin_limit : (1LL << 24);  // ~seconds with the back-off
+        if (atomicAdd(&s->bar_count, 1u) == nblocks + s->bar_extra - 1) {
             atomicExch(&s->bar_count, 0u);
             __threadfence();
             atomicAdd(&s->bar_gen, 1u);
         } else {
             long long it = 0;
             while (*gen == g) {
-                if (++it > (1LL << 24)) {  // ~seconds with the back-off below
+                if (++it > limit) {
                     atomicCAS(&s->error, 0u, (unsigned)GPK_ERR_TIMEOUT);
                     ok = 0;
                     break;

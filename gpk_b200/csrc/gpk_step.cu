@@ -982,8 +982,9 @@ template <typename real>
 __global__ void k_alpha(Dims D, const int32_t* __restrict__ active, const unsigned* __restrict__ n_active,
                         const int32_t* __restrict__ phi, const int32_t* __restrict__ phi_comp,
                         const real* __restrict__ vn, const real* __restrict__ T, real* __restrict__ alpha,
-                        real* __restrict__ alpha_new_a, uint8_t* __restrict__ cand_flag, const StepScalars* s, real dx,
-                        int do_noise_flag, real M0, real kB, real noise_scale, uint64_t step_id) {
+                        real* __restrict__ alpha_new_a, uint8_t* __restrict__ cand_flag, StepScalars* s, real dx,
+                        int do_noise_flag, real M0, real kB, real noise_scale, uint64_t step_id,
+                        real near_tol, int32_t* __restrict__ near_list, int near_cap) {
     const real dt = (real)s->dt;
     const real idt = dt / dx;
     const real cell_vol = dx * dx * dx;
@@ -997,9 +998,16 @@ __global__ void k_alpha(Dims D, const int32_t* __restrict__ active, const unsign
         if (do_noise) vn_eff += noise_amp * sqrt(dmax(T[i], (real)1)) * normal_from_cell_step<real>(i, step_id, 0xabcddcbaULL);
         const real an = dmin(alpha[i] + vn_eff * idt, (real)1);
         alpha_new_a[a] = an;
-        const bool cand = an <= (real)1e-6 && phi_comp[i] != phi[i];
+        const bool other = phi_comp[i] != phi[i];
+        const bool cand = an <= (real)1e-6 && other;
         cand_flag[a] = cand ? 1 : 0;
         if (!cand) alpha[i] = an;
+        // near-threshold listing: the switching margin an - 1e-6 within
+        // near_tol of zero (order restored when the list is read)
+        if (other && fabs(an - (real)1e-6) <= near_tol) {
+            const unsigned q = atomicAdd(&s->n_near, 1u);
+            if (q < (unsigned)near_cap) near_list[q] = i;
+        }
     }
 }
 
@@ -1217,7 +1225,8 @@ template <typename real>
 __global__ void __launch_bounds__(PDX * PDY) k_diffusion_partitioned_tiled(Dims D, const real* __restrict__ c,
                                                                            const real* __restrict__ s,
                                                                            real* __restrict__ c_new, real Dc, real k,
-                                                                           const StepScalars* st, real dx, int zc) {
+                                                                           const StepScalars* st, real dx, int zc,
+                                                                           real rsk) {
     __shared__ real ts[PDY + 2][PDX + 2];
     __shared__ real tl[PDY + 2][PDX + 2];
     const int Nx = D.Nx, Ny = D.Ny, Nz = D.Nz;
@@ -1271,9 +1280,17 @@ __global__ void __launch_bounds__(PDX * PDY) k_diffusion_partitioned_tiled(Dims 
         __syncthreads();
         const real li = (real)1 - s_cur;
         real flux = 0;
+        // rsk = (solid/liquid diffusivity ratio) x k: the solid composition
+        // k cL diffuses through the face's shared solid fraction; with
+        // rsk = 0 this is the reference's liquid-fraction face weight
         auto face = [&](real sj, real lj) {
             const real lf = dmin(li, (real)1 - sj);
-            if (lf > (real)0) flux += lf * (lj - l_cur);
+            if (rsk > (real)0) {
+                const real w = lf + rsk * dmin(s_cur, sj);
+                if (w > (real)0) flux += w * (lj - l_cur);
+            } else if (lf > (real)0) {
+                flux += lf * (lj - l_cur);
+            }
         };
         face(ts[ty + 1][tx + 2], tl[ty + 1][tx + 2]);  // x+
         face(ts[ty + 1][tx], tl[ty + 1][tx]);          // x-
@@ -1302,7 +1319,7 @@ __global__ void k_advance_time(StepScalars* s) { s->time += s->dt; }
 
 __global__ void k_reset_step(StepScalars* s) {
     s->accepted = 0; s->deferred = 0; s->exchanges = 0; s->exch_pass = 0;
-    s->n_cand = 0; s->n_prop = 0; s->waves = 0;
+    s->n_cand = 0; s->n_prop = 0; s->waves = 0; s->n_near = 0;
 }
 
 }  // namespace gpk_dev
@@ -1556,7 +1573,7 @@ static int transport(gpk_grid* G) {
             const dim3 tg(bx, by, (unsigned)((D.Nz + zc - 1) / zc));
             k_diffusion_partitioned_tiled<real><<<tg, dim3(PDX, PDY), 0, G->stream>>>(
                 D, (const real*)G->f[GPK_FIELD_C], (const real*)G->s_new, (real*)G->c_new, Dc, k, G->scal, dx,
-                (int)zc);
+                (int)zc, (real)G->solid_ratio * k);
             std::swap(G->f[GPK_FIELD_C], G->c_new);
             G->launches++;
         }
@@ -1683,7 +1700,7 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
                                              (const real*)G->f[GPK_FIELD_VN], (const real*)G->f[GPK_FIELD_T],
                                              (real*)G->f[GPK_FIELD_ALPHA], (real*)G->alpha_new_a, cflag, G->scal,
                                              (real)G->dx, th.stochastic, (real)th.M0, (real)th.kB, (real)th.noise_scale,
-                                             G->step_id);
+                                             G->step_id, (real)G->near_tol, G->near_list, D.N);
     const int nt = (D.N + MASK_TILE - 1) / MASK_TILE;
     int32_t* ctile = G->tile_off + nt + 1;
     k_count_u8<<<nt, MASK_TPB, 0, G->stream>>>(cflag, &G->scal->n_active, ctile);

@@ -1107,8 +1107,24 @@ static int coop_grid(gpk_grid* G, const void* kernel, int block, int want_items)
 static int launch_coop(gpk_grid* G, const void* kernel, int grid, int block, void** args) {
     GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->bar_count, 0, sizeof(unsigned), G->stream));
     GPK_CUDA_TRY(cudaMemsetAsync(G->scal->wave_rem, 0, sizeof(G->scal->wave_rem), G->stream));
+    const bool inject = G->inject_spin_limit > 0;
+    if (inject) {
+        // failure injection (gpk_grid_inject_wait_timeout): the first grid
+        // barrier waits for one block more than launched and gives up after
+        // the given number of spins, so the kernel returns GPK_ERR_TIMEOUT
+        const long long lim = G->inject_spin_limit;
+        const unsigned extra = 1;
+        GPK_CUDA_TRY(cudaMemcpyAsync(&G->scal->spin_limit, &lim, sizeof(lim), cudaMemcpyHostToDevice, G->stream));
+        GPK_CUDA_TRY(cudaMemcpyAsync(&G->scal->bar_extra, &extra, sizeof(extra), cudaMemcpyHostToDevice, G->stream));
+        GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));  // the host values above are locals
+        G->inject_spin_limit = 0;
+    }
     GPK_CUDA_TRY(cudaLaunchCooperativeKernel(kernel, dim3(grid), dim3(block), args, 0, G->stream));
     G->launches++;
+    if (inject) {
+        GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->spin_limit, 0, sizeof(long long), G->stream));
+        GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->bar_extra, 0, sizeof(unsigned), G->stream));
+    }
     return GPK_OK;
 }
 

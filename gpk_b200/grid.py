@@ -239,6 +239,27 @@ class GPKGrid:
                                            s[2].ctypes.data, sg.ctypes.data, C.byref(moved)))
         return moved.value
 
+    def set_near_threshold(self, tol: float = 1e-12) -> None:
+        """Tolerance of the near-threshold listing (see near_threshold)."""
+        check(lib().gpk_grid_set_near_threshold(self._h, float(tol)))
+
+    def near_threshold(self) -> np.ndarray:
+        """Cells of the last step whose crossing decision lies within the
+        tolerance of its threshold: interface cells with phi_comp != phi and
+        |alpha_new - 1e-6| <= tol (src/gpk_transitions.cpp:291-292), in
+        increasing cell order."""
+        n = C.c_int()
+        check(lib().gpk_grid_near_threshold(self._h, None, 0, C.byref(n)))
+        out = np.empty(n.value, dtype=np.int32)
+        if n.value:
+            check(lib().gpk_grid_near_threshold(self._h, out.ctypes.data, n.value, C.byref(n)))
+        return out
+
+    def set_solid_diffusivity_ratio(self, ratio: float) -> None:
+        """Solid/liquid diffusivity ratio of the partitioned transport
+        (0, the default, is the reference's transport)."""
+        check(lib().gpk_grid_set_solid_diffusivity_ratio(self._h, float(ratio)))
+
     def geometry(self) -> None:
         """Mask and geometry of the current labels, without stepping."""
         check(lib().gpk_grid_geometry(self._h))

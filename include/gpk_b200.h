@@ -258,6 +258,39 @@ int gpk_grid_set_geometry_kernel(gpk_grid* grid, int kind);
  * proxy (src/gpk_physics.cpp:10-63) is not run.                            */
 int gpk_grid_set_external_elastic(gpk_grid* grid, int on);
 
+/* Near-threshold listing (no counterpart in the reference).  The crossing
+ * decision of src/gpk_transitions.cpp:291-292 is
+ *     alpha_new <= 1e-6  &&  phi_comp != phi
+ * with alpha_new = min(alpha + v dt / dx, 1) (:251-271).  Every step lists
+ * the interface cells with phi_comp != phi whose margin alpha_new - 1e-6
+ * lies within tol of zero: the decisions that an arithmetic of another
+ * precision or operation order could flip.  tol defaults to 1e-12 and is
+ * compared in the grid's real type.
+ * gpk_grid_near_threshold returns in *n the number of cells listed by the
+ * last step and writes the first min(*n, cap) of them, in increasing cell
+ * order, to cells.                                                         */
+int gpk_grid_set_near_threshold(gpk_grid* grid, double tol);
+int gpk_grid_near_threshold(gpk_grid* grid, int32_t* cells, int cap, int* n);
+
+/* Solid/liquid diffusivity ratio of the partitioned solute transport (no
+ * counterpart in the reference, whose face flux is D x the smaller liquid
+ * fraction of the two cells times the jump of cL, src/gpk_transport.cpp:
+ * 102-135).  With ratio r > 0 the solid composition k cL also diffuses, with
+ * r D, through the face's shared solid fraction: the face weight becomes
+ * min(l_i, l_j) + r k min(s_i, s_j).  r = 0 (the default) is the reference's
+ * transport bit for bit; r must lie in [0, 1] (r <= 1 keeps the reference's
+ * stable time step valid).                                                  */
+int gpk_grid_set_solid_diffusivity_ratio(gpk_grid* grid, double ratio);
+
+/* Failure injection for tests (no counterpart in the reference).  The next
+ * cooperative launch of the grid (the ordered crossing sweep, or a remap
+ * exchange loop) waits at its first grid barrier for one block more than it
+ * launched, gives up after spin_limit polls (1 .. 2^24; about 100 ns each),
+ * and returns; the step then fails with GPK_ERR_TIMEOUT.  The grid's state
+ * is unspecified afterwards and it keeps reporting the error; the CUDA
+ * context stays usable for other grids.                                    */
+int gpk_grid_inject_wait_timeout(gpk_grid* grid, long long spin_limit);
+
 #ifdef __cplusplus
 }
 #endif

@@ -242,6 +242,26 @@ class OracleGrid(_GridBase):
     def interface_mask(self):
         self._fn("or_interface_mask")(self.h)
 
+    def set_near_threshold(self, tol=1e-12):
+        f = self._fn("or_set_near_tol")
+        f.argtypes = [C.c_void_p, C.c_double]
+        f(self.h, float(tol))
+
+    def near_threshold(self) -> np.ndarray:
+        f = self._fn("or_near_threshold")
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        f.restype = C.c_int
+        n = f(self.h, None, 0)
+        out = np.empty(n, dtype=np.int32)
+        if n:
+            f(self.h, out.ctypes.data, n)
+        return out
+
+    def set_solid_diffusivity_ratio(self, ratio):
+        f = self._fn("or_set_solid_ratio")
+        f.argtypes = [C.c_void_p, C.c_double]
+        f(self.h, float(ratio))
+
     def __del__(self):
         h = getattr(self, "h", None)
         if h:

@@ -2,7 +2,7 @@
 
 TEST INFRASTRUCTURE ONLY.  Only the tests, the smoke check and the CPU
 baseline leg of the benchmark use this file; the product path
-(gpk_b200.alcu over the CUDA library) never does.
+(gpk.alcu over the CUDA library) never does.
 
 Restates, in numpy, the functions of the reference's
 scripts/run_alcu_gpk_microstructure.py that move Cu and relabel cells once

@@ -159,6 +159,13 @@ typedef struct OrGrid {
     real* solid_old; int have_solid_old;
     uint64_t step_id;
     uint32_t* ff_stamp; uint32_t ff_epoch; int* ff_stack;   /* flood-fill scratch */
+    /* near-threshold listing (builder-defined, no reference counterpart):
+     * interface cells with phi_comp != phi whose alpha_new lies within
+     * near_tol of the switching threshold 1e-6, in increasing cell order   */
+    double near_tol; int* near; int n_near;
+    /* solid/liquid diffusivity ratio of the partitioned transport
+     * (builder-defined; 0 is the reference's transport)                    */
+    double solid_ratio;
 } OrGrid;
 
 static inline int IDX(const OrGrid* G, int z, int y, int x) { return z * G->Ny * G->Nx + y * G->Nx + x; }
@@ -373,6 +380,8 @@ OrGrid* SFX(or_create)(int Nz, int Ny, int Nx, double dx, const gpk_thermo_desc*
     G->solid_old = ralloc(N, RL(0.));
     G->ff_stamp = (uint32_t*)calloc((size_t)N, sizeof(uint32_t));
     G->ff_stack = (int*)malloc(sizeof(int) * (size_t)N);
+    G->near = (int*)malloc(sizeof(int) * (size_t)N);
+    G->near_tol = 1e-12;
     build_geometry_kernels(G);
     G->geom_global_separable = Nz > 1 && G->geom_radius > 18;
     if (G->geom_global_separable) {
@@ -389,7 +398,7 @@ void SFX(or_destroy)(OrGrid* G) {
     free(G->phi_comp); free(G->g_comp); free(G->mask);
     free(G->gauss.w); free(G->velocity_gauss.w); free(G->remap_gauss.w);
     free(G->alpha_new); free(G->c_new); free(G->eps_star); free(G->eps_smooth); free(G->eps_tmp);
-    free(G->active); free(G->solid_old); free(G->ff_stamp); free(G->ff_stack);
+    free(G->active); free(G->solid_old); free(G->ff_stamp); free(G->ff_stack); free(G->near);
     free(G->geom_w0); free(G->geom_w1); free(G->geom_w2);
     free(G->geom_I); free(G->geom_smooth); free(G->geom_tmp1); free(G->geom_tmp2);
     free(G);
@@ -425,6 +434,13 @@ void SFX(or_counters)(OrGrid* G, uint64_t out[3]) {
 }
 void SFX(or_set_thermo)(OrGrid* G, const gpk_thermo_desc* th) { G->th = *th; }
 int SFX(or_nactive)(OrGrid* G) { return G->nactive; }
+void SFX(or_set_near_tol)(OrGrid* G, double tol) { G->near_tol = tol; }
+/* cells of the last step's near-threshold list (at most cap written); returns its length */
+int SFX(or_near_threshold)(OrGrid* G, int* out, int cap) {
+    for (int k = 0; k < G->n_near && k < cap; ++k) out[k] = G->near[k];
+    return G->n_near;
+}
+void SFX(or_set_solid_ratio)(OrGrid* G, double r) { G->solid_ratio = r; }
 const int* SFX(or_active)(OrGrid* G) { return G->active; }
 
 /* ----------------------------------------------------------------------- */
@@ -1176,6 +1192,14 @@ static void step_alpha(OrGrid* G, real dt) {
             vn_eff += noise_amp * R_SQRT(rmax(G->T[i], RL(1.))) * normal_from_cell_step(i, G->step_id, 0xabcddcbaULL);
         G->alpha_new[i] = rmin(G->alpha[i] + vn_eff * idt, RL(1.));
     }
+    /* the decision alpha_new <= 1e-6 && phi_comp != phi, listed where the
+     * margin alpha_new - 1e-6 lies within near_tol of zero */
+    G->n_near = 0;
+    const real near_tol = (real)G->near_tol;
+    for (int a = 0; a < G->nactive; ++a) {
+        const int i = G->active[a];
+        if (G->phi_comp[i] != G->phi[i] && R_FABS(G->alpha_new[i] - RL(1e-6)) <= near_tol) G->near[G->n_near++] = i;
+    }
     lmap cnt; lmap_init(&cnt, 256);
     for (int i = 0; i < N; ++i) ++*lmap_ref(&cnt, G->phi[i]);
     G->topology_accepted_last = 0;
@@ -1294,6 +1318,10 @@ static void step_diffusion_partitioned(OrGrid* G, real dt) {
     cell_solid_fraction(G, s);
     for (int i = 0; i < N; ++i) cL[i] = G->c[i] / rmax(RL(1.) - s[i] * (RL(1.) - k), RL(1e-6));
     const real coef = dt * G->D / (G->dx * G->dx);
+    /* solid diffusion (builder-defined): the solid composition k cL diffuses
+     * with ratio x D through the face's shared solid fraction, so the face
+     * weight is lf + ratio k min(s_i, s_j); ratio 0 is the reference */
+    const real rsk = (real)G->solid_ratio * k;
     for (int i = 0; i < N; ++i) {
         int nb[6]; const int nn = faces_transport(G, i, nb);
         const real li = RL(1.) - s[i];
@@ -1301,7 +1329,12 @@ static void step_diffusion_partitioned(OrGrid* G, real dt) {
         for (int a = 0; a < nn; ++a) {
             const int j = nb[a];
             const real lf = rmin(li, RL(1.) - s[j]);
-            if (lf > RL(0.)) flux += lf * (cL[j] - cL[i]);
+            if (rsk > RL(0.)) {
+                const real w = lf + rsk * rmin(s[i], s[j]);
+                if (w > RL(0.)) flux += w * (cL[j] - cL[i]);
+            } else if (lf > RL(0.)) {
+                flux += lf * (cL[j] - cL[i]);
+            }
         }
         G->c_new[i] = G->c[i] + coef * flux;
     }

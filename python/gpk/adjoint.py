@@ -7,11 +7,9 @@ solve, interface velocities v = M_l (e(q) - e(i) - sigma_a(n, g) kappa) with
 four anisotropy coefficients a_m and one mobility per grain, the reference's
 pair projection, and the loss 1/2 |v - v*|^2 + w_E sum e dx^2.
 
-`GPKLoss` is the torch.autograd.Function over it: forward runs one FP64
-forward pass; backward re-runs the forward (nothing from it is kept) and the
-adjoint, and returns the gradients for the eigenstrain, anisotropy and
-mobility tensors.  The reference has no adjoint: the gradients are checked
-against FP64 central differences of the forward.
+The torch.autograd.Function over it is `gpk.autograd.GPKLoss`.  The
+reference has no adjoint: the gradients are checked against FP64 central
+differences of the forward.
 """
 from __future__ import annotations
 
@@ -19,7 +17,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import check, lib
+from gpk_b200._lib import check, lib
 
 
 class AdjointProblem:
@@ -80,41 +78,6 @@ class AdjointProblem:
             pass
 
 
-def _torch_function():
-    import torch
-
-    class GPKLoss(torch.autograd.Function):
-        """loss = GPKLoss.apply(problem, eigenstrain (3), anisotropy (4), mobility (n_mob)), float64."""
-
-        @staticmethod
-        def forward(ctx, problem, eig, aniso, mob):
-            theta = torch.cat([eig.detach(), aniso.detach(), mob.detach()]).cpu().numpy()
-            ctx.problem = problem
-            ctx.save_for_backward(eig, aniso, mob)
-            return torch.tensor(problem.forward(theta), dtype=torch.float64, device=eig.device)
-
-        @staticmethod
-        def backward(ctx, grad_out):
-            eig, aniso, mob = ctx.saved_tensors
-            theta = torch.cat([eig.detach(), aniso.detach(), mob.detach()]).cpu().numpy()
-            _, g = ctx.problem.gradient(theta)
-            g = torch.from_numpy(g).to(device=eig.device, dtype=torch.float64) * grad_out
-            return None, g[:3], g[3:7], g[7:]
-
-    return GPKLoss
-
-
-_fn = None
-
-
-def gpk_loss(problem: AdjointProblem, eig, aniso, mob):
-    """Differentiable loss of `problem` at (eigenstrain, anisotropy, mobility)."""
-    global _fn
-    if _fn is None:
-        _fn = _torch_function()
-    return _fn.apply(problem, eig, aniso, mob)
-
-
 def calibration_case(n: int = 512, grains: int = 256, precipitates: int = 64, seed: int = 11,
                      r_range=(6, 20)):
     """2-D periodic polycrystal of `grains` Voronoi grains (labels 1..grains,
@@ -122,7 +85,7 @@ def calibration_case(n: int = 512, grains: int = 256, precipitates: int = 64, se
     U[r_range] (labels grains+1..grains+precipitates, orientation 0).
     Returns (phi, g, mob_index) with mob_index[l] = l - 1 for grains and -1
     for precipitates."""
-    from .grid import voronoi
+    from gpk_b200.grid import voronoi
     phi, g = voronoi(1, n, n, grains, seed)
     g = g.astype(np.float64)
     rng = np.random.default_rng(seed + 1)

@@ -29,7 +29,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import CAlCuParams, check, lib
+from gpk_b200._lib import CAlCuParams, check, lib
 
 __all__ = ["AlCuTransport", "gauss_taps", "neighbor_competitor", "precip_fraction", "variant_fraction_fields",
            "matrix_composition",

@@ -15,7 +15,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import check, lib
+from gpk_b200._lib import check, lib
 
 
 def variant_eigenstrains(eigen_small: float, eigen_large: float) -> np.ndarray:

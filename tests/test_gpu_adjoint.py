@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 from gpk_b200 import GPKError, GPKGrid, thermo
-from gpk_b200.adjoint import AdjointProblem, calibration_case, gpk_loss
+from gpk.adjoint import AdjointProblem, calibration_case
+from gpk.autograd import gpk_loss
 from oracle import adjoint_oracle
 
 pytestmark = pytest.mark.gpu

@@ -35,7 +35,7 @@ def test_host_taps_agree_with_numpy_to_rounding():
     """gpk_alcu_gauss_taps uses the C library's exp: equal to numpy's taps up
     to the last bit (numpy's vectorised exp rounds differently at times)."""
     from gpk_b200._lib import lib
-    from gpk_b200.alcu import gauss_taps
+    from gpk.alcu import gauss_taps
 
     for s in (0.1, 0.7, 0.75, 0.85, 1.2, 2.0, 8.0 / 3.0, 7.0):
         t = np.zeros(2 * 32 + 1)
@@ -79,7 +79,7 @@ def params(dx=1.5e-9):
 @gpu
 @pytest.mark.parametrize("name", ["2d", "3d"])
 def test_golden_competitor_fraction_composition(torch_cuda, z, name):
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     h = AlCuTransport(z[f"{name}_labels"].shape, params(float(z[f"{name}_dx"])))
@@ -97,7 +97,7 @@ def test_golden_competitor_fraction_composition(torch_cuda, z, name):
 @gpu
 @pytest.mark.parametrize("name", ["2d", "3d"])
 def test_golden_diffusion(torch_cuda, z, name):
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     h = AlCuTransport(z[f"{name}_labels"].shape, params(float(z[f"{name}_dx"])))
@@ -111,7 +111,7 @@ def test_golden_diffusion(torch_cuda, z, name):
 @pytest.mark.parametrize("kind", ["grow", "shrink", "none"])
 @pytest.mark.parametrize("name", ["2d", "3d"])
 def test_golden_partition_transfer(torch_cuda, z, name, kind):
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     h = AlCuTransport(z[f"{name}_labels"].shape, params(float(z[f"{name}_dx"])))
@@ -125,7 +125,7 @@ def test_golden_partition_transfer(torch_cuda, z, name, kind):
 @pytest.mark.parametrize("sigma", [70, 120])
 @pytest.mark.parametrize("name", ["2d", "3d"])
 def test_golden_gaussian_remap(torch_cuda, z, name, sigma):
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     h = AlCuTransport(z[f"{name}_labels"].shape, params())
@@ -140,7 +140,7 @@ def test_golden_gaussian_remap(torch_cuda, z, name, sigma):
 @gpu
 def test_dropins_on_numpy_match_golden(torch_cuda, z):
     """The module-level functions take and return numpy like the reference."""
-    from gpk_b200 import alcu
+    from gpk import alcu
 
     name = "3d"
     p = O.AlCuParams(dx=float(z[f"{name}_dx"]))
@@ -246,7 +246,7 @@ def case_state(shape, kind, seed):
 @gpu
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
 def test_transport_against_oracle(torch_cuda, case):
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     name, shape, kind = case
@@ -298,7 +298,7 @@ def test_transport_against_oracle(torch_cuda, case):
 @pytest.mark.parametrize("sigma", [0.70, 1.2, 2.0])
 @pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
 def test_gaussian_remap_against_oracle(torch_cuda, case, sigma):
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     name, shape, kind = case
@@ -326,7 +326,7 @@ def test_gaussian_remap_against_oracle(torch_cuda, case, sigma):
 @gpu
 def test_partition_transfer_errors_match_oracle(torch_cuda):
     from gpk_b200 import GPKError
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     p = params()
@@ -353,7 +353,7 @@ def test_partition_transfer_errors_match_oracle(torch_cuda):
 def test_full_size_properties_256(torch_cuda):
     """256^3: sums bit-equal to np.sum, the remap keeps every label's
     volume, diffusion and partition transfer keep the summed Cu."""
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     shape = (256, 256, 256)
@@ -396,7 +396,7 @@ def test_diffusion_wide_range_against_oracle(torch_cuda, shape, dx):
     """Compositions spread over twelve decades and several grid spacings, so
     that the substep's divisions by dx meet many operand magnitudes; every
     result is compared bit for bit with numpy's IEEE division."""
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     rng = np.random.default_rng(int(dx * 1e9) % 1000 + len(shape))
@@ -420,7 +420,7 @@ def test_diffusion_wide_range_against_oracle(torch_cuda, shape, dx):
 @pytest.mark.parametrize("sigma", [70, 120])
 @pytest.mark.parametrize("name", ["2d", "3d", "rough_2d", "rough_3d"])
 def test_golden_balanced_remap(torch_cuda, z, name, sigma):
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     h = AlCuTransport(z[f"{name}_labels"].shape, params())
@@ -435,7 +435,7 @@ def test_golden_balanced_remap(torch_cuda, z, name, sigma):
 @gpu
 @pytest.mark.parametrize("name", ["2d", "3d"])
 def test_golden_topology_transactions(torch_cuda, z, name):
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     h = AlCuTransport(z[f"{name}_labels"].shape, params())
@@ -450,7 +450,7 @@ def test_golden_topology_transactions(torch_cuda, z, name):
 def test_certificate_known_answers(torch_cuda, z):
     """The reference's verdicts (local form) on canonical configurations,
     each as a single-cell transaction."""
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     names = sorted({k[5:-7] for k in z.files if k.startswith("topo_") and k.endswith("_labels")})
@@ -488,7 +488,7 @@ TX_CASES = [("plates_96", (96, 96, 96)), ("odd_2d", (67, 45)), ("thin_3d", (5, 4
 @gpu
 @pytest.mark.parametrize("case", TX_CASES, ids=[c[0] for c in TX_CASES])
 def test_topology_transactions_against_oracle(torch_cuda, case):
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     name, shape = case
@@ -523,7 +523,7 @@ BGR_CASES = [("rough_128_2d", (128, 120), 2), ("rough_40_3d", (40, 36, 30), 3), 
 @pytest.mark.parametrize("sigma", [0.70, 1.2])
 @pytest.mark.parametrize("case", BGR_CASES, ids=[c[0] for c in BGR_CASES])
 def test_balanced_remap_against_oracle(torch_cuda, case, sigma):
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     name, shape, variants = case
@@ -557,7 +557,7 @@ def test_balanced_remap_against_oracle(torch_cuda, case, sigma):
 def test_golden_variant_fractions(torch_cuda, z, name):
     """The spectral solve's input, negative fractions (alpha < 0) included:
     their products with 0.0 keep numpy's -0.0."""
-    from gpk_b200 import alcu
+    from gpk import alcu
 
     torch = torch_cuda
     h = alcu.AlCuTransport(z[f"{name}_labels"].shape, params())
@@ -578,7 +578,7 @@ def test_replays_the_reference_trajectory(torch_cuda):
 
     sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
     import alcu_replay as R
-    from gpk_b200.alcu import AlCuTransport
+    from gpk.alcu import AlCuTransport
 
     torch = torch_cuda
     handles = {}

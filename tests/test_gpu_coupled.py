@@ -8,8 +8,8 @@ zero elastic energy the external mode must leave the step unchanged.
 import numpy as np
 import pytest
 
-from gpk_b200 import GPKGrid, SpectralElasticity, thermo
-from gpk_b200.spectral import variant_eigenstrains
+from gpk import GPKGrid, SpectralElasticity, thermo
+from gpk.spectral import variant_eigenstrains
 
 from _cases import PUBLIC_FIELDS
 

@@ -11,8 +11,8 @@ import types
 import numpy as np
 import pytest
 
-from gpk_b200 import GPKError, SpectralElasticity, spectral_elasticity
-from gpk_b200.spectral import variant_eigenstrains
+from gpk import GPKError, SpectralElasticity, spectral_elasticity
+from gpk.spectral import variant_eigenstrains
 from oracle import spectral_oracle
 
 from test_spectral_oracle import golden_cases, rel_err
@@ -117,7 +117,7 @@ def test_gpu_on_the_reference_trajectory():
 
     sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
     import alcu_replay as R
-    from gpk_b200 import spectral_elasticity as gpu_spectral
+    from gpk import spectral_elasticity as gpu_spectral
 
     for vf, p, ref, res in R.spectral_cases():
         d, e, h, r = gpu_spectral(vf, p)
