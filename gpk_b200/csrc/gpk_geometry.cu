@@ -117,6 +117,45 @@ __device__ __forceinline__ void padd(uint32_t b, double& a0, double& a1, double&
         : "r"(b), "d"(w0), "d"(w1), "d"(w2), "d"(w3));
 }
 
+// One predicate for all additions of a tap: nine (3-D, no zero factor) or
+// five (2-D) accumulators.
+__device__ __forceinline__ void padd9(uint32_t b, float& a0, float& a1, float& a2, float& a3, float& a4, float& a5,
+                                      float& a6, float& a7, float& a8, float w0, float w1, float w2, float w3,
+                                      float w4, float w5, float w6, float w7, float w8) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %9, 0;\n\t"
+        "@p add.rn.f32 %0, %0, %10;\n\t@p add.rn.f32 %1, %1, %11;\n\t@p add.rn.f32 %2, %2, %12;\n\t"
+        "@p add.rn.f32 %3, %3, %13;\n\t@p add.rn.f32 %4, %4, %14;\n\t@p add.rn.f32 %5, %5, %15;\n\t"
+        "@p add.rn.f32 %6, %6, %16;\n\t@p add.rn.f32 %7, %7, %17;\n\t@p add.rn.f32 %8, %8, %18;\n\t}"
+        : "+f"(a0), "+f"(a1), "+f"(a2), "+f"(a3), "+f"(a4), "+f"(a5), "+f"(a6), "+f"(a7), "+f"(a8)
+        : "r"(b), "f"(w0), "f"(w1), "f"(w2), "f"(w3), "f"(w4), "f"(w5), "f"(w6), "f"(w7), "f"(w8));
+}
+__device__ __forceinline__ void padd9(uint32_t b, double& a0, double& a1, double& a2, double& a3, double& a4,
+                                      double& a5, double& a6, double& a7, double& a8, double w0, double w1,
+                                      double w2, double w3, double w4, double w5, double w6, double w7, double w8) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %9, 0;\n\t"
+        "@p add.rn.f64 %0, %0, %10;\n\t@p add.rn.f64 %1, %1, %11;\n\t@p add.rn.f64 %2, %2, %12;\n\t"
+        "@p add.rn.f64 %3, %3, %13;\n\t@p add.rn.f64 %4, %4, %14;\n\t@p add.rn.f64 %5, %5, %15;\n\t"
+        "@p add.rn.f64 %6, %6, %16;\n\t@p add.rn.f64 %7, %7, %17;\n\t@p add.rn.f64 %8, %8, %18;\n\t}"
+        : "+d"(a0), "+d"(a1), "+d"(a2), "+d"(a3), "+d"(a4), "+d"(a5), "+d"(a6), "+d"(a7), "+d"(a8)
+        : "r"(b), "d"(w0), "d"(w1), "d"(w2), "d"(w3), "d"(w4), "d"(w5), "d"(w6), "d"(w7), "d"(w8));
+}
+__device__ __forceinline__ void padd5(uint32_t b, float& a0, float& a1, float& a2, float& a3, float& a4, float w0,
+                                      float w1, float w2, float w3, float w4) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %5, 0;\n\t"
+        "@p add.rn.f32 %0, %0, %6;\n\t@p add.rn.f32 %1, %1, %7;\n\t@p add.rn.f32 %2, %2, %8;\n\t"
+        "@p add.rn.f32 %3, %3, %9;\n\t@p add.rn.f32 %4, %4, %10;\n\t}"
+        : "+f"(a0), "+f"(a1), "+f"(a2), "+f"(a3), "+f"(a4)
+        : "r"(b), "f"(w0), "f"(w1), "f"(w2), "f"(w3), "f"(w4));
+}
+__device__ __forceinline__ void padd5(uint32_t b, double& a0, double& a1, double& a2, double& a3, double& a4,
+                                      double w0, double w1, double w2, double w3, double w4) {
+    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %5, 0;\n\t"
+        "@p add.rn.f64 %0, %0, %6;\n\t@p add.rn.f64 %1, %1, %7;\n\t@p add.rn.f64 %2, %2, %8;\n\t"
+        "@p add.rn.f64 %3, %3, %9;\n\t@p add.rn.f64 %4, %4, %10;\n\t}"
+        : "+d"(a0), "+d"(a1), "+d"(a2), "+d"(a3), "+d"(a4)
+        : "r"(b), "d"(w0), "d"(w1), "d"(w2), "d"(w3), "d"(w4));
+}
+
 template <typename real> struct Quad;
 template <> struct Quad<float> {
     float x, y, z, w;
@@ -194,10 +233,9 @@ __device__ __forceinline__ void geo_row(const real* __restrict__ trow, const uin
             if (!zx0 && !ZY0) {
                 const Quad<real> A = Quad<real>::load(t), B = Quad<real>::load(t + 4);
 #pragma unroll
-                for (int s = 0; s < SLOTS; ++s) {
-                    padd(wd[s] & bit, acc[s][0], acc[s][2], acc[s][4], A.x, A.y, A.z);
-                    padd(wd[s] & bit, acc[s][1], acc[s][3], B.x, B.y);
-                }
+                for (int s = 0; s < SLOTS; ++s)
+                    padd5(wd[s] & bit, acc[s][0], acc[s][2], acc[s][4], acc[s][1], acc[s][3], A.x, A.y, A.z, B.x,
+                          B.y);
             } else if (zx0 && !ZY0) {
                 const Quad<real> A = Quad<real>::load(t);
 #pragma unroll
@@ -216,11 +254,9 @@ __device__ __forceinline__ void geo_row(const real* __restrict__ trow, const uin
         if (!zx0 && !ZY0 && !ZZ0) {
             const Quad<real> A = Quad<real>::load(t), B = Quad<real>::load(t + 4), C = Quad<real>::load(t + 8);
 #pragma unroll
-            for (int s = 0; s < SLOTS; ++s) {
-                padd(wd[s] & bit, acc[s][0], acc[s][2], acc[s][4], acc[s][7], A.x, A.y, A.z, A.w);
-                padd(wd[s] & bit, acc[s][1], acc[s][3], acc[s][8], B.x, B.y, B.w);
-                padd(wd[s] & bit, acc[s][5], acc[s][6], C.x, C.y);
-            }
+            for (int s = 0; s < SLOTS; ++s)
+                padd9(wd[s] & bit, acc[s][0], acc[s][2], acc[s][4], acc[s][7], acc[s][1], acc[s][3], acc[s][8],
+                      acc[s][5], acc[s][6], A.x, A.y, A.z, A.w, B.x, B.y, B.w, C.x, C.y);
         } else if (zx0 && !ZY0 && !ZZ0) {
             const Quad<real> A = Quad<real>::load(t);
 #pragma unroll

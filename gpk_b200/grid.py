@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import weakref
 from typing import Callable, Optional
 
 import numpy as np
@@ -36,9 +37,18 @@ class GPKGrid:
         check(L.gpk_grid_create(self.Nz, self.Ny, self.Nx, self.dx, C.byref(self._cthermo), float(D),
                                 float(gaussian_sigma), PRECISIONS[precision], C.byref(h)))
         self._h = h
+        self._dependents = weakref.WeakSet()
 
     # ---- lifetime --------------------------------------------------------
+    def attach(self, dependent) -> None:
+        """Registers a handle built on this grid (an adjoint problem) whose
+        close() must run before the grid is destroyed, whatever order the
+        garbage collector finalises them in."""
+        self._dependents.add(dependent)
+
     def close(self) -> None:
+        for dep in list(getattr(self, "_dependents", ())):
+            dep.close()
         if getattr(self, "_h", None) is not None and self._h.value:
             lib().gpk_grid_destroy(self._h)
         self._h = None

@@ -34,6 +34,7 @@ class AdjointProblem:
         check(lib().gpk_adjoint_create(grid._h, len(mi), mi.ctypes.data_as(C.POINTER(C.c_int32)), self.n_mob,
                                        float(m_fixed), float(sigma0), float(c11), float(c12), float(c44),
                                        float(energy_weight), C.byref(self._h)))
+        grid.attach(self)  # the grid closes this handle first if it goes away first
         self.shape = (grid.Ny, grid.Nx)
 
     @property
@@ -67,9 +68,10 @@ class AdjointProblem:
         return loss.value, g
 
     def close(self) -> None:
-        if self._h:
-            lib().gpk_adjoint_destroy(self._h)
+        h = getattr(self, "_h", None)
+        if h:
             self._h = C.c_void_p()
+            lib().gpk_adjoint_destroy(h)
 
     def __del__(self) -> None:
         try:

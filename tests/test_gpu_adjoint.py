@@ -3,8 +3,12 @@ the hand-written adjoint gradient against FP64 central differences
 (h = 1e-6) of the forward.
 
 Tolerances: forward loss and velocity within 1e-10 relative of the oracle;
-each gradient component within 1e-6 of the largest component plus 1e-4 of
-itself, against central differences.
+each gradient component within 1e-6 relative of its central difference
+wherever that difference is itself accurate to 1e-7 (its change between
+steps h and 2h, which measures its truncation and rounding error, is below
+1e-7 of it); elsewhere within 1e-6 plus four times that measured error.  The
+largest relative error and the number of components held to 1e-6 are
+printed.
 """
 import numpy as np
 import pytest
@@ -45,9 +49,27 @@ def _oracle_forward(grid, mob_index, theta, target):
                                   lambda r2: float(np.exp(-r2 * inv)))
 
 
-def _check_grad(g, fd):
-    scale = np.max(np.abs(fd))
-    assert np.all(np.abs(g - fd) <= 1e-6 * scale + 1e-4 * np.abs(fd)), np.max(np.abs(g - fd)) / scale
+def _central(f, theta, k, h):
+    tp, tm = theta.copy(), theta.copy()
+    tp[k] += h
+    tm[k] -= h
+    return (f(tp) - f(tm)) / (2 * h)
+
+
+def _check_grad(g, f, theta):
+    """g against central differences of the loss f at steps H and 2H."""
+    fd = np.array([_central(f, theta, k, H) for k in range(len(theta))])
+    fd2 = np.array([_central(f, theta, k, 2 * H) for k in range(len(theta))])
+    fd_err = np.abs(fd - fd2)
+    err = np.abs(g - fd)
+    resolved = fd_err <= 1e-7 * np.abs(fd)
+    rel = err[resolved] / np.abs(fd[resolved])
+    worst = float(rel.max()) if rel.size else 0.0
+    print(f"adjoint vs central differences: {int(resolved.sum())} of {len(fd)} components resolved to 1e-7, "
+          f"max relative error there {worst:.3e}; max relative error over all {float(np.max(err / np.abs(fd))):.3e}")
+    assert resolved.sum() >= len(fd) // 2, int(resolved.sum())
+    assert worst <= 1e-6, worst
+    assert np.all(err <= 1e-6 * np.abs(fd) + 4 * fd_err)
 
 
 def test_forward_matches_oracle_and_gradient_matches_central_differences():
@@ -58,13 +80,7 @@ def test_forward_matches_oracle_and_gradient_matches_central_differences():
     assert np.max(np.abs(v - vo)) <= 1e-10 * np.max(np.abs(vo))
     loss2, g = prob.gradient(theta)
     assert loss2 == loss
-    fd = np.empty_like(theta)
-    for k in range(len(theta)):
-        tp, tm = theta.copy(), theta.copy()
-        tp[k] += H
-        tm[k] -= H
-        fd[k] = (_oracle_forward(grid, mob_index, tp, v_star)[0] - _oracle_forward(grid, mob_index, tm, v_star)[0]) / (2 * H)
-    _check_grad(g, fd)
+    _check_grad(g, lambda t: _oracle_forward(grid, mob_index, t, v_star)[0], theta)
 
 
 def test_calibration_512_gradient_all_components():
@@ -73,13 +89,7 @@ def test_calibration_512_gradient_all_components():
     grid, prob, theta, mob_index, v_star = _problem(512, 256, 64, 11, (6, 20))
     loss, g = prob.gradient(theta)
     assert loss > 0 and np.all(np.isfinite(g))
-    fd = np.empty_like(theta)
-    for k in range(len(theta)):
-        tp, tm = theta.copy(), theta.copy()
-        tp[k] += H
-        tm[k] -= H
-        fd[k] = (prob.forward(tp) - prob.forward(tm)) / (2 * H)
-    _check_grad(g, fd)
+    _check_grad(g, prob.forward, theta)
     # deterministic reductions: the same bits every call
     assert np.array_equal(prob.gradient(theta)[1], g)
 

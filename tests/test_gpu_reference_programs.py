@@ -30,7 +30,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden", "validate")
 
 PROGRAMS = [("validate_topology_transactions", 120), ("validate_extended_base_models", 600),
             ("validate_real_materials", 600), ("validate_dimensional_multiphase", 300),
-            ("validate_interface_local_geometry", 300)]
+            ("validate_interface_local_geometry", 300), ("validate_theory_foundations", 600)]
 
 
 def _storage_line(line: str) -> bool:
