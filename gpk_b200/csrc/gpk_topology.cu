@@ -185,6 +185,58 @@ __device__ __forceinline__ bool bounded_branches_connected(const Dims& D, const 
     return true;
 }
 
+// The same two tests from a 5^d occupancy mask already gathered (bit
+// b = lz*25 + ly*5 + lx, lz = 0 in 2-D): the topological number of the inner
+// 3^d box (centre removed) and the bounded branch connectivity.
+__device__ __forceinline__ int topological_number_mask(u128 occ5, bool is3d) {
+    uint32_t occ = 0;
+    const int lzn = is3d ? 3 : 1;
+    for (int lz = 0; lz < lzn; ++lz)
+        for (int ly = 0; ly < 3; ++ly)
+            for (int lx = 0; lx < 3; ++lx) {
+                const int b5 = (is3d ? (lz + 1) * 25 : 0) + (ly + 1) * 5 + lx + 1;
+                occ |= (uint32_t)((occ5 >> b5) & 1) << (lz * 9 + ly * 3 + lx);
+            }
+    occ &= ~(1u << (is3d ? 13 : 4));
+    return count_face_components(occ, is3d);
+}
+
+__device__ __forceinline__ bool bounded_branches_connected_mask(u128 occ, bool is3d, bool exclude_centre) {
+    const int centre = (is3d ? 2 * 25 : 0) + 12;
+    u128 lx0 = 0, lx4 = 0, ly0 = 0, ly4 = 0;
+    const int zcount = is3d ? 5 : 1;
+    for (int lz = 0; lz < zcount; ++lz)
+        for (int l = 0; l < 5; ++l) {
+            lx0 |= bit128(lz * 25 + l * 5);
+            lx4 |= bit128(lz * 25 + l * 5 + 4);
+            ly0 |= bit128(lz * 25 + l);
+            ly4 |= bit128(lz * 25 + 20 + l);
+        }
+    if (exclude_centre) occ &= ~bit128(centre);
+    const int branch_bit[6] = {centre - 1, centre + 1, centre - 5, centre + 5, centre - 25, centre + 25};
+    const int nf = is3d ? 6 : 4;
+    int branches[6], nb = 0;
+    for (int k = 0; k < nf; ++k)
+        if (occ & bit128(branch_bit[k])) branches[nb++] = branch_bit[k];
+    if (nb <= 1) return true;
+    const u128 all = is3d ? ((((u128)1) << 125) - 1) : ((((u128)1) << 25) - 1);
+    u128 comp = bit128(branches[0]);
+    for (;;) {
+        u128 r = comp;
+        r |= (comp << 1) & ~lx0;
+        r |= (comp >> 1) & ~lx4;
+        r |= (comp << 5) & ~ly0;
+        r |= (comp >> 5) & ~ly4;
+        if (is3d) { r |= (comp << 25); r |= (comp >> 25); }
+        r &= all & occ;
+        if (r == comp) break;
+        comp = r;
+    }
+    for (int k = 1; k < nb; ++k)
+        if (!(comp & bit128(branches[k]))) return false;
+    return true;
+}
+
 // ---------------------------------------------------------------------------
 // global flood fill (src/gpk_connectivity.cpp:79-115).  `cap` bounds the
 // stack; overflowing it (only possible if the label counts were wrong)
@@ -530,48 +582,73 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
     unsigned prev_left = (unsigned)m;
     for (int w = 0; w < max_waves; ++w) {
         // ---- phase A: locality, local certificate parts, label-wide needs;
-        //      earliest pending candidate touching each label
+        //      earliest pending candidate touching each label.  One warp per
+        //      pending candidate: the lanes read the 5^d box around its cell
+        //      at once (labels in the serial-time view, and the earlier
+        //      pending candidates there), and ballots give the occupancy
+        //      masks of its old and new label.
         if (tid == 0) { rem[(w + 1) % 3] = 0; a.s->ff_pool = 0; }
-        for (int k = tid; k < m; k += nthr) {
-            if (a.cres[k] != 0) continue;
-            const int4 ci = a.cinfo[k];
-            atomicMin(&a.minL[ci.y], k);
-            atomicMin(&a.minL[ci.z], k);
-            int z0, y0, x0;
-            D.decode(ci.x, z0, y0, x0);
-            bool local = true;
-            for (int dz = (is3d ? -2 : 0); dz <= (is3d ? 2 : 0) && local; ++dz)
-                for (int dy = -2; dy <= 2 && local; ++dy)
-                    for (int dx = -2; dx <= 2; ++dx) {
-                        if (!dz && !dy && !dx) continue;
-                        const int j = D.idx(is3d ? wrap_any(z0 + dz, D.Nz) : z0, wrap_any(y0 + dy, D.Ny),
-                                            wrap_any(x0 + dx, D.Nx));
-                        const int q = a.cmap[j];
-                        if (q >= 0 && q < k && a.cres[q] == 0) {
-                            const int4 cq = a.cinfo[q];
-                            if (cq.y == ci.y || cq.y == ci.z || cq.z == ci.y || cq.z == ci.z) { local = false; break; }
+        {
+            const int lane = threadIdx.x & 31;
+            const int gwarp = tid >> 5, nwarps = nthr >> 5;
+            const int nbox = is3d ? 125 : 25, centre = is3d ? 62 : 12;
+            for (int k = gwarp; k < m; k += nwarps) {
+                if (a.cres[k] != 0) continue;
+                const int4 ci = a.cinfo[k];
+                if (lane == 0) {
+                    atomicMin(&a.minL[ci.y], k);
+                    atomicMin(&a.minL[ci.z], k);
+                }
+                int z0, y0, x0;
+                D.decode(ci.x, z0, y0, x0);
+                bool conflict = false;
+                uint32_t wo[4] = {0u, 0u, 0u, 0u}, wn[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int e = q * 32 + lane;
+                    int32_t lbl = -1;
+                    if (e < nbox) {
+                        const int lz = e / 25, ly = (e / 5) % 5, lx = e % 5;
+                        const int j = D.idx(is3d ? wrap_any(z0 + lz - 2, D.Nz) : z0, wrap_any(y0 + ly - 2, D.Ny),
+                                            wrap_any(x0 + lx - 2, D.Nx));
+                        const int c = a.cmap[j];
+                        lbl = a.phi[j];
+                        if (c > k) {
+                            if (a.cres[c] == 2) lbl = a.cinfo[c].y;  // accepted later: the old label
+                        } else if (c >= 0 && c < k && e != centre && a.cres[c] == 0) {
+                            const int4 cq = a.cinfo[c];
+                            conflict |= cq.y == ci.y || cq.y == ci.z || cq.z == ci.y || cq.z == ci.z;
                         }
                     }
-            int st = 0;
-            if (local) {
-                const SerialView view{a.phi, a.cmap, a.cres, a.cinfo, k};
-                const int to = topological_number(D, view, ci.x, ci.y);
-                const int tn = topological_number(D, view, ci.x, ci.z);
-                st = CS_LOCAL | (min(to, 2) << CS_TO_SHIFT) | (min(tn, 2) << CS_TN_SHIFT);
-                if (to == 0) {
-                    // at k's serial time the label holds at least count0 - (its other candidates) cells
-                    if (a.count0[ci.y] - (a.n_old[ci.y] - 1) >= 2) st |= CS_CNT_REJECT;
-                    else st |= CS_GC;
-                } else if (to > 1) {
-                    if (bounded_branches_connected(D, view, ci.x, ci.y, true)) st |= CS_OLD_LOCAL;
-                    else st |= CS_GO;
+                    wo[q] = __ballot_sync(0xffffffffu, lbl == ci.y);
+                    wn[q] = __ballot_sync(0xffffffffu, lbl == ci.z);
+                    if (nbox <= 32) break;
                 }
-                if (tn > 1) {
-                    if (bounded_branches_connected(D, view, ci.x, ci.z, false)) st |= CS_NEW_LOCAL;
-                    else st |= CS_GN;
+                const bool local = !__any_sync(0xffffffffu, conflict);
+                if (lane == 0) {
+                    int st = 0;
+                    if (local) {
+                        const u128 occ_o = (u128)wo[0] | ((u128)wo[1] << 32) | ((u128)wo[2] << 64) | ((u128)wo[3] << 96);
+                        const u128 occ_n = (u128)wn[0] | ((u128)wn[1] << 32) | ((u128)wn[2] << 64) | ((u128)wn[3] << 96);
+                        const int to = topological_number_mask(occ_o, is3d);
+                        const int tn = topological_number_mask(occ_n, is3d);
+                        st = CS_LOCAL | (min(to, 2) << CS_TO_SHIFT) | (min(tn, 2) << CS_TN_SHIFT);
+                        if (to == 0) {
+                            // at k's serial time the label holds at least count0 - (its other candidates) cells
+                            if (a.count0[ci.y] - (a.n_old[ci.y] - 1) >= 2) st |= CS_CNT_REJECT;
+                            else st |= CS_GC;
+                        } else if (to > 1) {
+                            if (bounded_branches_connected_mask(occ_o, is3d, true)) st |= CS_OLD_LOCAL;
+                            else st |= CS_GO;
+                        }
+                        if (tn > 1) {
+                            if (bounded_branches_connected_mask(occ_n, is3d, false)) st |= CS_NEW_LOCAL;
+                            else st |= CS_GN;
+                        }
+                    }
+                    a.cinfo[k].w = st;
                 }
             }
-            a.cinfo[k].w = st;
         }
         if (!grid_barrier(a.s, nblocks)) return;
         // ---- phase B: readiness; decisions that need only local reads
@@ -885,6 +962,21 @@ __device__ __forceinline__ bool certificate_local(const Dims& D, const int32_t* 
     return true;
 }
 
+// certificate_local from the 5^d occupancy masks of the old and new label
+__device__ __forceinline__ bool certificate_mask(u128 occ_old, u128 occ_new, int old_count, bool is3d) {
+    const int old_object = topological_number_mask(occ_old, is3d);
+    if (old_object == 0 && !(old_count <= 1)) return false;
+    if (old_object > 1 && !bounded_branches_connected_mask(occ_old, is3d, true)) return false;
+    const int new_object = topological_number_mask(occ_new, is3d);
+    if (new_object == 0) return false;
+    if (new_object > 1 && !bounded_branches_connected_mask(occ_new, is3d, false)) return false;
+    return true;
+}
+
+__device__ __forceinline__ u128 mask128(const uint32_t w[4]) {
+    return (u128)w[0] | ((u128)w[1] << 32) | ((u128)w[2] << 64) | ((u128)w[3] << 96);
+}
+
 struct ExchArgs {
     Dims D;
     int32_t* phi; int32_t* pmap; const int32_t* count;
@@ -909,42 +1001,67 @@ __global__ void __launch_bounds__(256) k_bgr_exchange_waves(ExchArgs a, int n, i
     for (int w = 0; w < max_waves; ++w) {
         if (tid == 0) rem[(w + 1) % 3] = 0;
         // ---- phase 1: readiness (no earlier pending exchange of an
-        //      intersecting label pair within Chebyshev distance 2) + decision
-        for (int t = tid; t < n; t += nthr) {
-            const int32_t st = a.estate[t];
-            if (!(st & ES_PENDING)) continue;
-            const int4 e = a.exch[t];
-            bool ready = true;
-            for (int side = 0; side < 2 && ready; ++side) {
-                int z0, y0, x0;
-                D.decode(side ? e.y : e.x, z0, y0, x0);
-                for (int dz = (is3d ? -2 : 0); dz <= (is3d ? 2 : 0) && ready; ++dz)
-                    for (int dy = -2; dy <= 2 && ready; ++dy)
-                        for (int dx = -2; dx <= 2; ++dx) {
-                            const int j = D.idx(is3d ? wrap_any(z0 + dz, D.Nz) : z0, wrap_any(y0 + dy, D.Ny),
-                                                wrap_any(x0 + dx, D.Nx));
-                            const int q = a.pmap[j];
-                            if (q >= 0 && q < t) {
-                                const int4 o = a.exch[q];
-                                if (o.z == e.z || o.z == e.w || o.w == e.z || o.w == e.w) { ready = false; break; }
+        //      intersecting label pair within Chebyshev distance 2) + decision.
+        //      One warp per pending exchange: the lanes read the 5^d boxes
+        //      around both cells at once; ballots give the occupancy masks
+        //      of the two labels that the certificates test.
+        {
+            const int lane = threadIdx.x & 31;
+            const int gwarp = tid >> 5, nwarps = nthr >> 5;
+            const int nbox = is3d ? 125 : 25;
+            for (int t = gwarp; t < n; t += nwarps) {
+                const int32_t st = a.estate[t];
+                if (!(st & ES_PENDING)) continue;
+                const int4 e = a.exch[t];
+                const int A = e.x, B = e.y;
+                const int32_t low = e.z, high = e.w;
+                bool blocked = false;
+                uint32_t aLow[4] = {0u, 0u, 0u, 0u}, aHigh[4] = {0u, 0u, 0u, 0u};
+                uint32_t bLow[4] = {0u, 0u, 0u, 0u}, bHigh[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                for (int side = 0; side < 2; ++side) {
+                    int z0, y0, x0;
+                    D.decode(side ? B : A, z0, y0, x0);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int b = q * 32 + lane;
+                        int32_t lbl = -1;
+                        if (b < nbox) {
+                            const int lz = b / 25, ly = (b / 5) % 5, lx = b % 5;
+                            const int j = D.idx(is3d ? wrap_any(z0 + lz - 2, D.Nz) : z0, wrap_any(y0 + ly - 2, D.Ny),
+                                                wrap_any(x0 + lx - 2, D.Nx));
+                            const int pq = a.pmap[j];
+                            if (pq >= 0 && pq < t) {
+                                const int4 o = a.exch[pq];
+                                blocked |= o.z == e.z || o.z == e.w || o.w == e.z || o.w == e.w;
                             }
+                            lbl = a.phi[j];
+                            if (side == 1 && j == A) lbl = high;  // B's certificate sees A already exchanged
                         }
-            }
-            if (!ready) continue;
-            const int A = e.x, B = e.y;
-            const int32_t low = e.z, high = e.w;
-            bool acc = false;
-            if (a.phi[A] == low && a.phi[B] == high) {
-                const int before = mismatch_count(D, a.phi, A, low, B, high) + mismatch_count(D, a.phi, B, high, A, low);
-                const int after = mismatch_count(D, a.phi, A, high, B, low) + mismatch_count(D, a.phi, B, low, A, high);
-                if (after < before) {
-                    const int cl = a.count[low], ch = a.count[high];
-                    if (certificate_local(D, a.phi, A, low, high, cl, -1, 0) &&
-                        certificate_local(D, a.phi, B, high, low, ch + 1, A, high))
-                        acc = true;
+                        const uint32_t ml = __ballot_sync(0xffffffffu, lbl == low);
+                        const uint32_t mh = __ballot_sync(0xffffffffu, lbl == high);
+                        if (side) { bLow[q] = ml; bHigh[q] = mh; } else { aLow[q] = ml; aHigh[q] = mh; }
+                        if (nbox <= 32) break;
+                    }
+                }
+                if (__any_sync(0xffffffffu, blocked)) continue;
+                if (lane == 0) {
+                    bool acc = false;
+                    if (a.phi[A] == low && a.phi[B] == high) {
+                        const int before =
+                            mismatch_count(D, a.phi, A, low, B, high) + mismatch_count(D, a.phi, B, high, A, low);
+                        const int after =
+                            mismatch_count(D, a.phi, A, high, B, low) + mismatch_count(D, a.phi, B, low, A, high);
+                        if (after < before) {
+                            const int cl = a.count[low], ch = a.count[high];
+                            if (certificate_mask(mask128(aLow), mask128(aHigh), cl, is3d) &&
+                                certificate_mask(mask128(bHigh), mask128(bLow), ch + 1, is3d))
+                                acc = true;
+                        }
+                    }
+                    a.estate[t] = st | ES_READY | (acc ? ES_ACCEPT : 0);
                 }
             }
-            a.estate[t] = st | ES_READY | (acc ? ES_ACCEPT : 0);
         }
         if (!grid_barrier(a.s, nblocks)) return;
         // ---- phase 2: commit
@@ -1156,7 +1273,8 @@ int gpk_crossings(gpk_grid* G, int m) {
     int max_waves = m + 1;
     void* args[] = {&a, &m, &max_waves};
     const void* kern = (const void*)k_crossing_sweep<real>;
-    const int grid = coop_grid(G, kern, 256, m);
+    // phase A runs one warp per pending candidate
+    const int grid = coop_grid(G, kern, 256, (int)std::min<long long>(32LL * m, 1LL << 30));
     GPK_TRY(launch_coop(G, kern, grid, 256, args));
     k_cross_cleanup<<<(m + B - 1) / B, B, 0, G->stream>>>(m, (const int4*)G->cand_info, G->pmap, G->n_old);
     G->launches++;
@@ -1228,7 +1346,8 @@ int gpk_remap_pass(gpk_grid* G) {
     int nn = n;
     void* args[] = {&a, &nn, &max_waves};
     const void* kern = (const void*)k_bgr_exchange_waves<real>;
-    return launch_coop(G, kern, coop_grid(G, kern, 256, n), 256, args);
+    // phase 1 runs one warp per pending exchange
+    return launch_coop(G, kern, coop_grid(G, kern, 256, (int)std::min<long long>(32LL * n, 1LL << 30)), 256, args);
 }
 
 template <typename real>
