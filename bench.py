@@ -470,12 +470,16 @@ def alcu_measurement(with_cpu: bool, steps: int = 10, warmup: int = 3):
     return out
 
 
-def batched_measurement(n_inst: int = 512, steps: int = 10, warmup: int = 3, ws: int = 1, rank: int = 0):
+def batched_measurement(n_inst: int = 512, steps: int = 10, warmup: int = 4, ws: int = 1, rank: int = 0):
     """The lamellar-precipitate sweep: n_inst 2-D instances of sides
-    U{64..512} (FP64, OstwaldThermo), advanced together by the batch engine
-    and, for comparison, as a plain loop over instances (one worker).  With
-    ws > 1 ranks the instances are sharded by cell count (no exchange); the
-    time is the max over ranks and the plain loop is not run."""
+    U{64..512} (FP64, OstwaldThermo), all advanced by one captured CUDA graph
+    per two steps (each instance's captured step a child graph), beside the
+    plain loop over instances and the worker-pool engine (instances on their
+    own streams, worker count autotuned).  Each figure times `steps` steps
+    with CUDA events on the stream the work is issued on; the three run one
+    after another on the same evolving instances.  With ws > 1 ranks the
+    instances are sharded by cell count (no exchange); the time is the max
+    over ranks and only the graph form runs."""
     import torch
     from gpk_b200 import GPKBatch
     from gpk_b200.sweep import lamellar_grid, lamellar_side, shard
@@ -483,20 +487,18 @@ def batched_measurement(n_inst: int = 512, steps: int = 10, warmup: int = 3, ws:
     sizes = [lamellar_side(s) ** 2 for s in seeds]
     mine = shard(sizes, ws)[rank] if ws > 1 else list(range(n_inst))
     grids = [lamellar_grid(seeds[i], precision="f64")[0] for i in mine]
-    cells = sum(sizes)
+    cells = sum(sizes) if ws == 1 else sum(sizes[i] for i in mine)
+    total_cells = sum(sizes)
     streams = [torch.cuda.ExternalStream(g.stream_ptr()) for g in grids]
     batch = GPKBatch(grids)
-    workers, tune_steps = batch.autotune(trial_steps=1)
-    batch.step(warmup)
 
-    def timed(nsteps):
+    def timed_streams(nsteps):
         ts = torch.cuda.Stream()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(ts)
         for st in streams:
             st.wait_event(e0)
-        l0 = sum(g.launch_count() for g in grids)
         batch.step(nsteps)
         for st in streams:
             ev = torch.cuda.Event()
@@ -504,22 +506,47 @@ def batched_measurement(n_inst: int = 512, steps: int = 10, warmup: int = 3, ws:
             ts.wait_event(ev)
         e1.record(ts)
         e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    gs = torch.cuda.ExternalStream(batch.graph_stream_ptr())
+
+    def timed_graph(nsteps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        l0 = sum(g.launch_count() for g in grids)
+        e0.record(gs)
+        batch.step_graph(nsteps)
+        e1.record(gs)
+        e1.synchronize()
         return e0.elapsed_time(e1), sum(g.launch_count() for g in grids) - l0
 
-    _barrier(ws)
-    ms_b, launches = timed(steps)
-    ms_b = _allmax(ms_b, ws)
     res = {"workload": f"{n_inst} lamellar-precipitate 2-D instances, sides U{{64..512}}, stripe thickness "
                        "U{4..16}, spacing/thickness U[2,12], OstwaldThermo, FP64, sigma 1.5",
-           "instances": n_inst, "cells": cells, "steps": steps, "warmup": warmup + tune_steps,
-           "value": cells * steps / (ms_b / 1e3), "unit": "cell-updates/s", "ms": ms_b,
-           "workers": workers, "gpu_launches_rank0": launches, "ranks": ws,
-           "how": "native worker pool, one CUDA stream per instance, worker count autotuned; plain = "
-                  "the same instances stepped one after another"}
+           "instances": n_inst, "cells": total_cells, "steps": steps, "ranks": ws, "unit": "cell-updates/s"}
     if ws == 1:
         batch.workers = 1
-        ms_p, _ = timed(steps)
-        res.update({"plain_value": cells * steps / (ms_p / 1e3), "plain_ms": ms_p, "speedup_vs_plain": ms_p / ms_b})
+        batch.step(2)
+        ms_p = timed_streams(steps)
+        workers, tune_steps = batch.autotune(trial_steps=1)
+        ms_w = timed_streams(steps)
+        res.update({"plain_value": cells * steps / (ms_p / 1e3), "plain_ms": ms_p,
+                    "pool_value": cells * steps / (ms_w / 1e3), "pool_ms": ms_w, "pool_workers": workers})
+    tiles, tile_steps = batch.autotune_tiles(trial_steps=2)
+    batch.step_graph(warmup)  # one ordinary step where fresh, then capture and replays
+    _barrier(ws)
+    ms_g, launches = timed_graph(steps)
+    ms_g = _allmax(ms_g, ws)
+    res.update({"value": total_cells * steps / (ms_g / 1e3), "ms": ms_g, "warmup": warmup,
+                "tile_rows_divisor_by_side": {"<=160": tiles[0], "161-320": tiles[1], ">320": tiles[2]},
+                "autotune_steps": tile_steps,
+                "gpu_launches_rank0": launches,
+                "how": "each instance's step captured once (two steps per graph, counts read on the device, the "
+                       "remap under a device-side gate), the instances' graphs the independent children of one "
+                       "graph, launched once per two steps; plain = the instances stepped one after another; "
+                       "pool = worker threads driving the instances' streams"})
+    if ws == 1:
+        res["speedup_vs_plain"] = ms_p / ms_g
+        res["pool_speedup_vs_plain"] = ms_p / ms_w
     batch.close()
     for g in grids:
         g.close()

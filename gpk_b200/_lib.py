@@ -90,6 +90,12 @@ def lib() -> C.CDLL:
         "gpk_grid_near_threshold": ([vp, vp, i32, C.POINTER(i32)], i32),
         "gpk_grid_set_solid_diffusivity_ratio": ([vp, dbl], i32),
         "gpk_grid_inject_wait_timeout": ([vp, C.c_longlong], i32),
+        "gpk_grid_step_graph": ([vp, i32, dbl, dbl, C.POINTER(dbl)], i32),
+        "gpk_grid_graph_supported": ([vp, C.POINTER(i32)], i32),
+        "gpk_batch_step_graph": ([vp, i32, dbl, dbl], i32),
+        "gpk_batch_graph_stream": ([vp, C.POINTER(vp)], i32),
+        "gpk_batch_autotune_tiles": ([vp, i32, C.POINTER(i32), C.POINTER(i32)], i32),
+        "gpk_grid_set_tile_rows": ([vp, i32], i32),
         "gpk_spectral_create": ([i32, C.POINTER(i32), dbl, dbl, dbl, dbl, C.POINTER(dbl), C.POINTER(vp)], i32),
         "gpk_spectral_destroy": ([vp], i32),
         "gpk_spectral_set_constants": ([vp, dbl, dbl, dbl, dbl, C.POINTER(dbl)], i32),

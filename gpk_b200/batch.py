@@ -35,6 +35,17 @@ class GPKBatch:
     def step(self, steps: int = 1, dt: float = -1.0, dt_cap: float = 1e30) -> None:
         check(lib().gpk_batch_step(self._h, int(steps), float(dt), float(dt_cap)))
 
+    def step_graph(self, steps: int = 2, dt: float = -1.0, dt_cap: float = 1e30) -> None:
+        """The same steps with the whole sweep as one captured CUDA graph (two
+        steps per launch); bit-identical to step()."""
+        check(lib().gpk_batch_step_graph(self._h, int(steps), float(dt), float(dt_cap)))
+
+    def graph_stream_ptr(self) -> int:
+        """cudaStream_t of the sweep graph's launches (for timing events)."""
+        p = C.c_void_p()
+        check(lib().gpk_batch_graph_stream(self._h, C.byref(p)))
+        return p.value or 0
+
     def run(self, t_end: float, dt: float = -1.0, max_steps: int = 1 << 30) -> list:
         out = (C.c_int * len(self.grids))()
         check(lib().gpk_batch_run(self._h, float(t_end), float(dt), int(max_steps), out))
@@ -45,6 +56,14 @@ class GPKBatch:
         w, n = C.c_int(), C.c_int()
         check(lib().gpk_batch_autotune(self._h, int(trial_steps), C.byref(w), C.byref(n)))
         return w.value, n.value
+
+    def autotune_tiles(self, trial_steps: int = 2) -> tuple:
+        """Picks the sweep graph's 2-D geometry tile height per instance-size
+        group; returns (divisor per group (side <= 160, <= 320, larger),
+        steps every instance took while timing)."""
+        ch, n = (C.c_int * 3)(), C.c_int()
+        check(lib().gpk_batch_autotune_tiles(self._h, int(trial_steps), ch, C.byref(n)))
+        return list(ch), n.value
 
     def close(self) -> None:
         if self._h:

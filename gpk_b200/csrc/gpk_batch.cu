@@ -26,6 +26,17 @@ struct gpk_batch {
     std::vector<int> order;  // instance indices, most cells first
     int workers = 1;
     int device = 0;
+    // the whole sweep as one graph: each instance's captured two-step graph
+    // as a child node, no edges between instances
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaGraph_t> children;  // the instance graphs it was built from
+    ~gpk_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (stream) cudaStreamDestroy(stream);
+    }
 };
 
 namespace {
@@ -173,6 +184,133 @@ extern "C" int gpk_batch_run(gpk_batch* b, double t_end, double dt, int max_step
         if (rc != GPK_OK) return rc;
         return gpk_grid_sync(b->grids[i]);
     });
+}
+
+// ---- the sweep as one captured graph -------------------------------------------
+static int batch_graph_build(gpk_batch* b, double dt, double dt_cap) {
+    const int n = (int)b->grids.size();
+    // each instance's two-step graph, captured on its own stream (in parallel)
+    GPK_TRY(for_each_instance(b, [&](int i) { return gpk_grid_graph_prepare(b->grids[i], dt, dt_cap); }));
+    bool same = b->exec && (int)b->children.size() == n;
+    for (int i = 0; same && i < n; ++i) same = b->children[i] == b->grids[i]->step_graph;
+    if (same) return GPK_OK;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    b->children.assign(n, nullptr);
+    GPK_CUDA_TRY(cudaGraphCreate(&b->graph, 0));
+    for (int k = 0; k < n; ++k) {
+        const int i = b->order[k];
+        cudaGraphNode_t node;
+        GPK_CUDA_TRY(cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, b->grids[i]->step_graph));
+        b->children[i] = b->grids[i]->step_graph;
+    }
+    GPK_CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    return GPK_OK;
+}
+
+extern "C" int gpk_batch_graph_stream(gpk_batch* b, void** stream) {
+    if (!b || !stream) return GPK_ERR_INVALID_ARGUMENT;
+    if (!b->stream) {
+        if (cudaSetDevice(b->device) != cudaSuccess) return GPK_ERR_CUDA;
+        GPK_CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    }
+    *stream = (void*)b->stream;
+    return GPK_OK;
+}
+
+extern "C" int gpk_batch_step_graph(gpk_batch* b, int steps, double dt, double dt_cap) {
+    if (!b || steps < 0) {
+        gpk_set_error("batch: null handle or negative step count");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    if (cudaSetDevice(b->device) != cudaSuccess) {
+        gpk_set_error("batch: cudaSetDevice failed");
+        return GPK_ERR_CUDA;
+    }
+    if (!b->stream) GPK_CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    int done = 0;
+    bool fresh = false;
+    for (gpk_grid* G : b->grids) fresh |= G->step_id == 0;
+    if (steps > 0 && fresh) {
+        // one ordinary step makes the buffers and settings a captured step relies on
+        GPK_TRY(gpk_batch_step(b, 1, dt, dt_cap));
+        ++done;
+    }
+    if (steps - done >= 2) {
+        GPK_TRY(batch_graph_build(b, dt, dt_cap));
+        for (gpk_grid* G : b->grids) GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+        for (; steps - done >= 2; done += 2) {
+            GPK_CUDA_TRY(cudaGraphLaunch(b->exec, b->stream));
+            for (gpk_grid* G : b->grids) {
+                G->step_id += 2;
+                G->launches += G->graph_launches;
+            }
+        }
+        GPK_CUDA_TRY(cudaStreamSynchronize(b->stream));
+        // a device-side failure of any instance's steps
+        GPK_TRY(for_each_instance(b, [&](int i) { return gpk_grid_sync(b->grids[i]); }));
+    }
+    if (steps - done > 0) GPK_TRY(gpk_batch_step(b, steps - done, dt, dt_cap));
+    return GPK_OK;
+}
+
+extern "C" int gpk_batch_autotune_tiles(gpk_batch* b, int trial_steps, int* choice_out, int* steps_taken) {
+    if (!b || trial_steps < 1) {
+        gpk_set_error("batch: null handle or trial_steps < 1");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    const int steps = trial_steps + (trial_steps & 1);
+    auto group = [&](gpk_grid* G) {
+        const int side = std::max(G->d.Nx, G->d.Ny);
+        return side <= 160 ? 0 : (side <= 320 ? 1 : 2);
+    };
+    int choice[3] = {1, 1, 1}, taken = 0;
+    if (!b->stream) {
+        void* st = nullptr;
+        GPK_TRY(gpk_batch_graph_stream(b, &st));
+    }
+    // a first call captures the graphs (and steps fresh instances once)
+    GPK_TRY(gpk_batch_step_graph(b, steps, -1.0, 1e30));
+    taken += steps;
+    cudaEvent_t e0, e1;
+    GPK_CUDA_TRY(cudaEventCreate(&e0));
+    GPK_CUDA_TRY(cudaEventCreate(&e1));
+    int rc = GPK_OK;
+    for (int gidx = 0; gidx < 3 && rc == GPK_OK; ++gidx) {
+        bool any = false;
+        for (gpk_grid* G : b->grids) any |= group(G) == gidx;
+        if (!any) continue;
+        float best = 3.4e38f;
+        int best_d = choice[gidx];
+        for (int d : {1, 2, 4}) {
+            for (gpk_grid* G : b->grids)
+                if (group(G) == gidx) G->tile_rows_div = d;
+            // capture for the new tiles outside the timed region
+            rc = gpk_batch_step_graph(b, 2, -1.0, 1e30);
+            taken += 2;
+            if (rc != GPK_OK) break;
+            cudaEventRecord(e0, b->stream);
+            rc = gpk_batch_step_graph(b, steps, -1.0, 1e30);
+            cudaEventRecord(e1, b->stream);
+            taken += steps;
+            if (rc != GPK_OK) break;
+            cudaEventSynchronize(e1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) { best = ms; best_d = d; }
+        }
+        choice[gidx] = best_d;
+        for (gpk_grid* G : b->grids)
+            if (group(G) == gidx) G->tile_rows_div = best_d;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (choice_out)
+        for (int k = 0; k < 3; ++k) choice_out[k] = choice[k];
+    if (steps_taken) *steps_taken = taken;
+    return rc;
 }
 
 extern "C" int gpk_batch_autotune(gpk_batch* b, int trial_steps, int* workers_out, int* steps_taken) {

@@ -399,6 +399,7 @@ extern "C" int gpk_grid_create(int Nz, int Ny, int Nx, double dx, const gpk_ther
 extern "C" int gpk_grid_destroy(gpk_grid* G) {
     if (!G) return GPK_OK;
     if (G->stream) cudaStreamSynchronize(G->stream);
+    gpk_grid_graph_release(G);
     for (void* p : G->allocations) cudaFree(p);
     G->allocations.clear();
     if (G->h_scal) cudaFreeHost(G->h_scal);
@@ -528,6 +529,110 @@ extern "C" int gpk_grid_step(gpk_grid* G, double dt, double dt_cap, double* dt_u
         GPK_TRY(gpk_sync_scalars(G));
         *dt_used = G->h_scal->dt;
     }
+    return GPK_OK;
+}
+
+// ---- the step as a captured graph ---------------------------------------------
+// What a captured step depends on besides device memory: the buffers the
+// host swaps (two steps swap each pair back), the arguments frozen into its
+// launches, and the model.
+static std::vector<uint64_t> graph_signature(gpk_grid* G, double dt, double dt_cap) {
+    std::vector<uint64_t> v;
+    auto P = [&](const void* p) { v.push_back((uint64_t)(uintptr_t)p); };
+    auto D = [&](double d) { uint64_t u; std::memcpy(&u, &d, 8); v.push_back(u); };
+    for (int f = 0; f < GPK_NUM_FIELDS; ++f) P(G->f[f]);
+    P(G->vn2); P(G->c_new); P(G->eps_star); P(G->eps_smooth); P(G->eps_tmp); P(G->solid_old); P(G->s_new);
+    v.push_back((uint64_t)G->have_solid_old);
+    D(dt); D(dt_cap); D(G->near_tol); D(G->solid_ratio); D(G->D); D(G->dx);
+    v.push_back((uint64_t)G->external_elastic);
+    v.push_back((uint64_t)G->geometry_kernel);
+    v.push_back((uint64_t)G->tile_rows_div);
+    v.push_back((uint64_t)G->label_cap);
+    P(G->count);
+    const uint64_t* th = reinterpret_cast<const uint64_t*>(&G->th);
+    for (size_t k = 0; k < sizeof(gpk_thermo_desc) / 8; ++k) v.push_back(th[k]);
+    return v;
+}
+
+void gpk_grid_graph_release(gpk_grid* G) {
+    if (G->step_exec) cudaGraphExecDestroy(G->step_exec);
+    if (G->step_graph) cudaGraphDestroy(G->step_graph);
+    G->step_exec = nullptr;
+    G->step_graph = nullptr;
+    G->graph_sig.clear();
+}
+
+int gpk_grid_graph_prepare(gpk_grid* G, double dt, double dt_cap) {
+    std::string why;
+    if (!gpk_step_graph_supported(G, &why)) {
+        gpk_set_error("captured step unsupported: " + why);
+        return GPK_ERR_UNSUPPORTED_MODEL;
+    }
+    const std::vector<uint64_t> sig = graph_signature(G, dt, dt_cap);
+    if (G->step_graph && sig == G->graph_sig) return GPK_OK;
+    gpk_grid_graph_release(G);
+    GPK_CUDA_TRY(cudaStreamSynchronize(G->stream));
+    const uint64_t step0 = G->step_id, launches0 = G->launches;
+    GPK_CUDA_TRY(cudaStreamBeginCapture(G->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = GPK_OK;
+    for (int k = 0; k < 2 && rc == GPK_OK; ++k)
+        rc = G->precision == GPK_PREC_F64 ? gpk_step_graph_body<double>(G, dt, dt_cap)
+                                          : gpk_step_graph_body<float>(G, dt, dt_cap);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(G->stream, &graph);
+    G->step_id = step0;  // nothing ran yet
+    G->graph_launches = G->launches - launches0;
+    G->launches = launches0;
+    if (rc != GPK_OK || ce != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (rc == GPK_OK) {
+            gpk_set_error(std::string("step capture failed: ") + cudaGetErrorString(ce));
+            rc = GPK_ERR_CUDA;
+        }
+        return rc;
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    if (ie != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        gpk_set_error(std::string("step graph instantiation failed: ") + cudaGetErrorString(ie));
+        return GPK_ERR_CUDA;
+    }
+    G->step_graph = graph;
+    G->step_exec = exec;
+    G->graph_sig = graph_signature(G, dt, dt_cap);  // two steps swap every buffer pair back
+    return G->graph_sig == sig ? GPK_OK : (gpk_grid_graph_release(G), gpk_set_error("step capture left swapped buffers"),
+                                           GPK_ERR_INTERNAL);
+}
+
+extern "C" int gpk_grid_step_graph(gpk_grid* G, int n, double dt, double dt_cap, double* time_out) {
+    if (!G || n < 0) return GPK_ERR_INVALID_ARGUMENT;
+    int done = 0;
+    if (n > 0 && G->step_id == 0) {
+        // the first ordinary step makes the buffers and settings a captured step relies on
+        GPK_TRY(step_once(G, dt, dt_cap));
+        ++done;
+    }
+    if (n - done >= 2) {
+        GPK_TRY(gpk_grid_graph_prepare(G, dt, dt_cap));
+        for (; n - done >= 2; done += 2) {
+            GPK_CUDA_TRY(cudaGraphLaunch(G->step_exec, G->stream));
+            G->step_id += 2;
+            G->launches += G->graph_launches;
+        }
+    }
+    for (; done < n; ++done) GPK_TRY(step_once(G, dt, dt_cap));
+    GPK_TRY(gpk_sync_scalars(G));  // reports a device-side failure of any step
+    if (time_out) *time_out = G->h_scal->time;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_graph_supported(gpk_grid* G, int* supported) {
+    if (!G || !supported) return GPK_ERR_INVALID_ARGUMENT;
+    std::string why;
+    *supported = gpk_step_graph_supported(G, &why);
+    if (!*supported) gpk_set_error(why);
     return GPK_OK;
 }
 
@@ -737,6 +842,15 @@ extern "C" int gpk_grid_inject_wait_timeout(gpk_grid* G, long long spin_limit) {
         return GPK_ERR_INVALID_ARGUMENT;
     }
     G->inject_spin_limit = spin_limit;
+    return GPK_OK;
+}
+
+extern "C" int gpk_grid_set_tile_rows(gpk_grid* G, int divisor) {
+    if (!G || (divisor != 1 && divisor != 2 && divisor != 4)) {
+        gpk_set_error("tile row divisor must be 1, 2 or 4");
+        return GPK_ERR_INVALID_ARGUMENT;
+    }
+    G->tile_rows_div = divisor;
     return GPK_OK;
 }
 

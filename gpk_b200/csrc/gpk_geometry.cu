@@ -187,11 +187,13 @@ struct GeoArgs {
     StepScalars* s;
 };
 
-template <int R, bool IS3D>
+// TD divides the rows of a 2-D tile (1: 1024 cells, 2: 512, 4: 256); smaller
+// tiles give small grids more CTAs (chosen per grid, gpk_grid_set_tile_rows)
+template <int R, bool IS3D, int TD = 1>
 struct GeoShape {
     static constexpr int W = 2 * R + 1;
     static constexpr int TX = 32 - 2 * R;  // halo row = 32 cells = one bitmap word
-    static constexpr int TY = IS3D ? 8 : 1024 / TX;
+    static constexpr int TY = IS3D ? 8 : 1024 / TX / TD;
     static constexpr int TZ = IS3D ? 1024 / (TX * 8) : 1;
     static constexpr int HY = TY + 2 * R, HZ = IS3D ? TZ + 2 * R : 1;
     static constexpr int NROW = HZ * HY;
@@ -206,9 +208,9 @@ struct GeoShape {
     static_assert(NCELL <= 1024 && NLB >= 1, "tile shape");
 };
 
-template <typename real, int R, bool IS3D>
+template <typename real, int R, bool IS3D, int TD>
 constexpr size_t geo_smem_bytes() {
-    typedef GeoShape<R, IS3D> S;
+    typedef GeoShape<R, IS3D, TD> S;
     // table planes | bitmaps | core labels | distinct labels | cells | cell label
     // index | batch cells | 2 mbarriers
     return (size_t)2 * S::PLANE * sizeof(real) + (size_t)S::BM_WORDS * 4 + (size_t)S::NCORE * 4 + (size_t)S::NCELL * 4 +
@@ -291,13 +293,13 @@ __device__ __forceinline__ void geo_row(const real* __restrict__ trow, const uin
 // The tap planes of one label batch.  gp0 = planes streamed before this
 // batch (buffer of global plane g: g & 1, its phase parity: (g >> 1) & 1);
 // gp_total = planes of all batches (the last plane prefetches nothing).
-template <typename real, int R, bool IS3D, int SLOTS>
+template <typename real, int R, bool IS3D, int TD, int SLOTS>
 __device__ __forceinline__ void geo_accumulate(const GeoArgs<real>& a, const uint32_t* __restrict__ bm,
                                                const real* __restrict__ tab0, const real* __restrict__ tab1,
                                                uint64_t* bars, int gp0, int gp_total, int nact, int tid,
                                                real acc[SLOTS][9], const int bmrow[SLOTS], const int lx[SLOTS],
                                                const uint32_t vmask[SLOTS], bool& ok) {
-    typedef GeoShape<R, IS3D> S;
+    typedef GeoShape<R, IS3D, TD> S;
     constexpr int W = S::W;
 #pragma unroll
     for (int s = 0; s < SLOTS; ++s)
@@ -400,9 +402,9 @@ constexpr int GEO_MIN_SLOTS = 2;
 
 // three CTAs per SM in float (80 registers); two in double, whose 36
 // accumulators of a 4-cell thread take 72 registers
-template <typename real, int R, bool IS3D>
+template <typename real, int R, bool IS3D, int TD>
 __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) k_geometry_tiled(GeoArgs<real> a) {
-    typedef GeoShape<R, IS3D> S;
+    typedef GeoShape<R, IS3D, TD> S;
     extern __shared__ __align__(128) unsigned char smem[];
     real* tab0 = reinterpret_cast<real*>(smem);
     real* tab1 = tab0 + S::PLANE;
@@ -579,9 +581,9 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) k_geometry_til
         real acc[4][9];
         const int gp0 = b * S::NPLANES;
         switch (slots) {
-        case 2: geo_accumulate<real, R, IS3D, 2>(a, bm, tab0, tab1, bars, gp0, gp_total, nact, tid, acc, bmrow, lx, vmask, ok); break;
-        case 3: geo_accumulate<real, R, IS3D, 3>(a, bm, tab0, tab1, bars, gp0, gp_total, nact, tid, acc, bmrow, lx, vmask, ok); break;
-        default: geo_accumulate<real, R, IS3D, 4>(a, bm, tab0, tab1, bars, gp0, gp_total, nact, tid, acc, bmrow, lx, vmask, ok); break;
+        case 2: geo_accumulate<real, R, IS3D, TD, 2>(a, bm, tab0, tab1, bars, gp0, gp_total, nact, tid, acc, bmrow, lx, vmask, ok); break;
+        case 3: geo_accumulate<real, R, IS3D, TD, 3>(a, bm, tab0, tab1, bars, gp0, gp_total, nact, tid, acc, bmrow, lx, vmask, ok); break;
+        default: geo_accumulate<real, R, IS3D, TD, 4>(a, bm, tab0, tab1, bars, gp0, gp_total, nact, tid, acc, bmrow, lx, vmask, ok); break;
         }
         if (ok) {
 #pragma unroll
@@ -596,20 +598,20 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) k_geometry_til
     }
 }
 
-template <typename real, int R, bool IS3D>
+template <typename real, int R, bool IS3D, int TD = 1>
 static int launch_tiled(gpk_grid* G, const GeoArgs<real>& a0) {
-    typedef GeoShape<R, IS3D> S;
+    typedef GeoShape<R, IS3D, TD> S;
     GeoArgs<real> a = a0;
     a.ntx = (G->d.Nx + S::TX - 1) / S::TX;
     a.nty = (G->d.Ny + S::TY - 1) / S::TY;
     a.ntz = (G->d.Nz + S::TZ - 1) / S::TZ;
-    const size_t smem = geo_smem_bytes<real, R, IS3D>();
+    const size_t smem = geo_smem_bytes<real, R, IS3D, TD>();
     // set once per process (thread-safe initialisation of a function-local static)
     static const cudaError_t attr_rc = cudaFuncSetAttribute(
-        k_geometry_tiled<real, R, IS3D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_geometry_tiled<real, R, IS3D, TD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     GPK_CUDA_TRY(attr_rc);
     const int ntiles = a.ntx * a.nty * a.ntz;
-    k_geometry_tiled<real, R, IS3D><<<ntiles, 256, smem, G->stream>>>(a);
+    k_geometry_tiled<real, R, IS3D, TD><<<ntiles, 256, smem, G->stream>>>(a);
     G->launches++;
     GPK_CUDA_TRY(cudaGetLastError());
     return GPK_OK;
@@ -651,7 +653,11 @@ int gpk_geometry_tiled(gpk_grid* G, int R, real inv_dx, real inv_dx2, real dx, r
     case 5: return launch_tiled<real, 5, false>(G, a);
     case 6: return launch_tiled<real, 6, false>(G, a);
     case 7: return launch_tiled<real, 7, false>(G, a);
-    case 8: return launch_tiled<real, 8, false>(G, a);
+    case 8:
+        // the sweep's sigma 1.5: tile height per grid
+        if (G->tile_rows_div == 4) return launch_tiled<real, 8, false, 4>(G, a);
+        if (G->tile_rows_div == 2) return launch_tiled<real, 8, false, 2>(G, a);
+        return launch_tiled<real, 8, false>(G, a);
     case 9: return launch_tiled<real, 9, false>(G, a);
     case 10: return launch_tiled<real, 10, false>(G, a);
     default: return -1;

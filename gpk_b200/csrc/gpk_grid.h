@@ -104,6 +104,9 @@ struct gpk_grid {
     // waves of the crossing sweeps, waves of the remap exchange loops,
     // crossing candidates, remap proposals (summed since last read)
     uint64_t wave_stats[4] = {};
+    // rows of a 2-D geometry tile at kernel radius 8 divided by 1, 2 or 4
+    // (1024, 512 or 256 cells; gpk_grid_set_tile_rows)
+    int tile_rows_div = 1;
     // geometry kernel choice: 0 = tiled (per-cell kernel where no tiled
     // instantiation exists), 1 = per-cell kernel
     int geometry_kernel = 0;
@@ -115,6 +118,12 @@ struct gpk_grid {
     double near_tol = 1e-12;
     // solid/liquid diffusivity ratio of the partitioned transport (0: the reference)
     double solid_ratio = 0;
+    // captured two-step graph (gpk_grid_step_graph / gpk_batch_step_graph)
+    // and what it was captured with; it replays only while these still hold
+    cudaGraph_t step_graph = nullptr;
+    cudaGraphExec_t step_exec = nullptr;
+    std::vector<uint64_t> graph_sig;
+    uint64_t graph_launches = 0;           // kernel launches per replay
     // gpk_grid_inject_wait_timeout: spin limit for the next cooperative
     // launch, whose grid barrier then also awaits one block that never comes
     long long inject_spin_limit = 0;
@@ -136,15 +145,24 @@ int gpk_stage_collect(gpk_grid* G);
 template <typename real> int gpk_build_tables(gpk_grid* G);
 template <typename real> int gpk_step_impl(gpk_grid* G, double dt, double dt_cap);
 template <typename real> int gpk_geometry_only(gpk_grid* G);
-template <typename real> int gpk_interface_mask(gpk_grid* G);
+template <typename real> int gpk_interface_mask(gpk_grid* G, const unsigned long long* gate = nullptr);
 template <typename real> int gpk_max_dt_impl(gpk_grid* G, double* out);
 template <typename real> int gpk_phase_volume_impl(gpk_grid* G, int32_t label, double* out);
 template <typename real>
 int gpk_geometry_tiled(gpk_grid* G, int R, real inv_dx, real inv_dx2, real dx, real kappa_limit);
-template <typename real> int gpk_bgr_scores_tiled(gpk_grid* G, int radius, real* res, real* best);
+template <typename real>
+int gpk_bgr_scores_tiled(gpk_grid* G, int radius, real* res, real* best, const unsigned long long* gate = nullptr);
 template <typename real> int gpk_projection_tiled(gpk_grid* G, int radius);
 int gpk_recount_labels(gpk_grid* G);
 int gpk_topology_simple_move_impl(gpk_grid* G, int cell, int32_t new_label, int* result);
 int gpk_alloc(gpk_grid* G, void** p, size_t bytes);
 int gpk_ensure_label_capacity(gpk_grid* G, int cap);
 int gpk_sync_scalars(gpk_grid* G);
+template <typename real> int gpk_remap_pass_graph(gpk_grid* G, const unsigned long long* gate);
+template <typename real> int gpk_step_graph_body(gpk_grid* G, double dt_req, double dt_cap);
+int gpk_step_graph_supported(gpk_grid* G, std::string* why);
+// captures (or keeps) the grid's two-step graph for (dt, dt_cap); GPK_OK
+// when G->step_graph holds a graph that replays two of its steps
+int gpk_grid_graph_prepare(gpk_grid* G, double dt, double dt_cap);
+void gpk_grid_graph_release(gpk_grid* G);
+int gpk_remap_gates(gpk_grid* G, int stage);

@@ -87,6 +87,9 @@ struct StepScalars {
     long long spin_limit;
     unsigned bar_extra;
     unsigned pad2;
+    // remap passes inside a captured step: the first pass's exchanges and
+    // the gate of the second (3-D) pass
+    unsigned long long exch_first, gate2;
     // instrumentation of the label-wide work (summed until read)
     unsigned long long flood_tasks, flood_cells, count_tasks, count_scanned;
 };

@@ -1,6 +1,6 @@
 // gpk_local.cu — tiled kernels for the small-radius Gaussian boxes of a step:
 // the pair velocity projection (src/gpk_physics.cpp:152-193) and the
-// balanced-remap scores (src/gpk_transitions.cpp:53-91, on label bitmaps).
+// balanced-remap scores (src/gpk_transitions.cpp:53-91).
 //
 // Both visit a (2R+1)^d box (R = 3 at the configured sigmas) around every
 // interface cell and accumulate, in double and in the reference's z -> y -> x
@@ -91,6 +91,75 @@ __device__ __forceinline__ void score_box_impl(const int32_t* __restrict__ lab, 
             }
         }
 }
+template <int R, bool IS3D, int NC>
+__device__ __forceinline__ void score_box(const int32_t* __restrict__ lab, int base, const double* __restrict__ w,
+                                          int32_t pi, const int32_t cand[6], double& resident, double sup[6]) {
+    typedef LocShape<R, IS3D> S;
+    score_box_impl<R, IS3D, NC, S::HX, S::HY>(lab, base, w, pi, cand, resident, sup);
+}
+template <typename real, int R, bool IS3D>
+__global__ void __launch_bounds__(256) k_bgr_scores_tiled(Dims D, const int32_t* __restrict__ phi,
+                                                          const uint8_t* __restrict__ mask, int ntx, int nty,
+                                                          const double* __restrict__ wtab, int32_t* __restrict__ phi_comp,
+                                                          real* __restrict__ res_out, real* __restrict__ best_out,
+                                                          const unsigned long long* __restrict__ gate) {
+    if (gate && *gate == 0ull) return;  // device-side skip inside a captured step
+    typedef LocShape<R, IS3D> S;
+    __shared__ int32_t lab[S::NH];
+    __shared__ int16_t cells[S::NCELL];
+    __shared__ double w[S::R2MAX + 1];
+    const int t = blockIdx.x;
+    const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
+    const int x0 = tx * S::TX, y0 = ty * S::TY, z0 = tz * S::TZ;
+    const int ncell = tile_interface_cells<R, IS3D>(D, mask, x0, y0, z0, cells);
+    if (ncell == 0) return;
+    for (int e = threadIdx.x; e < S::NH; e += 256) {
+        const int hx = e % S::HX, hy = (e / S::HX) % S::HY, hz = e / (S::HX * S::HY);
+        const int x = wrap_any(x0 + hx - R, D.Nx), y = wrap_any(y0 + hy - R, D.Ny);
+        const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
+        lab[e] = phi[D.idx(z, y, x)];
+    }
+    for (int e = threadIdx.x; e <= S::R2MAX; e += 256) w[e] = wtab[e];
+    __syncthreads();
+    const int plane = S::HX * S::HY;
+    for (int c = threadIdx.x; c < ncell; c += 256) {
+        const int lc = cells[c];
+        const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
+        const int cb = ((IS3D ? lz + R : 0) * S::HY + ly + R) * S::HX + lx + R;
+        const int32_t pi = lab[cb];
+        // distinct unlike face-neighbour labels in face order; -1 pads
+        const int fo[6] = {-1, +1, -S::HX, +S::HX, -plane, +plane};
+        int32_t cand[6] = {-1, -1, -1, -1, -1, -1};
+        int nc = 0;
+        for (int k = 0; k < (IS3D ? 6 : 4); ++k) {
+            const int32_t v = lab[cb + fo[k]];
+            if (v == pi) continue;
+            bool known = false;
+            for (int q = 0; q < nc; ++q) known |= cand[q] == v;
+            if (!known) cand[nc++] = v;
+        }
+        double resident = 0.0, sup[6] = {0, 0, 0, 0, 0, 0};
+        const int base = cb - (IS3D ? R * plane : 0) - R * S::HX - R;
+        // candidate slots beyond the warp's largest count are skipped
+        const int ncw = __reduce_max_sync(__activemask(), nc);
+        switch (ncw) {
+        case 0: score_box<R, IS3D, 0>(lab, base, w, pi, cand, resident, sup); break;
+        case 1: score_box<R, IS3D, 1>(lab, base, w, pi, cand, resident, sup); break;
+        case 2: score_box<R, IS3D, 2>(lab, base, w, pi, cand, resident, sup); break;
+        case 3: score_box<R, IS3D, 3>(lab, base, w, pi, cand, resident, sup); break;
+        default: score_box<R, IS3D, 6>(lab, base, w, pi, cand, resident, sup); break;
+        }
+        double best = -1.0;
+        int32_t best_label = pi;
+        for (int q = 0; q < nc; ++q)
+            if (sup[q] > best) { best = sup[q]; best_label = cand[q]; }
+        const int i = D.idx(z0 + lz, y0 + ly, x0 + lx);
+        res_out[i] = (real)resident;
+        best_out[i] = (real)best;
+        phi_comp[i] = best_label;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // pair projection
 // ---------------------------------------------------------------------------
@@ -166,248 +235,14 @@ __global__ void __launch_bounds__(256) k_projection_tiled(Dims D, const int32_t*
     }
 }
 
-// ---------------------------------------------------------------------------
-// balanced-remap scores on label bitmaps
-// ---------------------------------------------------------------------------
-// A tile of 26 x TY x TZ cells has halo rows of exactly 32 cells (R = 3), so
-// for one label a halo row is one 32-bit word.  The CTA lists the labels the
-// scores need (each interface cell's resident label and its unlike face
-// neighbours), builds one word per halo row and listed label with warp
-// match_any, and then adds, for each label of a cell, the weight of every
-// tap whose bit is set, in z -> y -> x order, under a predicate: the
-// reference's `if (value == label) acc += w` (src/gpk_transitions.cpp:67-85)
-// without a label load or compare per tap.  A tile that needs more labels
-// than the bitmap budget runs the per-tap comparison on its staged labels.
-template <bool IS3D> struct BitTile;
-template <> struct BitTile<true> { static constexpr int TY = 8, TZ = 8; };
-template <> struct BitTile<false> { static constexpr int TY = 32, TZ = 1; };
-
-template <bool IS3D>
-struct BitShape {
-    static constexpr int R = 3;
-    static constexpr int TX = 32 - 2 * R, HX = 32;
-    static constexpr int TY = BitTile<IS3D>::TY, TZ = BitTile<IS3D>::TZ;
-    static constexpr int HY = TY + 2 * R, HZ = IS3D ? TZ + 2 * R : 1;
-    static constexpr int NROW = HY * HZ;
-    static constexpr int NROWP = NROW | 1;
-    static constexpr int NCELL = TX * TY * TZ;
-    static constexpr int NH = NROW * HX;
-    static constexpr int R2MAX = (IS3D ? 3 : 2) * R * R;
-    static constexpr int NL = 20;       // bitmaps per tile (static shared memory stays under 48 KB)
-    static constexpr int HSLOT = 64;    // label hash slots
-};
-
-// acc += w when bit b of m is set; one predicate per tap for all labels
-__device__ __forceinline__ void badd(uint32_t m, double& a, double w) {
-    asm("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %1, 0;\n\t@p add.rn.f64 %0, %0, %2;\n\t}"
-        : "+d"(a)
-        : "r"(m), "d"(w));
-}
-
-// the hash slot of label v, inserting it when absent (-1: table full)
-__device__ __forceinline__ int label_slot_insert(int32_t* keys, int32_t v, int nslot) {
-    unsigned h = ((unsigned)v * 2654435761u) >> 26;  // 6 bits
-    for (int k = 0; k < nslot; ++k) {
-        const int sl = (int)((h + k) & (nslot - 1));
-        const int32_t old = atomicCAS(&keys[sl], -1, v);
-        if (old == -1 || old == v) return sl;
-    }
-    return -1;
-}
-__device__ __forceinline__ int label_slot_find(const int32_t* keys, int32_t v, int nslot) {
-    unsigned h = ((unsigned)v * 2654435761u) >> 26;
-    for (int k = 0; k < nslot; ++k) {
-        const int sl = (int)((h + k) & (nslot - 1));
-        const int32_t key = keys[sl];
-        if (key == v) return sl;
-        if (key == -1) return -1;
-    }
-    return -1;
-}
-
-// Resident and NC candidate sums of one cell over its 7^d box, rows z -> y,
-// taps x ascending; li[k] is the bitmap base of label k (0: resident).
-template <bool IS3D, int NC>
-__device__ __forceinline__ void score_bits(const uint32_t* __restrict__ bm, const double* __restrict__ w,
-                                           const int li[7], int lx, int ly, int lz, double& resident,
-                                           double sup[6]) {
-    typedef BitShape<IS3D> S;
-    constexpr int R = S::R;
-#pragma unroll 1
-    for (int dz = (IS3D ? -R : 0); dz <= (IS3D ? R : 0); ++dz)
-#pragma unroll 1
-        for (int dy = -R; dy <= R; ++dy) {
-            const int row = ((IS3D ? lz + R + dz : 0) * S::HY) + ly + R + dy;
-            const int r2 = dy * dy + dz * dz;
-            const double w0 = w[r2 + 9], w1 = w[r2 + 4], w2 = w[r2 + 1], w3 = w[r2];
-            const uint32_t m0 = bm[li[0] + row] >> lx;
-            badd(m0 & 1u, resident, w0); badd(m0 & 2u, resident, w1); badd(m0 & 4u, resident, w2);
-            badd(m0 & 8u, resident, w3); badd(m0 & 16u, resident, w2); badd(m0 & 32u, resident, w1);
-            badd(m0 & 64u, resident, w0);
-#pragma unroll
-            for (int q = 0; q < NC; ++q) {
-                const uint32_t m = bm[li[q + 1] + row] >> lx;
-                badd(m & 1u, sup[q], w0); badd(m & 2u, sup[q], w1); badd(m & 4u, sup[q], w2);
-                badd(m & 8u, sup[q], w3); badd(m & 16u, sup[q], w2); badd(m & 32u, sup[q], w1);
-                badd(m & 64u, sup[q], w0);
-            }
-        }
-}
-
-template <typename real, bool IS3D>
-__global__ void __launch_bounds__(256) k_bgr_scores_bits(Dims D, const int32_t* __restrict__ phi,
-                                                         const uint8_t* __restrict__ mask, int ntx, int nty,
-                                                         const double* __restrict__ wtab, int nl_cap,
-                                                         int32_t* __restrict__ phi_comp, real* __restrict__ res_out,
-                                                         real* __restrict__ best_out) {
-    typedef BitShape<IS3D> S;
-    constexpr int R = S::R;
-    __shared__ int32_t lab[S::NH];
-    __shared__ uint32_t bm[S::NL * S::NROWP];
-    __shared__ int16_t cells[S::NCELL];
-    __shared__ double w[S::R2MAX + 1];
-    __shared__ int32_t keys[S::HSLOT];
-    __shared__ int8_t dense[S::HSLOT];   // bitmap index of a slot, -1 when unused
-    __shared__ int s_ncell, s_nl, s_full;
-    typedef cub::BlockScan<int, 256> BS;
-    __shared__ typename BS::TempStorage scan;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int t = blockIdx.x;
-    const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
-    const int x0 = tx * S::TX, y0 = ty * S::TY, z0 = tz * S::TZ;
-    // 1. interface cells of the tile, in flat tile order
-    {
-        constexpr int PER = (S::NCELL + 255) / 256;
-        int flags[PER];
-        int cnt = 0;
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            const int c = tid * PER + k;
-            int f = 0;
-            if (c < S::NCELL) {
-                const int lx = c % S::TX, ly = (c / S::TX) % S::TY, lz = c / (S::TX * S::TY);
-                const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
-                if (x < D.Nx && y < D.Ny && z < D.Nz) f = mask[D.idx(z, y, x)];
-            }
-            flags[k] = f;
-            cnt += f;
-        }
-        int ex, total;
-        BS(scan).ExclusiveSum(cnt, ex, total);
-#pragma unroll
-        for (int k = 0; k < PER; ++k)
-            if (flags[k]) cells[ex++] = (int16_t)(tid * PER + k);
-        if (tid == 0) { s_ncell = total; s_full = 0; }
-    }
-    if (tid < S::HSLOT) keys[tid] = -1;
-    __syncthreads();
-    const int ncell = s_ncell;
-    if (ncell == 0) return;
-    // 2. halo labels: one warp per row of 32 consecutive cells
-    for (int r = warp; r < S::NROW; r += 8) {
-        const int hy = r % S::HY, hz = r / S::HY;
-        const int x = wrap_any(x0 + lane - R, D.Nx), y = wrap_any(y0 + hy - R, D.Ny);
-        const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
-        lab[r * S::HX + lane] = phi[D.idx(z, y, x)];
-    }
-    for (int e = tid; e <= S::R2MAX; e += 256) w[e] = wtab[e];
-    __syncthreads();
-    const int plane = S::HX * S::HY;
-    const int fo[6] = {-1, +1, -S::HX, +S::HX, -plane, +plane};
-    // 3. labels the scores need
-    for (int c = tid; c < ncell; c += 256) {
-        const int lc = cells[c];
-        const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
-        const int cb = ((IS3D ? lz + R : 0) * S::HY + ly + R) * S::HX + lx + R;
-        if (label_slot_insert(keys, lab[cb], S::HSLOT) < 0) s_full = 1;
-        for (int k = 0; k < (IS3D ? 6 : 4); ++k)
-            if (label_slot_insert(keys, lab[cb + fo[k]], S::HSLOT) < 0) s_full = 1;
-    }
-    __syncthreads();
-    if (warp == 0) {
-        // dense bitmap index per used slot, in slot order
-        for (int base = 0; base < S::HSLOT; base += 32) {
-            const bool used = keys[base + lane] != -1;
-            const unsigned bal = __ballot_sync(0xffffffffu, used);
-            const int before = (base == 0 ? 0 : s_nl) + __popc(bal & ((1u << lane) - 1u));
-            __syncwarp();
-            dense[base + lane] = (int8_t)(used ? before : -1);
-            if (lane == 0) s_nl = (base == 0 ? 0 : s_nl) + __popc(bal);
-            __syncwarp();
-        }
-    }
-    __syncthreads();
-    const int nl = s_nl;
-    const bool bitmaps = !s_full && nl <= (nl_cap < S::NL ? nl_cap : S::NL);
-    if (bitmaps) {
-        // 4. one word per halo row and listed label (words of absent labels stay 0)
-        for (int e = tid; e < nl * S::NROWP; e += 256) bm[e] = 0u;
-        __syncthreads();
-        for (int r = warp; r < S::NROW; r += 8) {
-            const int32_t v = lab[r * S::HX + lane];
-            const unsigned grp = __match_any_sync(0xffffffffu, v);
-            if (lane == __ffs(grp) - 1) {
-                const int sl = label_slot_find(keys, v, S::HSLOT);
-                if (sl >= 0 && dense[sl] >= 0) bm[dense[sl] * S::NROWP + r] = grp;
-            }
-        }
-        __syncthreads();
-    }
-    // 5. scores
-    for (int c = tid; c < ncell; c += 256) {
-        const int lc = cells[c];
-        const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
-        const int cb = ((IS3D ? lz + R : 0) * S::HY + ly + R) * S::HX + lx + R;
-        const int32_t pi = lab[cb];
-        int32_t cand[6] = {-1, -1, -1, -1, -1, -1};
-        int nc = 0;
-        for (int k = 0; k < (IS3D ? 6 : 4); ++k) {
-            const int32_t v = lab[cb + fo[k]];
-            if (v == pi) continue;
-            bool known = false;
-            for (int q = 0; q < nc; ++q) known |= cand[q] == v;
-            if (!known) cand[nc++] = v;
-        }
-        double resident = 0.0, sup[6] = {0, 0, 0, 0, 0, 0};
-        if (bitmaps) {
-            // bitmap rows of the resident label and the candidates; slots
-            // past nc read label 0's rows into sums that are never used
-            int li[7];
-            li[0] = dense[label_slot_find(keys, pi, S::HSLOT)] * S::NROWP;
-#pragma unroll
-            for (int q = 0; q < 6; ++q)
-                li[q + 1] = q < nc ? dense[label_slot_find(keys, cand[q], S::HSLOT)] * S::NROWP : li[0];
-            const int ncw = __reduce_max_sync(__activemask(), nc);
-            switch (ncw) {
-            case 0: score_bits<IS3D, 0>(bm, w, li, lx, ly, lz, resident, sup); break;
-            case 1: score_bits<IS3D, 1>(bm, w, li, lx, ly, lz, resident, sup); break;
-            case 2: score_bits<IS3D, 2>(bm, w, li, lx, ly, lz, resident, sup); break;
-            case 3: score_bits<IS3D, 3>(bm, w, li, lx, ly, lz, resident, sup); break;
-            default: score_bits<IS3D, 6>(bm, w, li, lx, ly, lz, resident, sup); break;
-            }
-        } else {
-            const int base = cb - (IS3D ? R * plane : 0) - R * S::HX - R;
-            score_box_impl<R, IS3D, 6, S::HX, S::HY>(lab, base, w, pi, cand, resident, sup);
-        }
-        double best = -1.0;
-        int32_t best_label = pi;
-        for (int q = 0; q < nc; ++q)
-            if (sup[q] > best) { best = sup[q]; best_label = cand[q]; }
-        const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
-        const int i = D.idx(z, y, x);
-        res_out[i] = (real)resident;
-        best_out[i] = (real)best;
-        phi_comp[i] = best_label;
-    }
-}
-
-template <typename real, bool IS3D>
-static int launch_scores_bits(gpk_grid* G, real* res, real* best) {
-    typedef BitShape<IS3D> S;
+template <typename real, int R, bool IS3D>
+static int launch_scores(gpk_grid* G, real* res, real* best, const unsigned long long* gate) {
+    typedef LocShape<R, IS3D> S;
     const Dims D = G->d;
     const int ntx = (D.Nx + S::TX - 1) / S::TX, nty = (D.Ny + S::TY - 1) / S::TY, ntz = (D.Nz + S::TZ - 1) / S::TZ;
-    k_bgr_scores_bits<real, IS3D><<<ntx * nty * ntz, 256, 0, G->stream>>>(
-        D, G->phi, G->mask, ntx, nty, G->d_remap_w, G->geometry_kernel == 2 ? 1 : S::NL, G->phi_comp, res, best);
+    k_bgr_scores_tiled<real, R, IS3D><<<ntx * nty * ntz, 256, 0, G->stream>>>(D, G->phi, G->mask, ntx, nty,
+                                                                               G->d_remap_w, G->phi_comp, res, best,
+                                                                               gate);
     G->launches++;
     GPK_CUDA_TRY(cudaGetLastError());
     return GPK_OK;
@@ -437,9 +272,10 @@ using namespace gpk_dev;
 // Tiled remap scores for radius 3 (the remap radius ceil(3 s) at every sigma:
 // s = clamp(sigma / 8, 0.7, 1)); -1 when no tiled instantiation applies.
 template <typename real>
-int gpk_bgr_scores_tiled(gpk_grid* G, int radius, real* res, real* best) {
+int gpk_bgr_scores_tiled(gpk_grid* G, int radius, real* res, real* best, const unsigned long long* gate) {
     if (radius != 3) return -1;
-    return G->d.is3d() ? launch_scores_bits<real, true>(G, res, best) : launch_scores_bits<real, false>(G, res, best);
+    return G->d.is3d() ? launch_scores<real, 3, true>(G, res, best, gate)
+                       : launch_scores<real, 3, false>(G, res, best, gate);
 }
 
 // Tiled projection for the radii ceil(3 s) of the velocity kernel (s =
@@ -473,7 +309,7 @@ int gpk_projection_tiled(gpk_grid* G, int radius) {
     }
 }
 
-template int gpk_bgr_scores_tiled<float>(gpk_grid*, int, float*, float*);
-template int gpk_bgr_scores_tiled<double>(gpk_grid*, int, double*, double*);
+template int gpk_bgr_scores_tiled<float>(gpk_grid*, int, float*, float*, const unsigned long long*);
+template int gpk_bgr_scores_tiled<double>(gpk_grid*, int, double*, double*, const unsigned long long*);
 template int gpk_projection_tiled<float>(gpk_grid*, int);
 template int gpk_projection_tiled<double>(gpk_grid*, int);

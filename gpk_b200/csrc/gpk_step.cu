@@ -30,8 +30,12 @@ static constexpr int MASK_TPB = 256;
 static constexpr int MASK_IPT = 8;
 static constexpr int MASK_TILE = MASK_TPB * MASK_IPT;
 
+// `gate` (may be null): when it points to zero the launch does nothing
+// (device-side skip of a stage inside a captured step)
 __global__ void __launch_bounds__(MASK_TPB) k_mask_tiles(Dims D, const int32_t* __restrict__ phi,
-                                                         uint8_t* __restrict__ mask, int32_t* __restrict__ tile_cnt) {
+                                                         uint8_t* __restrict__ mask, int32_t* __restrict__ tile_cnt,
+                                                         const unsigned long long* gate = nullptr) {
+    if (gate && *gate == 0ull) return;
     typedef cub::BlockReduce<int, MASK_TPB> BR;
     __shared__ typename BR::TempStorage tmp;
     const int base = blockIdx.x * MASK_TILE;
@@ -54,7 +58,9 @@ __global__ void __launch_bounds__(MASK_TPB) k_mask_tiles(Dims D, const int32_t* 
 }
 
 // Exclusive scan of tile counts in one block; writes the total.
-__global__ void __launch_bounds__(1024) k_scan_tiles(int32_t* __restrict__ tile, int ntiles, unsigned* __restrict__ total) {
+__global__ void __launch_bounds__(1024) k_scan_tiles(int32_t* __restrict__ tile, int ntiles, unsigned* __restrict__ total,
+                                                     const unsigned long long* gate = nullptr) {
+    if (gate && *gate == 0ull) return;
     typedef cub::BlockScan<int, 1024> BS;
     __shared__ typename BS::TempStorage tmp;
     __shared__ int carry;
@@ -75,7 +81,9 @@ __global__ void __launch_bounds__(1024) k_scan_tiles(int32_t* __restrict__ tile,
 
 // Writes the flat indices of flagged cells in increasing order.
 __global__ void __launch_bounds__(MASK_TPB) k_compact_u8(int n, const uint8_t* __restrict__ flag,
-                                                         const int32_t* __restrict__ tile_off, int32_t* __restrict__ out) {
+                                                         const int32_t* __restrict__ tile_off, int32_t* __restrict__ out,
+                                                         const unsigned long long* gate = nullptr) {
+    if (gate && *gate == 0ull) return;
     typedef cub::BlockScan<int, MASK_TPB> BS;
     __shared__ typename BS::TempStorage tmp;
     const int base = blockIdx.x * MASK_TILE;
@@ -1017,6 +1025,7 @@ __global__ void k_accept_all(const int32_t* __restrict__ active, const int32_t* 
                              int32_t* __restrict__ phi, const int32_t* __restrict__ phi_comp, real* __restrict__ g,
                              const real* __restrict__ g_comp, real* __restrict__ alpha, real* __restrict__ rho,
                              int32_t* __restrict__ count, StepScalars* s, int sweep_rho, real rho_rex) {
+    if (m < 0) m = (int)s->n_cand;  // count read on the device (captured step)
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
         const int i = active[cpos[k]];
         const int32_t o = phi[i], n = phi_comp[i];
@@ -1428,11 +1437,11 @@ static int sep_gauss3(const Dims& D, const real* in, const int32_t* phi, int32_t
 
 // mask + sorted interface list (src/gpk_geometry.cpp:42-82)
 template <typename real>
-int gpk_interface_mask(gpk_grid* G) {
+int gpk_interface_mask(gpk_grid* G, const unsigned long long* gate) {
     const int nt = (G->d.N + MASK_TILE - 1) / MASK_TILE;
-    k_mask_tiles<<<nt, MASK_TPB, 0, G->stream>>>(G->d, G->phi, G->mask, G->tile_off);
-    k_scan_tiles<<<1, 1024, 0, G->stream>>>(G->tile_off, nt, &G->scal->n_active);
-    k_compact_u8<<<nt, MASK_TPB, 0, G->stream>>>(G->d.N, G->mask, G->tile_off, G->active);
+    k_mask_tiles<<<nt, MASK_TPB, 0, G->stream>>>(G->d, G->phi, G->mask, G->tile_off, gate);
+    k_scan_tiles<<<1, 1024, 0, G->stream>>>(G->tile_off, nt, &G->scal->n_active, gate);
+    k_compact_u8<<<nt, MASK_TPB, 0, G->stream>>>(G->d.N, G->mask, G->tile_off, G->active, gate);
     G->launches += 3;
     GPK_CUDA_TRY(cudaGetLastError());
     return GPK_OK;
@@ -1841,10 +1850,134 @@ extern "C" int gpk_gaussian_filter_3d(const float* in, float* out, int Nz, int N
     return done(rc);
 }
 
-template int gpk_interface_mask<float>(gpk_grid*);
-template int gpk_interface_mask<double>(gpk_grid*);
+template int gpk_interface_mask<float>(gpk_grid*, const unsigned long long*);
+template int gpk_interface_mask<double>(gpk_grid*, const unsigned long long*);
 template int gpk_step_impl<float>(gpk_grid*, double, double);
 template int gpk_step_impl<double>(gpk_grid*, double, double);
+
+// ---------------------------------------------------------------------------
+// The step as a captured CUDA graph.
+//
+// gpk_step_impl reads counts back on the host and branches on them (the
+// crossing candidates, the remap passes, the extinction schedule).  For the
+// configurations below the same kernels in the same order can run with no
+// host decision: every launch is sized for the worst case and reads its
+// count on the device, the remap stages run under a device-side gate on the
+// step's accepted crossings (and, in 3-D, on the first pass's exchanges),
+// and the proposals are ordered by one block instead of the radix sorts.
+// Results are the step's, bit for bit.  Not covered (gpk_step_graph_supported
+// says why): region-identity crossings with topology certificates (the
+// ordered sweep's label-wide flood fills size their queues on the host),
+// the extinction pass that goes with them, stochastic noise (its step index
+// would be frozen into the graph), recovery (its decay is formed on the
+// host from the step's dt) and the global-separable geometry (host loop
+// over the interface labels).
+// ---------------------------------------------------------------------------
+int gpk_step_graph_supported(gpk_grid* G, std::string* why) {
+    auto no = [&](const char* m) {
+        if (why) *why = m;
+        return 0;
+    };
+    const gpk_thermo_desc& th = G->th;
+    if (th.grain_network) return no("region-identity crossings (grain_network) need the ordered sweep");
+    if (th.stochastic) return no("stochastic noise depends on the step index");
+    if (th.dislocation_enabled && th.recovery_rate > 0.f) return no("recovery forms its decay on the host");
+    if (G->profile) return no("stage profiling is on");
+    if (G->geometry_kernel == 1) return no("the per-cell kernels were selected");
+    const bool sep = G->precision == GPK_PREC_F32 ? ((HostKernels<float>*)G->host_kernels)->global_separable
+                                                  : ((HostKernels<double>*)G->host_kernels)->global_separable;
+    if (sep) return no("the global-separable geometry loops over labels on the host");
+    const int rr = G->precision == GPK_PREC_F32 ? ((HostKernels<float>*)G->host_kernels)->remap_radius
+                                                : ((HostKernels<double>*)G->host_kernels)->remap_radius;
+    if (rr != 3) return no("no tiled remap-score kernel for this remap radius");
+    return 1;
+}
+
+template <typename real>
+int gpk_step_graph_body(gpk_grid* G, double dt_req, double dt_cap) {
+    HostKernels<real>* hk = (HostKernels<real>*)G->host_kernels;
+    const Dims D = G->d;
+    const gpk_thermo_desc& th = G->th;
+    // grid-stride launches over at most N items, sized for the grid's cells
+    const int ga = (int)std::max(1LL, std::min((long long)G->num_sms * 8, ((long long)D.N + 255) / 256));
+    k_reset_step<<<1, 1, 0, G->stream>>>(G->scal);
+    G->launches++;
+    GPK_TRY(gpk_interface_mask<real>(G));
+    GPK_TRY(geometry<real>(G));
+    GPK_TRY(elastic<real>(G));
+    ThermoDev TD = make_thermo_dev(th);
+    if (G->external_elastic) TD.t.elastic_enabled = 1;
+    GPK_CUDA_TRY(cudaMemsetAsync(G->f[GPK_FIELD_VN], 0, G->rsz * D.N, G->stream));
+    k_velocities<real><<<ga, 256, 0, G->stream>>>(
+        D, TD, G->active, &G->scal->n_active, G->phi, G->phi_comp, (const real*)G->f[GPK_FIELD_C],
+        (const real*)G->f[GPK_FIELD_T], (const real*)G->f[GPK_FIELD_G], (const real*)G->f[GPK_FIELD_RHO],
+        (const real*)G->f[GPK_FIELD_NX], (const real*)G->f[GPK_FIELD_NY], (const real*)G->f[GPK_FIELD_NZ],
+        (const real*)G->f[GPK_FIELD_KAPPA], (const real*)G->f[GPK_FIELD_E_EL], (real*)G->f[GPK_FIELD_VN],
+        (real*)G->f[GPK_FIELD_G_COMP]);
+    GPK_CUDA_TRY(cudaMemsetAsync(G->vn2, 0, G->rsz * D.N, G->stream));
+    const int prc = gpk_projection_tiled<real>(G, hk->proj_radius);
+    if (prc == -1)
+        k_projection<real><<<ga, 256, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, G->phi_comp, G->mask,
+                                                      (const real*)G->f[GPK_FIELD_VN], (real*)G->vn2, G->d_proj_w,
+                                                      hk->proj_radius);
+    else if (prc != GPK_OK)
+        return prc;
+    std::swap(G->f[GPK_FIELD_VN], G->vn2);
+    typedef typename RealBits<real>::U U;
+    U* vbits = (U*)&G->scal->vmax;
+    GPK_CUDA_TRY(cudaMemsetAsync(vbits, 0, sizeof(double), G->stream));
+    k_vmax<real><<<ga, 256, 0, G->stream>>>(G->active, &G->scal->n_active, (const real*)G->f[GPK_FIELD_VN], vbits);
+    k_select_dt<real><<<1, 1, 0, G->stream>>>(G->scal, vbits, (real)G->dx, (real)G->D, D.is3d() ? 1 : 0, dt_req, dt_cap);
+    G->launches += 4;
+    if (th.solute_rejection) {
+        if (!G->solid_old) {
+            gpk_set_error("captured step: solute buffers are made by a first ordinary step");
+            return GPK_ERR_INVALID_ARGUMENT;
+        }
+        k_solid_fraction<real><<<grid_for(G, D.N), 256, 0, G->stream>>>(D.N, G->phi, (const real*)G->f[GPK_FIELD_ALPHA],
+                                                                         (real*)G->solid_old);
+        G->have_solid_old = 1;
+        G->launches++;
+    }
+    uint8_t* cflag = (uint8_t*)G->ero_target;
+    k_alpha<real><<<ga, 256, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, G->phi_comp,
+                                             (const real*)G->f[GPK_FIELD_VN], (const real*)G->f[GPK_FIELD_T],
+                                             (real*)G->f[GPK_FIELD_ALPHA], (real*)G->alpha_new_a, cflag, G->scal,
+                                             (real)G->dx, th.stochastic, (real)th.M0, (real)th.kB, (real)th.noise_scale,
+                                             G->step_id, (real)G->near_tol, G->near_list, D.N);
+    const int nt = (D.N + MASK_TILE - 1) / MASK_TILE;
+    int32_t* ctile = G->tile_off + nt + 1;
+    k_count_u8<<<nt, MASK_TPB, 0, G->stream>>>(cflag, &G->scal->n_active, ctile);
+    k_scan_tiles<<<1, 1024, 0, G->stream>>>(ctile, nt, &G->scal->n_cand);
+    k_compact_u8_dyn<<<nt, MASK_TPB, 0, G->stream>>>(&G->scal->n_active, cflag, ctile, G->cand);
+    // every candidate switches (no region identity); the count is read on the device
+    k_accept_all<real><<<ga, 256, 0, G->stream>>>(
+        G->active, G->cand, -1, G->phi, G->phi_comp, (real*)G->f[GPK_FIELD_G], (const real*)G->f[GPK_FIELD_G_COMP],
+        (real*)G->f[GPK_FIELD_ALPHA], (real*)G->f[GPK_FIELD_RHO], G->count, G->scal, th.dislocation_enabled,
+        (real)th.rho_rex);
+    G->launches += 5;
+    GPK_CUDA_TRY(cudaGetLastError());
+    // balanced remap under the accepted-crossings gate; a second 3-D pass
+    // under the first pass's exchanges
+    const unsigned long long* gate = &G->scal->accepted;
+    GPK_TRY(gpk_interface_mask<real>(G, gate));
+    GPK_TRY(gpk_remap_pass_graph<real>(G, gate));
+    GPK_TRY(gpk_interface_mask<real>(G, gate));
+    if (D.is3d()) {
+        GPK_TRY(gpk_remap_gates(G, 0));
+        GPK_TRY(gpk_remap_pass_graph<real>(G, &G->scal->gate2));
+        GPK_TRY(gpk_interface_mask<real>(G, &G->scal->gate2));
+    }
+    GPK_TRY(gpk_remap_gates(G, 1));
+    GPK_TRY(transport<real>(G));
+    k_advance_time<<<1, 1, 0, G->stream>>>(G->scal);
+    G->launches++;
+    GPK_CUDA_TRY(cudaGetLastError());
+    ++G->step_id;
+    return GPK_OK;
+}
+template int gpk_step_graph_body<float>(gpk_grid*, double, double);
+template int gpk_step_graph_body<double>(gpk_grid*, double, double);
 
 // The mask and geometry stages of GPKGrid::step on the current labels
 // (src/gpk_geometry.cpp:42-183), without moving any interface.

@@ -298,7 +298,8 @@ enum : int32_t {
 
 struct CrossArgs {
     Dims D;
-    int32_t* phi; int32_t* cmap; int8_t* cres; int32_t* minL; int32_t* count; const int32_t* count0;
+    int32_t* phi; int32_t* cmap; int8_t* cres; int32_t* count; const int32_t* count0;
+    int32_t* minL[2];      // earliest pending candidate per label, by wave parity (both INT_BIG between sweeps)
     const int32_t* n_old;  // candidates per old label
     int4* cinfo;           // cell, old label, new label, state
     const int32_t* cpos;   // active position of the candidate
@@ -579,7 +580,7 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
     const Dims D = a.D;
     const bool is3d = D.is3d();
     unsigned* rem = a.s->wave_rem;  // three rotating counters
-    unsigned prev_left = (unsigned)m;
+    unsigned prev_left = (unsigned)m + 1u;  // pending counts at wave starts: m, then strictly fewer
     for (int w = 0; w < max_waves; ++w) {
         // ---- phase A: locality, local certificate parts, label-wide needs;
         //      earliest pending candidate touching each label.  One warp per
@@ -587,17 +588,26 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
         //      at once (labels in the serial-time view, and the earlier
         //      pending candidates there), and ballots give the occupancy
         //      masks of its old and new label.
-        if (tid == 0) { rem[(w + 1) % 3] = 0; a.s->ff_pool = 0; }
+        int32_t* minA = a.minL[w & 1];        // this wave's per-label minima
+        int32_t* minN = a.minL[(w + 1) & 1];  // the next wave's, cleared here
+        if (tid == 0) a.s->ff_pool = 0;
+        __shared__ unsigned s_pending;
+        if (threadIdx.x == 0) s_pending = 0;
+        __syncthreads();
         {
             const int lane = threadIdx.x & 31;
             const int gwarp = tid >> 5, nwarps = nthr >> 5;
             const int nbox = is3d ? 125 : 25, centre = is3d ? 62 : 12;
+            unsigned pending = 0;
             for (int k = gwarp; k < m; k += nwarps) {
                 if (a.cres[k] != 0) continue;
                 const int4 ci = a.cinfo[k];
+                ++pending;
                 if (lane == 0) {
-                    atomicMin(&a.minL[ci.y], k);
-                    atomicMin(&a.minL[ci.z], k);
+                    atomicMin(&minA[ci.y], k);
+                    atomicMin(&minA[ci.z], k);
+                    minN[ci.y] = INT_BIG;
+                    minN[ci.z] = INT_BIG;
                 }
                 int z0, y0, x0;
                 D.decode(ci.x, z0, y0, x0);
@@ -649,16 +659,36 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
                     a.cinfo[k].w = st;
                 }
             }
+            if (lane == 0 && pending) atomicAdd(&s_pending, pending);
         }
+        __syncthreads();
+        if (threadIdx.x == 0 && s_pending) atomicAdd(&rem[w % 3], s_pending);
         if (!grid_barrier(a.s, nblocks)) return;
-        // ---- phase B: readiness; decisions that need only local reads
+        const unsigned left = *((volatile unsigned*)&rem[w % 3]);
+        if (left == 0) {
+            if (tid == 0) a.s->waves = w;
+            return;
+        }
+        // the earliest pending candidate is always decided, so every wave
+        // decides at least one; every thread holds the previous count in a
+        // register (the shared counter of wave w-1 is recycled by wave w+2)
+        if (left >= prev_left) {
+            if (threadIdx.x == 0) atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
+            return;
+        }
+        prev_left = left;
+        if (tid == 0) rem[(w + 1) % 3] = 0;
+        // ---- phase B: readiness; decisions that need only local reads are
+        //      committed at once (they depend on nothing another decision of
+        //      this wave writes: their local reads hold no earlier pending
+        //      candidate, and later ones read back through the serial view)
         for (int k = tid; k < m; k += nthr) {
             if (a.cres[k] != 0) continue;
             const int4 ci = a.cinfo[k];
             const int st = ci.w;
             if (!(st & CS_LOCAL)) continue;
-            if ((st & (CS_GO | CS_GC)) && a.minL[ci.y] < k) continue;
-            if ((st & CS_GN) && a.minL[ci.z] < k) continue;
+            if ((st & (CS_GO | CS_GC)) && minA[ci.y] < k) continue;
+            if ((st & CS_GN) && minA[ci.z] < k) continue;
             if (st & (CS_GO | CS_GN | CS_GC)) {
                 // label-wide work: one warp per candidate in phase B2
                 a.tasks[atomicAdd(&a.s->n_tasks, 1u)] = k;
@@ -668,14 +698,15 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
             // to == 0 without GC is CS_CNT_REJECT; to > 1 without GO passed the 5^d proof
             bool acc = to != 0;
             if (acc && tn == 0) acc = false;
-            a.cinfo[k].w = st | CS_READY | (acc ? CS_ACCEPT : 0);
+            cross_commit<real>(a, k, ci, acc);
         }
         if (!grid_barrier(a.s, nblocks)) return;
+        const unsigned ntask = *((volatile unsigned*)&a.s->n_tasks);
+        if (ntask == 0) continue;  // no label-wide work: the next wave reads these commits
         // ---- phase B2: global flood fills and exact counts, a warp per candidate
         {
             const int lane = threadIdx.x & 31;
             const int gwarp = tid >> 5, nwarps = nthr >> 5;
-            const unsigned ntask = *((volatile unsigned*)&a.s->n_tasks);
             for (unsigned t = gwarp; t < ntask; t += nwarps) {
                 const int k = a.tasks[t];
                 const int4 ci = a.cinfo[k];
@@ -734,30 +765,15 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
             }
         }
         if (!grid_barrier(a.s, nblocks)) return;
-        if (tid == 0) a.s->n_tasks = 0;
-        // ---- phase C: commit ready candidates, reset per-label minima
-        for (int k = tid; k < m; k += nthr) {
-            if (a.cres[k] != 0) continue;
+        // ---- phase C: commit the label-wide decisions (after all of them
+        //      were taken, on the labels as they stood)
+        for (unsigned t = tid; t < ntask; t += nthr) {
+            const int k = a.tasks[t];
             const int4 ci = a.cinfo[k];
-            a.minL[ci.y] = INT_BIG;
-            a.minL[ci.z] = INT_BIG;
-            if (ci.w & CS_READY) cross_commit<real>(a, k, ci, (ci.w & CS_ACCEPT) != 0);
-            else atomicAdd(&rem[w % 3], 1u);
+            cross_commit<real>(a, k, ci, (ci.w & CS_ACCEPT) != 0);
         }
         if (!grid_barrier(a.s, nblocks)) return;
-        const unsigned left = *((volatile unsigned*)&rem[w % 3]);
-        if (left == 0) {
-            if (tid == 0) a.s->waves = w + 1;
-            return;
-        }
-        // the earliest pending candidate is always ready, so every wave
-        // decides at least one; every thread holds the previous count in a
-        // register (the shared counter of wave w-1 is recycled by wave w+1)
-        if (left >= prev_left) {
-            if (threadIdx.x == 0) atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
-            return;
-        }
-        prev_left = left;
+        if (tid == 0) a.s->n_tasks = 0;
     }
     if (tid == 0) atomicCAS(&a.s->error, 0u, (unsigned)GPK_ERR_INTERNAL);
 }
@@ -778,12 +794,15 @@ __global__ void k_cross_setup(const int32_t* __restrict__ active, const int32_t*
 }
 
 // Clears the cell map and the per-label candidate counts after the sweep.
-__global__ void k_cross_cleanup(int m, const int4* __restrict__ cinfo, int32_t* cmap, int32_t* n_old) {
+__global__ void k_cross_cleanup(int m, const int4* __restrict__ cinfo, int32_t* cmap, int32_t* n_old, int32_t* minL,
+                                int32_t* minF) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= m) return;
     const int4 ci = cinfo[k];
     cmap[ci.x] = -1;
     n_old[ci.y] = 0;
+    minL[ci.y] = INT_BIG; minL[ci.z] = INT_BIG;
+    minF[ci.y] = INT_BIG; minF[ci.z] = INT_BIG;
 }
 
 // ---------------------------------------------------------------------------
@@ -847,7 +866,9 @@ template <typename real>
 __global__ void k_bgr_proposals(const int32_t* __restrict__ active, const unsigned* __restrict__ n_active,
                                 const int32_t* __restrict__ phi, const int32_t* __restrict__ phi_comp,
                                 const real* __restrict__ res_a, const real* __restrict__ best_a,
-                                unsigned long long* __restrict__ key2, int32_t* __restrict__ val, StepScalars* s) {
+                                unsigned long long* __restrict__ key2, int32_t* __restrict__ val, StepScalars* s,
+                                const unsigned long long* gate = nullptr) {
+    if (gate && *gate == 0ull) return;
     const int na = (int)*n_active;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += gridDim.x * blockDim.x) {
         const int i = active[a];
@@ -896,9 +917,10 @@ __device__ __forceinline__ int lower_bound_u64(const unsigned long long* a, int 
 // label pair (src/gpk_transitions.cpp:147-155).  Slot t (a forward element)
 // becomes exchange t; unmatched slots get a = -1.
 __global__ void k_bgr_match(int n, const unsigned long long* __restrict__ key1, const int32_t* __restrict__ val,
-                            int4* __restrict__ exch, int32_t* __restrict__ estate, int32_t* __restrict__ pmap) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
+                            int4* __restrict__ exch, int32_t* __restrict__ estate, int32_t* __restrict__ pmap,
+                            const unsigned* n_dev = nullptr) {
+    if (n_dev) n = (int)*n_dev;  // count read on the device (captured step); grid-stride below
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
     const unsigned long long k = key1[t];
     int4 e = make_int4(-1, -1, 0, 0);
     int32_t st = 0;
@@ -921,6 +943,7 @@ __global__ void k_bgr_match(int n, const unsigned long long* __restrict__ key1, 
     }
     exch[t] = e;
     estate[t] = st;
+    }
 }
 
 template <typename real>
@@ -978,6 +1001,7 @@ __device__ __forceinline__ u128 mask128(const uint32_t w[4]) {
 }
 
 struct ExchArgs {
+    const unsigned* n_dev;  // exchange slots read on the device (captured step), else null
     Dims D;
     int32_t* phi; int32_t* pmap; const int32_t* count;
     const int4* exch; int32_t* estate;
@@ -990,6 +1014,11 @@ enum : int32_t { ES_PENDING = 1, ES_READY = 2, ES_ACCEPT = 4 };
 
 template <typename real>
 __global__ void __launch_bounds__(256) k_bgr_exchange_waves(ExchArgs a, int n, int max_waves) {
+    if (a.n_dev) {
+        n = (int)*a.n_dev;
+        max_waves = n + 1;
+        if (n == 0) return;
+    }
     const int nblocks = gridDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nthr = nblocks * blockDim.x;
@@ -1204,6 +1233,110 @@ __global__ void k_fill_i32(int32_t* p, int n, int32_t v) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
 }
 
+// ---------------------------------------------------------------------------
+// captured-step form of the remap ordering
+// ---------------------------------------------------------------------------
+// The proposals in the reference's order — pair (low, high), direction,
+// gain descending, cell ascending; the cell makes every key distinct — by
+// one block: a merge sort whose run width doubles each pass, each element
+// placed by a binary search in the neighbouring run.  The count is read on
+// the device, so the launch can sit in a captured step.  Input: gain keys in
+// k2[0], cells in v[0] (as k_bgr_proposals writes them).  Output: primary
+// keys in k1[0] and cells in v[0], what k_bgr_match reads.
+struct SortItem {
+    unsigned long long k1, k2;
+    int32_t v;
+};
+__device__ __forceinline__ bool item_less(const SortItem& a, const SortItem& b) {
+    if (a.k1 != b.k1) return a.k1 < b.k1;
+    if (a.k2 != b.k2) return a.k2 < b.k2;
+    return a.v < b.v;
+}
+
+__global__ void __launch_bounds__(1024) k_sort_proposals(const unsigned* __restrict__ n_dev,
+                                                         const unsigned long long* __restrict__ gate,
+                                                         const int32_t* __restrict__ phi,
+                                                         const int32_t* __restrict__ phi_comp,
+                                                         unsigned long long* k1a, unsigned long long* k2a, int32_t* va,
+                                                         unsigned long long* k1b, unsigned long long* k2b, int32_t* vb) {
+    if (gate && *gate == 0ull) return;
+    const int n = (int)*n_dev;
+    if (n <= 1) {
+        if (n == 1) {
+            const int i = va[0];
+            const int32_t p = phi[i], q = phi_comp[i];
+            k1a[0] = ((unsigned long long)min(p, q) << 37) | ((unsigned long long)max(p, q) << 11) |
+                     ((p == min(p, q) ? 0ull : 1ull) << 10);
+        }
+        return;
+    }
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int i = va[t];
+        const int32_t p = phi[i], q = phi_comp[i];
+        const unsigned long long low = (unsigned long long)min(p, q), high = (unsigned long long)max(p, q);
+        k1a[t] = (low << 37) | (high << 11) | ((p == min(p, q) ? 0ull : 1ull) << 10);
+    }
+    __syncthreads();
+    unsigned long long *s1 = k1a, *s2 = k2a, *d1 = k1b, *d2 = k2b;
+    int32_t *sv = va, *dv = vb;
+    for (int width = 1; width < n; width *= 2) {
+        for (int t = threadIdx.x; t < n; t += blockDim.x) {
+            const SortItem it{s1[t], s2[t], sv[t]};
+            const int run = t / width;
+            const int lo_self = run * width;
+            // the neighbouring run
+            const int other = (run & 1) ? lo_self - width : lo_self + width;
+            int pos;
+            if (other >= n) {
+                pos = t;  // an odd run at the end stays in place
+            } else {
+                const int olo = other, ohi = min(other + width, n);
+                int a = olo, b = ohi;  // elements of the other run smaller than it
+                while (a < b) {
+                    const int mid = (a + b) >> 1;
+                    const SortItem o{s1[mid], s2[mid], sv[mid]};
+                    if (item_less(o, it)) a = mid + 1;
+                    else b = mid;
+                }
+                const int base = min(lo_self, olo);
+                pos = base + (t - lo_self) + (a - olo);
+            }
+            d1[pos] = it.k1;
+            d2[pos] = it.k2;
+            dv[pos] = it.v;
+        }
+        __syncthreads();
+        unsigned long long* x = s1; s1 = d1; d1 = x;
+        x = s2; s2 = d2; d2 = x;
+        int32_t* y = sv; sv = dv; dv = y;
+    }
+    if (s1 != k1a) {
+        for (int t = threadIdx.x; t < n; t += blockDim.x) {
+            k1a[t] = s1[t];
+            va[t] = sv[t];
+        }
+    }
+}
+
+// Second remap pass of a 3-D step inside a captured step: it runs when the
+// first pass (gated on accepted crossings) exchanged cells; the two passes'
+// exchanges are summed into the step's counter afterwards.
+__global__ void k_remap_second_gate(StepScalars* s) {
+    s->exch_first = s->exch_pass;
+    s->gate2 = (s->accepted > 0 && s->exch_pass > 0) ? 1ull : 0ull;
+    s->exch_pass = 0;
+    s->waves = 0;
+}
+__global__ void k_remap_total(StepScalars* s, int is3d) {
+    if (is3d) s->exchanges = s->exch_first + (s->gate2 ? s->exch_pass : 0ull);
+    else s->exchanges = s->exch_pass;
+}
+__global__ void k_copy_i32_gated(int n, const int32_t* __restrict__ src, int32_t* __restrict__ dst,
+                                 const unsigned long long* __restrict__ gate) {
+    if (gate && *gate == 0ull) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
+}
+
 }  // namespace gpk_dev
 
 using namespace gpk_dev;
@@ -1211,10 +1344,14 @@ using namespace gpk_dev;
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
+// Blocks of a persistent wave kernel: enough for want_items threads, at most
+// two per SM (a grid barrier costs more the more blocks arrive at it) and
+// never more than can be resident at once.
 static int coop_grid(gpk_grid* G, const void* kernel, int block, int want_items) {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
     if (per_sm < 1) per_sm = 1;
+    if (per_sm > 2) per_sm = 2;
     int maxb = per_sm * G->num_sms;
     int need = (want_items + block - 1) / block;
     if (need < 1) need = 1;
@@ -1260,7 +1397,8 @@ int gpk_crossings(gpk_grid* G, int m) {
     GPK_CUDA_TRY(cudaGetLastError());
     CrossArgs a;
     a.D = G->d;
-    a.phi = G->phi; a.cmap = G->pmap; a.cres = cres; a.minL = G->minL; a.count = G->count; a.count0 = G->count0;
+    a.phi = G->phi; a.cmap = G->pmap; a.cres = cres; a.count = G->count; a.count0 = G->count0;
+    a.minL[0] = G->minL; a.minL[1] = G->minF;
     a.n_old = G->n_old;
     a.cinfo = (int4*)G->cand_info; a.cpos = G->cand;
     a.alpha_new_a = G->alpha_new_a; a.alpha = G->f[GPK_FIELD_ALPHA]; a.g = G->f[GPK_FIELD_G];
@@ -1276,7 +1414,8 @@ int gpk_crossings(gpk_grid* G, int m) {
     // phase A runs one warp per pending candidate
     const int grid = coop_grid(G, kern, 256, (int)std::min<long long>(32LL * m, 1LL << 30));
     GPK_TRY(launch_coop(G, kern, grid, 256, args));
-    k_cross_cleanup<<<(m + B - 1) / B, B, 0, G->stream>>>(m, (const int4*)G->cand_info, G->pmap, G->n_old);
+    k_cross_cleanup<<<(m + B - 1) / B, B, 0, G->stream>>>(m, (const int4*)G->cand_info, G->pmap, G->n_old, G->minL,
+                                                        G->minF);
     G->launches++;
     GPK_CUDA_TRY(cudaGetLastError());
     return GPK_OK;
@@ -1336,6 +1475,7 @@ int gpk_remap_pass(gpk_grid* G) {
     G->launches++;
     GPK_CUDA_TRY(cudaGetLastError());
     ExchArgs a;
+    a.n_dev = nullptr;
     a.D = D;
     a.phi = G->phi; a.pmap = G->pmap; a.count = G->count;
     a.exch = (const int4*)G->exch; a.estate = G->val_b;
@@ -1407,7 +1547,69 @@ int gpk_topology_simple_move_impl(gpk_grid* G, int cell, int32_t new_label, int*
 
 template int gpk_crossings<float>(gpk_grid*, int);
 template int gpk_crossings<double>(gpk_grid*, int);
+// One balanced-remap pass inside a captured step: every launch is sized for
+// the worst case and reads its counts on the device, and nothing runs when
+// *gate is zero.  Same kernels and order as gpk_remap_pass (the proposals
+// ordered by k_sort_proposals instead of the radix sorts).
+template <typename real>
+int gpk_remap_pass_graph(gpk_grid* G, const unsigned long long* gate) {
+    const Dims D = G->d;
+    HostKernels<real>* hk = (HostKernels<real>*)G->host_kernels;
+    const int B = 256;
+    const int grid = 4 * G->num_sms;
+    k_copy_i32_gated<<<grid, B, 0, G->stream>>>(D.N, G->phi, G->phi_comp, gate);
+    const int rc = G->geometry_kernel != 1
+                       ? gpk_bgr_scores_tiled<real>(G, hk->remap_radius, (real*)G->bgr_res, (real*)G->bgr_best, gate)
+                       : -1;
+    if (rc == -1) {
+        gpk_set_error("captured step: the remap radius has no tiled score kernel");
+        return GPK_ERR_UNSUPPORTED_MODEL;
+    }
+    if (rc != GPK_OK) return rc;
+    GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->n_prop, 0, sizeof(unsigned), G->stream));
+    k_bgr_proposals<real><<<grid, B, 0, G->stream>>>(G->active, &G->scal->n_active, G->phi, G->phi_comp,
+                                                     (const real*)G->bgr_res, (const real*)G->bgr_best, G->key_b,
+                                                     G->val_b, G->scal, gate);
+    // k_sort_proposals reads gain keys in key_b, cells in val_b; ping-pong
+    // through the candidate record buffer (free while no crossing sweep runs)
+    unsigned long long* k1b = (unsigned long long*)G->cand_info;
+    unsigned long long* k2b = k1b + D.N;
+    k_sort_proposals<<<1, 1024, 0, G->stream>>>(&G->scal->n_prop, gate, G->phi, G->phi_comp, G->key_a, G->key_b,
+                                                G->val_b, k1b, k2b, G->val_a);
+    // sorted: primary keys in key_a, cells in val_b
+    k_bgr_match<<<grid, B, 0, G->stream>>>(0, G->key_a, G->val_b, (int4*)G->exch, G->val_a, G->pmap,
+                                           &G->scal->n_prop);
+    G->launches += 4;
+    GPK_CUDA_TRY(cudaGetLastError());
+    ExchArgs a;
+    a.n_dev = &G->scal->n_prop;
+    a.D = D;
+    a.phi = G->phi; a.pmap = G->pmap; a.count = G->count;
+    a.exch = (const int4*)G->exch; a.estate = G->val_a;
+    a.g = G->f[GPK_FIELD_G]; a.alpha = G->f[GPK_FIELD_ALPHA]; a.rho = G->f[GPK_FIELD_RHO];
+    a.s = G->scal;
+    a.sweep_rho = G->th.dislocation_enabled; a.rho_rex_f = G->th.rho_rex; a.rho_rex_d = (double)G->th.rho_rex;
+    int max_waves = 1, nn = 0;
+    void* args[] = {&a, &nn, &max_waves};
+    const void* kern = (const void*)k_bgr_exchange_waves<real>;
+    // the slot count is known only on the device: one block per 8192 cells
+    // (at most the usual cap), so that the exchange loops of many small grids
+    // captured side by side fit on the GPU together
+    const long long want = std::max(1LL, ((long long)D.N + 8191) / 8192) * 256;
+    return launch_coop(G, kern, coop_grid(G, kern, 256, (int)std::min<long long>(want, 1LL << 30)), 256, args);
+}
+
 template int gpk_remap_pass<float>(gpk_grid*);
 template int gpk_remap_pass<double>(gpk_grid*);
+template int gpk_remap_pass_graph<float>(gpk_grid*, const unsigned long long*);
+template int gpk_remap_pass_graph<double>(gpk_grid*, const unsigned long long*);
+
+int gpk_remap_gates(gpk_grid* G, int stage) {
+    if (stage == 0) k_remap_second_gate<<<1, 1, 0, G->stream>>>(G->scal);
+    else k_remap_total<<<1, 1, 0, G->stream>>>(G->scal, G->d.is3d() ? 1 : 0);
+    G->launches++;
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
+}
 template int gpk_extinction<float>(gpk_grid*);
 template int gpk_extinction<double>(gpk_grid*);

@@ -127,6 +127,22 @@ class GPKGrid:
         check(lib().gpk_grid_step(self._h, float(dt), float(dt_cap), C.byref(used)))
         return used.value
 
+    def step_graph(self, n: int, dt: float = -1.0, dt_cap: float = 1.0e30) -> float:
+        """n steps through a captured two-step CUDA graph (bit-identical to
+        step_n); returns the grid time."""
+        t = C.c_double()
+        check(lib().gpk_grid_step_graph(self._h, int(n), float(dt), float(dt_cap), C.byref(t)))
+        return t.value
+
+    def set_tile_rows(self, divisor: int) -> None:
+        """2-D geometry tile height at kernel radius 8: rows divided by 1, 2 or 4."""
+        check(lib().gpk_grid_set_tile_rows(self._h, int(divisor)))
+
+    def graph_supported(self) -> bool:
+        s = C.c_int()
+        check(lib().gpk_grid_graph_supported(self._h, C.byref(s)))
+        return bool(s.value)
+
     def step_n(self, n: int, dt: float = -1.0, dt_cap: float = 1.0e30) -> float:
         t = C.c_double()
         check(lib().gpk_grid_step_n(self._h, int(n), float(dt), float(dt_cap), C.byref(t)))

@@ -282,6 +282,27 @@ int gpk_grid_near_threshold(gpk_grid* grid, int32_t* cells, int cap, int* n);
  * stable time step valid).                                                  */
 int gpk_grid_set_solid_diffusivity_ratio(gpk_grid* grid, double ratio);
 
+/* The step as a captured CUDA graph (no counterpart in the reference, whose
+ * step is host code).  gpk_grid_step_graph takes n steps of
+ * GPKGrid::step(dt, dt_cap) like gpk_grid_step_n, replaying a graph of two
+ * captured steps that takes no decision on the host: counts are read on
+ * the device, the remap runs under a device-side gate on the step's
+ * accepted crossings, and its proposals are ordered by one block.  The
+ * results are bit-identical to gpk_grid_step_n.  The graph is captured on
+ * first use (a fresh grid first takes one ordinary step) and again when the
+ * model, a setting or the step arguments change; an odd last step is
+ * ordinary.  gpk_grid_graph_supported tells whether the grid's model
+ * qualifies (no region-identity topology certificates, no stochastic noise,
+ * no recovery, no global-separable geometry; gpk_last_error says why not);
+ * gpk_grid_step_graph returns GPK_ERR_UNSUPPORTED_MODEL otherwise.       */
+int gpk_grid_step_graph(gpk_grid* grid, int n, double dt, double dt_cap, double* time_out);
+/* Height of the 2-D geometry tiles at kernel radius 8 (sigma 1.5): the
+ * 1024-cell tile's rows divided by 1, 2 or 4 (1024, 512 or 256 cells per
+ * CTA).  Results do not depend on it; small grids get more CTAs from
+ * smaller tiles.  gpk_batch_autotune_tiles picks it per instance size.     */
+int gpk_grid_set_tile_rows(gpk_grid* grid, int divisor);
+int gpk_grid_graph_supported(gpk_grid* grid, int* supported);
+
 /* Failure injection for tests (no counterpart in the reference).  The next
  * cooperative launch of the grid (the ordered crossing sweep, or a remap
  * exchange loop) waits at its first grid barrier for one block more than it

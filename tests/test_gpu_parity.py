@@ -95,6 +95,20 @@ def test_geometry_kernels_agree_2d(oracle_mod, sigma):
         assert not compare_all(gpu, ora), kind
 
 
+@pytest.mark.parametrize("divisor", [2, 4])
+def test_geometry_tile_heights_2d(oracle_mod, divisor):
+    """The 2-D tiles of 512 and 256 cells at sigma 1.5 (kernel radius 8),
+    the shapes the sweep's autotuner chooses among, against the oracle."""
+    phi, g = polycrystal(1, 70, 90, 40, 5)
+    ora = oracle_mod.OracleGrid(1, 70, 90, 1.0, thermo.isotropic(1.0, 1.0), 0.0, 1.5)
+    gpu = GPKGrid(1, 70, 90, 1.0, thermo.isotropic(1.0, 1.0), 0.0, 1.5)
+    gpu.set_tile_rows(divisor)
+    _load((gpu, ora), phi=phi, g=g, alpha=1.0)
+    for _ in range(10):
+        assert gpu.step() == ora.step()
+    assert not compare_all(gpu, ora)
+
+
 def test_config1_256_128_grains_200_steps(oracle_mod):
     """The CPU-runnable configuration: 256^2, 128 grains, sigma 1.5, 200 steps."""
     phi, g = polycrystal(1, 256, 256, 128, 42)
