@@ -855,7 +855,7 @@ extern "C" int gpk_grid_set_tile_rows(gpk_grid* G, int divisor) {
 }
 
 extern "C" int gpk_grid_set_geometry_kernel(gpk_grid* G, int kind) {
-    if (!G || kind < 0 || kind > 2) return GPK_ERR_INVALID_ARGUMENT;
+    if (!G || kind < 0 || kind > 3) return GPK_ERR_INVALID_ARGUMENT;
     G->geometry_kernel = kind;
     return GPK_OK;
 }

@@ -235,6 +235,309 @@ __global__ void __launch_bounds__(256) k_projection_tiled(Dims D, const int32_t*
     }
 }
 
+// ---------------------------------------------------------------------------
+// balanced-remap scores: screening on label bitmaps, exact sums where needed
+// ---------------------------------------------------------------------------
+// The scores only matter through three outcomes: the best candidate label
+// (phi_comp, public), whether gain = best - resident exceeds 1e-7 (a
+// proposal) and, for proposals, the gain itself (their order).  A tile of
+// 26 x TY x TZ cells has halo rows of exactly 32 cells (R = 3), so for one
+// label a halo row is one 32-bit word; a 7-tap window of a row is a 7-bit
+// pattern, and a table of the weight sums of all 128 patterns per (dy, dz)
+// gives every score in 49 lookups.  Those sums are added in another order
+// than the reference's, so they differ from its sums by far less than
+// 1e-9.  A cell whose screened gain is below -1e-5 and whose best candidate
+// leads the others by more than 1e-9 cannot make a proposal nor pick
+// another candidate, whatever the rounding: it keeps the screened values
+// (read only by the proposal test).  Every other cell is queued and summed
+// exactly, tap by tap in z -> y -> x order as the reference adds them
+// (src/gpk_transitions.cpp:67-85), by all threads of the CTA together.
+template <bool IS3D> struct BitTile;
+template <> struct BitTile<true> { static constexpr int TY = 8, TZ = 8; };
+template <> struct BitTile<false> { static constexpr int TY = 32, TZ = 1; };
+
+template <bool IS3D>
+struct BitShape {
+    static constexpr int R = 3;
+    static constexpr int TX = 32 - 2 * R, HX = 32;
+    static constexpr int TY = BitTile<IS3D>::TY, TZ = BitTile<IS3D>::TZ;
+    static constexpr int HY = TY + 2 * R, HZ = IS3D ? TZ + 2 * R : 1;
+    static constexpr int NROW = HY * HZ;
+    static constexpr int NROWP = NROW | 1;
+    static constexpr int NCELL = TX * TY * TZ;
+    static constexpr int NH = NROW * HX;
+    static constexpr int R2MAX = (IS3D ? 3 : 2) * R * R;
+    static constexpr int NL = 16;       // bitmaps per tile
+    static constexpr int HSLOT = 64;    // label hash slots
+    static constexpr int NRS = 10;      // distinct dy^2 + dz^2 of a 7 x 7 row block
+};
+
+// index of dy^2 + dz^2 in {0, 1, 2, 4, 5, 8, 9, 10, 13, 18}
+__device__ __forceinline__ int rsum_index(int r2) {
+    switch (r2) {
+    case 0: return 0; case 1: return 1; case 2: return 2; case 4: return 3; case 5: return 4;
+    case 8: return 5; case 9: return 6; case 10: return 7; case 13: return 8; default: return 9;
+    }
+}
+__host__ __device__ constexpr int rsum_value(int k) {
+    return k == 0 ? 0 : k == 1 ? 1 : k == 2 ? 2 : k == 3 ? 4 : k == 4 ? 5 : k == 5 ? 8 : k == 6 ? 9 : k == 7 ? 10
+           : k == 8 ? 13 : 18;
+}
+
+// the hash slot of label v, inserting it when absent (-1: table full)
+__device__ __forceinline__ int label_slot_insert(int32_t* keys, int32_t v, int nslot) {
+    unsigned h = ((unsigned)v * 2654435761u) >> 26;  // 6 bits
+    for (int k = 0; k < nslot; ++k) {
+        const int sl = (int)((h + k) & (nslot - 1));
+        const int32_t old = atomicCAS(&keys[sl], -1, v);
+        if (old == -1 || old == v) return sl;
+    }
+    return -1;
+}
+__device__ __forceinline__ int label_slot_find(const int32_t* keys, int32_t v, int nslot) {
+    unsigned h = ((unsigned)v * 2654435761u) >> 26;
+    for (int k = 0; k < nslot; ++k) {
+        const int sl = (int)((h + k) & (nslot - 1));
+        const int32_t key = keys[sl];
+        if (key == v) return sl;
+        if (key == -1) return -1;
+    }
+    return -1;
+}
+
+// screened sums of the resident label and NC candidates: one table lookup
+// per row of 7 taps; li[k] is the bitmap base of label k (0: resident)
+template <bool IS3D, int NC>
+__device__ __forceinline__ void screen_rows(const uint32_t* __restrict__ bm, const double* __restrict__ rtab,
+                                            const int li[7], int lx, int ly, int lz, double& resident,
+                                            double sup[6]) {
+    typedef BitShape<IS3D> S;
+    constexpr int R = S::R;
+#pragma unroll 1
+    for (int dz = (IS3D ? -R : 0); dz <= (IS3D ? R : 0); ++dz)
+#pragma unroll
+        for (int dy = -R; dy <= R; ++dy) {
+            const int row = ((IS3D ? lz + R + dz : 0) * S::HY) + ly + R + dy;
+            const double* t = rtab + rsum_index(dy * dy + dz * dz) * 128;
+            resident += t[(bm[li[0] + row] >> lx) & 0x7Fu];
+#pragma unroll
+            for (int q = 0; q < NC; ++q) sup[q] += t[(bm[li[q + 1] + row] >> lx) & 0x7Fu];
+        }
+}
+
+template <typename real, bool IS3D>
+__global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t* __restrict__ phi,
+                                                           const uint8_t* __restrict__ mask, int ntx, int nty,
+                                                           const double* __restrict__ wtab, int nl_cap,
+                                                           int32_t* __restrict__ phi_comp, real* __restrict__ res_out,
+                                                           real* __restrict__ best_out,
+                                                           const unsigned long long* __restrict__ gate) {
+    if (gate && *gate == 0ull) return;  // device-side skip inside a captured step
+    typedef BitShape<IS3D> S;
+    constexpr int R = S::R;
+    extern __shared__ __align__(16) int32_t lab[];  // S::NH halo labels (dynamic: the rest is static)
+    __shared__ uint32_t bm[S::NL * S::NROWP];
+    __shared__ int16_t cells[S::NCELL];
+    __shared__ int16_t exact[S::NCELL];
+    __shared__ double w[S::R2MAX + 1];
+    __shared__ double rtab[S::NRS * 128];
+    __shared__ int32_t keys[S::HSLOT];
+    __shared__ int8_t dense[S::HSLOT];   // bitmap index of a slot, -1 when unused
+    __shared__ int s_ncell, s_nl, s_full, s_nexact;
+    typedef cub::BlockScan<int, 256> BS;
+    __shared__ typename BS::TempStorage scan;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int t = blockIdx.x;
+    const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
+    const int x0 = tx * S::TX, y0 = ty * S::TY, z0 = tz * S::TZ;
+    // 1. interface cells of the tile, in flat tile order
+    {
+        constexpr int PER = (S::NCELL + 255) / 256;
+        int flags[PER];
+        int cnt = 0;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int c = tid * PER + k;
+            int f = 0;
+            if (c < S::NCELL) {
+                const int lx = c % S::TX, ly = (c / S::TX) % S::TY, lz = c / (S::TX * S::TY);
+                const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+                if (x < D.Nx && y < D.Ny && z < D.Nz) f = mask[D.idx(z, y, x)];
+            }
+            flags[k] = f;
+            cnt += f;
+        }
+        int ex, total;
+        BS(scan).ExclusiveSum(cnt, ex, total);
+#pragma unroll
+        for (int k = 0; k < PER; ++k)
+            if (flags[k]) cells[ex++] = (int16_t)(tid * PER + k);
+        if (tid == 0) { s_ncell = total; s_full = 0; s_nexact = 0; }
+    }
+    if (tid < S::HSLOT) keys[tid] = -1;
+    __syncthreads();
+    const int ncell = s_ncell;
+    if (ncell == 0) return;
+    // 2. halo labels (one warp per row of 32 consecutive cells), weights, and
+    //    the row table: rtab[k][p] = sum of the weights of pattern p's taps
+    for (int r = warp; r < S::NROW; r += 8) {
+        const int hy = r % S::HY, hz = r / S::HY;
+        const int x = wrap_any(x0 + lane - R, D.Nx), y = wrap_any(y0 + hy - R, D.Ny);
+        const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
+        lab[r * S::HX + lane] = phi[D.idx(z, y, x)];
+    }
+    for (int e = tid; e <= S::R2MAX; e += 256) w[e] = wtab[e];
+    __syncthreads();
+    for (int e = tid; e < S::NRS * 128; e += 256) {
+        const int k = e >> 7, p = e & 127, r2 = rsum_value(k);
+        double sum = 0.0;
+        for (int j = 0; j < 7; ++j)
+            if (p & (1 << j)) sum += w[r2 + (j - 3) * (j - 3)];
+        rtab[e] = sum;
+    }
+    const int plane = S::HX * S::HY;
+    const int fo[6] = {-1, +1, -S::HX, +S::HX, -plane, +plane};
+    // 3. labels the scores need
+    for (int c = tid; c < ncell; c += 256) {
+        const int lc = cells[c];
+        const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
+        const int cb = ((IS3D ? lz + R : 0) * S::HY + ly + R) * S::HX + lx + R;
+        if (label_slot_insert(keys, lab[cb], S::HSLOT) < 0) s_full = 1;
+        for (int k = 0; k < (IS3D ? 6 : 4); ++k)
+            if (label_slot_insert(keys, lab[cb + fo[k]], S::HSLOT) < 0) s_full = 1;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // dense bitmap index per used slot, in slot order
+        int total = 0;
+        for (int base = 0; base < S::HSLOT; base += 32) {
+            const bool used = keys[base + lane] != -1;
+            const unsigned bal = __ballot_sync(0xffffffffu, used);
+            dense[base + lane] = (int8_t)(used ? total + __popc(bal & ((1u << lane) - 1u)) : -1);
+            total += __popc(bal);
+        }
+        if (lane == 0) s_nl = total;
+    }
+    __syncthreads();
+    const int nl = s_nl;
+    const bool screen = !s_full && nl <= (nl_cap < S::NL ? nl_cap : S::NL);
+    if (screen) {
+        // 4. one word per halo row and listed label (words of absent labels stay 0)
+        for (int e = tid; e < nl * S::NROWP; e += 256) bm[e] = 0u;
+        __syncthreads();
+        for (int r = warp; r < S::NROW; r += 8) {
+            const int32_t v = lab[r * S::HX + lane];
+            const unsigned grp = __match_any_sync(0xffffffffu, v);
+            if (lane == __ffs(grp) - 1) {
+                const int sl = label_slot_find(keys, v, S::HSLOT);
+                if (sl >= 0 && dense[sl] >= 0) bm[dense[sl] * S::NROWP + r] = grp;
+            }
+        }
+        __syncthreads();
+    }
+    // 5. screening; cells it cannot settle are queued
+    for (int c = tid; c < ncell; c += 256) {
+        bool settled = false;
+        if (screen) {
+            const int lc = cells[c];
+            const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
+            const int cb = ((IS3D ? lz + R : 0) * S::HY + ly + R) * S::HX + lx + R;
+            const int32_t pi = lab[cb];
+            int32_t cand[6] = {-1, -1, -1, -1, -1, -1};
+            int nc = 0;
+            for (int k = 0; k < (IS3D ? 6 : 4); ++k) {
+                const int32_t v = lab[cb + fo[k]];
+                if (v == pi) continue;
+                bool known = false;
+                for (int q = 0; q < nc; ++q) known |= cand[q] == v;
+                if (!known) cand[nc++] = v;
+            }
+            int li[7];
+            li[0] = dense[label_slot_find(keys, pi, S::HSLOT)] * S::NROWP;
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+                li[q + 1] = q < nc ? dense[label_slot_find(keys, cand[q], S::HSLOT)] * S::NROWP : li[0];
+            double resident = 0.0, sup[6] = {0, 0, 0, 0, 0, 0};
+            const int ncw = __reduce_max_sync(__activemask(), nc);
+            switch (ncw) {
+            case 0: screen_rows<IS3D, 0>(bm, rtab, li, lx, ly, lz, resident, sup); break;
+            case 1: screen_rows<IS3D, 1>(bm, rtab, li, lx, ly, lz, resident, sup); break;
+            case 2: screen_rows<IS3D, 2>(bm, rtab, li, lx, ly, lz, resident, sup); break;
+            case 3: screen_rows<IS3D, 3>(bm, rtab, li, lx, ly, lz, resident, sup); break;
+            default: screen_rows<IS3D, 6>(bm, rtab, li, lx, ly, lz, resident, sup); break;
+            }
+            double best = -1.0, second = -1.0;
+            int32_t best_label = pi;
+            for (int q = 0; q < nc; ++q) {
+                if (sup[q] > best) { second = best; best = sup[q]; best_label = cand[q]; }
+                else if (sup[q] > second) second = sup[q];
+            }
+            if (best - resident < -1e-5 && (nc < 2 || best - second > 1e-9)) {
+                settled = true;
+                const int i = D.idx(z0 + lz, y0 + ly, x0 + lx);
+                res_out[i] = (real)resident;
+                best_out[i] = (real)best;
+                phi_comp[i] = best_label;
+            }
+        }
+        if (!settled) exact[atomicAdd(&s_nexact, 1)] = (int16_t)c;
+    }
+    __syncthreads();
+    // 6. exact sums of the queued cells, all threads together
+    const int nexact = s_nexact;
+    for (int e = tid; e < nexact; e += 256) {
+        const int lc = cells[exact[e]];
+        const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
+        const int cb = ((IS3D ? lz + R : 0) * S::HY + ly + R) * S::HX + lx + R;
+        const int32_t pi = lab[cb];
+        int32_t cand[6] = {-1, -1, -1, -1, -1, -1};
+        int nc = 0;
+        for (int k = 0; k < (IS3D ? 6 : 4); ++k) {
+            const int32_t v = lab[cb + fo[k]];
+            if (v == pi) continue;
+            bool known = false;
+            for (int q = 0; q < nc; ++q) known |= cand[q] == v;
+            if (!known) cand[nc++] = v;
+        }
+        double resident = 0.0, sup[6] = {0, 0, 0, 0, 0, 0};
+        const int base = cb - (IS3D ? R * plane : 0) - R * S::HX - R;
+        const int ncw = __reduce_max_sync(__activemask(), nc);
+        switch (ncw) {
+        case 0: score_box_impl<R, IS3D, 0, S::HX, S::HY>(lab, base, w, pi, cand, resident, sup); break;
+        case 1: score_box_impl<R, IS3D, 1, S::HX, S::HY>(lab, base, w, pi, cand, resident, sup); break;
+        case 2: score_box_impl<R, IS3D, 2, S::HX, S::HY>(lab, base, w, pi, cand, resident, sup); break;
+        case 3: score_box_impl<R, IS3D, 3, S::HX, S::HY>(lab, base, w, pi, cand, resident, sup); break;
+        default: score_box_impl<R, IS3D, 6, S::HX, S::HY>(lab, base, w, pi, cand, resident, sup); break;
+        }
+        double best = -1.0;
+        int32_t best_label = pi;
+        for (int q = 0; q < nc; ++q)
+            if (sup[q] > best) { best = sup[q]; best_label = cand[q]; }
+        const int i = D.idx(z0 + lz, y0 + ly, x0 + lx);
+        res_out[i] = (real)resident;
+        best_out[i] = (real)best;
+        phi_comp[i] = best_label;
+    }
+}
+
+template <typename real, bool IS3D>
+static int launch_scores_screen(gpk_grid* G, real* res, real* best, const unsigned long long* gate) {
+    typedef BitShape<IS3D> S;
+    const Dims D = G->d;
+    const int ntx = (D.Nx + S::TX - 1) / S::TX, nty = (D.Ny + S::TY - 1) / S::TY, ntz = (D.Nz + S::TZ - 1) / S::TZ;
+    const size_t smem = sizeof(int32_t) * S::NH;
+    // set once per process (thread-safe initialisation of a function-local static)
+    static const cudaError_t attr_rc = cudaFuncSetAttribute(
+        k_bgr_scores_screen<real, IS3D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    GPK_CUDA_TRY(attr_rc);
+    k_bgr_scores_screen<real, IS3D><<<ntx * nty * ntz, 256, smem, G->stream>>>(
+        D, G->phi, G->mask, ntx, nty, G->d_remap_w, G->geometry_kernel == 2 ? 1 : S::NL, G->phi_comp, res, best,
+        gate);
+    G->launches++;
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
+}
+
 template <typename real, int R, bool IS3D>
 static int launch_scores(gpk_grid* G, real* res, real* best, const unsigned long long* gate) {
     typedef LocShape<R, IS3D> S;
@@ -274,8 +577,11 @@ using namespace gpk_dev;
 template <typename real>
 int gpk_bgr_scores_tiled(gpk_grid* G, int radius, real* res, real* best, const unsigned long long* gate) {
     if (radius != 3) return -1;
-    return G->d.is3d() ? launch_scores<real, 3, true>(G, res, best, gate)
-                       : launch_scores<real, 3, false>(G, res, best, gate);
+    if (G->geometry_kernel == 3)  // the all-exact tiled kernel (comparison runs)
+        return G->d.is3d() ? launch_scores<real, 3, true>(G, res, best, gate)
+                           : launch_scores<real, 3, false>(G, res, best, gate);
+    return G->d.is3d() ? launch_scores_screen<real, true>(G, res, best, gate)
+                       : launch_scores_screen<real, false>(G, res, best, gate);
 }
 
 // Tiled projection for the radii ceil(3 s) of the velocity kernel (s =

@@ -236,7 +236,8 @@ class GPKGrid:
                 "exact_counts": int(out[6]), "count_scanned": int(out[7])}
 
     def set_geometry_kernel(self, kind: str) -> None:
-        check(lib().gpk_grid_set_geometry_kernel(self._h, {"tiled": 0, "per_cell": 1, "tiled_batched": 2}[kind]))
+        check(lib().gpk_grid_set_geometry_kernel(
+            self._h, {"tiled": 0, "per_cell": 1, "tiled_batched": 2, "tiled_exact_scores": 3}[kind]))
 
     def set_external_elastic(self, on: bool = True) -> None:
         """E_el is supplied by the caller (e.g. SpectralElasticity.couple) and

@@ -248,7 +248,9 @@ int gpk_grid_wave_stats(gpk_grid* grid, uint64_t out[8]);
 /* Kernel selection (all give identical results): 0 = tiled shared-memory
  * kernels where an instantiation exists (default), 1 = the per-interface-
  * cell kernels, 2 = tiled kernels with one label per geometry bitmap batch
- * (exercises the many-label path of the tiled geometry kernel).           */
+ * (exercises the many-label path of the tiled geometry kernel; the remap
+ * scores then skip their bitmap screening), 3 = tiled kernels with every
+ * remap score summed tap by tap (no screening).                           */
 int gpk_grid_set_geometry_kernel(gpk_grid* grid, int kind);
 /* External elastic energy (no counterpart in the reference): when on, the
  * E_el field is what the caller last wrote (an upload, a device write, or

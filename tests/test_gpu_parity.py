@@ -95,6 +95,29 @@ def test_geometry_kernels_agree_2d(oracle_mod, sigma):
         assert not compare_all(gpu, ora), kind
 
 
+@pytest.mark.parametrize("shape,grains", [((40, 44, 36), 120), ((1, 160, 150), 90)])
+def test_remap_screening_equals_exact_scores(oracle_mod, shape, grains):
+    """The remap scores settle most cells from bitmap row sums and sum the
+    rest tap by tap; every field equals the all-tap-by-tap kernel's and the
+    oracle's after each step, through many remap exchanges."""
+    phi, g = oracle_mod.voronoi(*shape, grains, 21)
+    iso = thermo.isotropic(1.0, 1.0)
+    a = GPKGrid(*shape, 1.0, iso, 0.0, 1.5)
+    b = GPKGrid(*shape, 1.0, iso, 0.0, 1.5)
+    b.set_geometry_kernel("tiled_exact_scores")
+    ora = oracle_mod.OracleGrid(*shape, 1.0, iso, 0.0, 1.5)
+    _load((a, b, ora), phi=phi, g=g, alpha=1.0)
+    exchanges = 0
+    for s in range(24):
+        da, db, do = a.step(), b.step(), ora.step()
+        assert da == db == do, s
+        assert not compare_all(a, b), s
+        assert not compare_all(a, ora, ["phi", "alpha", "phi_comp", "g"]), s
+        exchanges += a.counters()[2]
+    if shape[0] > 1:
+        assert exchanges > 0   # the 3-D case runs both remap passes with exchanges
+
+
 @pytest.mark.parametrize("divisor", [2, 4])
 def test_geometry_tile_heights_2d(oracle_mod, divisor):
     """The 2-D tiles of 512 and 256 cells at sigma 1.5 (kernel radius 8),
