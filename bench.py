@@ -43,10 +43,10 @@ CPU_SIZE = 128
 CPU_GRAINS = 512
 # DRAM read + write bytes of one k_geometry_tiled launch on the 256^3 / 4096
 # grain / sigma 1.5 workload, measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum, one-pass metrics, one launch after the settling steps)
-GEOMETRY_TRAFFIC_256 = 463.91e6
-GEOMETRY_TRAFFIC_NOTE = ("DRAM bytes of one launch of the kernel, scaled by cell count from a 160^3 ncu capture "
-                         "of the same kernel and grain size")
+# dram__bytes_write.sum, one-pass metrics, the launch of the third warm-up step)
+GEOMETRY_TRAFFIC_256 = 530.12e6
+GEOMETRY_TRAFFIC_NOTE = ("DRAM bytes (read 303.10 MB + write 227.02 MB) of one launch of the kernel on this "
+                         "256^3 workload, measured by ncu with the one-pass dram__bytes metrics")
 
 
 def _peaks():
@@ -685,9 +685,11 @@ def separable_measurement(n: int = 256, grains: int = 32, sigma: float = 5.0, se
     grains, sigma 5 cells (Gaussian radius 18, geometry radius 20 > 18), FP32
     reference arithmetic.  Per step and interface label: the x pass of the
     indicator, the y and z passes, the evaluation on the label's interface
-    cells; algorithmic bytes of the geometry stage: labels in and the
-    smoothed field out per pass (8 B per cell), the evaluation's labels,
-    mask and smoothed field (9 B per cell), per label."""
+    cells.  Algorithmic bytes of the geometry stage: the labels read once
+    per interface label (4 B per cell) and the normals and curvature of the
+    interface cells written once (16 B each); the intermediate smoothed
+    fields between the passes are not algorithmic bytes (the traffic they
+    cause is in `intermediate_bytes_per_step`)."""
     import torch
     from gpk_b200 import GPKGrid, thermo
     g = GPKGrid(n, n, n, 1.0, thermo.isotropic(1.0, 1.0), 0.0, sigma)
@@ -711,7 +713,9 @@ def separable_measurement(n: int = 256, grains: int = 32, sigma: float = 5.0, se
     g.profile(False)
     geo_ms = st["geometry"][0] / max(1, st["geometry"][1])
     cells = n ** 3
-    geo_bytes = grains * cells * 33.0
+    n_active = g.interface_fraction() * cells
+    geo_bytes = grains * cells * 4.0 + n_active * 16.0
+    inter_bytes = grains * cells * 29.0  # x-pass output, y and z passes in/out, evaluation reads
     peak, peak_kind = _peaks()
     res = {"workload": f"3-D isotropic grain growth {n}^3, {grains} Voronoi grains, sigma {sigma} cells "
                        "(separable geometry: per-label x/y/z Gaussian passes + interface evaluation), FP32",
@@ -720,7 +724,7 @@ def separable_measurement(n: int = 256, grains: int = 32, sigma: float = 5.0, se
            "stages_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in st.items()},
            "roofline": {"kernels": "k_sep_x_indicator_f2, k_sep_pass (y, z), k_separable_eval per label",
                         "bound": "fp32 issue (the reference's unfused multiply + add per tap)",
-                        "algorithmic_bytes_per_step": geo_bytes,
+                        "algorithmic_bytes_per_step": geo_bytes, "intermediate_bytes_per_step": inter_bytes,
                         "achieved": geo_bytes / (geo_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                         "frac": geo_bytes / (geo_ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind}}
     g.close()
@@ -836,10 +840,9 @@ def run_gpu_arm(args):
     tap_adds = n_active * W ** 3 * 9 / (geo_ms / 1e3)
     separable = (W - 1) // 2 > 18
     if separable:
-        # per interface label: x pass (labels in, 4 B; t1 out, 4 B), y and z
-        # passes (8 B each), evaluation (labels, mask, S: 9 B); the interface
-        # cells' normals and curvature (16 B) once
-        geo_bytes = GRAINS * cells * 33.0 + n_active * 16
+        # per interface label the labels once (4 B per cell); the interface
+        # cells' normals and curvature (16 B) once; intermediates excluded
+        geo_bytes = GRAINS * cells * 4.0 + n_active * 16
         achieved = geo_bytes / (geo_ms / 1e3) / 1e9
     roofline = {"kernel": "k_geometry_tiled (label-bitmap Gaussian-Hessian tensor stencil + competitor)",
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -781,7 +781,7 @@ extern "C" int gpk_grid_stage_times(gpk_grid* G, double ms[GPK_NUM_STAGES], uint
     return GPK_OK;
 }
 
-extern "C" int gpk_grid_wave_stats(gpk_grid* G, uint64_t out[8]) {
+extern "C" int gpk_grid_wave_stats(gpk_grid* G, uint64_t out[10]) {
     if (!G || !out) return GPK_ERR_INVALID_ARGUMENT;
     for (int k = 0; k < 4; ++k) {
         out[k] = G->wave_stats[k];
@@ -792,7 +792,9 @@ extern "C" int gpk_grid_wave_stats(gpk_grid* G, uint64_t out[8]) {
     out[5] = G->h_scal->flood_cells;
     out[6] = G->h_scal->count_tasks;
     out[7] = G->h_scal->count_scanned;
-    GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->flood_tasks, 0, 4 * sizeof(unsigned long long), G->stream));
+    out[8] = G->h_scal->score_cells;
+    out[9] = G->h_scal->score_exact;
+    GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->flood_tasks, 0, 6 * sizeof(unsigned long long), G->stream));
     return GPK_OK;
 }
 

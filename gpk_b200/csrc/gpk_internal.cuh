@@ -92,6 +92,8 @@ struct StepScalars {
     unsigned long long exch_first, gate2;
     // instrumentation of the label-wide work (summed until read)
     unsigned long long flood_tasks, flood_cells, count_tasks, count_scanned;
+    // remap scores: interface cells scored, and those summed tap by tap
+    unsigned long long score_cells, score_exact;
 };
 
 // bounded grid-wide barrier for persistent kernels launched cooperatively.

@@ -331,7 +331,8 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
                                                            const double* __restrict__ wtab, int nl_cap,
                                                            int32_t* __restrict__ phi_comp, real* __restrict__ res_out,
                                                            real* __restrict__ best_out,
-                                                           const unsigned long long* __restrict__ gate) {
+                                                           const unsigned long long* __restrict__ gate,
+                                                           StepScalars* stats) {
     if (gate && *gate == 0ull) return;  // device-side skip inside a captured step
     typedef BitShape<IS3D> S;
     constexpr int R = S::R;
@@ -485,6 +486,10 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
     __syncthreads();
     // 6. exact sums of the queued cells, all threads together
     const int nexact = s_nexact;
+    if (tid == 0 && stats) {
+        atomicAdd(&stats->score_cells, (unsigned long long)ncell);
+        atomicAdd(&stats->score_exact, (unsigned long long)nexact);
+    }
     for (int e = tid; e < nexact; e += 256) {
         const int lc = cells[exact[e]];
         const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
@@ -532,7 +537,7 @@ static int launch_scores_screen(gpk_grid* G, real* res, real* best, const unsign
     GPK_CUDA_TRY(attr_rc);
     k_bgr_scores_screen<real, IS3D><<<ntx * nty * ntz, 256, smem, G->stream>>>(
         D, G->phi, G->mask, ntx, nty, G->d_remap_w, G->geometry_kernel == 2 ? 1 : S::NL, G->phi_comp, res, best,
-        gate);
+        gate, G->scal);
     G->launches++;
     GPK_CUDA_TRY(cudaGetLastError());
     return GPK_OK;

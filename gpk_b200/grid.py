@@ -229,11 +229,12 @@ class GPKGrid:
               "extinction", "transport")
 
     def wave_stats(self) -> dict:
-        out = (C.c_uint64 * 8)()
+        out = (C.c_uint64 * 10)()
         check(lib().gpk_grid_wave_stats(self._h, out))
         return {"crossing_waves": int(out[0]), "remap_waves": int(out[1]), "candidates": int(out[2]),
                 "remap_proposals": int(out[3]), "flood_fills": int(out[4]), "flood_cells": int(out[5]),
-                "exact_counts": int(out[6]), "count_scanned": int(out[7])}
+                "exact_counts": int(out[6]), "count_scanned": int(out[7]), "score_cells": int(out[8]),
+                "score_cells_exact": int(out[9])}
 
     def set_geometry_kernel(self, kind: str) -> None:
         check(lib().gpk_grid_set_geometry_kernel(

@@ -242,9 +242,10 @@ int gpk_grid_profile(gpk_grid* grid, int enable);
 int gpk_grid_stage_times(gpk_grid* grid, double ms[GPK_NUM_STAGES], uint64_t calls[GPK_NUM_STAGES]);
 /* out = {waves of the crossing sweeps, waves of the remap exchange loops,
  * crossing candidates, remap proposals, global flood fills, cells they
- * visited, exact label counts, candidates those counts scanned}, summed
- * since the last read.                                                     */
-int gpk_grid_wave_stats(gpk_grid* grid, uint64_t out[8]);
+ * visited, exact label counts, candidates those counts scanned, interface
+ * cells given remap scores, those of them summed tap by tap}, summed since
+ * the last read.                                                           */
+int gpk_grid_wave_stats(gpk_grid* grid, uint64_t out[10]);
 /* Kernel selection (all give identical results): 0 = tiled shared-memory
  * kernels where an instantiation exists (default), 1 = the per-interface-
  * cell kernels, 2 = tiled kernels with one label per geometry bitmap batch
