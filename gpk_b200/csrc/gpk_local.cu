@@ -313,16 +313,43 @@ __device__ __forceinline__ void screen_rows(const uint32_t* __restrict__ bm, con
                                             double sup[6]) {
     typedef BitShape<IS3D> S;
     constexpr int R = S::R;
-#pragma unroll 1
+    const int row0 = (IS3D ? lz * S::HY : 0) + ly;  // halo row of tap (-R, -R) (2-D: (0, -R))
+#pragma unroll
     for (int dz = (IS3D ? -R : 0); dz <= (IS3D ? R : 0); ++dz)
 #pragma unroll
         for (int dy = -R; dy <= R; ++dy) {
-            const int row = ((IS3D ? lz + R + dz : 0) * S::HY) + ly + R + dy;
+            const int row = row0 + (IS3D ? (dz + R) * S::HY : 0) + dy + R;
             const double* t = rtab + rsum_index(dy * dy + dz * dz) * 128;
             resident += t[(bm[li[0] + row] >> lx) & 0x7Fu];
 #pragma unroll
             for (int q = 0; q < NC; ++q) sup[q] += t[(bm[li[q + 1] + row] >> lx) & 0x7Fu];
         }
+}
+
+// Distinct face-neighbour labels other than pi, in face order, kept in
+// registers (no indexed arrays): c[q] for q < n, -1 beyond.
+template <bool IS3D>
+__device__ __forceinline__ int face_candidates(const int32_t* __restrict__ lab, int cb, int32_t pi, int32_t c[6]) {
+    typedef BitShape<IS3D> S;
+    constexpr int NF = IS3D ? 6 : 4;
+    const int fo[6] = {-1, +1, -S::HX, +S::HX, -S::HX * S::HY, +S::HX * S::HY};
+    int32_t v[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { v[k] = k < NF ? lab[cb + fo[k]] : pi; c[k] = -1; }
+    int n = 0;
+#pragma unroll
+    for (int k = 0; k < NF; ++k) {
+        bool fresh = v[k] != pi;
+#pragma unroll
+        for (int j = 0; j < k; ++j) fresh &= v[j] != v[k];
+        if (fresh) {
+#pragma unroll
+            for (int q = 0; q <= k; ++q)
+                if (q == n) c[q] = v[k];
+            ++n;
+        }
+    }
+    return n;
 }
 
 template <typename real, bool IS3D>
@@ -348,9 +375,15 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
     typedef cub::BlockScan<int, 256> BS;
     __shared__ typename BS::TempStorage scan;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ int rowbase[S::NROW];  // flat index of halo row r's periodic (z, y) row
     const int t = blockIdx.x;
     const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
     const int x0 = tx * S::TX, y0 = ty * S::TY, z0 = tz * S::TZ;
+    const int xw = wrap_any(x0 + lane - R, D.Nx);  // periodic x of halo column `lane`
+    for (int r = tid; r < S::NROW; r += 256) {
+        const int hy = r % S::HY, hz = r / S::HY;
+        rowbase[r] = D.idx(IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0, wrap_any(y0 + hy - R, D.Ny), 0);
+    }
     // 1. interface cells of the tile, in flat tile order
     {
         constexpr int PER = (S::NCELL + 255) / 256;
@@ -381,11 +414,14 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
     if (ncell == 0) return;
     // 2. halo labels (one warp per row of 32 consecutive cells), weights, and
     //    the row table: rtab[k][p] = sum of the weights of pattern p's taps
-    for (int r = warp; r < S::NROW; r += 8) {
-        const int hy = r % S::HY, hz = r / S::HY;
-        const int x = wrap_any(x0 + lane - R, D.Nx), y = wrap_any(y0 + hy - R, D.Ny);
-        const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
-        lab[r * S::HX + lane] = phi[D.idx(z, y, x)];
+    for (int r0 = warp; r0 < S::NROW; r0 += 64) {  // eight rows per warp at a time, loads issued together
+        int32_t v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (r0 + 8 * u < S::NROW) v[u] = phi[rowbase[r0 + 8 * u] + xw];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (r0 + 8 * u < S::NROW) lab[(r0 + 8 * u) * S::HX + lane] = v[u];
     }
     for (int e = tid; e <= S::R2MAX; e += 256) w[e] = wtab[e];
     __syncthreads();
@@ -398,14 +434,24 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
     }
     const int plane = S::HX * S::HY;
     const int fo[6] = {-1, +1, -S::HX, +S::HX, -plane, +plane};
-    // 3. labels the scores need
-    for (int c = tid; c < ncell; c += 256) {
-        const int lc = cells[c];
-        const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
-        const int cb = ((IS3D ? lz + R : 0) * S::HY + ly + R) * S::HX + lx + R;
-        if (label_slot_insert(keys, lab[cb], S::HSLOT) < 0) s_full = 1;
-        for (int k = 0; k < (IS3D ? 6 : 4); ++k)
-            if (label_slot_insert(keys, lab[cb + fo[k]], S::HSLOT) < 0) s_full = 1;
+    // 3. labels the scores need: a cell's label and its distinct other face
+    //    labels; of the lanes of a warp holding one label, one inserts it
+    for (int c0 = 0; c0 < ncell; c0 += 256) {
+        const int c = c0 + tid;
+        int32_t own = -1, cn[6] = {-1, -1, -1, -1, -1, -1};
+        if (c < ncell) {
+            const int lc = cells[c];
+            const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
+            const int cb = ((IS3D ? lz + R : 0) * S::HY + ly + R) * S::HX + lx + R;
+            own = lab[cb];
+            face_candidates<IS3D>(lab, cb, own, cn);
+        }
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            const int32_t v = q == 0 ? own : cn[q - 1];
+            const unsigned grp = __match_any_sync(0xffffffffu, v);
+            if (v >= 0 && lane == __ffs(grp) - 1 && label_slot_insert(keys, v, S::HSLOT) < 0) s_full = 1;
+        }
     }
     __syncthreads();
     if (warp == 0) {
@@ -444,15 +490,8 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
             const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
             const int cb = ((IS3D ? lz + R : 0) * S::HY + ly + R) * S::HX + lx + R;
             const int32_t pi = lab[cb];
-            int32_t cand[6] = {-1, -1, -1, -1, -1, -1};
-            int nc = 0;
-            for (int k = 0; k < (IS3D ? 6 : 4); ++k) {
-                const int32_t v = lab[cb + fo[k]];
-                if (v == pi) continue;
-                bool known = false;
-                for (int q = 0; q < nc; ++q) known |= cand[q] == v;
-                if (!known) cand[nc++] = v;
-            }
+            int32_t cand[6];
+            const int nc = face_candidates<IS3D>(lab, cb, pi, cand);
             int li[7];
             li[0] = dense[label_slot_find(keys, pi, S::HSLOT)] * S::NROWP;
 #pragma unroll
@@ -469,7 +508,9 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
             }
             double best = -1.0, second = -1.0;
             int32_t best_label = pi;
-            for (int q = 0; q < nc; ++q) {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                if (q >= nc) break;
                 if (sup[q] > best) { second = best; best = sup[q]; best_label = cand[q]; }
                 else if (sup[q] > second) second = sup[q];
             }
@@ -523,6 +564,280 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
         best_out[i] = (real)best;
         phi_comp[i] = best_label;
     }
+}
+
+// ---------------------------------------------------------------------------
+// pair projection on pair bitmaps (radius 3)
+// ---------------------------------------------------------------------------
+// A tap of the projection counts when its cell is an interface cell with the
+// centre's unordered label pair (src/gpk_physics.cpp:152-193).  A tile of
+// 26 x TY x TZ cells lists the distinct pairs of its interface cells; per
+// pair, one 32-bit word per halo row marks the halo cells holding that pair
+// (a halo row is 32 cells), so a row of 7 taps is a 7-bit pattern and only
+// its set bits add: num += w * (orientation_j * vn_j), den += w, in double,
+// z -> y -> x, as the reference adds them.  The 28 weights by squared
+// distance are kernel parameters (constant-bank operands of the products).
+// Tiles with more than 64 distinct pairs sum their cells straight from global
+// memory in the same order.
+struct ProjW {
+    double w[28];  // (double)expf(-r2 / (2 s^2)) for r2 = 0..27
+};
+
+__device__ __forceinline__ unsigned long long pair_key(int32_t p, int32_t q) {
+    const int32_t lo = p < q ? p : q, hi = p < q ? q : p;
+    return ((unsigned long long)(uint32_t)lo << 32) | (uint32_t)hi;
+}
+__device__ __forceinline__ int pair_slot_insert(unsigned long long* keys, unsigned long long v) {
+    const unsigned h = (unsigned)((v * 0x9E3779B97F4A7C15ull) >> 58);  // 6 bits: 64 slots
+    for (int k = 0; k < 64; ++k) {
+        const int sl = (int)((h + k) & 63u);
+        const unsigned long long old = atomicCAS(&keys[sl], ~0ull, v);
+        if (old == ~0ull || old == v) return sl;
+    }
+    return -1;
+}
+__device__ __forceinline__ int pair_slot_find(const unsigned long long* keys, unsigned long long v) {
+    const unsigned h = (unsigned)((v * 0x9E3779B97F4A7C15ull) >> 58);
+    for (int k = 0; k < 64; ++k) {
+        const int sl = (int)((h + k) & 63u);
+        const unsigned long long key = keys[sl];
+        if (key == v) return sl;
+        if (key == ~0ull) return -1;
+    }
+    return -1;
+}
+
+// One cell's sums read from global memory (tiles whose pairs overflow the
+// slot table): the same taps, order and operations as the bitmap path.
+template <typename real, bool IS3D>
+__device__ void proj_cell_global(const Dims& D, const int32_t* __restrict__ phi, const int32_t* __restrict__ phi_comp,
+                                 const uint8_t* __restrict__ mask, const real* __restrict__ vn, const ProjW& pw,
+                                 int x, int y, int z, unsigned long long key, double& num, double& den) {
+    constexpr int R = 3, RZ = IS3D ? 3 : 0;
+#pragma unroll 1
+    for (int dz = -RZ; dz <= RZ; ++dz)
+#pragma unroll 1
+        for (int dy = -R; dy <= R; ++dy)
+#pragma unroll
+            for (int dx = -R; dx <= R; ++dx) {
+                const int j = D.idx(IS3D ? wrap_any(z + dz, D.Nz) : 0, wrap_any(y + dy, D.Ny), wrap_any(x + dx, D.Nx));
+                const int32_t pj = phi[j], qj = phi_comp[j];
+                if (mask[j] && pj != qj && pair_key(pj, qj) == key) {
+                    const double wt = pw.w[dz * dz + dy * dy + dx * dx];
+                    const double sv = pj < qj ? (double)vn[j] : -(double)vn[j];
+                    num = num + wt * sv;
+                    den = den + wt;
+                }
+            }
+}
+
+template <typename real, bool IS3D>
+__global__ void __launch_bounds__(256) k_projection_bits(Dims D, const int32_t* __restrict__ phi,
+                                                         const int32_t* __restrict__ phi_comp,
+                                                         const uint8_t* __restrict__ mask, const real* __restrict__ vn,
+                                                         real* __restrict__ vn_out, int ntx, int nty, int nl_cap,
+                                                         ProjW pw) {
+    typedef BitShape<IS3D> S;
+    constexpr int R = S::R, RZ = IS3D ? R : 0;
+    constexpr unsigned long long NONE = ~0ull;
+    extern __shared__ __align__(16) double svn[];  // S::NH signed velocities of the halo
+    __shared__ uint32_t bm[S::NL * S::NROWP];
+    __shared__ int16_t cells[S::NCELL];
+    __shared__ int8_t cslot[S::NCELL];  // pair slot of a listed cell; -1: no competitor, -2: slots full
+    __shared__ unsigned long long keys[64];
+    __shared__ int8_t dense[64];
+    __shared__ int rowbase[S::NROW];  // flat index of halo row r's periodic (z, y) row
+    __shared__ int s_ncell, s_np, s_full;
+    typedef cub::BlockScan<int, 256> BS;
+    __shared__ typename BS::TempStorage scan;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int t = blockIdx.x;
+    const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
+    const int x0 = tx * S::TX, y0 = ty * S::TY, z0 = tz * S::TZ;
+    const int xw = wrap_any(x0 + lane - R, D.Nx);  // periodic x of halo column `lane`
+    for (int r = tid; r < S::NROW; r += 256) {
+        const int hy = r % S::HY, hz = r / S::HY;
+        rowbase[r] = D.idx(IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0, wrap_any(y0 + hy - R, D.Ny), 0);
+    }
+    // 1. interface cells of the tile, in flat tile order
+    {
+        constexpr int PER = (S::NCELL + 255) / 256;
+        int flags[PER];
+        int cnt = 0;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int c = tid * PER + k;
+            int f = 0;
+            if (c < S::NCELL) {
+                const int lx = c % S::TX, ly = (c / S::TX) % S::TY, lz = c / (S::TX * S::TY);
+                const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+                if (x < D.Nx && y < D.Ny && z < D.Nz) f = mask[D.idx(z, y, x)];
+            }
+            flags[k] = f;
+            cnt += f;
+        }
+        int ex, total;
+        BS(scan).ExclusiveSum(cnt, ex, total);
+#pragma unroll
+        for (int k = 0; k < PER; ++k)
+            if (flags[k]) cells[ex++] = (int16_t)(tid * PER + k);
+        if (tid == 0) { s_ncell = total; s_full = 0; }
+    }
+    if (tid < 64) keys[tid] = NONE;
+    __syncthreads();
+    const int ncell = s_ncell;
+    if (ncell == 0) return;
+    // 2. the pair of every listed cell (of the lanes of a warp holding one
+    //    pair, one inserts it); cells without a competitor keep vn
+    for (int c0 = 0; c0 < ncell; c0 += 256) {
+        const int c = c0 + tid;
+        unsigned long long key = NONE;
+        if (c < ncell) {
+            const int lc = cells[c];
+            const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
+            const int i = D.idx(z0 + lz, y0 + ly, x0 + lx);
+            const int32_t p = phi[i], q = phi_comp[i];
+            if (p != q) key = pair_key(p, q);
+            else vn_out[i] = vn[i];
+        }
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        const int leader = __ffs(grp) - 1;
+        int sl = -1;
+        if (key != NONE && lane == leader) {
+            sl = pair_slot_insert(keys, key);
+            if (sl < 0) s_full = 1;
+        }
+        sl = __shfl_sync(0xffffffffu, sl, leader);
+        if (c < ncell) cslot[c] = (int8_t)(key == NONE ? -1 : (sl < 0 ? -2 : sl));
+    }
+    __syncthreads();
+    if (s_full) {
+        for (int c = tid; c < ncell; c += 256) {
+            if (cslot[c] == -1) continue;
+            const int lc = cells[c];
+            const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
+            const int i = D.idx(z0 + lz, y0 + ly, x0 + lx);
+            const int32_t p = phi[i], q = phi_comp[i];
+            double num = 0.0, den = 0.0;
+            proj_cell_global<real, IS3D>(D, phi, phi_comp, mask, vn, pw, x0 + lx, y0 + ly, z0 + lz, pair_key(p, q),
+                                         num, den);
+            real out = vn[i];
+            if (den > 0.0) out = (p < q ? (real)1 : (real)-1) * (real)(num / den);
+            vn_out[i] = out;
+        }
+        return;
+    }
+    if (warp == 0) {
+        // dense pair index per used slot, in slot order
+        int total = 0;
+        for (int base = 0; base < 64; base += 32) {
+            const bool used = keys[base + lane] != NONE;
+            const unsigned bal = __ballot_sync(0xffffffffu, used);
+            dense[base + lane] = (int8_t)(used ? total + __popc(bal & ((1u << lane) - 1u)) : -1);
+            total += __popc(bal);
+        }
+        if (lane == 0) s_np = total;
+    }
+    __syncthreads();
+    const int np = s_np;
+    const int nlb = nl_cap < S::NL ? nl_cap : S::NL;
+    // 3. per batch of pairs: halo bitmaps (the first batch also stages the
+    //    signed velocities), then the batch's cells
+    for (int b0 = 0; b0 < np; b0 += nlb) {
+        const int nb = np - b0 < nlb ? np - b0 : nlb;
+        for (int e = tid; e < nb * S::NROWP; e += 256) bm[e] = 0u;
+        __syncthreads();
+        // a warp takes four rows at a time, their loads issued together
+        for (int r0 = warp; r0 < S::NROW; r0 += 32) {
+            int32_t pj[4], qj[4];
+            uint8_t mj[4];
+            real vj[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int r = r0 + 8 * u;
+                if (r < S::NROW) {
+                    const int j = rowbase[r] + xw;
+                    pj[u] = phi[j];
+                    qj[u] = phi_comp[j];
+                    mj[u] = mask[j];
+                    vj[u] = vn[j];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int r = r0 + 8 * u;
+                if (r >= S::NROW) break;
+                const bool valid = mj[u] && pj[u] != qj[u];
+                const unsigned long long key = valid ? pair_key(pj[u], qj[u]) : NONE;
+                if (b0 == 0) svn[r * S::HX + lane] = valid ? (pj[u] < qj[u] ? (double)vj[u] : -(double)vj[u]) : 0.0;
+                const unsigned grp = __match_any_sync(0xffffffffu, key);
+                if (key != NONE && lane == __ffs(grp) - 1) {
+                    const int sl = pair_slot_find(keys, key);
+                    if (sl >= 0) {
+                        const int d = dense[sl] - b0;
+                        if (d >= 0 && d < nb) bm[d * S::NROWP + r] = grp;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        for (int c = tid; c < ncell; c += 256) {
+            const int sl = cslot[c];
+            if (sl < 0) continue;
+            const int d = dense[sl] - b0;
+            if (d < 0 || d >= nb) continue;
+            const int lc = cells[c];
+            const int lx = lc % S::TX, ly = (lc / S::TX) % S::TY, lz = lc / (S::TX * S::TY);
+            const int rc = (IS3D ? lz * S::HY : 0) + ly;  // halo row of tap (-RZ, -R)
+            const uint32_t* bmb = bm + d * S::NROWP + rc;
+            const double* sv = svn + rc * S::HX + lx;
+            double num = 0.0, den = 0.0;
+#pragma unroll
+            for (int dz = -RZ; dz <= RZ; ++dz)
+#pragma unroll
+                for (int dy = -R; dy <= R; ++dy) {
+                    const int ro = (dz + RZ) * S::HY + dy + R;
+                    const uint32_t bits = (bmb[ro] >> lx) & 0x7Fu;
+                    if (!bits) continue;
+                    const double* s = sv + ro * S::HX;
+#pragma unroll
+                    for (int k = 0; k < 2 * R + 1; ++k)
+                        if (bits & (1u << k)) {
+                            const double wt = pw.w[dz * dz + dy * dy + (k - R) * (k - R)];
+                            num = num + wt * s[k];
+                            den = den + wt;
+                        }
+                }
+            const int i = D.idx(z0 + lz, y0 + ly, x0 + lx);
+            const int32_t p = phi[i], q = phi_comp[i];
+            real out = vn[i];
+            if (den > 0.0) out = (p < q ? (real)1 : (real)-1) * (real)(num / den);
+            vn_out[i] = out;
+        }
+        __syncthreads();  // the next batch rewrites the bitmaps
+    }
+}
+
+template <typename real, bool IS3D>
+static int launch_projection_bits(gpk_grid* G) {
+    typedef BitShape<IS3D> S;
+    const HostKernels<real>* hk = (const HostKernels<real>*)G->host_kernels;
+    if (hk->proj_w.size() > 28) return -1;
+    ProjW pw{};
+    for (size_t k = 0; k < hk->proj_w.size(); ++k) pw.w[k] = hk->proj_w[k];
+    const Dims D = G->d;
+    const int ntx = (D.Nx + S::TX - 1) / S::TX, nty = (D.Ny + S::TY - 1) / S::TY, ntz = (D.Nz + S::TZ - 1) / S::TZ;
+    const size_t smem = sizeof(double) * S::NH;
+    // set once per process (thread-safe initialisation of a function-local static)
+    static const cudaError_t attr_rc = cudaFuncSetAttribute(
+        k_projection_bits<real, IS3D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    GPK_CUDA_TRY(attr_rc);
+    k_projection_bits<real, IS3D><<<ntx * nty * ntz, 256, smem, G->stream>>>(
+        D, G->phi, G->phi_comp, G->mask, (const real*)G->f[GPK_FIELD_VN], (real*)G->vn2, ntx, nty,
+        G->geometry_kernel == 2 ? 1 : S::NL, pw);
+    G->launches++;
+    GPK_CUDA_TRY(cudaGetLastError());
+    return GPK_OK;
 }
 
 template <typename real, bool IS3D>
@@ -609,7 +924,11 @@ static int projection_r(gpk_grid* G) {
 template <typename real>
 int gpk_projection_tiled(gpk_grid* G, int radius) {
     switch (radius) {
-        case 3: return projection_r<real, 3>(G);
+        case 3:
+            // pair bitmaps; kind 3 keeps the pair-compare tiles (comparison runs)
+            if (G->geometry_kernel != 3)
+                return G->d.is3d() ? launch_projection_bits<real, true>(G) : launch_projection_bits<real, false>(G);
+            return projection_r<real, 3>(G);
         case 4: return projection_r<real, 4>(G);
         case 5: return projection_r<real, 5>(G);
         case 6: return projection_r<real, 6>(G);

@@ -61,14 +61,14 @@ def test_polycrystal_3d_bitexact(oracle_mod):
 # sigma 0.5 / 1.0 / 1.5 / 2.0 / 2.2 give geometry radii 4 / 6 / 8 / 9 / 10
 @pytest.mark.parametrize("sigma", [0.5, 1.0, 1.5, 2.0, 2.2])
 def test_geometry_kernels_agree_3d(oracle_mod, sigma):
-    """Tiled (one and many bitmap batches) and per-cell kernels give the
-    oracle's fields bit for bit."""
+    """Tiled (one and many bitmap batches; pair-bitmap and pair-compare
+    projection) and per-cell kernels give the oracle's fields bit for bit."""
     phi, g = polycrystal(24, 30, 36, 20, 12)
     ora = oracle_mod.OracleGrid(24, 30, 36, 1.0, thermo.isotropic(1.0, 1.0), 0.0, sigma)
     _load((ora,), phi=phi, g=g, alpha=1.0)
     for _ in range(10):
         ora.step()
-    for kind in ("tiled", "per_cell", "tiled_batched"):
+    for kind in ("tiled", "per_cell", "tiled_batched", "tiled_exact_scores"):
         gpu = GPKGrid(24, 30, 36, 1.0, thermo.isotropic(1.0, 1.0), 0.0, sigma)
         gpu.set_geometry_kernel(kind)
         _load((gpu,), phi=phi, g=g, alpha=1.0)
@@ -86,7 +86,7 @@ def test_geometry_kernels_agree_2d(oracle_mod, sigma):
     _load((ora,), phi=phi, g=g, alpha=1.0)
     for _ in range(10):
         ora.step()
-    for kind in ("tiled", "tiled_batched"):
+    for kind in ("tiled", "tiled_batched", "tiled_exact_scores"):
         gpu = GPKGrid(1, 70, 90, 1.0, thermo.isotropic(1.0, 1.0), 0.0, sigma)
         gpu.set_geometry_kernel(kind)
         _load((gpu,), phi=phi, g=g, alpha=1.0)
@@ -116,6 +116,27 @@ def test_remap_screening_equals_exact_scores(oracle_mod, shape, grains):
         exchanges += a.counters()[2]
     if shape[0] > 1:
         assert exchanges > 0   # the 3-D case runs both remap passes with exchanges
+
+
+@pytest.mark.parametrize("shape", [(12, 20, 40), (1, 48, 64)])
+def test_projection_many_pairs_per_tile(oracle_mod, shape):
+    """Label noise: nearly every cell is an interface cell and a projection
+    tile holds far more than the 64 label pairs its slot table takes (those
+    tiles sum from global memory); two steps against the oracle and the
+    pair-compare kernel, every public field bit for bit."""
+    rng = np.random.default_rng(3)
+    phi = rng.integers(0, 400, size=shape).astype(np.int32)
+    iso = thermo.isotropic(1.0, 1.0)
+    a = GPKGrid(*shape, 1.0, iso, 0.0, 1.5)
+    b = GPKGrid(*shape, 1.0, iso, 0.0, 1.5)
+    b.set_geometry_kernel("tiled_exact_scores")
+    ora = oracle_mod.OracleGrid(*shape, 1.0, iso, 0.0, 1.5)
+    _load((a, b, ora), phi=phi, g=0.0, alpha=1.0)
+    for s in range(2):
+        da, db, do = a.step(), b.step(), ora.step()
+        assert da == db == do, s
+        assert not compare_all(a, b), s
+        assert not compare_all(a, ora), s
 
 
 @pytest.mark.parametrize("divisor", [2, 4])
