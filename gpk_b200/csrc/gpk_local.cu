@@ -307,23 +307,31 @@ __device__ __forceinline__ int label_slot_find(const int32_t* keys, int32_t v, i
 
 // screened sums of the resident label and NC candidates: one table lookup
 // per row of 7 taps; li[k] is the bitmap base of label k (0: resident)
-template <bool IS3D, int NC>
+template <bool IS3D, int NC, bool RES = true>
 __device__ __forceinline__ void screen_rows(const uint32_t* __restrict__ bm, const double* __restrict__ rtab,
                                             const int li[7], int lx, int ly, int lz, double& resident,
                                             double sup[6]) {
     typedef BitShape<IS3D> S;
     constexpr int R = S::R;
     const int row0 = (IS3D ? lz * S::HY : 0) + ly;  // halo row of tap (-R, -R) (2-D: (0, -R))
-#pragma unroll
-    for (int dz = (IS3D ? -R : 0); dz <= (IS3D ? R : 0); ++dz)
+    // the dz loop stays rolled (code size); the table row of (dy, dz) is
+    // rsum_index(dy^2 + dz^2), with dz^2 in {0, 1, 4, 9}
+#pragma unroll 1
+    for (int dz = (IS3D ? -R : 0); dz <= (IS3D ? R : 0); ++dz) {
+        const int az = dz < 0 ? -dz : dz;
+        // rsum_index(ay^2 + az^2) for ay = 0..3: four bits each, az's 16-bit row of
+        // 0x9876'8543'7421'6310
+        const unsigned idx4 = (unsigned)(0x9876854374216310ull >> (16 * az)) & 0xFFFFu;
 #pragma unroll
         for (int dy = -R; dy <= R; ++dy) {
             const int row = row0 + (IS3D ? (dz + R) * S::HY : 0) + dy + R;
-            const double* t = rtab + rsum_index(dy * dy + dz * dz) * 128;
-            resident += t[(bm[li[0] + row] >> lx) & 0x7Fu];
+            const int ay = dy < 0 ? -dy : dy;
+            const double* t = rtab + ((idx4 >> (4 * ay)) & 0xFu) * 128;
+            if (RES) resident += t[(bm[li[0] + row] >> lx) & 0x7Fu];
 #pragma unroll
             for (int q = 0; q < NC; ++q) sup[q] += t[(bm[li[q + 1] + row] >> lx) & 0x7Fu];
         }
+    }
 }
 
 // Distinct face-neighbour labels other than pi, in face order, kept in
@@ -372,6 +380,7 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
     __shared__ int32_t keys[S::HSLOT];
     __shared__ int8_t dense[S::HSLOT];   // bitmap index of a slot, -1 when unused
     __shared__ int s_ncell, s_nl, s_full, s_nexact;
+    __shared__ double s_wtot;  // weight of the whole box
     typedef cub::BlockScan<int, 256> BS;
     __shared__ typename BS::TempStorage scan;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -463,10 +472,17 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
             dense[base + lane] = (int8_t)(used ? total + __popc(bal & ((1u << lane) - 1u)) : -1);
             total += __popc(bal);
         }
-        if (lane == 0) s_nl = total;
+        if (lane == 0) {
+            s_nl = total;
+            double wt = 0.0;
+            for (int dz = (IS3D ? -R : 0); dz <= (IS3D ? R : 0); ++dz)
+                for (int dy = -R; dy <= R; ++dy) wt += rtab[rsum_index(dy * dy + dz * dz) * 128 + 127];
+            s_wtot = wt;
+        }
     }
     __syncthreads();
     const int nl = s_nl;
+    const double wtot = s_wtot;
     const bool screen = !s_full && nl <= (nl_cap < S::NL ? nl_cap : S::NL);
     if (screen) {
         // 4. one word per halo row and listed label (words of absent labels stay 0)
@@ -498,14 +514,21 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
             for (int q = 0; q < 6; ++q)
                 li[q + 1] = q < nc ? dense[label_slot_find(keys, cand[q], S::HSLOT)] * S::NROWP : li[0];
             double resident = 0.0, sup[6] = {0, 0, 0, 0, 0, 0};
-            const int ncw = __reduce_max_sync(__activemask(), nc);
+            screen_rows<IS3D, 0>(bm, rtab, li, lx, ly, lz, resident, sup);
+            // One candidate: it is the best, and its score is at most the
+            // weight of the box outside the resident label, wtot - resident;
+            // when that bound already puts the gain below -1e-5 (with 1e-9 to
+            // spare for the other summation order) its sum is not needed.
+            const bool bounded = nc == 1 && wtot - resident - resident < -1e-5 - 1e-9;
+            const int ncw = __reduce_max_sync(__activemask(), bounded ? 0 : nc);
             switch (ncw) {
-            case 0: screen_rows<IS3D, 0>(bm, rtab, li, lx, ly, lz, resident, sup); break;
-            case 1: screen_rows<IS3D, 1>(bm, rtab, li, lx, ly, lz, resident, sup); break;
-            case 2: screen_rows<IS3D, 2>(bm, rtab, li, lx, ly, lz, resident, sup); break;
-            case 3: screen_rows<IS3D, 3>(bm, rtab, li, lx, ly, lz, resident, sup); break;
-            default: screen_rows<IS3D, 6>(bm, rtab, li, lx, ly, lz, resident, sup); break;
+            case 0: break;
+            case 1: screen_rows<IS3D, 1, false>(bm, rtab, li, lx, ly, lz, resident, sup); break;
+            case 2: screen_rows<IS3D, 2, false>(bm, rtab, li, lx, ly, lz, resident, sup); break;
+            case 3: screen_rows<IS3D, 3, false>(bm, rtab, li, lx, ly, lz, resident, sup); break;
+            default: screen_rows<IS3D, 6, false>(bm, rtab, li, lx, ly, lz, resident, sup); break;
             }
+            if (bounded) sup[0] = wtot - resident;
             double best = -1.0, second = -1.0;
             int32_t best_label = pi;
 #pragma unroll
