@@ -731,6 +731,56 @@ def separable_measurement(n: int = 256, grains: int = 32, sigma: float = 5.0, se
     return res
 
 
+def throughput_measurement(n: int = 256, grains: int = 4096, settle: int = 16, steps: int = 4, warmup: int = 2):
+    """The FP64 step of the headline workload (n^3, `grains` Voronoi grains,
+    sigma 1.5) with the direct FP64 geometry tiles and with the separable
+    tiles (the throughput geometry: each tile label's indicator smoothed, then
+    fourth-order differences), from the same settled state.  Algorithmic
+    bytes of the geometry stage: the labels read once (4 B per cell) and, per
+    interface cell, the normals and curvature written (4 x 8 B) and the
+    competitor (4 B), i.e. 4 B per cell + 36 B per interface cell."""
+    import torch
+    from gpk_b200 import GPKGrid, thermo
+    res = {"workload": f"3-D isotropic grain growth {n}^3, {grains} Voronoi grains, sigma 1.5 cells, FP64",
+           "steps": steps, "warmup": warmup}
+    peak, peak_kind = _peaks()
+    cells = n ** 3
+    for kind in ("tiled", "separable_tiles"):
+        g = GPKGrid(n, n, n, 1.0, thermo.isotropic(1.0, 1.0), 0.0, 1.5, precision="f64")
+        g.voronoi(grains, SEED)
+        g.set("alpha", 1.0)
+        g.step_n(settle)
+        g.set_geometry_kernel(kind)
+        for _ in range(warmup):
+            g.step()
+        g.sync()
+        g.profile(True)
+        g.stage_times()
+        stream = torch.cuda.ExternalStream(g.stream_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            g.step()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        st = g.stage_times()
+        g.profile(False)
+        geo_ms = st["geometry"][0] / max(1, st["geometry"][1])
+        geo_bytes = cells * 4.0 + g.interface_fraction() * cells * 36.0
+        res[kind] = {"ms_per_step": ms, "value": cells / (ms / 1e3), "unit": "cell-updates/s",
+                     "geometry_ms_per_step": geo_ms,
+                     "stages_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in st.items() if v[1]},
+                     "geometry_roofline": {"algorithmic_bytes": geo_bytes,
+                                           "achieved": geo_bytes / (geo_ms / 1e3) / 1e9, "peak": peak,
+                                           "unit": "GB/s", "frac": geo_bytes / (geo_ms / 1e3) / 1e9 / peak,
+                                           "peak_kind": peak_kind}}
+        g.close()
+    res["geometry_speedup"] = res["tiled"]["geometry_ms_per_step"] / res["separable_tiles"]["geometry_ms_per_step"]
+    res["step_speedup"] = res["tiled"]["ms_per_step"] / res["separable_tiles"]["ms_per_step"]
+    return res
+
+
 def _summary(line):
     """A compact digest of the line's main figures, printed last so that a
     reader who keeps only the end of the output still has them."""
@@ -755,7 +805,9 @@ def _summary(line):
            "adjoint_gradients_per_s": r3(g(line, "adjoint", "gradients_per_s")),
            "spectral_ms_128": r3(g(line, "spectral", "ms_per_solve")),
            "coupled_ms_128": r3(g(line, "coupled", "ms_per_step")),
-           "near_threshold_cells": g(line, "near_threshold", "cells_last_step")}
+           "near_threshold_cells": g(line, "near_threshold", "cells_last_step"),
+           "f64_step_ms_direct": r3(g(line, "throughput_f64", "tiled", "ms_per_step")),
+           "f64_step_ms_separable_tiles": r3(g(line, "throughput_f64", "separable_tiles", "ms_per_step"))}
     st = line.get("stages_ms_per_step") or {}
     out["stages_ms"] = {k: r3(v) for k, v in st.items() if isinstance(v, (int, float)) and v > 0.01}
     return out
@@ -898,7 +950,7 @@ def run_gpu_arm(args):
             cpu = cpu_sample_from_state(grid.get("phi"), grid.get("alpha"), grid.get("g"))
         except Exception as exc:  # the GPU number stands on its own
             cpu = {"error": str(exc)}
-    spectral = batched = adjoint = coupled = alcu = separable = transport = None
+    spectral = batched = adjoint = coupled = alcu = separable = transport = throughput = None
     # the sweep shards over all ranks (same collective order on every rank)
     if not args.headline_only:
         try:
@@ -930,6 +982,10 @@ def run_gpu_arm(args):
             transport = coupled_measurement(5, 3, 256, elastic=False)
         except Exception as exc:
             transport = {"error": str(exc)}
+        try:
+            throughput = throughput_measurement()
+        except Exception as exc:
+            throughput = {"error": str(exc)}
     if rank == 0:
         line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -939,7 +995,7 @@ def run_gpu_arm(args):
                 "stages_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in stages.items()},
                 "interface_fraction": iface, "counters_last_step": list(grid.counters()),
                 "per_step_topology": waves, "near_threshold": near,
-                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "spectral": spectral, "batched": batched, "adjoint": adjoint, "coupled": coupled, "alcu": alcu, "separable": separable, "transport": transport, "init": init,
+                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches, "spectral": spectral, "batched": batched, "adjoint": adjoint, "coupled": coupled, "alcu": alcu, "separable": separable, "transport": transport, "throughput_f64": throughput, "init": init,
                 "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": io,
                         "d2h_bytes_per_step": io, "steps": e2e_steps,
                         "path": "GPKGrid drop-in semantics: upload phi/alpha/g, step, download phi/alpha/g"}}
@@ -969,6 +1025,8 @@ def main():
                     help="time only the 128^3 solidification step with a spectral solve per step")
     ap.add_argument("--separable-only", action="store_true",
                     help="time only the 256^3 sigma-5 grain-growth step (separable geometry)")
+    ap.add_argument("--throughput-only", action="store_true",
+                    help="time only the FP64 256^3 step with direct and with separable-tile geometry")
     ap.add_argument("--transport-only", action="store_true",
                     help="time only the solidification step without the elastic solve, on a --size cube")
     ap.add_argument("--sigma", type=float, default=SIGMA,
@@ -992,6 +1050,9 @@ def main():
         return 0
     if args.separable_only:
         print(json.dumps({"separable": separable_measurement()}))
+        return 0
+    if args.throughput_only:
+        print(json.dumps({"throughput_f64": throughput_measurement()}))
         return 0
     if args.transport_only:
         print(json.dumps({"transport": coupled_measurement(args.steps, args.warmup, args.size, elastic=False)}))

@@ -857,7 +857,19 @@ extern "C" int gpk_grid_set_tile_rows(gpk_grid* G, int divisor) {
 }
 
 extern "C" int gpk_grid_set_geometry_kernel(gpk_grid* G, int kind) {
-    if (!G || kind < 0 || kind > 3) return GPK_ERR_INVALID_ARGUMENT;
+    if (!G || kind < 0 || kind > 4) return GPK_ERR_INVALID_ARGUMENT;
+    if (kind == 4) {
+        // separable tiles: FP64 grids at kernel radii 4..10 (Gaussian radius 2..8)
+        if (G->precision != GPK_PREC_F64) {
+            gpk_set_error("separable tiles are an FP64 mode; FP32 grids keep the reference's arithmetic");
+            return GPK_ERR_INVALID_ARGUMENT;
+        }
+        const HostKernels<double>* hk = (const HostKernels<double>*)G->host_kernels;
+        if (hk->global_separable || hk->geom_radius < 4 || hk->geom_radius > 10) {
+            gpk_set_error("separable tiles need a kernel radius of 4..10 (sigma 0.5..2.2)");
+            return GPK_ERR_INVALID_ARGUMENT;
+        }
+    }
     G->geometry_kernel = kind;
     return GPK_OK;
 }

@@ -150,6 +150,9 @@ template <typename real> int gpk_max_dt_impl(gpk_grid* G, double* out);
 template <typename real> int gpk_phase_volume_impl(gpk_grid* G, int32_t label, double* out);
 template <typename real>
 int gpk_geometry_tiled(gpk_grid* G, int R, real inv_dx, real inv_dx2, real dx, real kappa_limit);
+// FP64 separable tiles (throughput geometry); -1 when they do not apply
+int gpk_geometry_sep_tiles(gpk_grid* G, int R, const double* gauss, int gauss_radius, double dx,
+                           double kappa_limit);
 template <typename real>
 int gpk_bgr_scores_tiled(gpk_grid* G, int radius, real* res, real* best, const unsigned long long* gate = nullptr);
 template <typename real> int gpk_projection_tiled(gpk_grid* G, int radius);

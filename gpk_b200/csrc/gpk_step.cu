@@ -1506,6 +1506,13 @@ static int geometry(gpk_grid* G) {
     if (!hk->global_separable) {
         const real inv_dx = (real)1 / dx;
         const real inv_dx2 = inv_dx * inv_dx;
+        if constexpr (sizeof(real) == 8) {
+            if (G->geometry_kernel == 4) {
+                const int rc = gpk_geometry_sep_tiles(G, hk->geom_radius, (const double*)hk->gauss_w.data(),
+                                                      hk->gauss_radius, (double)dx, (double)kappa_limit);
+                if (rc != -1) return rc;
+            }
+        }
         if (G->geometry_kernel != 1) {
             const int rc = gpk_geometry_tiled<real>(G, hk->geom_radius, inv_dx, inv_dx2, dx, kappa_limit);
             if (rc != -1) return rc;

@@ -238,7 +238,8 @@ class GPKGrid:
 
     def set_geometry_kernel(self, kind: str) -> None:
         check(lib().gpk_grid_set_geometry_kernel(
-            self._h, {"tiled": 0, "per_cell": 1, "tiled_batched": 2, "tiled_exact_scores": 3}[kind]))
+            self._h, {"tiled": 0, "per_cell": 1, "tiled_batched": 2, "tiled_exact_scores": 3,
+                      "separable_tiles": 4}[kind]))
 
     def set_external_elastic(self, on: bool = True) -> None:
         """E_el is supplied by the caller (e.g. SpectralElasticity.couple) and

@@ -251,7 +251,15 @@ int gpk_grid_wave_stats(gpk_grid* grid, uint64_t out[10]);
  * cell kernels, 2 = tiled kernels with one label per geometry bitmap batch
  * (exercises the many-label path of the tiled geometry kernel; the remap
  * scores then skip their bitmap screening), 3 = tiled kernels with every
- * remap score summed tap by tap (no screening).                           */
+ * remap score summed tap by tap (no screening) and the pair-compare
+ * projection tiles.  4 = separable tiles, FP64 grids only (the throughput
+ * geometry): the reference's separable geometry (src/gpk_geometry.cpp:
+ * 185-347: Gaussian smoothing of each label's indicator, fourth-order
+ * differences) evaluated per tile; the fields agree with the direct stencil
+ * to rounding (far below 1e-10), not bit for bit, so a label may differ
+ * where a decision lies within rounding of its threshold (see the
+ * near-threshold listing).  Kind 4 on an FP32 grid, or at a kernel radius
+ * outside 4..10, returns GPK_ERR_INVALID_ARGUMENT.                        */
 int gpk_grid_set_geometry_kernel(gpk_grid* grid, int kind);
 /* External elastic energy (no counterpart in the reference): when on, the
  * E_el field is what the caller last wrote (an upload, a device write, or
