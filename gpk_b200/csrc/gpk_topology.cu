@@ -599,8 +599,14 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
             const int gwarp = tid >> 5, nwarps = nthr >> 5;
             const int nbox = is3d ? 125 : 25, centre = is3d ? 62 : 12;
             unsigned pending = 0;
-            for (int k = gwarp; k < m; k += nwarps) {
-                if (a.cres[k] != 0) continue;
+            // warp w takes candidates w, w + nwarps, ...; its lanes read the
+            // states of 32 of them at once, then it walks the pending ones
+            for (int k0 = gwarp; k0 < m; k0 += 32 * nwarps) {
+                const int kl = k0 + lane * nwarps;
+                unsigned todo = __ballot_sync(0xffffffffu, kl < m && a.cres[kl] == 0);
+            while (todo) {
+                const int k = k0 + (__ffs(todo) - 1) * nwarps;
+                todo &= todo - 1;
                 const int4 ci = a.cinfo[k];
                 ++pending;
                 if (lane == 0) {
@@ -619,8 +625,11 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
                     int32_t lbl = -1;
                     if (e < nbox) {
                         const int lz = e / 25, ly = (e / 5) % 5, lx = e % 5;
-                        const int j = D.idx(is3d ? wrap_any(z0 + lz - 2, D.Nz) : z0, wrap_any(y0 + ly - 2, D.Ny),
-                                            wrap_any(x0 + lx - 2, D.Nx));
+                        // offsets of at most 2: one period at extents of 3 or more
+                        const int zz = !is3d ? z0 : (D.Nz >= 3 ? wrap1(z0 + lz - 2, D.Nz) : wrap_any(z0 + lz - 2, D.Nz));
+                        const int yy = D.Ny >= 3 ? wrap1(y0 + ly - 2, D.Ny) : wrap_any(y0 + ly - 2, D.Ny);
+                        const int xx = D.Nx >= 3 ? wrap1(x0 + lx - 2, D.Nx) : wrap_any(x0 + lx - 2, D.Nx);
+                        const int j = D.idx(zz, yy, xx);
                         const int c = a.cmap[j];
                         lbl = a.phi[j];
                         if (c > k) {
@@ -658,6 +667,7 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
                     }
                     a.cinfo[k].w = st;
                 }
+            }
             }
             if (lane == 0 && pending) atomicAdd(&s_pending, pending);
         }
@@ -1038,9 +1048,17 @@ __global__ void __launch_bounds__(256) k_bgr_exchange_waves(ExchArgs a, int n, i
             const int lane = threadIdx.x & 31;
             const int gwarp = tid >> 5, nwarps = nthr >> 5;
             const int nbox = is3d ? 125 : 25;
-            for (int t = gwarp; t < n; t += nwarps) {
-                const int32_t st = a.estate[t];
-                if (!(st & ES_PENDING)) continue;
+            // warp w takes exchanges w, w + nwarps, ...; its lanes read the
+            // states of 32 of them at once, then it walks the pending ones
+            for (int t0 = gwarp; t0 < n; t0 += 32 * nwarps) {
+                const int tl = t0 + lane * nwarps;
+                const int32_t stl = tl < n ? a.estate[tl] : 0;
+                unsigned todo = __ballot_sync(0xffffffffu, (stl & ES_PENDING) != 0);
+            while (todo) {
+                const int j0 = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const int t = t0 + j0 * nwarps;
+                const int32_t st = __shfl_sync(0xffffffffu, stl, j0);
                 const int4 e = a.exch[t];
                 const int A = e.x, B = e.y;
                 const int32_t low = e.z, high = e.w;
@@ -1057,8 +1075,12 @@ __global__ void __launch_bounds__(256) k_bgr_exchange_waves(ExchArgs a, int n, i
                         int32_t lbl = -1;
                         if (b < nbox) {
                             const int lz = b / 25, ly = (b / 5) % 5, lx = b % 5;
-                            const int j = D.idx(is3d ? wrap_any(z0 + lz - 2, D.Nz) : z0, wrap_any(y0 + ly - 2, D.Ny),
-                                                wrap_any(x0 + lx - 2, D.Nx));
+                            // offsets of at most 2: one period at extents of 3 or more
+                            const int zz = !is3d ? z0
+                                                 : (D.Nz >= 3 ? wrap1(z0 + lz - 2, D.Nz) : wrap_any(z0 + lz - 2, D.Nz));
+                            const int yy = D.Ny >= 3 ? wrap1(y0 + ly - 2, D.Ny) : wrap_any(y0 + ly - 2, D.Ny);
+                            const int xx = D.Nx >= 3 ? wrap1(x0 + lx - 2, D.Nx) : wrap_any(x0 + lx - 2, D.Nx);
+                            const int j = D.idx(zz, yy, xx);
                             const int pq = a.pmap[j];
                             if (pq >= 0 && pq < t) {
                                 const int4 o = a.exch[pq];
@@ -1090,6 +1112,7 @@ __global__ void __launch_bounds__(256) k_bgr_exchange_waves(ExchArgs a, int n, i
                     }
                     a.estate[t] = st | ES_READY | (acc ? ES_ACCEPT : 0);
                 }
+            }
             }
         }
         if (!grid_barrier(a.s, nblocks)) return;
