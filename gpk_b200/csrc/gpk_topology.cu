@@ -617,53 +617,70 @@ __global__ void __launch_bounds__(256) k_crossing_sweep(CrossArgs a, int m, int 
                 }
                 int z0, y0, x0;
                 D.decode(ci.x, z0, y0, x0);
-                bool conflict = false;
-                uint32_t wo[4] = {0u, 0u, 0u, 0u}, wn[4] = {0u, 0u, 0u, 0u};
+                // the box in three rounds of loads: cell indices, then labels
+                // and candidate slots, then the candidates' states
+                int jq[4], cq4[4];
+                int32_t lq[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     const int e = q * 32 + lane;
-                    int32_t lbl = -1;
-                    if (e < nbox) {
+                    jq[q] = -1;
+                    if (e < nbox && (q == 0 || nbox > 32)) {
                         const int lz = e / 25, ly = (e / 5) % 5, lx = e % 5;
                         // offsets of at most 2: one period at extents of 3 or more
                         const int zz = !is3d ? z0 : (D.Nz >= 3 ? wrap1(z0 + lz - 2, D.Nz) : wrap_any(z0 + lz - 2, D.Nz));
                         const int yy = D.Ny >= 3 ? wrap1(y0 + ly - 2, D.Ny) : wrap_any(y0 + ly - 2, D.Ny);
                         const int xx = D.Nx >= 3 ? wrap1(x0 + lx - 2, D.Nx) : wrap_any(x0 + lx - 2, D.Nx);
-                        const int j = D.idx(zz, yy, xx);
-                        const int c = a.cmap[j];
-                        lbl = a.phi[j];
-                        if (c > k) {
-                            if (a.cres[c] == 2) lbl = a.cinfo[c].y;  // accepted later: the old label
-                        } else if (c >= 0 && c < k && e != centre && a.cres[c] == 0) {
-                            const int4 cq = a.cinfo[c];
-                            conflict |= cq.y == ci.y || cq.y == ci.z || cq.z == ci.y || cq.z == ci.z;
-                        }
+                        jq[q] = D.idx(zz, yy, xx);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    cq4[q] = jq[q] >= 0 ? a.cmap[jq[q]] : -1;
+                    lq[q] = jq[q] >= 0 ? a.phi[jq[q]] : -1;
+                }
+                bool conflict = false;
+                uint32_t wo[4] = {0u, 0u, 0u, 0u}, wn[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int e = q * 32 + lane;
+                    const int c = cq4[q];
+                    int32_t lbl = lq[q];
+                    if (c > k) {
+                        if (a.cres[c] == 2) lbl = a.cinfo[c].y;  // accepted later: the old label
+                    } else if (c >= 0 && c < k && e != centre && a.cres[c] == 0) {
+                        const int4 cq = a.cinfo[c];
+                        conflict |= cq.y == ci.y || cq.y == ci.z || cq.z == ci.y || cq.z == ci.z;
                     }
                     wo[q] = __ballot_sync(0xffffffffu, lbl == ci.y);
                     wn[q] = __ballot_sync(0xffffffffu, lbl == ci.z);
                     if (nbox <= 32) break;
                 }
                 const bool local = !__any_sync(0xffffffffu, conflict);
+                // lane 0 takes the old label's topology, lane 1 the new one's
+                // (the same code on two masks runs side by side)
+                int part = 0;
+                if (local && lane < 2) {
+                    const uint32_t* wv = lane == 0 ? wo : wn;
+                    const u128 occ = (u128)wv[0] | ((u128)wv[1] << 32) | ((u128)wv[2] << 64) | ((u128)wv[3] << 96);
+                    const int tv = topological_number_mask(occ, is3d);
+                    part = min(tv, 2);
+                    if (tv > 1) part |= bounded_branches_connected_mask(occ, is3d, lane == 0) ? 4 : 8;
+                }
+                const int part_n = __shfl_sync(0xffffffffu, part, 1);
                 if (lane == 0) {
                     int st = 0;
                     if (local) {
-                        const u128 occ_o = (u128)wo[0] | ((u128)wo[1] << 32) | ((u128)wo[2] << 64) | ((u128)wo[3] << 96);
-                        const u128 occ_n = (u128)wn[0] | ((u128)wn[1] << 32) | ((u128)wn[2] << 64) | ((u128)wn[3] << 96);
-                        const int to = topological_number_mask(occ_o, is3d);
-                        const int tn = topological_number_mask(occ_n, is3d);
-                        st = CS_LOCAL | (min(to, 2) << CS_TO_SHIFT) | (min(tn, 2) << CS_TN_SHIFT);
+                        const int to = part & 3, tn = part_n & 3;
+                        st = CS_LOCAL | (to << CS_TO_SHIFT) | (tn << CS_TN_SHIFT);
                         if (to == 0) {
                             // at k's serial time the label holds at least count0 - (its other candidates) cells
                             if (a.count0[ci.y] - (a.n_old[ci.y] - 1) >= 2) st |= CS_CNT_REJECT;
                             else st |= CS_GC;
                         } else if (to > 1) {
-                            if (bounded_branches_connected_mask(occ_o, is3d, true)) st |= CS_OLD_LOCAL;
-                            else st |= CS_GO;
+                            st |= (part & 4) ? CS_OLD_LOCAL : CS_GO;
                         }
-                        if (tn > 1) {
-                            if (bounded_branches_connected_mask(occ_n, is3d, false)) st |= CS_NEW_LOCAL;
-                            else st |= CS_GN;
-                        }
+                        if (tn > 1) st |= (part_n & 4) ? CS_NEW_LOCAL : CS_GN;
                     }
                     a.cinfo[k].w = st;
                 }
