@@ -62,6 +62,24 @@ struct SerialView {
         bool r;
         return get(j, r);
     }
+    // the first n of six cells at once: each round of loads is issued together
+    __device__ __forceinline__ void get6(const int j[6], int n, int32_t out[6], bool rev[6]) const {
+        int c[6];
+        int32_t p[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            c[q] = q < n ? cmap[j[q]] : -1;
+            p[q] = q < n ? phi[j[q]] : -1;
+        }
+        int8_t r[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) r[q] = c[q] > k ? cres[c[q]] : (int8_t)0;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            rev[q] = r[q] == 2;
+            out[q] = rev[q] ? cinfo[c[q]].y : p[q];
+        }
+    }
 };
 
 // ---------------------------------------------------------------------------
@@ -498,19 +516,30 @@ __device__ bool warp_branches_connected_ms(const Dims& D, const Lab& lab, int ce
             sid = qsid[head + lane];
             int nx[6];
             D.faces(cur, nx);
-            for (int k = 0; k < nf; ++k) {
+            // the six neighbours' labels, then their stamps, each round of
+            // loads issued together; the claims follow in face order
+            int32_t lv[6];
+            bool rv[6];
+            lab.get6(nx, nf, lv, rv);
+            bool want[6];
+            uint32_t sv[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                want[k] = k < nf && !(exclude_centre && nx[k] == cell) && lv[k] == label;
+                sv[k] = want[k] ? (rv[k] ? stamp_rev[nx[k]] : stamp[nx[k]]) : 0u;
+            }
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                if (!want[k]) continue;
                 const int next = nx[k];
-                if (exclude_centre && next == cell) continue;
-                bool rev;
-                if (lab.get(next, rev) != label) continue;
-                uint32_t* mark = rev ? &stamp_rev[next] : &stamp[next];
-                const uint32_t seen = *mark - my_stamp;
+                const uint32_t seen = sv[k] - my_stamp;
                 if (seen < 8u) {  // already claimed by a search of this test
                     if ((int)seen != sid) unions |= 1ull << (6 * sid + (int)seen);
                     continue;
                 }
+                uint32_t* mark = rv[k] ? &stamp_rev[next] : &stamp[next];
                 const uint32_t old = atomicExch(mark, my_stamp + (uint32_t)sid) - my_stamp;
-                if (old < 8u) {  // another lane claimed it first
+                if (old < 8u) {  // another lane (or an earlier face of this one) claimed it first
                     if ((int)old != sid) unions |= 1ull << (6 * sid + (int)old);
                     continue;
                 }
