@@ -1052,7 +1052,7 @@ def main():
         print(json.dumps({"separable": separable_measurement()}))
         return 0
     if args.throughput_only:
-        print(json.dumps({"throughput_f64": throughput_measurement()}))
+        print(json.dumps({"throughput_f64": throughput_measurement(args.size, args.grains)}))
         return 0
     if args.transport_only:
         print(json.dumps({"transport": coupled_measurement(args.steps, args.warmup, args.size, elastic=False)}))

@@ -794,7 +794,9 @@ extern "C" int gpk_grid_wave_stats(gpk_grid* G, uint64_t out[10]) {
     out[7] = G->h_scal->count_scanned;
     out[8] = G->h_scal->score_cells;
     out[9] = G->h_scal->score_exact;
-    GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->flood_tasks, 0, 6 * sizeof(unsigned long long), G->stream));
+    out[1] += G->h_scal->remap_waves_sum;  // remap passes ordered on the device
+    out[3] += G->h_scal->remap_props_sum;
+    GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->flood_tasks, 0, 8 * sizeof(unsigned long long), G->stream));
     return GPK_OK;
 }
 

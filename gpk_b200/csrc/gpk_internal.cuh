@@ -94,6 +94,8 @@ struct StepScalars {
     unsigned long long flood_tasks, flood_cells, count_tasks, count_scanned;
     // remap scores: interface cells scored, and those summed tap by tap
     unsigned long long score_cells, score_exact;
+    // remap passes ordered on the device: their exchange waves and proposals
+    unsigned long long remap_waves_sum, remap_props_sum;
 };
 
 // bounded grid-wide barrier for persistent kernels launched cooperatively.

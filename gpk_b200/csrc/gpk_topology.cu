@@ -1391,12 +1391,16 @@ __global__ void __launch_bounds__(1024) k_sort_proposals(const unsigned* __restr
 // first pass (gated on accepted crossings) exchanged cells; the two passes'
 // exchanges are summed into the step's counter afterwards.
 __global__ void k_remap_second_gate(StepScalars* s) {
+    s->remap_waves_sum += s->waves;
+    s->remap_props_sum += s->n_prop;
     s->exch_first = s->exch_pass;
     s->gate2 = (s->accepted > 0 && s->exch_pass > 0) ? 1ull : 0ull;
     s->exch_pass = 0;
     s->waves = 0;
 }
 __global__ void k_remap_total(StepScalars* s, int is3d) {
+    s->remap_waves_sum += s->waves;  // the last pass (a skipped pass left 0 in both)
+    s->remap_props_sum += s->n_prop;
     if (is3d) s->exchanges = s->exch_first + (s->gate2 ? s->exch_pass : 0ull);
     else s->exchanges = s->exch_pass;
 }
