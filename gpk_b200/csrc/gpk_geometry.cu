@@ -674,6 +674,7 @@ __global__ void __launch_bounds__(256) k_geometry_sep_tiles(SepArgs a) {
     uint16_t* cli = reinterpret_cast<uint16_t*>(cells + S::NCELL);
     int32_t* cand = reinterpret_cast<int32_t*>(bm);  // label candidates, before the first bitmap
     __shared__ int s_count, s_ncand, s_nl;
+    __shared__ int sbox[6 * P::NLB];  // per label of the batch: min x, y, z, max x, y, z of its cells
     typedef cub::BlockScan<int, 256> BS;
     __shared__ typename BS::TempStorage scan;
     constexpr int PER = (S::NCELL + 255) / 256;
@@ -772,9 +773,28 @@ __global__ void __launch_bounds__(256) k_geometry_sep_tiles(SepArgs a) {
                 if (lane == 0) bm[L * S::NROWP + r] = bits;
             }
         }
+        // each label's interface cells span a box of the tile; its smoothed
+        // values are needed there plus two cells each side (the differences)
+        if (tid < 6 * P::NLB) sbox[tid] = (tid % 6) < 3 ? 1 << 20 : -1;
+        __syncthreads();
+        for (int k = tid; k < ncell; k += 256) {
+            const int L = (int)cli[k] - lb0;
+            if (L < 0 || L >= nb) continue;
+            const int c = cells[k];
+            atomicMin(&sbox[6 * L + 0], c % S::TX);
+            atomicMin(&sbox[6 * L + 1], (c / S::TX) % S::TY);
+            atomicMin(&sbox[6 * L + 2], c / (S::TX * S::TY));
+            atomicMax(&sbox[6 * L + 3], c % S::TX);
+            atomicMax(&sbox[6 * L + 4], (c / S::TX) % S::TY);
+            atomicMax(&sbox[6 * L + 5], c / (S::TX * S::TY));
+        }
         for (int L = 0; L < nb; ++L) {
-            __syncthreads();  // bitmaps written / the previous label's S read
+            __syncthreads();  // bitmaps and boxes written / the previous label's S read
             const uint32_t* bml = bm + L * S::NROWP;
+            // the label's box in smoothed-value coordinates: x in [bx, bx + nsx)
+            const int bx = sbox[6 * L + 0], by = sbox[6 * L + 1], bz = IS3D ? sbox[6 * L + 2] : 0;
+            const int nsx = sbox[6 * L + 3] - bx + 5, nsy = sbox[6 * L + 4] - by + 5;
+            const int nhz = IS3D ? sbox[6 * L + 5] - bz + 5 + 2 * P::K : 1;
             // smoothed x value of the window starting at bit xs of halo row `row`
             auto xval = [&](int row, int xs) -> double {
                 const uint32_t w = bml[row] >> xs;
@@ -786,8 +806,10 @@ __global__ void __launch_bounds__(256) k_geometry_sep_tiles(SepArgs a) {
             if (IS3D) {
                 // a strip (x, halo plane): its x values down all halo rows, then
                 // the y sums of the tile's rows plus two each side
-                for (int st = tid; st < P::SX * S::HZ; st += 256) {
-                    const int xs = st % P::SX, hz = st / P::SX;
+                // (the strips and columns outside the label's box are skipped;
+                // their stale values are never read)
+                for (int st = tid; st < nsx * nhz; st += 256) {
+                    const int xs = bx + st % nsx, hz = bz + st / nsx;
                     double X[S::HY];
 #pragma unroll
                     for (int r = 0; r < S::HY; ++r) X[r] = xval(hz * S::HY + r, xs);
@@ -795,13 +817,14 @@ __global__ void __launch_bounds__(256) k_geometry_sep_tiles(SepArgs a) {
                     for (int ys = 0; ys < P::SY; ++ys) {
                         double acc = 0.0;
 #pragma unroll
-                        for (int j = 0; j < P::NT; ++j) acc += a.g[j] * X[ys + j];
+                        for (int j = 0; j < P::NT; ++j) acc = __fma_rn(a.g[j], X[ys + j], acc);
                         Ym[(hz * P::SY + ys) * P::SX + xs] = acc;
                     }
                 }
                 __syncthreads();
                 // a column (x, y): the z sums from its y-smoothed planes
-                for (int col = tid; col < P::SX * P::SY; col += 256) {
+                for (int cc = tid; cc < nsx * nsy; cc += 256) {
+                    const int col = (by + cc / nsx) * P::SX + bx + cc % nsx;
                     double Y[S::HZ];
 #pragma unroll
                     for (int hz = 0; hz < S::HZ; ++hz) Y[hz] = Ym[hz * P::SX * P::SY + col];
@@ -809,16 +832,16 @@ __global__ void __launch_bounds__(256) k_geometry_sep_tiles(SepArgs a) {
                     for (int zs = 0; zs < P::SZ; ++zs) {
                         double acc = 0.0;
 #pragma unroll
-                        for (int j = 0; j < P::NT; ++j) acc += a.g[j] * Y[zs + j];
+                        for (int j = 0; j < P::NT; ++j) acc = __fma_rn(a.g[j], Y[zs + j], acc);
                         Sm[zs * P::SX * P::SY + col] = acc;
                     }
                 }
             } else {
-                for (int pt = tid; pt < P::SX * P::SY; pt += 256) {
-                    const int xs = pt % P::SX, ys = pt / P::SX;
+                for (int pt = tid; pt < nsx * nsy; pt += 256) {
+                    const int xs = bx + pt % nsx, ys = by + pt / nsx;
                     double acc = 0.0;
 #pragma unroll
-                    for (int j = 0; j < P::NT; ++j) acc += a.g[j] * xval(ys + j, xs);
+                    for (int j = 0; j < P::NT; ++j) acc = __fma_rn(a.g[j], xval(ys + j, xs), acc);
                     Sm[ys * P::SX + xs] = acc;
                 }
             }
