@@ -1542,8 +1542,12 @@ int gpk_remap_pass(gpk_grid* G) {
     k_bgr_primary_keys<real><<<(n + B - 1) / B, B, 0, G->stream>>>(n, G->val_b, G->phi, G->phi_comp, G->key_b);
     G->launches++;
     bytes = G->cub_tmp_bytes;
+    // the keys' set bits lie in [10, 37 + bits of the largest label): sorting
+    // those bits alone gives the same order with fewer digit passes
+    int lbits = 1;
+    while (lbits < 27 && (1LL << lbits) < (long long)G->label_cap) ++lbits;
     GPK_CUDA_TRY(cub::DeviceRadixSort::SortPairs(G->cub_tmp, bytes, (const unsigned long long*)G->key_b, G->key_a,
-                                                 (const int32_t*)G->val_b, G->val_a, n, 0, 64, G->stream));
+                                                 (const int32_t*)G->val_b, G->val_a, n, 10, 37 + lbits, G->stream));
     k_bgr_match<<<(n + B - 1) / B, B, 0, G->stream>>>(n, G->key_a, G->val_a, (int4*)G->exch, G->val_b, G->pmap);
     G->launches++;
     GPK_CUDA_TRY(cudaGetLastError());
