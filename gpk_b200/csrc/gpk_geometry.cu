@@ -529,20 +529,31 @@ __global__ void __launch_bounds__(256, sizeof(real) == 4 ? 3 : 2) k_geometry_til
         const int nb = nl - lb0 < nlb ? nl - lb0 : nlb;
         __syncthreads();  // bitmaps, candidates and batch cells of the previous pass are free
 
-        // 3. one word per halo row and label of the batch
-        for (int r = warp; r < S::NROW; r += 8) {
-            const int hz = r / S::HY, hy = r % S::HY;
-            const int x = wrap_any(x0 - R + lane, D.Nx), y = wrap_any(y0 + hy - R, D.Ny);
-            const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
-            const int32_t g = a.phi[D.idx(z, y, x)];
-            for (int L0 = 0; L0 < nb; L0 += 32) {
-                const int cnt = nb - L0 < 32 ? nb - L0 : 32;
-                uint32_t mine = 0;
-                for (int L = 0; L < cnt; ++L) {
-                    const uint32_t bits = __ballot_sync(0xffffffffu, g == dl[lb0 + L0 + L]);
-                    if (lane == L) mine = bits;
+        // 3. one word per halo row and label of the batch; a warp takes two
+        //    rows at a time, their label loads issued together
+        for (int r0 = warp; r0 < S::NROW; r0 += 16) {
+            int32_t gv[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int r = r0 + 8 * u;
+                const int hz = r / S::HY, hy = r % S::HY;
+                const int x = wrap_any(x0 - R + lane, D.Nx), y = wrap_any(y0 + hy - R, D.Ny);
+                const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
+                gv[u] = r < S::NROW ? a.phi[D.idx(z, y, x)] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int r = r0 + 8 * u;
+                if (r >= S::NROW) break;
+                for (int L0 = 0; L0 < nb; L0 += 32) {
+                    const int cnt = nb - L0 < 32 ? nb - L0 : 32;
+                    uint32_t mine = 0;
+                    for (int L = 0; L < cnt; ++L) {
+                        const uint32_t bits = __ballot_sync(0xffffffffu, gv[u] == dl[lb0 + L0 + L]);
+                        if (lane == L) mine = bits;
+                    }
+                    if (lane < cnt) bm[(L0 + lane) * S::NROWP + r] = mine;
                 }
-                if (lane < cnt) bm[(L0 + lane) * S::NROWP + r] = mine;
             }
         }
         // cells of the batch, grouped by label (flat order within a label), so
