@@ -27,6 +27,15 @@ def _same(a, b, fields=PUBLIC_FIELDS):
     assert a.time == b.time
 
 
+def _same_remap_stats(a, b):
+    """Remap statistics: the captured passes sum theirs on the device, the
+    ordinary ones on the host; a captured pass without proposals still runs
+    (and counts) one empty exchange wave."""
+    sa, sb = a.wave_stats(), b.wave_stats()
+    assert sa["remap_proposals"] == sb["remap_proposals"]
+    assert sb["remap_waves"] >= sa["remap_waves"]
+
+
 @pytest.mark.parametrize("precision", ["f64", "f32"])
 @pytest.mark.parametrize("seed", [5003, 5011])
 def test_graph_step_equals_ordinary_steps_lamellar(seed, precision):
@@ -39,6 +48,7 @@ def test_graph_step_equals_ordinary_steps_lamellar(seed, precision):
     a.step_n(7)
     b.step_graph(7)           # the captured graph again, and an odd step
     _same(a, b)
+    _same_remap_stats(a, b)
 
 
 def test_graph_step_equals_ordinary_steps_3d_solidification():
@@ -58,6 +68,7 @@ def test_graph_step_equals_ordinary_steps_3d_solidification():
     a.step_n(25)
     b.step_graph(25)
     _same(a, b)
+    _same_remap_stats(a, b)
     assert a.counters()[0] > 0 or a.get("phi").sum() > 515   # the nucleus grew through crossings
 
 
