@@ -44,8 +44,8 @@ CPU_GRAINS = 512
 # DRAM read + write bytes of one k_geometry_tiled launch on the 256^3 / 4096
 # grain / sigma 1.5 workload, measured by ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum, one-pass metrics, the launch of the third warm-up step)
-GEOMETRY_TRAFFIC_256 = 530.12e6
-GEOMETRY_TRAFFIC_NOTE = ("DRAM bytes (read 303.10 MB + write 227.02 MB) of one launch of the kernel on this "
+GEOMETRY_TRAFFIC_256 = 527.80e6
+GEOMETRY_TRAFFIC_NOTE = ("DRAM bytes (read 300.98 MB + write 226.82 MB) of one launch of the kernel on this "
                          "256^3 workload, measured by ncu with the one-pass dram__bytes metrics")
 
 
