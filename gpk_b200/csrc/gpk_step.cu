@@ -1376,7 +1376,7 @@ __global__ void k_reset_step(StepScalars* s) {
 using namespace gpk_dev;
 
 template <typename real> int gpk_crossings(gpk_grid* G, int m);
-template <typename real> int gpk_remap_pass(gpk_grid* G);
+template <typename real> int gpk_remap_pass(gpk_grid* G, const unsigned long long* gate = nullptr);
 template <typename real> int gpk_extinction(gpk_grid* G);
 
 static inline int grid_for(gpk_grid* G, long long n, int block = 256) {
@@ -1794,24 +1794,37 @@ int gpk_step_impl(gpk_grid* G, double dt_req, double dt_cap) {
         GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->waves, 0, sizeof(unsigned), G->stream));
         GPK_TRY(gpk_remap_pass<real>(G));
         GPK_TRY(gpk_interface_mask<real>(G));
-        GPK_TRY(gpk_sync_scalars(G));
-        G->wave_stats[1] += G->h_scal->waves;
-        G->wave_stats[3] += G->h_scal->n_prop;
-        const unsigned long long first = G->h_scal->exch_pass;
-        unsigned long long total = first;
-        if (D.is3d() && first > 0) {
-            GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->exch_pass, 0, sizeof(unsigned long long), G->stream));
-            GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->waves, 0, sizeof(unsigned), G->stream));
-            GPK_TRY(gpk_remap_pass<real>(G));
-            GPK_TRY(gpk_interface_mask<real>(G));
+        const bool tiled_scores = G->geometry_kernel != 1 && hk->remap_radius == 3;
+        if (D.is3d() && tiled_scores) {
+            // the second pass under the device-side gate of the first pass's
+            // exchanges (no host round trip between the passes); the pass
+            // statistics and the exchange total are formed on the device
+            GPK_TRY(gpk_remap_gates(G, 0));
+            GPK_TRY(gpk_remap_pass<real>(G, &G->scal->gate2));
+            GPK_TRY(gpk_interface_mask<real>(G, &G->scal->gate2));
+            GPK_TRY(gpk_remap_gates(G, 1));
+        } else if (!D.is3d()) {
+            GPK_TRY(gpk_remap_gates(G, 1));
+        } else {
             GPK_TRY(gpk_sync_scalars(G));
-            total += G->h_scal->exch_pass;
             G->wave_stats[1] += G->h_scal->waves;
             G->wave_stats[3] += G->h_scal->n_prop;
+            const unsigned long long first = G->h_scal->exch_pass;
+            unsigned long long total = first;
+            if (first > 0) {
+                GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->exch_pass, 0, sizeof(unsigned long long), G->stream));
+                GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->waves, 0, sizeof(unsigned), G->stream));
+                GPK_TRY(gpk_remap_pass<real>(G));
+                GPK_TRY(gpk_interface_mask<real>(G));
+                GPK_TRY(gpk_sync_scalars(G));
+                total += G->h_scal->exch_pass;
+                G->wave_stats[1] += G->h_scal->waves;
+                G->wave_stats[3] += G->h_scal->n_prop;
+            }
+            G->h_scal->exchanges = total;
+            GPK_CUDA_TRY(cudaMemcpyAsync(&G->scal->exchanges, &G->h_scal->exchanges, sizeof(unsigned long long),
+                                         cudaMemcpyHostToDevice, G->stream));
         }
-        G->h_scal->exchanges = total;
-        GPK_CUDA_TRY(cudaMemcpyAsync(&G->scal->exchanges, &G->h_scal->exchanges, sizeof(unsigned long long),
-                                     cudaMemcpyHostToDevice, G->stream));
         GPK_TRY(gpk_stage_end(G, GPK_STAGE_REMAP));
     }
     if (th.grain_network && (G->step_id & 7ULL) == 0ULL) {

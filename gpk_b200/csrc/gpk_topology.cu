@@ -1497,26 +1497,35 @@ int gpk_crossings(gpk_grid* G, int m) {
 // One balanced-remap pass.  Precondition: the interface mask and the active
 // list have just been rebuilt from the current labels.
 template <typename real>
-int gpk_remap_pass(gpk_grid* G) {
+int gpk_remap_pass(gpk_grid* G, const unsigned long long* gate) {
     const Dims D = G->d;
     HostKernels<real>* hk = (HostKernels<real>*)G->host_kernels;
     const int B = 256;
     const int grid = 4 * G->num_sms;
-    // phi_comp <- phi everywhere, then the best candidate at interface cells
-    GPK_CUDA_TRY(cudaMemcpyAsync(G->phi_comp, G->phi, sizeof(int32_t) * D.N, cudaMemcpyDeviceToDevice, G->stream));
+    // phi_comp <- phi everywhere, then the best candidate at interface cells;
+    // under a device-side gate (the second 3-D pass) every kernel up to the
+    // proposals checks it, and a closed gate leaves no proposal
+    if (gate) {
+        k_copy_i32_gated<<<grid, B, 0, G->stream>>>(D.N, G->phi, G->phi_comp, gate);
+        G->launches++;
+    } else {
+        GPK_CUDA_TRY(cudaMemcpyAsync(G->phi_comp, G->phi, sizeof(int32_t) * D.N, cudaMemcpyDeviceToDevice, G->stream));
+    }
     const int rc = G->geometry_kernel != 1
-                       ? gpk_bgr_scores_tiled<real>(G, hk->remap_radius, (real*)G->bgr_res, (real*)G->bgr_best)
+                       ? gpk_bgr_scores_tiled<real>(G, hk->remap_radius, (real*)G->bgr_res, (real*)G->bgr_best, gate)
                        : -1;
-    if (rc == -1)
+    if (rc == -1) {
+        if (gate) return GPK_ERR_INTERNAL;  // callers gate only where a tiled score kernel exists
         k_bgr_scores<real><<<grid, B, 0, G->stream>>>(D, G->active, &G->scal->n_active, G->phi, G->phi_comp,
                                                       (real*)G->bgr_res, (real*)G->bgr_best, G->d_remap_w,
                                                       hk->remap_radius);
-    else if (rc != GPK_OK)
+    } else if (rc != GPK_OK) {
         return rc;
+    }
     GPK_CUDA_TRY(cudaMemsetAsync(&G->scal->n_prop, 0, sizeof(unsigned), G->stream));
     k_bgr_proposals<real><<<grid, B, 0, G->stream>>>(G->active, &G->scal->n_active, G->phi, G->phi_comp,
                                                      (const real*)G->bgr_res, (const real*)G->bgr_best, G->key_b,
-                                                     G->val_b, G->scal);
+                                                     G->val_b, G->scal, gate);
     G->launches += 2;
     GPK_CUDA_TRY(cudaGetLastError());
     GPK_TRY(gpk_sync_scalars(G));
@@ -1676,8 +1685,8 @@ int gpk_remap_pass_graph(gpk_grid* G, const unsigned long long* gate) {
     return launch_coop(G, kern, coop_grid(G, kern, 256, (int)std::min<long long>(want, 1LL << 30)), 256, args);
 }
 
-template int gpk_remap_pass<float>(gpk_grid*);
-template int gpk_remap_pass<double>(gpk_grid*);
+template int gpk_remap_pass<float>(gpk_grid*, const unsigned long long*);
+template int gpk_remap_pass<double>(gpk_grid*, const unsigned long long*);
 template int gpk_remap_pass_graph<float>(gpk_grid*, const unsigned long long*);
 template int gpk_remap_pass_graph<double>(gpk_grid*, const unsigned long long*);
 
