@@ -774,14 +774,26 @@ __global__ void __launch_bounds__(256) k_geometry_sep_tiles(SepArgs a) {
     for (int lb0 = 0; lb0 < nl; lb0 += P::NLB) {
         const int nb = nl - lb0 < P::NLB ? nl - lb0 : P::NLB;
         __syncthreads();  // the previous batch's bitmaps and smoothed values are free
-        for (int r = warp; r < S::NROW; r += 8) {
-            const int hz = r / S::HY, hy = r % S::HY;
-            const int x = wrap_any(x0 - R + lane, D.Nx), y = wrap_any(y0 + hy - R, D.Ny);
-            const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
-            const int32_t gl = a.phi[D.idx(z, y, x)];
-            for (int L = 0; L < nb; ++L) {
-                const uint32_t bits = __ballot_sync(0xffffffffu, gl == dl[lb0 + L]);
-                if (lane == 0) bm[L * S::NROWP + r] = bits;
+        // a warp takes four halo rows at a time, their label loads issued together
+        const int xw = wrap_any(x0 - R + lane, D.Nx);
+        for (int r0 = warp; r0 < S::NROW; r0 += 32) {
+            int32_t gv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int r = r0 + 8 * u;
+                const int hz = r / S::HY, hy = r % S::HY;
+                const int y = wrap_any(y0 + hy - R, D.Ny);
+                const int z = IS3D ? wrap_any(z0 + hz - R, D.Nz) : 0;
+                gv[u] = r < S::NROW ? a.phi[D.idx(z, y, xw)] : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int r = r0 + 8 * u;
+                if (r >= S::NROW) break;
+                for (int L = 0; L < nb; ++L) {
+                    const uint32_t bits = __ballot_sync(0xffffffffu, gv[u] == dl[lb0 + L]);
+                    if (lane == 0) bm[L * S::NROWP + r] = bits;
+                }
             }
         }
         // each label's interface cells span a box of the tile; its smoothed
