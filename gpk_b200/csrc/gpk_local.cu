@@ -8,9 +8,11 @@
 // label condition.  One CTA stages its tile's labels (and, for the
 // projection, each cell's label pair and signed velocity) with an R-cell
 // periodic halo in shared memory and walks the tile's interface cells.  The
-// conditional additions are written as fma(w, m, acc) with m in {0, 1}; a sum
-// that starts at +0 is never -0 in round-to-nearest, so adding a signed zero
-// changes nothing and the result is bit-identical to `if (cond) acc += w`.
+// pair-compare and tap-by-tap kernels write the conditional additions as
+// fma(w, m, acc) with m in {0, 1}; the bitmap kernels add only the taps whose
+// bit is set.  A sum that starts at +0 is never -0 in round-to-nearest, so
+// adding a signed zero changes nothing and both forms are bit-identical to
+// `if (cond) acc += w`.
 #include <cuda_runtime.h>
 
 #include <cub/cub.cuh>
