@@ -256,6 +256,21 @@ int gpk_build_tables(gpk_grid* G) {
     GPK_CUDA_TRY(cudaMemcpy(G->d_gauss, hk->gauss_w.data(), sizeof(real) * hk->gauss_w.size(), cudaMemcpyHostToDevice));
     GPK_TRY(gpk_alloc(G, (void**)&G->d_proj_w, sizeof(double) * hk->proj_w.size()));
     GPK_CUDA_TRY(cudaMemcpy(G->d_proj_w, hk->proj_w.data(), sizeof(double) * hk->proj_w.size(), cudaMemcpyHostToDevice));
+    if (hk->remap_radius == 3) {
+        // rows of the remap screening table, summed as the screening kernel
+        // reads them: bit j of a pattern is tap x-offset j - 3, ascending
+        const int r2s[10] = {0, 1, 2, 4, 5, 8, 9, 10, 13, 18};
+        std::vector<double> rt(10 * 128);
+        for (int k = 0; k < 10; ++k)
+            for (int p = 0; p < 128; ++p) {
+                double sum = 0.0;
+                for (int j = 0; j < 7; ++j)
+                    if (p & (1 << j)) sum += hk->remap_w[r2s[k] + (j - 3) * (j - 3)];
+                rt[k * 128 + p] = sum;
+            }
+        GPK_TRY(gpk_alloc(G, (void**)&G->d_remap_rtab, sizeof(double) * rt.size()));
+        GPK_CUDA_TRY(cudaMemcpy(G->d_remap_rtab, rt.data(), sizeof(double) * rt.size(), cudaMemcpyHostToDevice));
+    }
     GPK_TRY(gpk_alloc(G, (void**)&G->d_remap_w, sizeof(double) * hk->remap_w.size()));
     GPK_CUDA_TRY(cudaMemcpy(G->d_remap_w, hk->remap_w.data(), sizeof(double) * hk->remap_w.size(),
                             cudaMemcpyHostToDevice));

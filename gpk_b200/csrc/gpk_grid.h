@@ -96,6 +96,9 @@ struct gpk_grid {
     // tables
     void* d_geom_table = nullptr; void* d_w0 = nullptr; void* d_w1 = nullptr; void* d_w2 = nullptr;
     void* d_gauss = nullptr; double* d_proj_w = nullptr; double* d_remap_w = nullptr;
+    // remap screening: weight sums of the 128 patterns of a 7-tap row, for the
+    // ten distinct dy^2 + dz^2 of a 7 x 7 row block (radius 3 only)
+    double* d_remap_rtab = nullptr;
     gpk_dev::StepScalars* scal = nullptr;  // device scalars
     gpk_dev::StepScalars* h_scal = nullptr;  // pinned host mirror
     void* host_kernels = nullptr;          // HostKernels<real>*

@@ -365,7 +365,8 @@ __device__ __forceinline__ int face_candidates(const int32_t* __restrict__ lab, 
 template <typename real, bool IS3D>
 __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t* __restrict__ phi,
                                                            const uint8_t* __restrict__ mask, int ntx, int nty,
-                                                           const double* __restrict__ wtab, int nl_cap,
+                                                           const double* __restrict__ wtab,
+                                                           const double* __restrict__ rtab_g, int nl_cap,
                                                            int32_t* __restrict__ phi_comp, real* __restrict__ res_out,
                                                            real* __restrict__ best_out,
                                                            const unsigned long long* __restrict__ gate,
@@ -436,13 +437,7 @@ __global__ void __launch_bounds__(256) k_bgr_scores_screen(Dims D, const int32_t
     }
     for (int e = tid; e <= S::R2MAX; e += 256) w[e] = wtab[e];
     __syncthreads();
-    for (int e = tid; e < S::NRS * 128; e += 256) {
-        const int k = e >> 7, p = e & 127, r2 = rsum_value(k);
-        double sum = 0.0;
-        for (int j = 0; j < 7; ++j)
-            if (p & (1 << j)) sum += w[r2 + (j - 3) * (j - 3)];
-        rtab[e] = sum;
-    }
+    for (int e = tid; e < S::NRS * 128; e += 256) rtab[e] = rtab_g[e];  // built on the host
     const int plane = S::HX * S::HY;
     const int fo[6] = {-1, +1, -S::HX, +S::HX, -plane, +plane};
     // 3. labels the scores need: a cell's label and its distinct other face
@@ -876,7 +871,8 @@ static int launch_scores_screen(gpk_grid* G, real* res, real* best, const unsign
         k_bgr_scores_screen<real, IS3D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     GPK_CUDA_TRY(attr_rc);
     k_bgr_scores_screen<real, IS3D><<<ntx * nty * ntz, 256, smem, G->stream>>>(
-        D, G->phi, G->mask, ntx, nty, G->d_remap_w, G->geometry_kernel == 2 ? 1 : S::NL, G->phi_comp, res, best,
+        D, G->phi, G->mask, ntx, nty, G->d_remap_w, G->d_remap_rtab, G->geometry_kernel == 2 ? 1 : S::NL,
+        G->phi_comp, res, best,
         gate, G->scal);
     G->launches++;
     GPK_CUDA_TRY(cudaGetLastError());
