@@ -91,3 +91,57 @@ def test_separable_tiles_rejected_in_fp32():
     g64 = GPKGrid(8, 8, 8, 1.0, thermo.isotropic(1.0, 1.0), 0.0, 6.0, precision="f64")  # kernel radius 23
     with pytest.raises(GPKError):
         g64.set_geometry_kernel("separable_tiles")
+
+
+@pytest.mark.parametrize("shape", [(24, 30, 36), (1, 70, 90)])
+def test_separable_tiles_many_labels_per_tile(oracle_mod, shape):
+    """Hundreds of small grains: most tiles hold more labels than one bitmap
+    batch (four), so the per-batch bitmaps, label boxes and passes repeat."""
+    phi, g = oracle_mod.voronoi(*shape, 400, 7)
+    iso = thermo.isotropic(1.0, 1.0)
+    out = []
+    for kind in ("tiled", "separable_tiles"):
+        G = GPKGrid(*shape, 1.0, iso, 0.0, 1.5, precision="f64")
+        G.set_geometry_kernel(kind)
+        G.set("phi", phi)
+        G.set("g", g.astype(np.float64))
+        G.geometry()
+        out.append({f: G.get(f) for f in ("nx_f", "ny_f", "nz_f", "kappa_f", "phi_comp")})
+    for f in ("nx_f", "ny_f", "nz_f", "kappa_f"):
+        assert _close(out[1][f], out[0][f]), f
+    _competitors_equal_except_ties(phi, out[0], out[1])
+
+
+def _competitors_equal_except_ties(phi, a, b):
+    """The competitor (src/gpk_geometry.cpp:154-182) is the unlike face
+    neighbour with the most like cells among the 26 around the cell, ties
+    going to the larger outward-normal alignment.  Normals that agree to
+    rounding can still order two equally supported candidates differently
+    when their alignments agree to rounding; every other cell must match."""
+    diff = np.argwhere(a["phi_comp"] != b["phi_comp"])
+    Nz, Ny, Nx = phi.shape
+    for z, y, x in diff:
+        own = phi[z, y, x]
+
+        def support(q):
+            n = 0
+            for dz in ((-1, 0, 1) if Nz > 1 else (0,)):
+                for dy in (-1, 0, 1):
+                    for dx in (-1, 0, 1):
+                        if dz or dy or dx:
+                            n += phi[(z + dz) % Nz, (y + dy) % Ny, (x + dx) % Nx] == q
+            return n
+
+        qa, qb = a["phi_comp"][z, y, x], b["phi_comp"][z, y, x]
+        assert qa != own and qb != own, (z, y, x)
+        assert support(qa) == support(qb), (z, y, x)
+        faces = {(0, 0, -1): -a["nx_f"], (0, 0, 1): a["nx_f"], (0, -1, 0): -a["ny_f"], (0, 1, 0): a["ny_f"]}
+        if Nz > 1:
+            faces.update({(-1, 0, 0): -a["nz_f"], (1, 0, 0): a["nz_f"]})
+        score = {}
+        for (dz, dy, dx), field in faces.items():
+            q = phi[(z + dz) % Nz, (y + dy) % Ny, (x + dx) % Nx]
+            if q in (qa, qb):
+                score[q] = max(score.get(q, -2.0), float(field[z, y, x]))
+        assert abs(score[qa] - score[qb]) <= 1e-12, (z, y, x, score)
+    print(f"competitors differing at near-ties: {len(diff)} of {a['phi_comp'].size} cells")
